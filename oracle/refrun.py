@@ -1,0 +1,97 @@
+"""Runs the reference's own C++ sources (built by oracle/ref_build/Makefile into
+oracle/_ref/) on given inputs.  TEST INFRASTRUCTURE ONLY: used to pin the numpy
+oracle against the reference's code, and never by the product."""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+
+def driver_path(cpu_stencil: bool = False) -> str:
+    return os.path.join(REF_DIR, "ref_driver_cpufd" if cpu_stencil else "ref_driver")
+
+
+def available(cpu_stencil: bool = False) -> bool:
+    return os.path.exists(driver_path(cpu_stencil))
+
+
+def run(op: str, values, cpu_stencil: bool = False) -> np.ndarray:
+    flat = np.concatenate([np.ravel(np.asarray(v, dtype=np.float64)) for v in values])
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.f64")
+        fout = os.path.join(td, "out.f64")
+        flat.tofile(fin)
+        subprocess.run([driver_path(cpu_stencil), op, fin, fout], check=True,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1)))
+        return np.fromfile(fout, dtype=np.float64)
+
+
+def forward2d(vol, theta, nr):
+    ns, n2, n3 = vol.shape
+    out = run("forward2d", [[ns, n2, n3, len(theta), nr], theta, vol])
+    return out.reshape(ns, len(theta), nr)
+
+
+def backproj2d(sino, theta, n):
+    ns, nth, nr = sino.shape
+    out = run("backproj2d", [[ns, nth, nr, n, n], theta, sino])
+    return out.reshape(ns, n, n)
+
+
+def psf2d(theta, nr, n, x):
+    """Returns P, kernel_hat (P, P/2+1), Toeplitz sysmat2d(x), NUFFT sysmat2d(x)."""
+    ns = x.shape[0]
+    out = run("psf2d", [[len(theta), nr, n, ns], theta, x])
+    P = int(out[0])
+    nh = P * (P // 2 + 1)
+    kh = out[1:1 + 2 * nh].view(np.complex128).reshape(P, P // 2 + 1)
+    rest = out[1 + 2 * nh:]
+    nv = ns * n * n
+    return P, kh, rest[:nv].reshape(ns, n, n), rest[nv:2 * nv].reshape(ns, n, n)
+
+
+def mbir2d(sino, theta, n, method, iters, tol, xtol, lam=0.1, mu=10.0, inner=1):
+    ns, nth, nr = sino.shape
+    m = 0 if method == "cg" else 1
+    out = run("mbir2d", [[ns, nth, nr, n, m, iters, tol, xtol, lam, mu, inner], theta, sino])
+    return out.reshape(ns, n, n)
+
+
+def grad(u, cpu_stencil=False):
+    n1, n2, n3 = u.shape
+    out = run("grad", [[n1, n2, n3], u], cpu_stencil=cpu_stencil).reshape(4, n1, n2, n3)
+    return [out[0], out[1], out[2]], out[3]
+
+
+def proj3d(vol, proj, theta, gamma, beta, shifts):
+    """forward, backproj, backproj(shifts), sysmat(NUFFT), P dims, kernel_hat, sysmat(PSF)."""
+    n1, n2, n3 = vol.shape
+    nth, nrows, ncols = proj.shape
+    out = run("proj3d", [[nth, nrows, ncols, n1, n2, n3], theta, gamma, beta,
+                         np.asarray(shifts).ravel(), vol, proj])
+    o = 0
+    fw = out[o:o + proj.size].reshape(proj.shape); o += proj.size
+    bp = out[o:o + vol.size].reshape(vol.shape); o += vol.size
+    bps = out[o:o + vol.size].reshape(vol.shape); o += vol.size
+    sm = out[o:o + vol.size].reshape(vol.shape); o += vol.size
+    P = tuple(int(v) for v in out[o:o + 3]); o += 3
+    nk = P[0] * P[1] * (P[2] // 2 + 1)
+    kh = out[o:o + 2 * nk].view(np.complex128).reshape(P[0], P[1], P[2] // 2 + 1); o += 2 * nk
+    st = out[o:o + vol.size].reshape(vol.shape)
+    return dict(forward=fw, backproj=bp, backproj_shifted=bps, sysmat_nufft=sm, P=P,
+                kernel_hat=kh, sysmat_toeplitz=st)
+
+
+def mbir3d(projs, theta, gamma, beta, recon_dims, method, iters, tol, xtol, lam=0.1, mu=10.0,
+           inner=1):
+    nth, nrows, ncols = projs.shape
+    m = 0 if method == "cg" else 1
+    out = run("mbir3d", [[nth, nrows, ncols, *recon_dims, m, iters, tol, xtol, lam, mu, inner,
+                          gamma, beta], theta, projs])
+    return out.reshape(recon_dims)
