@@ -1,0 +1,164 @@
+/* laminocam_b200 C ABI: the MBIR reconstruction hot path of LaminoCam
+ * (aryabhatt/laminocam) on one NVIDIA B200.
+ *
+ * Conventions
+ *  - Every function returns 0 on success or a non-zero LC_ERR_* code; the
+ *    message of the last failure is lc_last_error(ctx).  This replaces the
+ *    reference's std::runtime_error / std::invalid_argument throws
+ *    (include/gpu/utils.h:31-49, include/finufft_plan.h:97-107).
+ *  - Arrays are row-major float32 with the last dimension fastest, exactly the
+ *    reference's Array<T> / DeviceArray<T> layout {n1, n2, n3}
+ *    (include/dtypes.h:29-60).
+ *  - Functions whose array arguments are described as "device" take device
+ *    pointers that the caller owns; functions named lc_mbir* take host
+ *    pointers and copy internally.
+ *  - All device work is issued on the context's stream; a context is used by
+ *    one host thread at a time.  Destroy handles before their context.
+ *  - NUFFT tolerance arguments follow FINUFFT (include/finufft_plan.h:48,71;
+ *    include/gpu/cufinufft_plan.h:49,75); pass <= 0 for the default 1e-6.
+ */
+#ifndef LAMINOCAM_H
+#define LAMINOCAM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LC_OK 0
+#define LC_ERR_INVALID 1  /* bad argument or size */
+#define LC_ERR_NOMEM 2    /* device allocation failed / over the memory budget */
+#define LC_ERR_CUDA 3     /* CUDA runtime error */
+#define LC_ERR_INTERNAL 4 /* anything else */
+
+typedef struct lc_context_s *lc_context;
+typedef struct lc_geometry_s *lc_geometry;
+typedef struct lc_psf_s *lc_psf;
+
+/* ---- context ---------------------------------------------------------- */
+int lc_version(void);
+/* stream: a cudaStream_t or NULL for a private non-blocking stream */
+int lc_context_create(int device, void *stream, lc_context *out);
+int lc_context_destroy(lc_context ctx);
+int lc_context_set_stream(lc_context ctx, void *stream);
+int lc_context_synchronize(lc_context ctx);
+const char *lc_last_error(lc_context ctx);
+
+/* ---- geometry --------------------------------------------------------- */
+/* Replaces cpu::PolarGrid2D / gpu::PolarGrid2D (include/polar_grid2d.h:35-66,
+ * include/gpu/polar_grid2d.h): x = r cos(theta), y = r sin(theta),
+ * r_k = (k+1/2) 2pi/nradial - pi.  theta: host, radians, ntheta values. */
+int lc_geometry2d_create(lc_context ctx, const double *theta, int ntheta, int nradial,
+                         lc_geometry *out);
+/* Replaces cpu::PolarGrid / gpu::PolarGrid (include/polar_grid.h:34-95,
+ * include/rotation.h:28-56) plus the per-projection centre-of-rotation shifts
+ * of backproj() (src/projection.cpp:100-131).  theta, gamma, beta: host,
+ * radians, one per projection; shifts: host, 2 floats (dx, dy) per projection
+ * in pixels, or NULL. */
+int lc_geometry3d_create(lc_context ctx, const double *theta, const double *gamma,
+                         const double *beta, const float *shifts, int ntheta, int nrows,
+                         int ncols, lc_geometry *out);
+int lc_geometry_destroy(lc_geometry g);
+
+/* ---- projection operators (device pointers) ---------------------------- */
+/* forward2d (src/projection.cpp:146-160): volume {ns, n2, n3} -> sino {ns, ntheta, nradial} */
+int lc_forward2d(lc_context ctx, lc_geometry g, const float *volume, int ns, int n2, int n3,
+                 float *sino, double tol);
+/* backproj2d (src/projection.cpp:168-182): sino {ns, ntheta, nradial} -> volume {ns, n2, n3} */
+int lc_backproj2d(lc_context ctx, lc_geometry g, const float *sino, int ns, int n2, int n3,
+                  float *volume, double tol);
+/* sysmat2d(x, PolarGrid2D) (src/gradient.cpp:55-69): Re(NUFFT1(NUFFT2(x))) / nradial */
+int lc_sysmat2d_nufft(lc_context ctx, lc_geometry g, const float *x, int ns, int n2, int n3,
+                      float *y, double tol);
+/* forward (src/projection.cpp:42-64, CPU semantics incl. the |q|<=pi mask):
+ * volume {n1, n2, n3} -> projections {ntheta, nrows, ncols} */
+int lc_forward3d(lc_context ctx, lc_geometry g, const float *volume, int n1, int n2, int n3,
+                 float *proj, double tol);
+/* backproj (src/projection.cpp:69-131): projections -> volume {n1, n2, n3};
+ * apply_shifts != 0 uses the geometry's per-projection shifts */
+int lc_backproj3d(lc_context ctx, lc_geometry g, const float *proj, int n1, int n2, int n3,
+                  int apply_shifts, float *volume, double tol);
+/* sysmat(x, PolarGrid) (src/gradient.cpp:32-45): Re(NUFFT1(NUFFT2(x))) / (nrows*ncols) */
+int lc_sysmat3d_nufft(lc_context ctx, lc_geometry g, const float *x, int n1, int n2, int n3,
+                      float *y, double tol);
+
+/* ---- Toeplitz PSF ------------------------------------------------------ */
+/* Replaces cpu/gpu::PointSpreadFunction2D (include/toeplitz2d.h:40-126) for a
+ * 2D geometry (n1 = number of slices, n2 == n3 = image size) and
+ * cpu/gpu::PointSpreadFunction (include/toeplitz.h:35-130) for a 3D geometry
+ * (volume {n1, n2, n3}).  The kernel is generated in FP64 on the device. */
+int lc_psf_create(lc_context ctx, lc_geometry g, int n1, int n2, int n3, lc_psf *out);
+int lc_psf_destroy(lc_psf psf);
+/* P[3]: PSF grid (P[0] = 1 for 2D); spectrum_elems: stored real spectrum size */
+int lc_psf_info(lc_psf psf, int *P, long *spectrum_elems);
+/* FP64 PSF K on the P grid in mode order (index k + P/2), host buffer */
+int lc_psf_kernel(lc_context ctx, lc_psf psf, double *host_out);
+/* real spectrum octant {P0/2+1, P1/2+1, P2/2+1} of the zero-centred PSF, host buffer */
+int lc_psf_spectrum(lc_context ctx, lc_psf psf, float *host_out);
+/* sysmat(x, PSF) / sysmat2d(x, PSF2D) (src/gradient.cpp:49-52,76-79):
+ * y = A^T A x, x and y device {n1, n2, n3} */
+int lc_sysmat_toeplitz(lc_context ctx, lc_psf psf, const float *x, float *y);
+
+/* ---- solvers ------------------------------------------------------------ */
+typedef struct {
+    int max_iters;    /* CG iterations, or Split-Bregman outer iterations */
+    int inner_iters;  /* CG iterations per Split-Bregman outer iteration */
+    float tol;        /* residual tolerance (0 disables) */
+    float xtol;       /* relative-step tolerance (0 disables) */
+    float lambda;     /* TV weight */
+    float mu;         /* Bregman penalty */
+    int fp32_scalars; /* 1: float dot products as the reference GPU path */
+    int poll_every;   /* iterations between host checks of the stop flag */
+} lc_solver_params;
+
+typedef struct {
+    int iters;          /* CG iterations, or Split-Bregman outer iterations */
+    int cg_iters_total;
+    double residual;    /* last CG ||r|| / (||y|| + 1e-8) */
+    double dx;          /* last relative change */
+    int stop_reason;    /* 0 max iters, 1 residual, 2 step, 3 |pAp| < 1e-10 */
+    double elapsed_ms;  /* device time of the call */
+} lc_solver_stats;
+
+void lc_solver_params_default(lc_solver_params *p);
+
+/* opt::cgsolver (include/optimize.h:89-91, src/conjgrad.cpp:33-76) with the
+ * Toeplitz operator of psf.  rhs, x: device {n1, n2, n3}; x holds x0 on entry. */
+int lc_cgsolver(lc_context ctx, lc_psf psf, const float *rhs, float *x, const lc_solver_params *p,
+                lc_solver_stats *stats);
+/* opt::split_bregman (include/optimize.h:74-77, src/bregman.cpp:36-94) */
+int lc_split_bregman(lc_context ctx, lc_psf psf, const float *rhs, float *x,
+                     const lc_solver_params *p, lc_solver_stats *stats);
+
+/* ---- reconstruction drivers (host buffers) ------------------------------ */
+typedef struct {
+    int method;           /* 0: CG (UNCONSTRAINED), 1: Split-Bregman */
+    lc_solver_params solver;
+    double nufft_tol;     /* <= 0: 1e-6 */
+    float pad_factor;     /* 3D only, ReconParams::PAD_FACTOR (1.4142) */
+} lc_recon_params;
+
+void lc_recon_params_default(lc_recon_params *p);
+
+/* gpu::MBIR2D (src/gpu/mbir2d.cu:36-85) on a prepared sinogram
+ * {ns, ntheta, nradial} (include/mbir2d_prep.h:44-65); recon {ns, n, n} with
+ * recon_dims = {ns, n, n}. */
+int lc_mbir2d(lc_context ctx, const float *sino, int ns, int ntheta, int nradial,
+              const double *theta, const int *recon_dims, const lc_recon_params *p, float *recon,
+              lc_solver_stats *stats);
+/* gpu::MBIR (src/gpu/mbir.cu:41-167): stacked projections {ntheta, nrows, ncols}
+ * with per-projection angles (radians); normalises by the maximum, pads by
+ * pad_factor (odd sizes), backprojects, builds the PSF, solves and crops to
+ * recon_dims {n1, n2, n3}. */
+int lc_mbir3d(lc_context ctx, const float *projs, int ntheta, int nrows, int ncols,
+              const double *theta, const double *gamma, const double *beta, const float *shifts,
+              const int *recon_dims, const lc_recon_params *p, float *recon,
+              lc_solver_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LAMINOCAM_H */

@@ -1,0 +1,250 @@
+// Shared device/host helpers for the laminocam_b200 kernels (sm_100a).
+//
+//  * complex helpers over float2 / double2
+//  * the exponential-of-semicircle (ES) spreading kernel
+//  * a shared-memory Stockham FFT core (radices 2, 3, 4, 8) used by every
+//    line-FFT kernel in this library
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <stdexcept>
+#include <string>
+
+namespace lc {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define LC_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            throw ::lc::Error(3, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+    } while (0)
+
+#define LC_CHECK_LAUNCH() LC_CUDA(cudaGetLastError())
+
+#define LC_REQUIRE(cond, msg)                                                           \
+    do {                                                                                \
+        if (!(cond)) throw ::lc::Error(1, std::string(msg));                           \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// complex arithmetic
+// ---------------------------------------------------------------------------
+template <typename T> struct C2;
+template <> struct C2<float> { using type = float2; };
+template <> struct C2<double> { using type = double2; };
+template <typename T> using cx = typename C2<T>::type;
+
+template <typename T> __host__ __device__ __forceinline__ cx<T> mk(T r, T i) {
+    cx<T> z;
+    z.x = r;
+    z.y = i;
+    return z;
+}
+template <typename V> __host__ __device__ __forceinline__ V cadd(V a, V b) {
+    a.x += b.x;
+    a.y += b.y;
+    return a;
+}
+template <typename V> __host__ __device__ __forceinline__ V csub(V a, V b) {
+    a.x -= b.x;
+    a.y -= b.y;
+    return a;
+}
+template <typename V> __host__ __device__ __forceinline__ V cmul(V a, V b) {
+    V z;
+    z.x = a.x * b.x - a.y * b.y;
+    z.y = a.x * b.y + a.y * b.x;
+    return z;
+}
+template <typename V> __host__ __device__ __forceinline__ V cconj(V a) {
+    a.y = -a.y;
+    return a;
+}
+template <typename V, typename S> __host__ __device__ __forceinline__ V cscale(V a, S s) {
+    a.x *= s;
+    a.y *= s;
+    return a;
+}
+// multiply by sign*i
+template <typename V> __device__ __forceinline__ V cmul_i(V a, int sign) {
+    V z;
+    if (sign > 0) {
+        z.x = -a.y;
+        z.y = a.x;
+    } else {
+        z.x = a.y;
+        z.y = -a.x;
+    }
+    return z;
+}
+
+// ---------------------------------------------------------------------------
+// line-FFT plans
+// ---------------------------------------------------------------------------
+constexpr int kMaxStages = 16;
+
+// Device-side description of one FFT length: radix sequence and twiddle table
+// tw[m] = exp(-2*pi*i*m/L), m in [0, L), in the plan's precision.
+struct FFTPlan {
+    int L;
+    int nst;
+    int radix[kMaxStages];
+    const void *tw;
+};
+
+template <typename V, int R>
+__device__ __forceinline__ void dft_small(V *v, int sign) {
+    using T = decltype(v[0].x);
+    if constexpr (R == 2) {
+        V a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 3) {
+        const T c1 = T(-0.5);
+        const T s1 = T(0.86602540378443864676) * T(sign);
+        V a = v[0], b = v[1], c = v[2];
+        V t1 = cadd(b, c);
+        V t2 = csub(b, c);
+        v[0] = cadd(a, t1);
+        V m = mk<T>(a.x + c1 * t1.x, a.y + c1 * t1.y);
+        // (b - c) * i * s1
+        V r = mk<T>(-s1 * t2.y, s1 * t2.x);
+        v[1] = cadd(m, r);
+        v[2] = csub(m, r);
+    } else if constexpr (R == 4) {
+        V a = v[0], b = v[1], c = v[2], d = v[3];
+        V t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), t3 = cmul_i(csub(b, d), sign);
+        v[0] = cadd(t0, t2);
+        v[2] = csub(t0, t2);
+        v[1] = cadd(t1, t3);
+        v[3] = csub(t1, t3);
+    } else if constexpr (R == 8) {
+        const T h = T(0.70710678118654752440);
+        // radix-2 over even/odd, then radix-4 each
+        V e[4] = {v[0], v[2], v[4], v[6]};
+        V o[4] = {v[1], v[3], v[5], v[7]};
+        dft_small<V, 4>(e, sign);
+        dft_small<V, 4>(o, sign);
+        // twiddles w8^k for k=0..3 with sign: exp(sign*i*2*pi*k/8)
+        V o1 = mk<T>(h * (o[1].x - T(sign) * o[1].y), h * (o[1].y + T(sign) * o[1].x));
+        V o2 = cmul_i(o[2], sign);
+        V o3 = mk<T>(h * (-o[3].x - T(sign) * o[3].y), h * (-o[3].y + T(sign) * o[3].x));
+        v[0] = cadd(e[0], o[0]);
+        v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], o1);
+        v[5] = csub(e[1], o1);
+        v[2] = cadd(e[2], o2);
+        v[6] = csub(e[2], o2);
+        v[3] = cadd(e[3], o3);
+        v[7] = csub(e[3], o3);
+    }
+}
+
+// One Stockham stage of radix R over C lines of length L, out of place:
+// element (i, c) of line c lives at src[i*C + c] / dst[i*C + c].
+template <typename T, int R>
+__device__ __forceinline__ void stockham_stage(const cx<T> *__restrict__ src, cx<T> *__restrict__ dst,
+                                               int L, int C, int Ns, const cx<T> *__restrict__ tw,
+                                               int sign) {
+    using V = cx<T>;
+    const int nb = L / R;
+    const int items = nb * C;
+    const int tstride = L / (Ns * R);
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int c = it % C;
+        const int j = it / C;
+        const int k = j % Ns;
+        V v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * C + c];
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                V w = tw[r * k * tstride];
+                if (sign > 0) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        dft_small<V, R>(v, sign);
+        const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[(base + r * Ns) * C + c] = v[r];
+    }
+}
+
+// Unnormalised DFT of C lines held in shared memory ([L][C] layout), natural
+// order in and out, ping-ponging between a and b.  Returns the buffer that
+// holds the result.  sign = -1: forward (e^{-i}); sign = +1: backward.
+// The data must be complete in `a` (__syncthreads() before the call); the
+// result is complete when the call returns.
+template <typename T>
+__device__ cx<T> *smem_fft(cx<T> *a, cx<T> *b, int C, const FFTPlan &pl, int sign) {
+    const cx<T> *tw = reinterpret_cast<const cx<T> *>(pl.tw);
+    cx<T> *src = a, *dst = b;
+    int Ns = 1;
+    for (int s = 0; s < pl.nst; ++s) {
+        const int R = pl.radix[s];
+        switch (R) {
+            case 2: stockham_stage<T, 2>(src, dst, pl.L, C, Ns, tw, sign); break;
+            case 3: stockham_stage<T, 3>(src, dst, pl.L, C, Ns, tw, sign); break;
+            case 4: stockham_stage<T, 4>(src, dst, pl.L, C, Ns, tw, sign); break;
+            default: stockham_stage<T, 8>(src, dst, pl.L, C, Ns, tw, sign); break;
+        }
+        __syncthreads();
+        cx<T> *t = src;
+        src = dst;
+        dst = t;
+        Ns *= R;
+    }
+    return src;
+}
+
+// ---------------------------------------------------------------------------
+// exponential-of-semicircle kernel  phi(z) = exp(beta*(sqrt(1-z^2)-1)), |z|<=1
+// (Barnett, Magland & af Klinteberg, SIAM J. Sci. Comput. 41(5), 2019)
+// ---------------------------------------------------------------------------
+struct ESParams {
+    int w;        // kernel width in fine-grid cells
+    float beta;   // shape parameter
+    float half_w; // w/2
+};
+
+template <typename T>
+__device__ __forceinline__ T es_eval(T z, T beta) {
+    T s = T(1) - z * z;
+    return s > T(0) ? exp(beta * (sqrt(s) - T(1))) : T(0);
+}
+
+__device__ __forceinline__ float es_evalf(float z, float beta) {
+    float s = 1.0f - z * z;
+    return s > 0.0f ? expf(beta * (sqrtf(s) - 1.0f)) : 0.0f;
+}
+
+// Fine-grid placement of a coordinate x (radians, any real value, taken
+// 2*pi-periodic) on a grid of nf cells of width 2*pi/nf.  Computes the first
+// covered cell l0 (not yet wrapped) and the offset of x from l0 in cells, in
+// double precision so that the float kernel evaluation sees an exact offset.
+__device__ __forceinline__ void es_place(double x, int nf, int w, int &l0, float &off) {
+    double u = x * (double)nf * 0.15915494309189533577;  // x / h, h = 2*pi/nf
+    double lo = ceil(u - 0.5 * (double)w);
+    l0 = (int)lo;
+    off = (float)(u - lo);  // in (w/2 - 1, w/2]; cell l0+m sits at z = (m - off)/(w/2)
+}
+
+__device__ __forceinline__ int wrap(int l, int n) {
+    l %= n;
+    return l < 0 ? l + n : l;
+}
+
+}  // namespace lc

@@ -1,0 +1,75 @@
+// Line transforms along one axis of a strided 3D array:
+//  * launch_axis_fft: 2^p*3^q shared-memory Stockham FFT with fused zero
+//    padding, mode (CMCL) placement/extraction, Hermitian expansion, per-index
+//    scale factors (NUFFT deapodisation), an optional spectral multiply between
+//    a forward and an inverse transform (Toeplitz), and real or complex output.
+//  * launch_axis_dft: direct DFT of arbitrary length with fused circular
+//    shifts (fftshift / ifftshift index maps), used for detector-domain
+//    transforms whose lengths are odd.
+#pragma once
+
+#include "lc_runtime.hpp"
+
+namespace lc {
+
+enum Elem { E_F32 = 0, E_C64 = 1, E_F64 = 2, E_C128 = 3 };  // float, float2, double, double2
+enum InMap { IN_DIRECT = 0, IN_MODES = 1, IN_HERM = 2 };
+enum OutMap { OUT_DIRECT = 0, OUT_MODES = 1, OUT_WINDOW = 2 };
+
+// Lines are indexed by (o, c), o in [0, n_outer), c in [0, n_inner); element i
+// of line (o, c) is at  o*ostride + i*n_inner + c  (input and output alike).
+//
+// Input maps (element j of the input line -> FFT index f):
+//   IN_DIRECT  f = j (j < n_in, zero padded to L)
+//   IN_MODES   f = (j - n_in/2) mod L        (mode k = j - floor(n_in/2))
+//   IN_HERM    f in [0, L): in[f] for f <= L/2, conj(in[L-f]) otherwise
+//              (n_in = L/2 + 1, half spectrum of a real line)
+// Output maps (output element j <- FFT index f):
+//   OUT_DIRECT f = j; OUT_MODES f = (j - n_out/2) mod L; OUT_WINDOW f = j + out_off
+struct AxisFFT {
+    const void *in = nullptr;
+    Elem in_t = E_C64;
+    void *out = nullptr;
+    Elem out_t = E_C64;
+    long n_outer = 1, n_inner = 1;
+    long in_ostride = 0, out_ostride = 0;
+    int n_in = 0, n_out = 0, L = 0;
+    InMap in_map = IN_DIRECT;
+    OutMap out_map = OUT_DIRECT;
+    int out_off = 0;
+    int sign = -1;
+    const void *pre = nullptr;      // real factor per input index j
+    const void *linefac = nullptr;  // real factor per line inner index c
+    const void *post = nullptr;     // real factor per output index j
+    double scale = 1.0;
+    // spectral multiply between a transform of `sign` and one of `sign2`:
+    // value at FFT index f of line (o, c) is multiplied by
+    // mid[fold(f, L)*mid_ra + fold(c / mid_p3h, mid_pmid)*mid_p3h + c % mid_p3h]
+    // with fold(k, n) = min(k, n - k).
+    const float *mid = nullptr;
+    long mid_ra = 0;
+    int mid_p3h = 1, mid_pmid = 1;
+    int sign2 = +1;
+    bool fp64 = false;  // compute precision
+    int lines_per_cta = 0;  // 0 = choose automatically
+};
+
+void launch_axis_fft(Context &ctx, const AxisFFT &a);
+
+struct AxisDFT {
+    const void *in = nullptr;
+    Elem in_t = E_C64;
+    void *out = nullptr;
+    Elem out_t = E_C64;
+    long n_outer = 1, n_inner = 1;
+    long in_ostride = 0, out_ostride = 0;
+    int n = 0;
+    int d_pre = 0;   // loaded line:  v[m] = in[(m + d_pre) % n]
+    int d_post = 0;  // stored line:  out[k] = DFT(v)[(k + d_post) % n]
+    int sign = -1;
+    float scale = 1.0f;
+};
+
+void launch_axis_dft(Context &ctx, const AxisDFT &a);
+
+}  // namespace lc

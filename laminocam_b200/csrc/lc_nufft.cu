@@ -1,0 +1,793 @@
+// Bin-sorted ES-kernel spreading (type 1) and tile-staged interpolation
+// (type 2) on polar grids, plus the pruned fine-grid FFT passes.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "lc_nufft.hpp"
+
+namespace lc {
+
+// ---------------------------------------------------------------------------
+// geometry
+// ---------------------------------------------------------------------------
+void geometry_init_2d(Context &ctx, PolarGeometry &g, const double *theta, int ntheta, int nr) {
+    LC_REQUIRE(ntheta > 0 && nr > 0, "geometry: ntheta and nradial must be positive");
+    g.theta.assign(theta, theta + ntheta);
+    std::vector<double2> cs(ntheta);
+    for (int i = 0; i < ntheta; ++i) cs[i] = make_double2(std::cos(theta[i]), std::sin(theta[i]));
+    g.cs.upload(cs.data(), ntheta, ctx.stream());
+    LC_CUDA(cudaStreamSynchronize(ctx.stream()));
+    g.pts = PolarPts{};
+    g.pts.dim = 2;
+    g.pts.ntheta = ntheta;
+    g.pts.nr = nr;
+    g.pts.M = (long)ntheta * nr;
+    g.pts.cs = g.cs.get();
+}
+
+void geometry_init_3d(Context &ctx, PolarGeometry &g, const double *theta, const double *gamma,
+                      const double *beta, const float *shifts, int ntheta, int nrows, int ncols) {
+    LC_REQUIRE(ntheta > 0 && nrows > 0 && ncols > 0, "geometry: sizes must be positive");
+    LC_REQUIRE((long)ntheta * nrows * ncols < (1L << 31), "geometry: too many points");
+    g.theta.assign(theta, theta + ntheta);
+    g.gamma.assign(gamma, gamma + ntheta);
+    g.beta.assign(beta, beta + ntheta);
+    std::vector<double> rot(6 * (size_t)ntheta);
+    for (int i = 0; i < ntheta; ++i) {
+        // transpose(Rx(theta) Ry(beta) Rz(gamma)), columns 0 and 1 (q has no z part)
+        double ct = std::cos(theta[i]), st = std::sin(theta[i]);
+        double cb = std::cos(beta[i]), sb = std::sin(beta[i]);
+        double cg = std::cos(gamma[i]), sg = std::sin(gamma[i]);
+        double *r = &rot[6 * (size_t)i];
+        r[0] = cb * cg;                 // R00
+        r[1] = ct * sg + st * sb * cg;  // R01
+        r[2] = -cb * sg;                // R10
+        r[3] = ct * cg - st * sb * sg;  // R11
+        r[4] = sb;                      // R20
+        r[5] = -st * cb;                // R21
+    }
+    g.rot.upload(rot.data(), rot.size(), ctx.stream());
+    g.shifts.assign(2 * (size_t)ntheta, 0.0f);
+    if (shifts) std::copy(shifts, shifts + 2 * (size_t)ntheta, g.shifts.begin());
+    g.dshifts.upload(reinterpret_cast<const float2 *>(g.shifts.data()), ntheta, ctx.stream());
+    LC_CUDA(cudaStreamSynchronize(ctx.stream()));
+    g.pts = PolarPts{};
+    g.pts.dim = 3;
+    g.pts.ntheta = ntheta;
+    g.pts.nrows = nrows;
+    g.pts.ncols = ncols;
+    g.pts.M = (long)ntheta * nrows * ncols;
+    g.pts.rot = g.rot.get();
+}
+
+// ---------------------------------------------------------------------------
+// ES kernel parameters and deapodisation
+// ---------------------------------------------------------------------------
+int es_width_for_tol(double tol) {
+    LC_REQUIRE(tol > 0 && tol < 1, "NUFFT tolerance must be in (0, 1)");
+    int w = (int)std::ceil(std::log10(1.0 / tol)) + 1;
+    return std::min(12, std::max(4, w));
+}
+
+double es_beta_for_width(int w) { return 2.30 * w; }
+
+// Gauss-Legendre nodes on [-1, 1] by Newton iteration on P_n.
+static void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &wt) {
+    x.assign(n, 0.0);
+    wt.assign(n, 0.0);
+    const double pi = 3.14159265358979323846;
+    for (int i = 0; i < (n + 1) / 2; ++i) {
+        double z = std::cos(pi * (i + 0.75) / (n + 0.5)), z1, pp;
+        do {
+            double p1 = 1.0, p2 = 0.0;
+            for (int j = 1; j <= n; ++j) {
+                double p3 = p2;
+                p2 = p1;
+                p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+            }
+            pp = n * (z * p1 - p2) / (z * z - 1.0);
+            z1 = z;
+            z = z1 - p1 / pp;
+        } while (std::fabs(z - z1) > 1e-15);
+        x[i] = -z;
+        x[n - 1 - i] = z;
+        wt[i] = wt[n - 1 - i] = 2.0 / ((1.0 - z * z) * pp * pp);
+    }
+}
+
+std::vector<double> es_correction(int n, int nf, int w, double beta) {
+    std::vector<double> x, wt;
+    gauss_legendre(4 * w + 60, x, wt);
+    std::vector<double> phi(x.size());
+    for (size_t q = 0; q < x.size(); ++q) phi[q] = std::exp(beta * (std::sqrt(1.0 - x[q] * x[q]) - 1.0));
+    std::vector<double> out(n);
+    const double pi = 3.14159265358979323846;
+    for (int j = 0; j < n; ++j) {
+        double k = (double)(j - n / 2);
+        double xi = k * w * pi / nf;
+        double s = 0;
+        for (size_t q = 0; q < x.size(); ++q) s += wt[q] * phi[q] * std::cos(xi * x[q]);
+        out[j] = 2.0 / (w * s);
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr double kInv2Pi = 0.15915494309189533577;
+constexpr double kPi = 3.14159265358979323846;
+
+struct GridCfg {
+    int nf[3];
+    int bs[3];
+    int nb[3];
+    int hw[3];
+    int td[3];   // tile extent per dim
+    float beta;
+};
+
+struct PointInfo {
+    double c[3];  // x, y, z
+    double qX, qY;
+    int angle;
+};
+
+__device__ __forceinline__ void point_at(const PolarPts &p, long j, PointInfo &pi) {
+    if (p.dim == 2) {
+        int i = (int)(j / p.nr);
+        int m = (int)(j - (long)i * p.nr);
+        double r = ((double)m + 0.5) * (2.0 * kPi / p.nr) - kPi;
+        double2 cs = p.cs[i];
+        pi.c[0] = cs.x * r;
+        pi.c[1] = cs.y * r;
+        pi.c[2] = 0.0;
+        pi.angle = i;
+        pi.qX = r;
+        pi.qY = 0.0;
+    } else {
+        long per = (long)p.nrows * p.ncols;
+        int i = (int)(j / per);
+        long rem = j - (long)i * per;
+        int a = (int)(rem / p.ncols);
+        int b = (int)(rem - (long)a * p.ncols);
+        double qX = ((double)b + 0.5) * (2.0 * kPi / p.ncols) - kPi;
+        double qY = ((double)a + 0.5) * (2.0 * kPi / p.nrows) - kPi;
+        const double *R = p.rot + 6 * (long)i;
+        pi.c[0] = R[0] * qX + R[1] * qY;
+        pi.c[1] = R[2] * qX + R[3] * qY;
+        pi.c[2] = R[4] * qX + R[5] * qY;
+        pi.qX = qX;
+        pi.qY = qY;
+        pi.angle = i;
+    }
+}
+
+__device__ __forceinline__ bool in_band(const PointInfo &pi) {
+    return fabs(pi.c[0]) <= kPi && fabs(pi.c[1]) <= kPi && fabs(pi.c[2]) <= kPi;
+}
+
+// wrapped fine-grid coordinate u in [0, nf), its cell, first covered cell l0
+// and the float offset u - l0
+__device__ __forceinline__ void place(double x, int nf, int W, int &cell, int &l0, float &off) {
+    double u = x * (double)nf * kInv2Pi;
+    u -= (double)nf * floor(u / (double)nf);
+    if (u >= (double)nf) u -= (double)nf;
+    if (u < 0.0) u = 0.0;
+    cell = (int)floor(u);
+    if (cell >= nf) cell = nf - 1;
+    double lo = ceil(u - 0.5 * (double)W);
+    l0 = (int)lo;
+    off = (float)(u - lo);
+}
+
+template <int DIM>
+__device__ __forceinline__ int bin_of(const PointInfo &pi, const GridCfg &g, int W) {
+    int b = 0, mul = 1;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        int cell, l0;
+        float off;
+        place(pi.c[d], g.nf[d], W, cell, l0, off);
+        b += (cell / g.bs[d]) * mul;
+        mul *= g.nb[d];
+    }
+    return b;
+}
+
+template <int DIM>
+__global__ void bin_count_kernel(PolarPts pts, GridCfg g, int W, int *counts) {
+    for (long j = (long)blockIdx.x * blockDim.x + threadIdx.x; j < pts.M;
+         j += (long)gridDim.x * blockDim.x) {
+        PointInfo pi;
+        point_at(pts, j, pi);
+        int b = bin_of<DIM>(pi, g, W);
+        unsigned act = __activemask();
+        unsigned peers = __match_any_sync(act, b);
+        int lane = threadIdx.x & 31;
+        int leader = __ffs(peers) - 1;
+        if (lane == leader) atomicAdd(&counts[b], __popc(peers));
+    }
+}
+
+template <int DIM>
+__global__ void bin_scatter_kernel(PolarPts pts, GridCfg g, int W, int *cursor, int *perm) {
+    for (long j = (long)blockIdx.x * blockDim.x + threadIdx.x; j < pts.M;
+         j += (long)gridDim.x * blockDim.x) {
+        PointInfo pi;
+        point_at(pts, j, pi);
+        int b = bin_of<DIM>(pi, g, W);
+        unsigned act = __activemask();
+        unsigned peers = __match_any_sync(act, b);
+        int lane = threadIdx.x & 31;
+        int leader = __ffs(peers) - 1;
+        int rank = __popc(peers & ((1u << lane) - 1u));
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&cursor[b], __popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        perm[base + rank] = (int)j;
+    }
+}
+
+// ---- spreading ----------------------------------------------------------
+template <int DIM, int W>
+__global__ void __launch_bounds__(256) spread_kernel(PolarPts pts, GridCfg g,
+                                                     const float2 *__restrict__ c, long cstride,
+                                                     int nvol, const int *__restrict__ perm,
+                                                     const int4 *__restrict__ subs,
+                                                     float2 *__restrict__ grid, long gstride,
+                                                     int mode, const float2 *__restrict__ shifts) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *tile = reinterpret_cast<float2 *>(smem_raw);
+    const int4 sp = subs[blockIdx.x];
+    const int bin = sp.x;
+    int bcoord[3] = {0, 0, 0};
+    {
+        int r = bin;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            bcoord[d] = r % g.nb[d];
+            r /= g.nb[d];
+        }
+    }
+    int S[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) S[d] = bcoord[d] * g.bs[d] - g.hw[d];
+    const int tx = g.td[0], ty = g.td[1], tz = DIM == 3 ? g.td[2] : 1;
+    const int tsize = tx * ty * tz;
+    for (int idx = threadIdx.x; idx < nvol * tsize; idx += blockDim.x) tile[idx] = make_float2(0.f, 0.f);
+    __syncthreads();
+
+    const float inv_hw = 2.0f / (float)W;
+    for (int p = threadIdx.x; p < sp.z; p += blockDim.x) {
+        const int j = perm[sp.y + p];
+        PointInfo pi;
+        point_at(pts, j, pi);
+        float2 mult = make_float2(1.f, 0.f);
+        if (mode != PT_PLAIN) {
+            if (!in_band(pi)) continue;
+            if (mode == PT_SHIFT) {
+                float2 sh = shifts[pi.angle];
+                double ph = pi.qX * (double)sh.x + pi.qY * (double)sh.y;
+                double sn, cs;
+                sincos(ph, &sn, &cs);
+                mult = make_float2((float)cs, (float)-sn);
+            }
+        }
+        float wk[2][W];
+        int lo[3] = {0, 0, 0};
+        float offz = 0.f;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            int cell, l0;
+            float off;
+            place(pi.c[d], g.nf[d], W, cell, l0, off);
+            lo[d] = l0 - S[d];
+            if (d < 2) {
+#pragma unroll
+                for (int m = 0; m < W; ++m) wk[d][m] = es_evalf(((float)m - off) * inv_hw, g.beta);
+            } else {
+                offz = off;
+            }
+        }
+        for (int s = 0; s < nvol; ++s) {
+            float2 v = c[(long)s * cstride + j];
+            if (mode == PT_SHIFT) v = cmul(v, mult);
+            float2 *ts = tile + (long)s * tsize;
+            if constexpr (DIM == 2) {
+#pragma unroll
+                for (int dy = 0; dy < W; ++dy) {
+                    float2 vy = make_float2(v.x * wk[1][dy], v.y * wk[1][dy]);
+                    float2 *row = ts + (lo[1] + dy) * tx + lo[0];
+#pragma unroll
+                    for (int dx = 0; dx < W; ++dx) {
+                        atomicAdd(&row[dx].x, vy.x * wk[0][dx]);
+                        atomicAdd(&row[dx].y, vy.y * wk[0][dx]);
+                    }
+                }
+            } else {
+                for (int dz = 0; dz < W; ++dz) {
+                    const float wz = es_evalf(((float)dz - offz) * inv_hw, g.beta);
+                    float2 vz = make_float2(v.x * wz, v.y * wz);
+#pragma unroll
+                    for (int dy = 0; dy < W; ++dy) {
+                        float2 vy = make_float2(vz.x * wk[1][dy], vz.y * wk[1][dy]);
+                        float2 *row = ts + ((lo[2] + dz) * ty + (lo[1] + dy)) * tx + lo[0];
+#pragma unroll
+                        for (int dx = 0; dx < W; ++dx) {
+                            atomicAdd(&row[dx].x, vy.x * wk[0][dx]);
+                            atomicAdd(&row[dx].y, vy.y * wk[0][dx]);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // flush: halos overlap neighbouring bins, so accumulate atomically
+    for (int idx = threadIdx.x; idx < nvol * tsize; idx += blockDim.x) {
+        float2 v = tile[idx];
+        if (v.x == 0.f && v.y == 0.f) continue;
+        int s = idx / tsize;
+        int r = idx - s * tsize;
+        int ix = r % tx;
+        int iy = (r / tx) % ty;
+        int iz = r / (tx * ty);
+        long gi = (long)wrap(S[0] + ix, g.nf[0]) + (long)wrap(S[1] + iy, g.nf[1]) * g.nf[0];
+        if (DIM == 3) gi += (long)wrap(S[2] + iz, g.nf[2]) * g.nf[0] * g.nf[1];
+        float2 *dst = grid + (long)s * gstride + gi;
+        atomicAdd(&dst->x, v.x);
+        atomicAdd(&dst->y, v.y);
+    }
+}
+
+// ---- interpolation --------------------------------------------------------
+template <int DIM, int W>
+__global__ void __launch_bounds__(256) interp_kernel(PolarPts pts, GridCfg g,
+                                                     const float2 *__restrict__ grid, long gstride,
+                                                     int nvol, const int *__restrict__ perm,
+                                                     const int4 *__restrict__ subs,
+                                                     float2 *__restrict__ c, long cstride, int mode) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *tile = reinterpret_cast<float2 *>(smem_raw);
+    const int4 sp = subs[blockIdx.x];
+    const int bin = sp.x;
+    int bcoord[3] = {0, 0, 0};
+    {
+        int r = bin;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            bcoord[d] = r % g.nb[d];
+            r /= g.nb[d];
+        }
+    }
+    int S[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) S[d] = bcoord[d] * g.bs[d] - g.hw[d];
+    const int tx = g.td[0], ty = g.td[1], tz = DIM == 3 ? g.td[2] : 1;
+    const int tsize = tx * ty * tz;
+    for (int idx = threadIdx.x; idx < nvol * tsize; idx += blockDim.x) {
+        int s = idx / tsize;
+        int r = idx - s * tsize;
+        int ix = r % tx;
+        int iy = (r / tx) % ty;
+        int iz = r / (tx * ty);
+        long gi = (long)wrap(S[0] + ix, g.nf[0]) + (long)wrap(S[1] + iy, g.nf[1]) * g.nf[0];
+        if (DIM == 3) gi += (long)wrap(S[2] + iz, g.nf[2]) * g.nf[0] * g.nf[1];
+        tile[idx] = __ldg(grid + (long)s * gstride + gi);
+    }
+    __syncthreads();
+    const float inv_hw = 2.0f / (float)W;
+    for (int p = threadIdx.x; p < sp.z; p += blockDim.x) {
+        const int j = perm[sp.y + p];
+        PointInfo pi;
+        point_at(pts, j, pi);
+        if (mode != PT_PLAIN && !in_band(pi)) {
+            for (int s = 0; s < nvol; ++s) c[(long)s * cstride + j] = make_float2(0.f, 0.f);
+            continue;
+        }
+        float wk[2][W];
+        int lo[3] = {0, 0, 0};
+        float offz = 0.f;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            int cell, l0;
+            float off;
+            place(pi.c[d], g.nf[d], W, cell, l0, off);
+            lo[d] = l0 - S[d];
+            if (d < 2) {
+#pragma unroll
+                for (int m = 0; m < W; ++m) wk[d][m] = es_evalf(((float)m - off) * inv_hw, g.beta);
+            } else {
+                offz = off;
+            }
+        }
+        for (int s = 0; s < nvol; ++s) {
+            const float2 *ts = tile + (long)s * tsize;
+            float ar = 0.f, ai = 0.f;
+            if constexpr (DIM == 2) {
+#pragma unroll
+                for (int dy = 0; dy < W; ++dy) {
+                    const float2 *row = ts + (lo[1] + dy) * tx + lo[0];
+                    float rr = 0.f, ri = 0.f;
+#pragma unroll
+                    for (int dx = 0; dx < W; ++dx) {
+                        float2 v = row[dx];
+                        rr = fmaf(v.x, wk[0][dx], rr);
+                        ri = fmaf(v.y, wk[0][dx], ri);
+                    }
+                    ar = fmaf(rr, wk[1][dy], ar);
+                    ai = fmaf(ri, wk[1][dy], ai);
+                }
+            } else {
+                for (int dz = 0; dz < W; ++dz) {
+                    float zr = 0.f, zi = 0.f;
+#pragma unroll
+                    for (int dy = 0; dy < W; ++dy) {
+                        const float2 *row = ts + ((lo[2] + dz) * ty + (lo[1] + dy)) * tx + lo[0];
+                        float rr = 0.f, ri = 0.f;
+#pragma unroll
+                        for (int dx = 0; dx < W; ++dx) {
+                            float2 v = row[dx];
+                            rr = fmaf(v.x, wk[0][dx], rr);
+                            ri = fmaf(v.y, wk[0][dx], ri);
+                        }
+                        zr = fmaf(rr, wk[1][dy], zr);
+                        zi = fmaf(ri, wk[1][dy], zi);
+                    }
+                    const float wz = es_evalf(((float)dz - offz) * inv_hw, g.beta);
+                    ar = fmaf(zr, wz, ar);
+                    ai = fmaf(zi, wz, ai);
+                }
+            }
+            c[(long)s * cstride + j] = make_float2(ar, ai);
+        }
+    }
+}
+
+template <int DIM, int W>
+void launch_spread_w(dim3 grid, int threads, size_t smem, cudaStream_t st, const PolarPts &pts,
+                     const GridCfg &g, const float2 *c, long cstride, int nvol, const int *perm,
+                     const int4 *subs, float2 *out, long gstride, int mode, const float2 *shifts) {
+    auto kern = spread_kernel<DIM, W>;
+    LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, threads, smem, st>>>(pts, g, c, cstride, nvol, perm, subs, out, gstride, mode,
+                                      shifts);
+    LC_CHECK_LAUNCH();
+}
+
+template <int DIM, int W>
+void launch_interp_w(dim3 grid, int threads, size_t smem, cudaStream_t st, const PolarPts &pts,
+                     const GridCfg &g, const float2 *gr, long gstride, int nvol, const int *perm,
+                     const int4 *subs, float2 *c, long cstride, int mode) {
+    auto kern = interp_kernel<DIM, W>;
+    LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, threads, smem, st>>>(pts, g, gr, gstride, nvol, perm, subs, c, cstride, mode);
+    LC_CHECK_LAUNCH();
+}
+
+#define LC_W_SWITCH(W, CALL)                           \
+    switch (W) {                                       \
+        case 4: { constexpr int WW = 4; CALL; } break; \
+        case 5: { constexpr int WW = 5; CALL; } break; \
+        case 6: { constexpr int WW = 6; CALL; } break; \
+        case 7: { constexpr int WW = 7; CALL; } break; \
+        case 8: { constexpr int WW = 8; CALL; } break; \
+        case 9: { constexpr int WW = 9; CALL; } break; \
+        case 10: { constexpr int WW = 10; CALL; } break; \
+        case 11: { constexpr int WW = 11; CALL; } break; \
+        case 12: { constexpr int WW = 12; CALL; } break; \
+        default: throw Error(1, "unsupported ES kernel width"); \
+    }
+
+GridCfg make_cfg(int dim, const int nf[3], const int bs[3], const int nb[3], int w, double beta) {
+    GridCfg g{};
+    int hw = (w + 1) / 2;
+    for (int d = 0; d < 3; ++d) {
+        g.nf[d] = nf[d];
+        g.bs[d] = bs[d];
+        g.nb[d] = nb[d];
+        g.hw[d] = d < dim ? hw : 0;
+        g.td[d] = d < dim ? bs[d] + 2 * hw : 1;
+    }
+    g.beta = (float)beta;
+    return g;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+NufftPlan::NufftPlan(Context &ctx, const PolarGeometry &g, const int modes[3], double tol) {
+    dim_ = g.pts.dim;
+    pts_ = g.pts;
+    shifts_ = g.dshifts.get();
+    w_ = es_width_for_tol(tol);
+    beta_ = es_beta_for_width(w_);
+    for (int d = 0; d < 3; ++d) {
+        modes_[d] = d < dim_ ? modes[d] : 1;
+        LC_REQUIRE(modes_[d] >= 1, "NUFFT: mode counts must be positive");
+        nf_[d] = d < dim_ ? (int)next_smooth23(std::max(2 * modes_[d], 2 * w_)) : 1;
+    }
+    const int bs2[3] = {32, 32, 1};
+    const int bs3[3] = {16, 16, 8};
+    for (int d = 0; d < 3; ++d) {
+        bs_[d] = std::min(dim_ == 2 ? bs2[d] : bs3[d], nf_[d]);
+        nb_[d] = (nf_[d] + bs_[d] - 1) / bs_[d];
+    }
+    cudaStream_t st = ctx.stream();
+    for (int d = 0; d < dim_; ++d) {
+        auto c = es_correction(modes_[d], nf_[d], w_, beta_);
+        std::vector<float> cf(c.begin(), c.end());
+        corr_[d].upload(cf.data(), cf.size(), st);
+    }
+    if (dim_ == 3) {
+        auto cx_ = es_correction(modes_[0], nf_[0], w_, beta_);
+        auto cy_ = es_correction(modes_[1], nf_[1], w_, beta_);
+        std::vector<float> xy((size_t)modes_[0] * modes_[1]);
+        for (int y = 0; y < modes_[1]; ++y)
+            for (int x = 0; x < modes_[0]; ++x) xy[(size_t)y * modes_[0] + x] = (float)(cy_[y] * cx_[x]);
+        corr_xy_.upload(xy.data(), xy.size(), st);
+    }
+    LC_CUDA(cudaStreamSynchronize(st));
+    sort_points(ctx);
+}
+
+void NufftPlan::sort_points(Context &ctx) {
+    cudaStream_t st = ctx.stream();
+    long nbins = (long)nb_[0] * nb_[1] * nb_[2];
+    GridCfg g = make_cfg(dim_, nf_, bs_, nb_, w_, beta_);
+    DevBuf<int> counts(nbins, st);
+    counts.zero(st);
+    int threads = 256;
+    long blocks = std::min<long>((pts_.M + threads - 1) / threads, (long)ctx.num_sms() * 16);
+    blocks = std::max<long>(blocks, 1);
+    if (dim_ == 2) bin_count_kernel<2><<<(unsigned)blocks, threads, 0, st>>>(pts_, g, w_, counts.get());
+    else bin_count_kernel<3><<<(unsigned)blocks, threads, 0, st>>>(pts_, g, w_, counts.get());
+    LC_CHECK_LAUNCH();
+    std::vector<int> hc(nbins);
+    LC_CUDA(cudaMemcpyAsync(hc.data(), counts.get(), nbins * sizeof(int), cudaMemcpyDeviceToHost, st));
+    LC_CUDA(cudaStreamSynchronize(st));
+    std::vector<int> off(nbins);
+    long acc = 0;
+    const int maxsub = dim_ == 2 ? 1024 : 2048;
+    std::vector<int4> subs;
+    for (long b = 0; b < nbins; ++b) {
+        off[b] = (int)acc;
+        for (int s = 0; s < hc[b]; s += maxsub)
+            subs.push_back(make_int4((int)b, (int)(acc + s), std::min(maxsub, hc[b] - s), 0));
+        acc += hc[b];
+    }
+    LC_REQUIRE(acc == pts_.M, "NUFFT: bin sort lost points");
+    nsub_ = (int)subs.size();
+    LC_REQUIRE(nsub_ > 0, "NUFFT: no points");
+    subs_.upload(subs.data(), subs.size(), st);
+    DevBuf<int> cursor;
+    cursor.upload(off.data(), off.size(), st);
+    perm_.alloc(pts_.M, st);
+    if (dim_ == 2) bin_scatter_kernel<2><<<(unsigned)blocks, threads, 0, st>>>(pts_, g, w_, cursor.get(), perm_.get());
+    else bin_scatter_kernel<3><<<(unsigned)blocks, threads, 0, st>>>(pts_, g, w_, cursor.get(), perm_.get());
+    LC_CHECK_LAUNCH();
+    LC_CUDA(cudaStreamSynchronize(st));
+}
+
+void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, PtMode mode) {
+    GridCfg g = make_cfg(dim_, nf_, bs_, nb_, w_, beta_);
+    const long gvol = (long)nf_[0] * nf_[1] * nf_[2];
+    const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(float2);
+    int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
+    for (int v0 = 0; v0 < nvol; v0 += vchunk) {
+        int nv = std::min(vchunk, nvol - v0);
+        size_t smem = tile_bytes * nv;
+        const float2 *cv = c + (long)v0 * pts_.M;
+        float2 *gv = grid + (long)v0 * gvol;
+        dim3 gd(nsub_);
+        if (dim_ == 2) {
+            LC_W_SWITCH(w_, (launch_spread_w<2, WW>(gd, 256, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
+                                                   perm_.get(), subs_.get(), gv, gvol, mode, shifts_)));
+        } else {
+            LC_W_SWITCH(w_, (launch_spread_w<3, WW>(gd, 256, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
+                                                   perm_.get(), subs_.get(), gv, gvol, mode, shifts_)));
+        }
+    }
+}
+
+void NufftPlan::interp(Context &ctx, const float2 *grid, int nvol, float2 *c, PtMode mode) {
+    GridCfg g = make_cfg(dim_, nf_, bs_, nb_, w_, beta_);
+    const long gvol = (long)nf_[0] * nf_[1] * nf_[2];
+    const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(float2);
+    int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
+    for (int v0 = 0; v0 < nvol; v0 += vchunk) {
+        int nv = std::min(vchunk, nvol - v0);
+        size_t smem = tile_bytes * nv;
+        const float2 *gv = grid + (long)v0 * gvol;
+        float2 *cv = c + (long)v0 * pts_.M;
+        dim3 gd(nsub_);
+        if (dim_ == 2) {
+            LC_W_SWITCH(w_, (launch_interp_w<2, WW>(gd, 256, smem, ctx.stream(), pts_, g, gv, gvol, nv,
+                                                   perm_.get(), subs_.get(), cv, pts_.M, mode)));
+        } else {
+            LC_W_SWITCH(w_, (launch_interp_w<3, WW>(gd, 256, smem, ctx.stream(), pts_, g, gv, gvol, nv,
+                                                   perm_.get(), subs_.get(), cv, pts_.M, mode)));
+        }
+    }
+}
+
+void NufftPlan::type1_real(Context &ctx, const float2 *c, int nvol, float *out, float scale,
+                           PtMode mode) {
+    cudaStream_t st = ctx.stream();
+    const long gvol = (long)nf_[0] * nf_[1] * nf_[2];
+    grid_.ensure(gvol * nvol, st);
+    LC_CUDA(cudaMemsetAsync(grid_.get(), 0, gvol * nvol * sizeof(float2), st));
+    spread(ctx, c, nvol, grid_.get(), mode);
+    const int n3 = modes_[0], n2 = modes_[1], n1 = modes_[2];
+    const int fx = nf_[0], fy = nf_[1], fz = nf_[2];
+    // x pass: fine rows -> n3 modes
+    h1_.ensure((long)nvol * fz * fy * n3, st);
+    {
+        AxisFFT a;
+        a.in = grid_.get();
+        a.in_t = E_C64;
+        a.out = h1_.get();
+        a.out_t = E_C64;
+        a.n_outer = (long)nvol * fz * fy;
+        a.n_inner = 1;
+        a.in_ostride = fx;
+        a.out_ostride = n3;
+        a.n_in = fx;
+        a.L = fx;
+        a.n_out = n3;
+        a.out_map = OUT_MODES;
+        a.sign = +1;
+        a.post = corr_[0].get();
+        launch_axis_fft(ctx, a);
+    }
+    if (dim_ == 2) {
+        AxisFFT a;
+        a.in = h1_.get();
+        a.in_t = E_C64;
+        a.out = out;
+        a.out_t = E_F32;
+        a.n_outer = nvol;
+        a.n_inner = n3;
+        a.in_ostride = (long)fy * n3;
+        a.out_ostride = (long)n2 * n3;
+        a.n_in = fy;
+        a.L = fy;
+        a.n_out = n2;
+        a.out_map = OUT_MODES;
+        a.sign = +1;
+        a.post = corr_[1].get();
+        a.scale = scale;
+        launch_axis_fft(ctx, a);
+        return;
+    }
+    h2_.ensure((long)nvol * fz * n2 * n3, st);
+    {
+        AxisFFT a;
+        a.in = h1_.get();
+        a.in_t = E_C64;
+        a.out = h2_.get();
+        a.out_t = E_C64;
+        a.n_outer = (long)nvol * fz;
+        a.n_inner = n3;
+        a.in_ostride = (long)fy * n3;
+        a.out_ostride = (long)n2 * n3;
+        a.n_in = fy;
+        a.L = fy;
+        a.n_out = n2;
+        a.out_map = OUT_MODES;
+        a.sign = +1;
+        a.post = corr_[1].get();
+        launch_axis_fft(ctx, a);
+    }
+    {
+        AxisFFT a;
+        a.in = h2_.get();
+        a.in_t = E_C64;
+        a.out = out;
+        a.out_t = E_F32;
+        a.n_outer = nvol;
+        a.n_inner = (long)n2 * n3;
+        a.in_ostride = (long)fz * n2 * n3;
+        a.out_ostride = (long)n1 * n2 * n3;
+        a.n_in = fz;
+        a.L = fz;
+        a.n_out = n1;
+        a.out_map = OUT_MODES;
+        a.sign = +1;
+        a.post = corr_[2].get();
+        a.scale = scale;
+        launch_axis_fft(ctx, a);
+    }
+}
+
+void NufftPlan::type2_real(Context &ctx, const float *in, int nvol, float2 *c, PtMode mode) {
+    cudaStream_t st = ctx.stream();
+    const int n3 = modes_[0], n2 = modes_[1], n1 = modes_[2];
+    const int fx = nf_[0], fy = nf_[1], fz = nf_[2];
+    const long gvol = (long)fx * fy * fz;
+    grid_.ensure(gvol * nvol, st);
+    h1_.ensure((long)nvol * fz * fy * n3, st);
+    if (dim_ == 2) {
+        AxisFFT a;
+        a.in = in;
+        a.in_t = E_F32;
+        a.out = h1_.get();
+        a.out_t = E_C64;
+        a.n_outer = nvol;
+        a.n_inner = n3;
+        a.in_ostride = (long)n2 * n3;
+        a.out_ostride = (long)fy * n3;
+        a.n_in = n2;
+        a.in_map = IN_MODES;
+        a.L = fy;
+        a.n_out = fy;
+        a.sign = -1;
+        a.pre = corr_[1].get();
+        a.linefac = corr_[0].get();
+        launch_axis_fft(ctx, a);
+    } else {
+        h2_.ensure((long)nvol * fz * n2 * n3, st);
+        {
+            AxisFFT a;
+            a.in = in;
+            a.in_t = E_F32;
+            a.out = h2_.get();
+            a.out_t = E_C64;
+            a.n_outer = nvol;
+            a.n_inner = (long)n2 * n3;
+            a.in_ostride = (long)n1 * n2 * n3;
+            a.out_ostride = (long)fz * n2 * n3;
+            a.n_in = n1;
+            a.in_map = IN_MODES;
+            a.L = fz;
+            a.n_out = fz;
+            a.sign = -1;
+            a.pre = corr_[2].get();
+            a.linefac = corr_xy_.get();
+            launch_axis_fft(ctx, a);
+        }
+        {
+            AxisFFT a;
+            a.in = h2_.get();
+            a.in_t = E_C64;
+            a.out = h1_.get();
+            a.out_t = E_C64;
+            a.n_outer = (long)nvol * fz;
+            a.n_inner = n3;
+            a.in_ostride = (long)n2 * n3;
+            a.out_ostride = (long)fy * n3;
+            a.n_in = n2;
+            a.in_map = IN_MODES;
+            a.L = fy;
+            a.n_out = fy;
+            a.sign = -1;
+            launch_axis_fft(ctx, a);
+        }
+    }
+    {
+        AxisFFT a;
+        a.in = h1_.get();
+        a.in_t = E_C64;
+        a.out = grid_.get();
+        a.out_t = E_C64;
+        a.n_outer = (long)nvol * fz * fy;
+        a.n_inner = 1;
+        a.in_ostride = n3;
+        a.out_ostride = fx;
+        a.n_in = n3;
+        a.in_map = IN_MODES;
+        a.L = fx;
+        a.n_out = fx;
+        a.sign = -1;
+        launch_axis_fft(ctx, a);
+    }
+    interp(ctx, grid_.get(), nvol, c, mode);
+}
+
+}  // namespace lc

@@ -1,0 +1,128 @@
+// Host runtime: context, FFT plan cache and twiddle tables.
+#include <cmath>
+#include <cstdint>
+
+#include "lc_runtime.hpp"
+
+namespace lc {
+
+bool is_smooth23(long n) {
+    if (n < 1) return false;
+    while (n % 2 == 0) n /= 2;
+    while (n % 3 == 0) n /= 3;
+    return n == 1;
+}
+
+long next_smooth23(long n) {
+    long best = 1;
+    while (best < n) best <<= 1;
+    for (long q3 = 3; q3 < best; q3 *= 3) {
+        long x = q3;
+        while (x < n) x <<= 1;
+        if (x < best) best = x;
+    }
+    return best;
+}
+
+static void factorise(int L, FFTPlan &pl) {
+    pl.L = L;
+    pl.nst = 0;
+    int r = L;
+    while (r % 8 == 0) {
+        pl.radix[pl.nst++] = 8;
+        r /= 8;
+    }
+    if (r % 4 == 0) {
+        pl.radix[pl.nst++] = 4;
+        r /= 4;
+    }
+    if (r % 2 == 0) {
+        pl.radix[pl.nst++] = 2;
+        r /= 2;
+    }
+    while (r % 3 == 0) {
+        pl.radix[pl.nst++] = 3;
+        r /= 3;
+    }
+    LC_REQUIRE(r == 1 && pl.nst <= kMaxStages, "FFT length must be 2^p*3^q");
+}
+
+const FFTPlan &PlanCache::get(int L, bool fp64, cudaStream_t s) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto key = std::make_pair(L, fp64);
+    auto it = plans_.find(key);
+    if (it != plans_.end()) return it->second->plan;
+    auto e = std::make_unique<PlanEntry>();
+    factorise(L, e->plan);
+    const double two_pi = 6.283185307179586476925286766559;
+    if (fp64) {
+        std::vector<double2> h(L);
+        for (int m = 0; m < L; ++m) {
+            double a = two_pi * (double)m / (double)L;
+            h[m] = make_double2(std::cos(a), -std::sin(a));
+        }
+        e->tw.alloc(sizeof(double2) * L, s);
+        LC_CUDA(cudaMemcpyAsync(e->tw.get(), h.data(), sizeof(double2) * L,
+                                cudaMemcpyHostToDevice, s));
+    } else {
+        std::vector<float2> h(L);
+        for (int m = 0; m < L; ++m) {
+            double a = two_pi * (double)m / (double)L;
+            h[m] = make_float2((float)std::cos(a), (float)-std::sin(a));
+        }
+        e->tw.alloc(sizeof(float2) * L, s);
+        LC_CUDA(cudaMemcpyAsync(e->tw.get(), h.data(), sizeof(float2) * L,
+                                cudaMemcpyHostToDevice, s));
+    }
+    // the host vectors die here; make the copy complete first
+    LC_CUDA(cudaStreamSynchronize(s));
+    e->plan.tw = e->tw.get();
+    auto &ref = e->plan;
+    plans_[key] = std::move(e);
+    return ref;
+}
+
+const float2 *PlanCache::dft_twiddles(int n, cudaStream_t s) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = dft_.find(n);
+    if (it != dft_.end()) return it->second->get();
+    std::vector<float2> h(n);
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int m = 0; m < n; ++m) {
+        double a = two_pi * (double)m / (double)n;
+        h[m] = make_float2((float)std::cos(a), (float)-std::sin(a));
+    }
+    auto b = std::make_unique<DevBuf<float2>>(n, s);
+    LC_CUDA(cudaMemcpyAsync(b->get(), h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, s));
+    LC_CUDA(cudaStreamSynchronize(s));
+    const float2 *p = b->get();
+    dft_[n] = std::move(b);
+    return p;
+}
+
+Context::Context(int device, cudaStream_t stream) : device_(device) {
+    DeviceGuard g(device);
+    LC_CUDA(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+    stream_ = stream ? stream : own_stream_;
+    cudaDeviceProp prop;
+    LC_CUDA(cudaGetDeviceProperties(&prop, device));
+    num_sms_ = prop.multiProcessorCount;
+    max_smem_ = prop.sharedMemPerBlockOptin;
+    // keep freed pool memory cached in the process instead of returning it
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+}
+
+Context::~Context() {
+    cudaSetDevice(device_);
+    plans_.clear();
+    if (own_stream_) {
+        cudaStreamSynchronize(own_stream_);
+        cudaStreamDestroy(own_stream_);
+    }
+}
+
+}  // namespace lc

@@ -1,0 +1,144 @@
+// Host runtime of laminocam_b200: device context, stream-ordered buffers and
+// the FFT plan cache.  Everything here is plain C++ over the CUDA runtime.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "lc_common.cuh"
+
+namespace lc {
+
+// Device buffer allocated from the stream-ordered pool of the context's device
+// (cudaMallocAsync): repeated create/destroy cycles reuse pool memory instead
+// of calling the driver allocator.
+template <typename T>
+class DevBuf {
+  public:
+    DevBuf() = default;
+    DevBuf(size_t n, cudaStream_t s) { alloc(n, s); }
+    ~DevBuf() { release(); }
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p_(o.p_), n_(o.n_), s_(o.s_) {
+        o.p_ = nullptr;
+        o.n_ = 0;
+    }
+    DevBuf &operator=(DevBuf &&o) noexcept {
+        if (this != &o) {
+            release();
+            p_ = o.p_;
+            n_ = o.n_;
+            s_ = o.s_;
+            o.p_ = nullptr;
+            o.n_ = 0;
+        }
+        return *this;
+    }
+    void alloc(size_t n, cudaStream_t s) {
+        release();
+        s_ = s;
+        n_ = n;
+        if (n) LC_CUDA(cudaMallocAsync((void **)&p_, n * sizeof(T), s));
+    }
+    // grow-only: keeps the buffer when it is already large enough
+    void ensure(size_t n, cudaStream_t s) {
+        if (n > n_) alloc(n, s);
+    }
+    void release() {
+        if (p_) cudaFreeAsync(p_, s_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    void zero(cudaStream_t s) {
+        if (n_) LC_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s));
+    }
+    void upload(const T *h, size_t n, cudaStream_t s) {
+        ensure(n, s);
+        LC_CUDA(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    T *get() const { return p_; }
+    size_t size() const { return n_; }
+
+  private:
+    T *p_ = nullptr;
+    size_t n_ = 0;
+    cudaStream_t s_ = nullptr;
+};
+
+// FFT plan: factorisation of L into radices 8/4/2/3 and a twiddle table in
+// the requested precision.  Lengths must be 2^p * 3^q.
+struct PlanEntry {
+    FFTPlan plan{};
+    DevBuf<char> tw;
+};
+
+bool is_smooth23(long n);
+long next_smooth23(long n);  // smallest 2^p 3^q >= n
+
+class Context;
+
+// Per-device cache of FFT plans and twiddle tables.
+class PlanCache {
+  public:
+    const FFTPlan &get(int L, bool fp64, cudaStream_t s);
+    // twiddle table exp(-2*pi*i*m/n) for a direct DFT of arbitrary n (float2)
+    const float2 *dft_twiddles(int n, cudaStream_t s);
+    void clear() {
+        std::lock_guard<std::mutex> lk(mu_);
+        plans_.clear();
+        dft_.clear();
+    }
+
+  private:
+    std::mutex mu_;
+    std::map<std::pair<int, bool>, std::unique_ptr<PlanEntry>> plans_;
+    std::map<int, std::unique_ptr<DevBuf<float2>>> dft_;
+};
+
+class Context {
+  public:
+    Context(int device, cudaStream_t stream);
+    ~Context();
+    int device() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
+    void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+    PlanCache &plans() { return plans_; }
+    int num_sms() const { return num_sms_; }
+    size_t max_smem() const { return max_smem_; }
+    std::string last_error;
+    int verbose = 0;
+
+  private:
+    int device_;
+    cudaStream_t stream_;
+    cudaStream_t own_stream_ = nullptr;
+    PlanCache plans_;
+    int num_sms_ = 148;
+    size_t max_smem_ = 227 * 1024;
+};
+
+// Makes `dev` current for the lifetime of the guard.
+class DeviceGuard {
+  public:
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev_);
+        if (prev_ != dev) LC_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() {
+        int cur;
+        cudaGetDevice(&cur);
+        if (cur != prev_) cudaSetDevice(prev_);
+    }
+
+  private:
+    int prev_ = 0;
+};
+
+}  // namespace lc

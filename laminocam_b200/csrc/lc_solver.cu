@@ -1,0 +1,412 @@
+// Fused solver kernels: CG updates with FP64 reductions finished by the last
+// CTA (deterministic fixed-order sum of per-CTA partials), and the
+// Split-Bregman stencil kernels (right-hand side, shrinkage + Bregman update).
+#include <algorithm>
+
+#include "lc_solver.hpp"
+#include "lc_toeplitz.hpp"
+
+namespace lc {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kParts = 4;  // partial sums per CTA
+
+template <typename A>
+__device__ __forceinline__ A warp_sum(A v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-reduce up to kParts sums and store them as this CTA's partials.
+// Returns true in every thread of the CTA that finished last.
+template <typename A, int K>
+__device__ bool block_partials(A (&v)[K], double *part, unsigned *counter) {
+    __shared__ A sh[K][kThreads / 32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        A s = warp_sum(v[k]);
+        if (lane == 0) sh[k][wid] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            A s = lane < (int)(blockDim.x >> 5) ? sh[k][lane] : A(0);
+            s = warp_sum(s);
+            if (lane == 0) part[(long)blockIdx.x * kParts + k] = (double)s;
+        }
+    }
+    __threadfence();
+    if (threadIdx.x == 0) {
+        unsigned t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    return last;
+}
+
+// Fixed-order total of partial k over all CTAs (called by the last CTA).
+template <typename A>
+__device__ double total(const double *part, int k, int nblk) {
+    __shared__ A sh[kThreads / 32];
+    A s = A(0);
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += (A)part[(long)b * kParts + k];
+    s = warp_sum(s);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = s;
+    __syncthreads();
+    A t = A(0);
+    if (threadIdx.x < 32) {
+        t = lane < (int)(blockDim.x >> 5) ? sh[lane] : A(0);
+        t = warp_sum(t);
+    }
+    __shared__ A res;
+    if (threadIdx.x == 0) res = t;
+    __syncthreads();
+    double out = (double)res;
+    __syncthreads();
+    return out;
+}
+
+// r = y - r(=A x0);  p = r;  partials y.y, r.r
+template <typename A>
+__global__ void __launch_bounds__(kThreads) cg_init_kernel(const float *__restrict__ y, float *r,
+                                                          float *p, long n, double *part,
+                                                          unsigned *counter, CGState *st) {
+    if (st->sb_done) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->done = 1;
+        return;
+    }
+    A v[2] = {A(0), A(0)};
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        float yi = y[i];
+        float ri = yi - r[i];
+        r[i] = ri;
+        p[i] = ri;
+        v[0] += (A)yi * (A)yi;
+        v[1] += (A)ri * (A)ri;
+    }
+    if (block_partials<A, 2>(v, part, counter)) {
+        double y2 = total<A>(part, 0, gridDim.x);
+        double r2 = total<A>(part, 1, gridDim.x);
+        if (threadIdx.x == 0) {
+            st->y2 = y2;
+            st->rs_old = r2;
+            st->iters = 0;
+            st->done = 0;
+            st->reason = 0;
+            st->res = 0;
+            st->dx = 0;
+            *counter = 0;
+        }
+    }
+}
+
+template <typename A>
+__global__ void __launch_bounds__(kThreads) dot_pap_kernel(const float *__restrict__ p,
+                                                          const float *__restrict__ ap, long n,
+                                                          double *part, unsigned *counter,
+                                                          CGState *st) {
+    if (st->done) return;
+    A v[1] = {A(0)};
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        v[0] += (A)p[i] * (A)ap[i];
+    if (block_partials<A, 1>(v, part, counter)) {
+        double pap = total<A>(part, 0, gridDim.x);
+        if (threadIdx.x == 0) {
+            st->pAp = pap;
+            if (fabs(pap) < 1e-10) {
+                st->done = 1;
+                st->reason = 3;
+            } else {
+                st->alpha = (double)((A)st->rs_old / (A)pap);
+            }
+            *counter = 0;
+        }
+    }
+}
+
+// x += a p; r -= a Ap; partials r.r, |a p|^2, x.x; then beta, stopping tests
+template <typename A>
+__global__ void __launch_bounds__(kThreads) cg_update_kernel(float *x, float *r,
+                                                            const float *__restrict__ p,
+                                                            const float *__restrict__ ap, long n,
+                                                            double *part, unsigned *counter,
+                                                            CGState *st, float tol, float xtol) {
+    if (st->done) return;
+    const float a = (float)st->alpha;
+    A v[3] = {A(0), A(0), A(0)};
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        float step = a * p[i];
+        float xi = x[i] + step;
+        float ri = fmaf(-a, ap[i], r[i]);
+        x[i] = xi;
+        r[i] = ri;
+        v[0] += (A)ri * (A)ri;
+        v[1] += (A)step * (A)step;
+        v[2] += (A)xi * (A)xi;
+    }
+    if (block_partials<A, 3>(v, part, counter)) {
+        double rs_new = total<A>(part, 0, gridDim.x);
+        double s2 = total<A>(part, 1, gridDim.x);
+        double x2 = total<A>(part, 2, gridDim.x);
+        if (threadIdx.x == 0) {
+            st->beta = (double)((A)rs_new / (A)st->rs_old);
+            st->rs_old = rs_new;
+            double res = sqrt(rs_new) / (sqrt(st->y2) + 1e-8);
+            double dx = sqrt(s2) / (sqrt(x2) + 1e-8);
+            st->res = res;
+            st->dx = dx;
+            st->iters += 1;
+            if (res < (double)tol) {
+                st->done = 1;
+                st->reason = 1;
+            } else if (dx < (double)xtol) {
+                st->done = 1;
+                st->reason = 2;
+            }
+            *counter = 0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) p_update_kernel(float *p, const float *__restrict__ r,
+                                                           long n, const CGState *st) {
+    if (st->done) return;
+    const float b = (float)st->beta;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        p[i] = fmaf(b, p[i], r[i]);
+}
+
+struct Dims {
+    long n1, n2, n3;
+};
+
+__device__ __forceinline__ float at(const float *f, long i, long j, long k, const Dims &d) {
+    return (i >= 0 && j >= 0 && k >= 0 && i < d.n1 && j < d.n2 && k < d.n3)
+               ? f[(i * d.n2 + j) * d.n3 + k]
+               : 0.f;
+}
+
+// rhs = yT - mu * div(d - b); div = D_n3(v0) + D_n2(v1) + D_n1(v2), zero padded
+__global__ void __launch_bounds__(kThreads) sb_rhs_kernel(const float *__restrict__ yT,
+                                                         const float *d0, const float *d1,
+                                                         const float *d2, const float *b0,
+                                                         const float *b1, const float *b2,
+                                                         float *rhs, Dims dm, float mu,
+                                                         const CGState *st) {
+    if (st->sb_done) return;
+    long total_n = dm.n1 * dm.n2 * dm.n3;
+    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total_n;
+         idx += (long)gridDim.x * blockDim.x) {
+        long i = idx / (dm.n2 * dm.n3);
+        long rr = idx - i * dm.n2 * dm.n3;
+        long j = rr / dm.n3, k = rr - j * dm.n3;
+        float dv = 0.5f * ((at(d0, i, j, k + 1, dm) - at(b0, i, j, k + 1, dm)) -
+                           (at(d0, i, j, k - 1, dm) - at(b0, i, j, k - 1, dm))) +
+                   0.5f * ((at(d1, i, j + 1, k, dm) - at(b1, i, j + 1, k, dm)) -
+                           (at(d1, i, j - 1, k, dm) - at(b1, i, j - 1, k, dm))) +
+                   0.5f * ((at(d2, i + 1, j, k, dm) - at(b2, i + 1, j, k, dm)) -
+                           (at(d2, i - 1, j, k, dm) - at(b2, i - 1, j, k, dm)));
+        rhs[idx] = fmaf(-mu, dv, yT[idx]);
+    }
+}
+
+// g = grad x; t = g + b; s = |t|; d = max(0, s - lam/mu) t / (s + 1e-8); b += g - d
+__global__ void __launch_bounds__(kThreads) sb_shrink_kernel(const float *__restrict__ x, float *d0,
+                                                            float *d1, float *d2, float *b0,
+                                                            float *b1, float *b2, Dims dm,
+                                                            float thresh, const CGState *st) {
+    if (st->sb_done) return;
+    long total_n = dm.n1 * dm.n2 * dm.n3;
+    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total_n;
+         idx += (long)gridDim.x * blockDim.x) {
+        long i = idx / (dm.n2 * dm.n3);
+        long rr = idx - i * dm.n2 * dm.n3;
+        long j = rr / dm.n3, k = rr - j * dm.n3;
+        float g0 = 0.5f * (at(x, i, j, k + 1, dm) - at(x, i, j, k - 1, dm));
+        float g1 = 0.5f * (at(x, i, j + 1, k, dm) - at(x, i, j - 1, k, dm));
+        float g2 = 0.5f * (at(x, i + 1, j, k, dm) - at(x, i - 1, j, k, dm));
+        float t0 = g0 + b0[idx], t1 = g1 + b1[idx], t2 = g2 + b2[idx];
+        float s = sqrtf(t0 * t0 + t1 * t1 + t2 * t2);
+        float m = fmaxf(0.f, s - thresh);
+        float inv = 1.0f / (s + 1e-8f);
+        float e0 = m * (t0 * inv), e1 = m * (t1 * inv), e2 = m * (t2 * inv);
+        d0[idx] = e0;
+        d1[idx] = e1;
+        d2[idx] = e2;
+        b0[idx] = b0[idx] + (g0 - e0);
+        b1[idx] = b1[idx] + (g1 - e1);
+        b2[idx] = b2[idx] + (g2 - e2);
+    }
+}
+
+template <typename A>
+__global__ void __launch_bounds__(kThreads) sb_diff_kernel(const float *__restrict__ x, float *xold,
+                                                          long n, double *part, unsigned *counter,
+                                                          CGState *st, float xtol) {
+    if (st->sb_done) return;
+    A v[2] = {A(0), A(0)};
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        float xi = x[i], xo = xold[i];
+        float df = xi - xo;
+        v[0] += (A)df * (A)df;
+        v[1] += (A)xo * (A)xo;
+        xold[i] = xi;
+    }
+    if (block_partials<A, 2>(v, part, counter)) {
+        double d2 = total<A>(part, 0, gridDim.x);
+        double o2 = total<A>(part, 1, gridDim.x);
+        if (threadIdx.x == 0) {
+            double rel = sqrt(d2) / (sqrt(o2) + 1e-8);
+            st->sb_rel = rel;
+            st->sb_iters += 1;
+            if (rel < (double)xtol) st->sb_done = 1;
+            *counter = 0;
+        }
+    }
+}
+
+__global__ void reset_state_kernel(CGState *st) {
+    CGState z{};
+    *st = z;
+}
+
+}  // namespace
+
+Solver::Solver(Context &ctx, long n) : n_(n) {
+    cudaStream_t s = ctx.stream();
+    nblk_ = (int)std::max<long>(1, std::min<long>((n + kThreads * 4 - 1) / (kThreads * 4),
+                                                  (long)ctx.num_sms() * 4));
+    r_.alloc(n, s);
+    p_.alloc(n, s);
+    ap_.alloc(n, s);
+    part_.alloc((long)nblk_ * kParts, s);
+    counter_.alloc(1, s);
+    counter_.zero(s);
+    st_.alloc(1, s);
+    LC_CUDA(cudaMallocHost((void **)&host_st_, sizeof(CGState)));
+}
+
+void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, int iters,
+                    float tol, float xtol, int fp32, int poll_every, bool in_sb) {
+    cudaStream_t s = ctx.stream();
+    A(x, ap_.get());
+    // r <- A x0 (moved), then r = y - r, p = r
+    LC_CUDA(cudaMemcpyAsync(r_.get(), ap_.get(), n_ * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    if (fp32)
+        cg_init_kernel<float><<<nblk_, kThreads, 0, s>>>(y, r_.get(), p_.get(), n_, part_.get(),
+                                                         counter_.get(), st_.get());
+    else
+        cg_init_kernel<double><<<nblk_, kThreads, 0, s>>>(y, r_.get(), p_.get(), n_, part_.get(),
+                                                          counter_.get(), st_.get());
+    LC_CHECK_LAUNCH();
+    for (int it = 0; it < iters; ++it) {
+        A(p_.get(), ap_.get());
+        if (fp32) {
+            dot_pap_kernel<float><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
+                                                             counter_.get(), st_.get());
+            cg_update_kernel<float><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), n_,
+                                                               part_.get(), counter_.get(),
+                                                               st_.get(), tol, xtol);
+        } else {
+            dot_pap_kernel<double><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
+                                                              counter_.get(), st_.get());
+            cg_update_kernel<double><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), n_,
+                                                                part_.get(), counter_.get(),
+                                                                st_.get(), tol, xtol);
+        }
+        p_update_kernel<<<nblk_, kThreads, 0, s>>>(p_.get(), r_.get(), n_, st_.get());
+        LC_CHECK_LAUNCH();
+        if (!in_sb && poll_every > 0 && (it + 1) % poll_every == 0 && it + 1 < iters) {
+            LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
+            LC_CUDA(cudaStreamSynchronize(s));
+            if (host_st_->done) break;
+        }
+    }
+}
+
+void Solver::cg(Context &ctx, const Operator &A, const float *y, float *x, const SolverParams &p,
+                SolverStats *stats) {
+    cudaStream_t s = ctx.stream();
+    reset_state_kernel<<<1, 1, 0, s>>>(st_.get());
+    LC_CHECK_LAUNCH();
+    int poll = (p.tol > 0 || p.xtol > 0) ? p.poll_every : 0;
+    cg_run(ctx, A, y, x, p.max_iters, p.tol, p.xtol, p.fp32_scalars, poll, false);
+    LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
+    LC_CUDA(cudaStreamSynchronize(s));
+    if (stats) {
+        stats->iters = host_st_->iters;
+        stats->cg_iters_total = host_st_->iters;
+        stats->residual = host_st_->res;
+        stats->dx = host_st_->dx;
+        stats->stop_reason = host_st_->reason;
+    }
+}
+
+void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3], const float *yT,
+                           float *x, const SolverParams &p, SolverStats *stats) {
+    cudaStream_t s = ctx.stream();
+    LC_REQUIRE(dims[0] * dims[1] * dims[2] == n_, "split_bregman: dims do not match the solver size");
+    for (int a = 0; a < 3; ++a) {
+        d_[a].ensure(n_, s);
+        b_[a].ensure(n_, s);
+        d_[a].zero(s);
+        b_[a].zero(s);
+    }
+    rhs_.ensure(n_, s);
+    xold_.ensure(n_, s);
+    LC_CUDA(cudaMemcpyAsync(xold_.get(), x, n_ * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    reset_state_kernel<<<1, 1, 0, s>>>(st_.get());
+    LC_CHECK_LAUNCH();
+    const float mu = p.mu;
+    long dcopy[3] = {dims[0], dims[1], dims[2]};
+    Operator Ap = [&](const float *in, float *out) {
+        AtA(in, out);
+        launch_neg_laplacian_axpy(ctx, in, out, dcopy, mu);
+    };
+    Dims dm{dims[0], dims[1], dims[2]};
+    unsigned gsz = (unsigned)std::max<long>(1, std::min<long>((n_ + kThreads - 1) / kThreads,
+                                                             (long)ctx.num_sms() * 16));
+    int total_cg = 0;
+    int poll = p.xtol > 0 ? std::max(1, p.poll_every) : 0;
+    for (int it = 0; it < p.max_iters; ++it) {
+        sb_rhs_kernel<<<gsz, kThreads, 0, s>>>(yT, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(),
+                                                b_[1].get(), b_[2].get(), rhs_.get(), dm, mu, st_.get());
+        LC_CHECK_LAUNCH();
+        cg_run(ctx, Ap, rhs_.get(), x, p.inner_iters, p.tol, p.xtol, p.fp32_scalars, 0, true);
+        total_cg += p.inner_iters;
+        sb_shrink_kernel<<<gsz, kThreads, 0, s>>>(x, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(),
+                                                   b_[1].get(), b_[2].get(), dm, p.lambda / p.mu,
+                                                   st_.get());
+        LC_CHECK_LAUNCH();
+        if (p.fp32_scalars)
+            sb_diff_kernel<float><<<nblk_, kThreads, 0, s>>>(x, xold_.get(), n_, part_.get(),
+                                                             counter_.get(), st_.get(), p.xtol);
+        else
+            sb_diff_kernel<double><<<nblk_, kThreads, 0, s>>>(x, xold_.get(), n_, part_.get(),
+                                                              counter_.get(), st_.get(), p.xtol);
+        LC_CHECK_LAUNCH();
+        if (poll > 0 && (it + 1) % poll == 0 && it + 1 < p.max_iters) {
+            LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
+            LC_CUDA(cudaStreamSynchronize(s));
+            if (host_st_->sb_done) break;
+        }
+    }
+    LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
+    LC_CUDA(cudaStreamSynchronize(s));
+    if (stats) {
+        stats->iters = host_st_->sb_iters;
+        stats->cg_iters_total = total_cg;
+        stats->residual = host_st_->res;
+        stats->dx = host_st_->sb_rel;
+        stats->stop_reason = host_st_->sb_done ? 2 : 0;
+    }
+}
+
+}  // namespace lc

@@ -1,0 +1,72 @@
+// CG and Split-Bregman (isotropic TV) on the device.
+//
+// Algorithms follow src/conjgrad.cpp:33-76 / src/gpu/conjgrad.cu:45-108 and
+// src/bregman.cpp:36-94 / src/gpu/bregman.cu:88-165 of the reference.  All
+// solver scalars (alpha, beta, r.r, p.Ap, the norms and the stopping tests)
+// live in device memory and are computed in FP64 by the last CTA of each
+// fused reduction, so an iteration never waits on the host.  Once a stopping
+// test fires, a device flag turns the remaining update kernels into no-ops.
+#pragma once
+
+#include <functional>
+
+#include "lc_runtime.hpp"
+
+namespace lc {
+
+struct SolverParams {
+    int max_iters = 50;   // CG iterations, or Split-Bregman outer iterations
+    int inner_iters = 1;  // CG iterations per Split-Bregman outer iteration
+    float tol = 1e-5f;
+    float xtol = 1e-5f;
+    float lambda = 0.1f;
+    float mu = 10.0f;
+    int fp32_scalars = 0;  // 1: float accumulation of dots (the reference GPU path)
+    int poll_every = 8;    // iterations between host checks of the stop flag (0: never)
+};
+
+struct SolverStats {
+    int iters = 0;          // CG iterations, or outer iterations for Split-Bregman
+    int cg_iters_total = 0;
+    double residual = 0;    // ||r|| / (||y|| + 1e-8) of the last CG iteration
+    double dx = 0;          // last CG relative step, or Split-Bregman relative change
+    int stop_reason = 0;    // 0 max iters, 1 residual, 2 step, 3 |pAp| tiny
+};
+
+// device-resident solver state
+struct CGState {
+    double rs_old, pAp, alpha, beta;
+    double y2;
+    double res, dx;
+    int iters, done, reason, pad;
+    // Split-Bregman
+    double sb_diff2, sb_old2, sb_rel;
+    int sb_iters, sb_done;
+};
+
+using Operator = std::function<void(const float *in, float *out)>;
+
+class Solver {
+  public:
+    Solver(Context &ctx, long n);
+    // x (in: x0, out: solution); y = right-hand side
+    void cg(Context &ctx, const Operator &A, const float *y, float *x, const SolverParams &p,
+            SolverStats *stats);
+    // A is the normal operator A^T A alone; mu * (-laplacian) is added here.
+    void split_bregman(Context &ctx, const Operator &AtA, const long dims[3], const float *yT,
+                       float *x, const SolverParams &p, SolverStats *stats);
+
+  private:
+    void cg_run(Context &ctx, const Operator &A, const float *y, float *x, int iters, float tol,
+                float xtol, int fp32, int poll_every, bool in_sb);
+    long n_;
+    int nblk_;
+    DevBuf<float> r_, p_, ap_, xold_;
+    DevBuf<float> d_[3], b_[3], rhs_;
+    DevBuf<double> part_;
+    DevBuf<unsigned> counter_;
+    DevBuf<CGState> st_;
+    CGState *host_st_ = nullptr;
+};
+
+}  // namespace lc

@@ -1,0 +1,55 @@
+// Toeplitz normal operator A^T A as a convolution with the point-spread
+// function of the polar grid (include/toeplitz.h:61-129 and
+// include/toeplitz2d.h:81-125 of the reference).
+//
+// The PSF is K(k) = Re sum_j exp(i k.x_j) on the P-grid, P = next 2^p3^q >=
+// 2n-1 per axis, with unit weights at every grid point (no mask).  On a polar
+// grid the sum over the radial samples of one angle is a Dirichlet kernel,
+//     sum_m exp(i u r_m) = sin(pi u) / sin(pi u / n),
+// so K is generated exactly, in FP64, as a sum over angles of products of
+// Dirichlet kernels (one factor in 2D, two in 3D) instead of a type-1 NUFFT of
+// ones.  K is real and even, so the spectrum of the zero-centred kernel K0 is
+// real and even too; only its first octant (quadrant in 2D) is kept, in FP32.
+// Convolving with K0 and cropping at offset 0 equals the reference's
+// convolution with the centred kernel cropped at P/2.
+#pragma once
+
+#include "lc_nufft.hpp"
+
+namespace lc {
+
+class Toeplitz {
+  public:
+    // dims = {n1, n2, n3}: volume (3D) or stack of n1 independent n2 x n3
+    // slices (2D, n2 == n3 required by the reference API).
+    Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], bool three_d);
+    void apply(Context &ctx, const float *x, float *y);
+    // y = A^T A x + mu * (-laplacian(x))
+    void apply_reg(Context &ctx, const float *x, float *y, float mu);
+
+    const long *dims() const { return n_; }
+    const int *P() const { return P_; }
+    bool three_d() const { return three_d_; }
+    long nvox() const { return n_[0] * n_[1] * n_[2]; }
+    long spectrum_elems() const { return (long)Ph_[0] * Ph_[1] * Ph_[2]; }
+    const float *spectrum() const { return R_.get(); }
+    // FP64 PSF K on the P-grid in mode order (k = j - P/2), for tests
+    void kernel_fp64(Context &ctx, double *host_out);
+    // bytes the apply must move at minimum (algorithmic traffic)
+    double algorithmic_bytes() const;
+
+  private:
+    void build_kernel(Context &ctx, DevBuf<double> &K);
+    bool three_d_;
+    long n_[3];
+    int P_[3];
+    int Ph_[3];
+    const PolarGeometry *g_;
+    DevBuf<float> R_;
+    DevBuf<float2> t1_, t2_;
+    double scale_;
+};
+
+void launch_neg_laplacian_axpy(Context &ctx, const float *x, float *y, const long dims[3], float mu);
+
+}  // namespace lc

@@ -1,0 +1,156 @@
+"""GPU parity of the CUDA path (through the C ABI) against the FP64 oracle and the
+golden fixtures.  Tolerances: projections, backprojections and A^T A within
+1e-5 relative L2 at NUFFT tol 1e-6; reconstructions after a fixed iteration
+count within 1e-4 relative L2."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+PROJ_TOL = 1e-5
+RECON_TOL = 1e-4
+
+
+def load(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+@pytest.fixture(scope="module")
+def lc(cuda):
+    import laminocam_b200 as lc
+    return lc
+
+
+def to_np(t):
+    return t.detach().cpu().numpy().astype(np.float64)
+
+
+@pytest.mark.parametrize("f", ["golden2d_odd.npz", "golden2d_even.npz", "golden2d_nr.npz"])
+def test_projection_ops_2d_golden(lc, f):
+    g = load(f)
+    th, nr = g["theta"], int(g["nr"])
+    vol, sino = g["vol"], g["sino"]
+    ns, n = vol.shape[0], vol.shape[1]
+    pg = lc.PolarGrid2D(th, nr)
+    assert O.rel_l2(to_np(lc.forward2d(vol, pg)), g["forward2d"]) < PROJ_TOL
+    assert O.rel_l2(to_np(lc.backproj2d(sino, pg, (ns, n, n))), g["backproj2d"]) < PROJ_TOL
+    assert O.rel_l2(to_np(lc.sysmat2d(vol, pg)), g["sysmat2d_nufft"]) < PROJ_TOL
+
+
+@pytest.mark.parametrize("f", ["golden2d_odd.npz", "golden2d_even.npz", "golden2d_nr.npz"])
+def test_toeplitz_2d_golden(lc, f):
+    g = load(f)
+    th, nr = g["theta"], int(g["nr"])
+    vol = g["vol"]
+    ns, n = vol.shape[0], vol.shape[1]
+    pg = lc.PolarGrid2D(th, nr)
+    psf = lc.PointSpreadFunction2D(pg, n, ns)
+    K = psf.kernel()
+    assert O.rel_l2(K, g["psf_kernel"]) < 1e-12          # FP64 closed form vs exact NUDFT
+    assert O.rel_l2(to_np(psf.convolve(vol)), g["toeplitz"]) < PROJ_TOL
+
+
+@pytest.mark.parametrize("f", ["golden2d_odd.npz", "golden2d_even.npz", "golden2d_nr.npz"])
+def test_solvers_2d_golden(lc, f):
+    g = load(f)
+    th, nr = g["theta"], int(g["nr"])
+    sino = g["sino"]
+    ns, n = sino.shape[0], g["vol"].shape[1]
+    p = lc.ReconParams(regularizer="unconstrained", recon_dims=(ns, n, n), max_iters=10, tol=0, xtol=0)
+    x = lc.MBIR2D(sino, th, p)
+    assert O.rel_l2(x, g["cg10"]) < RECON_TOL
+    p = lc.ReconParams(regularizer="split_bregman", recon_dims=(ns, n, n), max_iters=4, inner_iters=2,
+                       lam=0.05, mu=2.0, tol=0, xtol=0)
+    x = lc.MBIR2D(sino, th, p)
+    assert O.rel_l2(x, g["sb4"]) < RECON_TOL
+
+
+@pytest.mark.parametrize("f", ["golden3d_a.npz", "golden3d_b.npz"])
+def test_projection_ops_3d_golden(lc, f):
+    g = load(f)
+    vol, proj = g["vol"], g["proj"]
+    pg = lc.PolarGrid(g["theta"], g["gamma"], g["beta"], int(g["nrows"]), int(g["ncols"]),
+                      shifts=g["shifts"])
+    assert O.rel_l2(to_np(lc.forward(vol, pg)), g["forward3d"]) < PROJ_TOL
+    assert O.rel_l2(to_np(lc.backproj(proj, pg, vol.shape)), g["backproj3d"]) < PROJ_TOL
+    assert O.rel_l2(to_np(lc.backproj(proj, pg, vol.shape, shifts=True)), g["backproj3d_shifted"]) < PROJ_TOL
+    assert O.rel_l2(to_np(lc.sysmat(vol, pg)), g["sysmat3d_nufft"]) < PROJ_TOL
+
+
+@pytest.mark.parametrize("f", ["golden3d_a.npz", "golden3d_b.npz"])
+def test_toeplitz_3d_golden(lc, f):
+    g = load(f)
+    vol = g["vol"]
+    pg = lc.PolarGrid(g["theta"], g["gamma"], g["beta"], int(g["nrows"]), int(g["ncols"]))
+    psf = lc.PointSpreadFunction(pg, vol.shape)
+    assert O.rel_l2(psf.kernel(), g["psf_kernel"]) < 1e-12
+    assert O.rel_l2(to_np(psf.convolve(vol)), g["toeplitz"]) < PROJ_TOL
+
+
+def test_mbir3d_golden(lc):
+    g = load("golden_mbir3d.npz")
+    rd = tuple(int(v) for v in g["recon_dims"])
+    ds = [lc.Dataset(g["projs"], g["theta"], float(g["gamma"]), 0.0)]
+    x = lc.MBIR(ds, lc.ReconParams(regularizer="unconstrained", recon_dims=rd, max_iters=6, tol=0, xtol=0))
+    assert O.rel_l2(x, g["cg6"]) < RECON_TOL
+    x = lc.MBIR(ds, lc.ReconParams(regularizer="split_bregman", recon_dims=rd, max_iters=3, tol=0, xtol=0))
+    assert O.rel_l2(x, g["sb3"]) < RECON_TOL
+
+
+def test_config1_sized_operators(lc):
+    """n = 255, 180 angles over [0, pi): forward, backproj and Toeplitz vs the oracle."""
+    rng = np.random.default_rng(100)
+    n, nth = 255, 180
+    th = np.arange(nth) * np.pi / nth
+    x = rng.random((1, n, n)).astype(np.float32)
+    y = rng.random((1, nth, n)).astype(np.float32)
+    pg = lc.PolarGrid2D(th, n)
+    assert O.rel_l2(to_np(lc.forward2d(x, pg)), O.forward2d(x.astype(np.float64), th, n)) < PROJ_TOL
+    assert O.rel_l2(to_np(lc.backproj2d(y, pg, (1, n, n))), O.backproj2d(y.astype(np.float64), th, (1, n, n))) < PROJ_TOL
+    psf = lc.PointSpreadFunction2D(pg, n, 1)
+    opsf = O.psf2d(th, n, n)
+    assert O.rel_l2(psf.kernel(), opsf.kernel) < 1e-12
+    assert O.rel_l2(to_np(psf.convolve(x)), O.convolve2d(x.astype(np.float64), opsf)) < PROJ_TOL
+
+
+@pytest.mark.parametrize("n,nth", [(64, 40), (128, 90)])
+def test_adjoint_identity_gpu(lc, n, nth):
+    """<R x, y> = <x, R^T y> for even detector counts (tests/test_adjoint2d.cpp:56-115), to 1e-6."""
+    rng = np.random.default_rng(n)
+    th = (np.arange(nth) - nth / 2.0) * np.pi / nth
+    x = rng.random((1, n, n)).astype(np.float32)
+    y = rng.random((1, nth, n)).astype(np.float32)
+    pg = lc.PolarGrid2D(th, n)
+    lhs = np.vdot(to_np(lc.forward2d(x, pg)), y.astype(np.float64))
+    rhs = np.vdot(x.astype(np.float64), to_np(lc.backproj2d(y, pg, (1, n, n))))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-6
+
+
+def test_toeplitz_matches_nufft_normal_operator_gpu(lc):
+    """tests/test_sysmat_toeplitz2d_gpu.cu:104-120: NUFFT vs Toeplitz A^T A on the GPU."""
+    rng = np.random.default_rng(7)
+    n, nth = 96, 60
+    th = (np.arange(nth) - nth / 2.0) * np.pi / nth
+    x = rng.random((2, n, n)).astype(np.float32)
+    pg = lc.PolarGrid2D(th, n)
+    a = to_np(lc.sysmat2d(x, pg))
+    b = to_np(lc.PointSpreadFunction2D(pg, n, 2).convolve(x))
+    assert O.rel_l2(b, a) < 5e-5
+
+
+def test_toeplitz_slice_independence(lc):
+    """tests/test_sysmat_toeplitz2d.cpp:98-137: batched slices equal single-slice runs."""
+    rng = np.random.default_rng(8)
+    n, nth = 31, 20
+    th = np.arange(nth) * np.pi / nth
+    x = rng.random((3, n, n)).astype(np.float32)
+    pg = lc.PolarGrid2D(th, n)
+    batched = to_np(lc.PointSpreadFunction2D(pg, n, 3).convolve(x))
+    single = lc.PointSpreadFunction2D(pg, n, 1)
+    for i in range(3):
+        assert O.rel_l2(batched[i], to_np(single.convolve(x[i:i + 1]))[0]) < 1e-6

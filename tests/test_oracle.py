@@ -1,0 +1,190 @@
+"""CPU tests of the FP64 oracle: golden fixtures, known answers, the reference's
+own identities (tests/test_adjoint*.cpp, tests/test_sysmat_toeplitz*.cpp), and
+the pin against the reference's sources built with the shim headers."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle import refrun as R
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+def test_next_fast_dim_table():
+    # include/toeplitz.h:42-51 on the sizes the configs produce
+    table = {509: 512, 1441: 1458, 57: 64, 765: 768, 1021: 1024, 4093: 4096, 9: 9, 717: 729,
+             41: 48, 1533: 1536, 253: 256, 2045: 2048, 1: 1, 2: 2, 3: 3, 5: 6, 7: 8}
+    for n, want in table.items():
+        assert O.next_fast_dim(n) == want, n
+
+
+def test_pad_size_matches_reference_rounding():
+    # src/gpu/mbir.cu:46-60: int(n * 1.4142f), forced odd
+    assert O.pad_size(511) == 721
+    assert O.pad_size(21) == 29
+    assert O.pad_size(255) == 359
+    assert O.pad_size(383) == 541
+    assert O.pad_size(31) == 43
+    assert O.pad_size(15) == 21
+
+
+def test_nudft_single_point_known_answer():
+    x = np.array([0.3])
+    y = np.array([-1.1])
+    F = O.nudft1_2d(np.array([[2.0 + 1j]]), x, y, 5, 4, +1)[0]
+    kx = np.arange(-2, 2)
+    ky = np.arange(-2, 3)
+    want = (2.0 + 1j) * np.exp(1j * (kx[None, :] * 0.3 + ky[:, None] * -1.1))
+    assert np.abs(F - want).max() < 1e-13
+    c = O.nudft2_2d(want[None], x, y, -1)[0, 0]
+    assert abs(c - np.sum(want * np.exp(-1j * (kx[None, :] * 0.3 + ky[:, None] * -1.1)))) < 1e-12
+
+
+@pytest.mark.parametrize("f", sorted(os.path.basename(p) for p in glob.glob(os.path.join(GOLD, "golden2d_*.npz"))))
+def test_oracle_reproduces_golden_2d(f):
+    g = load(f)
+    th, nr = g["theta"], int(g["nr"])
+    vol = g["vol"].astype(np.float64)
+    sino = g["sino"].astype(np.float64)
+    ns, n = vol.shape[0], vol.shape[1]
+    assert O.rel_l2(O.forward2d(vol, th, nr), g["forward2d"]) < 1e-13
+    assert O.rel_l2(O.backproj2d(sino, th, (ns, n, n)), g["backproj2d"]) < 1e-13
+    psf = O.psf2d(th, nr, n)
+    assert O.rel_l2(psf.kernel_hat, g["psf_kernel_hat"]) < 1e-13
+    assert O.rel_l2(O.convolve2d(vol, psf), g["toeplitz"]) < 1e-13
+
+
+@pytest.mark.parametrize("f", ["golden3d_a.npz", "golden3d_b.npz"])
+def test_oracle_reproduces_golden_3d(f):
+    g = load(f)
+    grid = O.Grid3D(g["theta"], g["gamma"], g["beta"], int(g["nrows"]), int(g["ncols"]))
+    vol = g["vol"].astype(np.float64)
+    proj = g["proj"].astype(np.float64)
+    assert O.rel_l2(O.forward3d(vol, grid), g["forward3d"]) < 1e-13
+    assert O.rel_l2(O.backproj3d(proj, grid, vol.shape), g["backproj3d"]) < 1e-13
+    sh = g["shifts"].astype(np.float64)
+    assert O.rel_l2(O.backproj3d(proj, grid, vol.shape, sh), g["backproj3d_shifted"]) < 1e-13
+
+
+@pytest.mark.parametrize("dims,nang", [((5, 16, 16), 7), ((8, 32, 32), 13)])
+def test_adjoint_identity_2d(dims, nang):
+    # tests/test_adjoint2d.cpp:56-115 (holds for even detector counts)
+    rng = np.random.default_rng(3)
+    th = (np.arange(nang) - nang / 2.0) * np.pi / nang
+    x = rng.random(dims)
+    y = rng.random((dims[0], nang, dims[2]))
+    lhs = np.vdot(O.forward2d(x, th), y)
+    rhs = np.vdot(x, O.backproj2d(y, th, dims))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-12
+
+
+def test_adjoint_identity_3d():
+    rng = np.random.default_rng(4)
+    th = (np.arange(7) - 3.5) * np.pi / 7
+    grid = O.Grid3D(th, np.full(7, 0.3), np.zeros(7), 16, 16)
+    x = rng.random((5, 16, 16))
+    y = rng.random((7, 16, 16))
+    lhs = np.vdot(O.forward3d(x, grid), y)
+    rhs = np.vdot(x, O.backproj3d(y, grid, x.shape))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-12
+
+
+@pytest.mark.parametrize("dims,nang", [((5, 16, 16), 7), ((2, 15, 15), 9)])
+def test_toeplitz_equals_nufft_normal_operator_2d(dims, nang):
+    # tests/test_sysmat_toeplitz2d.cpp:58-137
+    rng = np.random.default_rng(5)
+    th = (np.arange(nang) - nang / 2.0) * np.pi / nang
+    x = rng.random(dims)
+    a = O.sysmat2d_nufft(x, th, dims[2])
+    b = O.convolve2d(x, O.psf2d(th, dims[2], dims[2]))
+    assert O.rel_l2(b, a) < 1e-12
+
+
+def test_dirichlet_closed_form_psf_matches_nudft():
+    """The closed form used by the CUDA PSF generator: sum_m e^{i u r_m} = sin(pi u)/sin(pi u/n)."""
+    rng = np.random.default_rng(6)
+    th = np.sort(rng.uniform(0, np.pi, 11))
+    nr, n = 13, 9
+    P = O.next_fast_dim(2 * n - 1)
+    K_exact = O.psf2d(th, nr, n).kernel
+    k = np.arange(P) - P // 2
+    kx, ky = np.meshgrid(k, k)
+    K = np.zeros((P, P))
+    for t in th:
+        u = kx * np.cos(t) + ky * np.sin(t)
+        den = np.sin(np.pi * u / nr)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            d = np.where(np.abs(den) < 1e-13, nr * np.cos(np.pi * u) / np.cos(np.pi * u / nr),
+                         np.sin(np.pi * u) / den)
+        K += d
+    assert np.abs(K - K_exact).max() / np.abs(K_exact).max() < 1e-12
+
+
+def test_zero_centred_spectrum_is_real_even():
+    th = np.arange(9) * np.pi / 9
+    for n in (8, 9, 15):
+        psf = O.psf2d(th, n, n)
+        K0 = np.roll(np.roll(psf.kernel, -(psf.psf_n // 2), 0), -(psf.psf_n // 2), 1)
+        R0 = np.fft.fft2(K0)
+        assert np.abs(R0.imag).max() < 1e-9 * np.abs(R0.real).max()
+        assert np.abs(R0.real - np.roll(R0.real[::-1, ::-1], 1, (0, 1))).max() < 1e-9 * np.abs(R0).max()
+
+
+def test_finite_differences_are_antisymmetric():
+    rng = np.random.default_rng(7)
+    u = rng.random((4, 5, 6))
+    v = [rng.random((4, 5, 6)) for _ in range(3)]
+    lhs = sum(np.vdot(g, w) for g, w in zip(O.grad(u), v))
+    rhs = -np.vdot(u, O.divergence(v))
+    assert abs(lhs - rhs) < 1e-12 * abs(lhs)
+
+
+needs_ref = pytest.mark.skipif(not R.available(), reason="reference build (oracle/_ref) not present")
+
+
+@needs_ref
+def test_pin_oracle_against_reference_sources_2d():
+    rng = np.random.default_rng(8)
+    th = np.arange(6) * np.pi / 6 + 0.05
+    x = rng.random((2, 11, 11))
+    y = rng.random((2, 6, 13))
+    assert O.rel_l2(O.forward2d(x, th, 13), R.forward2d(x, th, 13)) < 1e-12
+    assert O.rel_l2(O.backproj2d(y, th, (2, 11, 11)), R.backproj2d(y, th, 11)) < 1e-12
+    P, kh, st, sn = R.psf2d(th, 13, 11, x)
+    psf = O.psf2d(th, 13, 11)
+    assert P == psf.psf_n
+    assert O.rel_l2(psf.kernel_hat, kh) < 1e-12
+    assert O.rel_l2(O.convolve2d(x, psf), st) < 1e-12
+
+
+@needs_ref
+def test_pin_finite_differences_against_reference():
+    rng = np.random.default_rng(9)
+    u = rng.random((4, 6, 7))
+    g, d = R.grad(u)
+    go = O.grad(u)
+    for a in range(3):
+        assert O.rel_l2(go[a], g[a]) < 1e-14
+    assert O.rel_l2(O.divergence(go), d) < 1e-14
+    # the reference CPU stencil is interior-only (src/finitediff.cpp:26-90)
+    gc, _ = R.grad(u, cpu_stencil=True)
+    oc = O.grad_cpu(u)
+    for a in range(3):
+        assert O.rel_l2(oc[a], gc[a]) < 1e-14
+
+
+@needs_ref
+def test_pin_split_bregman_against_reference():
+    rng = np.random.default_rng(10)
+    th = np.arange(8) * np.pi / 8
+    sino = rng.random((1, 8, 11))
+    a = R.mbir2d(sino, th, 11, "sb", 3, 0.0, 0.0, lam=0.1, mu=5.0, inner=2)
+    b = O.mbir2d(sino, th, (1, 11, 11), "sb", 3, 0.0, 0.0, lam=0.1, mu=5.0, inner=2)
+    assert O.rel_l2(b, a) < 1e-10
