@@ -1,0 +1,343 @@
+#!/usr/bin/env python
+"""Benchmark: laminography MBIR reconstructions per second on one B200.
+
+Workload (the reference's laminography configuration): recon_dims [21, 511, 511]
+(padded to [29, 721, 721] inside the solver), 40 seeded random ellipsoids,
+360 projections over [0, 360 deg), tilt gamma = 30 deg (TOML key, negated
+internally like include/config.h:206), 511 x 511 detector, 1% Gaussian noise,
+Split-Bregman TV with lambda = 0.1, mu = 10, inner_iters = 1, 100 outer
+iterations (tol = 1e-5, xtol = 0 so that every step does the same work), NUFFT
+tolerance 1e-6.
+
+A step is one complete reconstruction: normalisation and padding of the
+projections, geometry and bin sort, backprojection (type-1 NUFFT), FP64 PSF
+generation (no cache), 100 Split-Bregman outer iterations and the final crop.
+`value` is measured with the projections resident in HBM (lc_mbir3d_device);
+`e2e` through the host-buffer API (lc_mbir3d) with a pinned host copy in and
+the reconstruction copied back out every step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (the path does not shard across GPUs; the
+reference's multi-GPU slice streaming has no single-volume exchange), launched
+with torch.distributed.run; rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RECON_DIMS = (21, 511, 511)
+NANGLES = 360
+DET = (511, 511)
+GAMMA_DEG = 30.0
+N_ELLIPSOIDS = 40
+OUTER = 100
+LAM, MU = 0.1, 10.0
+NOISE = 0.01
+METRIC = "laminography MBIR reconstructions/s (Split-Bregman TV, 100 outer iterations)"
+CONFIG = {
+    "workload": "laminography Split-Bregman: recon_dims [21,511,511] (padded [29,721,721]), "
+                "360 angles over [0,360), tilt 30 deg, 511x511 detector, 40 ellipsoids, 1% noise, "
+                "lambda 0.1, mu 10, inner 1, outer 100, NUFFT tol 1e-6",
+    "recon_dims": list(RECON_DIMS), "padded_dims": [29, 721, 721], "angles": NANGLES,
+    "detector": list(DET), "outer_iters": OUTER, "inner_iters": 1, "lambda": LAM, "mu": MU,
+    "tol": 1e-5, "xtol": 0.0, "nufft_tol": 1e-6,
+    "l2_policy": "inputs larger than L2 (projections 376 MB, fine grids >1 GB)",
+}
+
+
+def geometry():
+    theta = np.arange(NANGLES) * 2 * np.pi / NANGLES
+    gamma = -GAMMA_DEG * np.pi / 180.0
+    return theta, gamma
+
+
+def make_projections(lc):
+    """Seeded phantom, forward-projected on the GPU (like the reference's
+    forward_scalar tool, src/radon.cpp), plus 1% noise."""
+    import torch
+    from laminocam_b200 import synthetic as S
+    theta, gamma = geometry()
+    vol = S.ellipsoid_phantom(RECON_DIMS, N_ELLIPSOIDS, 1000)
+    pg = lc.PolarGrid(theta, np.full(NANGLES, gamma), np.zeros(NANGLES), DET[0], DET[1])
+    proj = lc.forward(torch.as_tensor(vol, device="cuda"), pg)
+    proj = proj + NOISE * proj.max() * torch.randn(proj.shape, device="cuda",
+                                                   generator=torch.Generator("cuda").manual_seed(2000))
+    torch.cuda.synchronize()
+    del pg
+    return vol, proj.contiguous()
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 3 + i and s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(sample_outer: int = 1):
+    """The FP64 oracle's Split-Bregman outer iteration at the padded size on host
+    cores (scipy.fft workers), extrapolated to 100 outer iterations."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_fft_workers(cores)
+    n = (29, 721, 721)
+    P = tuple(O.next_fast_dim(2 * v - 1) for v in n)
+    rng = np.random.default_rng(0)
+    # a real, point-symmetric spectrum of the right shape stands in for the PSF
+    khat = np.abs(rng.standard_normal((P[0], P[1], P[2] // 2 + 1))).astype(np.float64)
+    psf = O.PSF3D(P, None, khat)
+    yT = rng.random(n)
+    A = lambda v: O.convolve3d(v, psf)
+    t0 = time.perf_counter()
+    O.split_bregman(A, yT, np.zeros(n), LAM, MU, sample_outer, 1, 1e-5, 0.0)
+    dt = (time.perf_counter() - t0) / sample_outer
+    return {"value": 1.0 / (OUTER * dt), "unit": "recons/s", "cores": cores, "kind": "port",
+            "sample": f"{sample_outer} Split-Bregman outer iteration(s) of the FP64 oracle at the "
+                      f"padded size 29x721x721 ({dt:.2f} s each, scipy.fft with {cores} workers), "
+                      f"extrapolated to 100 outer iterations; backprojection and PSF setup excluded"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    steps = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        info = cpu_baseline(1)
+        if i >= args.warmup:
+            steps.append(1.0 / info["value"])
+    sec = float(np.mean(steps))
+    v = 1.0 / sec
+    line = {"metric": METRIC, "value": v, "unit": "recons/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": CONFIG, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "recons/s", "cores": info["cores"], "kind": "port",
+                             "sample": info["sample"]},
+            "e2e": {"value": v, "unit": "recons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import ctypes as C
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    import laminocam_b200 as lc
+    from laminocam_b200 import _lib
+
+    ctx = lc.Context.default(local)
+    lib = ctx.lib
+    theta, gamma = geometry()
+    vol, dproj = make_projections(lc)
+    nth, nr, nc = dproj.shape
+    gam = np.full(nth, gamma)
+    bet = np.zeros(nth)
+    params = lc.ReconParams(regularizer="split_bregman", recon_dims=RECON_DIMS, max_iters=OUTER,
+                            inner_iters=1, lam=LAM, mu=MU, tol=1e-5, xtol=0.0).to_c()
+    rd = (C.c_int * 3)(*RECON_DIMS)
+    _, tp = lc._dptr(theta)
+    _, gp = lc._dptr(gam)
+    _, bp = lc._dptr(bet)
+    th_keep = (np.ascontiguousarray(theta), np.ascontiguousarray(gam), np.ascontiguousarray(bet))
+    tp = th_keep[0].ctypes.data_as(C.POINTER(C.c_double))
+    gp = th_keep[1].ctypes.data_as(C.POINTER(C.c_double))
+    bp = th_keep[2].ctypes.data_as(C.POINTER(C.c_double))
+    drecon = torch.empty(RECON_DIMS, dtype=torch.float32, device="cuda")
+    host_proj = torch.empty(dproj.shape, dtype=torch.float32, pin_memory=True)
+    host_proj.copy_(dproj.cpu())
+    host_recon = torch.empty(RECON_DIMS, dtype=torch.float32, pin_memory=True)
+    stats = _lib.SolverStats()
+
+    def step_device():
+        ctx.sync_stream()
+        rc = lib.lc_mbir3d_device(ctx.handle, C.c_void_p(dproj.data_ptr()), nth, nr, nc, tp, gp, bp,
+                                  None, rd, C.byref(params), C.c_void_p(drecon.data_ptr()), C.byref(stats))
+        if rc:
+            raise RuntimeError(lib.lc_last_error(ctx.handle).decode())
+
+    def step_e2e():
+        ctx.sync_stream()
+        rc = lib.lc_mbir3d(ctx.handle, C.cast(host_proj.data_ptr(), C.POINTER(C.c_float)), nth, nr, nc,
+                           tp, gp, bp, None, rd, C.byref(params),
+                           C.cast(host_recon.data_ptr(), C.POINTER(C.c_float)), C.byref(stats))
+        if rc:
+            raise RuntimeError(lib.lc_last_error(ctx.handle).decode())
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, k):
+        lat = []
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            lat.append((a, b))
+        e1.record()
+        barrier()
+        total = e0.elapsed_time(e1)
+        lats = [a.elapsed_time(b) for a, b in lat]
+        if dist is not None:
+            t = torch.tensor([total], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        return total, lats
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+
+    with ClockSampler(local) as clk:
+        lib.lc_profile_enable(ctx.handle, 1)
+        launches0 = lib.lc_kernel_launches()
+        total_ms, lats = timed(step_device, args.steps)
+        launches = lib.lc_kernel_launches() - launches0
+        entries = (_lib.ProfileEntry * 32)()
+        nent = C.c_int()
+        lib.lc_profile_read(ctx.handle, entries, 32, C.byref(nent))
+        lib.lc_profile_enable(ctx.handle, 0)
+    value = args.steps * world / (total_ms / 1e3)
+
+    # end to end through the host-buffer API
+    step_e2e()
+    e2e_ms, _ = timed(step_e2e, max(1, min(args.steps, 3)))
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_value = e2e_steps * world / (e2e_ms / 1e3)
+
+    # roofline of the dominant kernel section
+    prof = []
+    for i in range(nent.value):
+        e = entries[i]
+        prof.append({"name": e.name.decode(), "launches": e.count, "total_ms": e.total_ms,
+                     "avg_ms": e.total_ms / max(e.count, 1), "gbs": e.bytes / max(e.total_ms, 1e-9) / 1e6,
+                     "bytes_per_launch": e.bytes / max(e.count, 1)})
+    prof.sort(key=lambda d: -d["total_ms"])
+    peak, peak_kind = measured_peak()
+    dom = next((p for p in prof if p["bytes_per_launch"] > 0), prof[0] if prof else None)
+    roof = None
+    if dom:
+        roof = {"bound": "hbm", "kernel": dom["name"], "achieved": dom["gbs"], "peak": peak,
+                "unit": "GB/s", "frac": dom["gbs"] / peak, "peak_source": peak_kind,
+                "bytes_per_launch": dom["bytes_per_launch"], "avg_launch_ms": dom["avg_ms"],
+                "traffic": None}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(1)
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": "recons/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"failed: {ex}"}
+
+    lats_sorted = sorted(lats)
+    line = {
+        "metric": METRIC, "value": value, "unit": "recons/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 PSF and solver scalars)",
+        "data": "synthetic", "config": CONFIG,
+        "latency_ms": {"p50": float(np.percentile(lats_sorted, 50)),
+                       "p99": float(np.percentile(lats_sorted, 99))},
+        "e2e": {"value": e2e_value, "unit": "recons/s",
+                "h2d_bytes_per_step": int(host_proj.numel() * 4),
+                "d2h_bytes_per_step": int(host_recon.numel() * 4)},
+        "roofline": roof, "kernels": prof[:8], "clocks": clk.summary(),
+        "gpu_launches": int(launches), "cpu_baseline": cpu,
+        "solver": {"outer_iters": stats.iters, "cg_iters": stats.cg_iters_total, "dx": stats.dx},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -95,7 +95,8 @@ int lc_psf_destroy(lc_psf psf);
 int lc_psf_info(lc_psf psf, int *P, long *spectrum_elems);
 /* FP64 PSF K on the P grid in mode order (index k + P/2), host buffer */
 int lc_psf_kernel(lc_context ctx, lc_psf psf, double *host_out);
-/* real spectrum octant {P0/2+1, P1/2+1, P2/2+1} of the zero-centred PSF, host buffer */
+/* real R2C half spectrum {P0, P1, P2/2+1} of the zero-centred PSF (its
+ * unpaired -P/2 planes zeroed), host buffer */
 int lc_psf_spectrum(lc_context ctx, lc_psf psf, float *host_out);
 /* sysmat(x, PSF) / sysmat2d(x, PSF2D) (src/gradient.cpp:49-52,76-79):
  * y = A^T A x, x and y device {n1, n2, n3} */
@@ -156,6 +157,29 @@ int lc_mbir3d(lc_context ctx, const float *projs, int ntheta, int nrows, int nco
               const double *theta, const double *gamma, const double *beta, const float *shifts,
               const int *recon_dims, const lc_recon_params *p, float *recon,
               lc_solver_stats *stats);
+
+/* As lc_mbir3d with device pointers: projs {ntheta, nrows, ncols} and recon
+ * {n1, n2, n3} stay in device memory (the DeviceArray overload of gpu::MBIR). */
+int lc_mbir3d_device(lc_context ctx, const float *projs, int ntheta, int nrows, int ncols,
+                     const double *theta, const double *gamma, const double *beta,
+                     const float *shifts, const int *recon_dims, const lc_recon_params *p,
+                     float *recon, lc_solver_stats *stats);
+
+/* ---- profiling (no counterpart in the reference, which has only a wall-clock
+ * Timer, include/timer.h:30-64) ---------------------------------------- */
+typedef struct {
+    char name[32];   /* kernel section, e.g. "toeplitz_z_mid" */
+    long count;      /* launches timed */
+    double total_ms; /* summed CUDA-event time */
+    double bytes;    /* summed algorithmic bytes */
+} lc_profile_entry;
+
+/* on != 0 starts timing every kernel section with CUDA events on the context
+ * stream (and clears the totals); 0 stops */
+int lc_profile_enable(lc_context ctx, int on);
+int lc_profile_read(lc_context ctx, lc_profile_entry *out, int max_entries, int *n_entries);
+/* number of kernels this library has launched in the process so far */
+long lc_kernel_launches(void);
 
 #ifdef __cplusplus
 }

@@ -252,12 +252,12 @@ class _PSFBase:
         return out
 
     def spectrum(self) -> np.ndarray:
-        """Real spectrum octant of the zero-centred PSF (float32)."""
-        Ph = tuple(p // 2 + 1 for p in self.P)
-        out = np.empty(Ph, dtype=np.float32)
+        """Real R2C half spectrum {P0, P1, P2/2+1} of the zero-centred PSF (float32)."""
+        shape = (self.P[0], self.P[1], self.P[2] // 2 + 1)
+        out = np.empty(shape, dtype=np.float32)
         _check(self.ctx.lib.lc_psf_spectrum(self.ctx.handle, self.handle,
                                             out.ctypes.data_as(C.POINTER(C.c_float))), self.ctx)
-        return out.reshape(Ph[1:]) if self.P[0] == 1 else out
+        return out[0] if self.P[0] == 1 else out
 
     def convolve(self, x):
         """A^T A x (Toeplitz)."""

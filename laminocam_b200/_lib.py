@@ -24,6 +24,11 @@ class ReconParamsC(C.Structure):
                 ("pad_factor", C.c_float)]
 
 
+class ProfileEntry(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("count", C.c_long), ("total_ms", C.c_double),
+                ("bytes", C.c_double)]
+
+
 vp = C.c_void_p
 i32 = C.c_int
 f64 = C.c_double
@@ -61,6 +66,11 @@ SIGNATURES = {
                         fptr, C.POINTER(SolverStats)]),
     "lc_mbir3d": (i32, [vp, fptr, i32, i32, i32, dptr, dptr, dptr, fptr, C.POINTER(C.c_int),
                         C.POINTER(ReconParamsC), fptr, C.POINTER(SolverStats)]),
+    "lc_mbir3d_device": (i32, [vp, vp, i32, i32, i32, dptr, dptr, dptr, fptr, C.POINTER(C.c_int),
+                               C.POINTER(ReconParamsC), vp, C.POINTER(SolverStats)]),
+    "lc_profile_enable": (i32, [vp, i32]),
+    "lc_kernel_launches": (C.c_long, []),
+    "lc_profile_read": (i32, [vp, C.POINTER(ProfileEntry), i32, C.POINTER(C.c_int)]),
 }
 
 _lib = None

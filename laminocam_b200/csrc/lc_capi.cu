@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
 #include <map>
 #include <memory>
 #include <tuple>
@@ -328,6 +329,8 @@ extern "C" {
 
 int lc_version(void) { return 100; }
 
+long lc_kernel_launches(void) { return kernel_launch_count(); }
+
 void lc_solver_params_default(lc_solver_params *p) {
     if (!p) return;
     p->max_iters = 50;
@@ -600,68 +603,120 @@ int lc_mbir2d(lc_context c, const float *sino, int ns, int ntheta, int nradial,
     });
 }
 
+static void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nrows, int ncols,
+                        const double *theta, const double *gamma, const double *beta,
+                        const float *shifts, const int *recon_dims, const lc_recon_params *p,
+                        float *dout, lc_solver_stats *stats) {
+    LC_REQUIRE(theta && gamma && beta && recon_dims && p, "NULL argument");
+    LC_REQUIRE(ntheta > 0 && nrows > 0 && ncols > 0, "sizes must be positive");
+    LC_REQUIRE(recon_dims[0] > 0 && recon_dims[1] > 0 && recon_dims[2] > 0,
+               "recon_dims must be positive");
+    LC_REQUIRE(p->method == 0 || p->method == 1, "method must be 0 (CG) or 1 (Split-Bregman)");
+    LC_REQUIRE(p->pad_factor >= 1.0f && p->pad_factor < 4.0f, "pad_factor must be in [1, 4)");
+    check_solver_params(&p->solver);
+    Context &ctx = *c->ctx;
+    cudaStream_t s = ctx.stream();
+    const float pf = p->pad_factor;
+    // padded reconstruction box (src/gpu/mbir.cu:46-60)
+    long N[3];
+    for (int d = 0; d < 3; ++d) {
+        N[d] = odd_pad(recon_dims[d], pf);
+        LC_REQUIRE(N[d] >= recon_dims[d], "recon_dims must be odd when pad_factor is 1");
+    }
+    // padded projections (symmetric, odd), normalised by the global maximum
+    long PR = odd_pad(nrows, pf), PC = odd_pad(ncols, pf);
+    if (pf - 1.0f < 1e-6f) {
+        PR = nrows;
+        PC = ncols;
+    }
+    const long np = (long)ntheta * nrows * ncols;
+    DevBuf<unsigned> mx(1, s);
+    mx.zero(s);
+    max_kernel<<<grid_for(np, 256, ctx.num_sms()), 256, 0, s>>>(dprojs_in, np, mx.get());
+    LC_CHECK_LAUNCH();
+    DevBuf<float> dproj((long)ntheta * PR * PC, s);
+    norm_pad_kernel<<<grid_for((long)ntheta * PR * PC, 256, ctx.num_sms()), 256, 0, s>>>(
+        dprojs_in, ntheta, nrows, ncols, dproj.get(), PR, PC, (PR - nrows) / 2, (PC - ncols) / 2,
+        mx.get());
+    LC_CHECK_LAUNCH();
+    lc_geometry g = nullptr;
+    int rc = lc_geometry3d_create(c, theta, gamma, beta, shifts, ntheta, (int)PR, (int)PC, &g);
+    if (rc) throw Error(rc == LC_ERR_INVALID ? 1 : 3, c->err);
+    std::unique_ptr<lc_geometry_s> gown(g);
+    const long nvp = N[0] * N[1] * N[2];
+    DevBuf<float> yT(nvp, s), x(nvp, s);
+    do_backproj3d(g, dproj.get(), (int)N[0], (int)N[1], (int)N[2], shifts != nullptr, yT.get(),
+                  eff_tol(p->nufft_tol));
+    dproj.release();
+    g->work.release();
+    g->plans.clear();
+    lc_psf_s psf;
+    psf.owner = c;
+    psf.geom = g;
+    psf.T = std::make_unique<Toeplitz>(ctx, g->g, N, true);
+    x.zero(s);
+    run_solver(&psf, p->method, yT.get(), x.get(), &p->solver, stats);
+    const long nv = (long)recon_dims[0] * recon_dims[1] * recon_dims[2];
+    crop_kernel<<<grid_for(nv, 256, ctx.num_sms()), 256, 0, s>>>(
+        x.get(), N[0], N[1], N[2], dout, recon_dims[0], recon_dims[1], recon_dims[2],
+        (N[0] - recon_dims[0]) / 2, (N[1] - recon_dims[1]) / 2, (N[2] - recon_dims[2]) / 2);
+    LC_CHECK_LAUNCH();
+}
+
 int lc_mbir3d(lc_context c, const float *projs, int ntheta, int nrows, int ncols,
               const double *theta, const double *gamma, const double *beta, const float *shifts,
               const int *recon_dims, const lc_recon_params *p, float *recon,
               lc_solver_stats *stats) {
     return guarded(c, [&] {
-        LC_REQUIRE(projs && theta && gamma && beta && recon_dims && p && recon, "NULL argument");
+        LC_REQUIRE(projs && recon && recon_dims, "NULL argument");
         LC_REQUIRE(ntheta > 0 && nrows > 0 && ncols > 0, "sizes must be positive");
-        LC_REQUIRE(recon_dims[0] > 0 && recon_dims[1] > 0 && recon_dims[2] > 0,
-                   "recon_dims must be positive");
-        LC_REQUIRE(p->method == 0 || p->method == 1, "method must be 0 (CG) or 1 (Split-Bregman)");
-        LC_REQUIRE(p->pad_factor >= 1.0f && p->pad_factor < 4.0f, "pad_factor must be in [1, 4)");
-        check_solver_params(&p->solver);
         Context &ctx = *c->ctx;
         cudaStream_t s = ctx.stream();
-        const float pf = p->pad_factor;
-        // padded reconstruction box (src/gpu/mbir.cu:46-60)
-        long N[3];
-        for (int d = 0; d < 3; ++d) N[d] = odd_pad(recon_dims[d], pf);
-        // padded projections (symmetric, odd), normalised by the global maximum
-        long PR = odd_pad(nrows, pf), PC = odd_pad(ncols, pf);
-        if (pf - 1.0f < 1e-6f) {
-            PR = nrows;
-            PC = ncols;
-        }
         const long np = (long)ntheta * nrows * ncols;
         DevBuf<float> draw;
         draw.upload(projs, np, s);
-        DevBuf<unsigned> mx(1, s);
-        mx.zero(s);
-        max_kernel<<<grid_for(np, 256, ctx.num_sms()), 256, 0, s>>>(draw.get(), np, mx.get());
-        LC_CHECK_LAUNCH();
-        DevBuf<float> dproj((long)ntheta * PR * PC, s);
-        norm_pad_kernel<<<grid_for((long)ntheta * PR * PC, 256, ctx.num_sms()), 256, 0, s>>>(
-            draw.get(), ntheta, nrows, ncols, dproj.get(), PR, PC, (PR - nrows) / 2, (PC - ncols) / 2,
-            mx.get());
-        LC_CHECK_LAUNCH();
-        draw.release();
-        lc_geometry g = nullptr;
-        int rc = lc_geometry3d_create(c, theta, gamma, beta, shifts, ntheta, (int)PR, (int)PC, &g);
-        if (rc) throw Error(rc == LC_ERR_INVALID ? 1 : 3, c->err);
-        std::unique_ptr<lc_geometry_s> gown(g);
-        const long nvp = N[0] * N[1] * N[2];
-        DevBuf<float> yT(nvp, s), x(nvp, s);
-        do_backproj3d(g, dproj.get(), (int)N[0], (int)N[1], (int)N[2], shifts != nullptr, yT.get(),
-                      eff_tol(p->nufft_tol));
-        dproj.release();
-        g->work.release();
-        g->plans.clear();
-        lc_psf_s psf;
-        psf.owner = c;
-        psf.geom = g;
-        psf.T = std::make_unique<Toeplitz>(ctx, g->g, N, true);
-        x.zero(s);
-        run_solver(&psf, p->method, yT.get(), x.get(), &p->solver, stats);
         const long nv = (long)recon_dims[0] * recon_dims[1] * recon_dims[2];
+        LC_REQUIRE(nv > 0, "recon_dims must be positive");
         DevBuf<float> out(nv, s);
-        crop_kernel<<<grid_for(nv, 256, ctx.num_sms()), 256, 0, s>>>(
-            x.get(), N[0], N[1], N[2], out.get(), recon_dims[0], recon_dims[1], recon_dims[2],
-            (N[0] - recon_dims[0]) / 2, (N[1] - recon_dims[1]) / 2, (N[2] - recon_dims[2]) / 2);
-        LC_CHECK_LAUNCH();
+        mbir3d_core(c, draw.get(), ntheta, nrows, ncols, theta, gamma, beta, shifts, recon_dims, p,
+                    out.get(), stats);
         LC_CUDA(cudaMemcpyAsync(recon, out.get(), nv * sizeof(float), cudaMemcpyDeviceToHost, s));
         LC_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int lc_mbir3d_device(lc_context c, const float *projs, int ntheta, int nrows, int ncols,
+                     const double *theta, const double *gamma, const double *beta,
+                     const float *shifts, const int *recon_dims, const lc_recon_params *p,
+                     float *recon, lc_solver_stats *stats) {
+    return guarded(c, [&] {
+        LC_REQUIRE(projs && recon, "NULL argument");
+        mbir3d_core(c, projs, ntheta, nrows, ncols, theta, gamma, beta, shifts, recon_dims, p,
+                    recon, stats);
+    });
+}
+
+int lc_profile_enable(lc_context c, int on) {
+    return guarded(c, [&] {
+        c->ctx->prof.reset();
+        c->ctx->prof.on = on != 0;
+    });
+}
+
+int lc_profile_read(lc_context c, lc_profile_entry *out, int max_entries, int *n_entries) {
+    return guarded(c, [&] {
+        LC_REQUIRE(out && n_entries, "NULL argument");
+        c->ctx->prof.collect();
+        int n = 0;
+        for (int sct = 0; sct < PS_COUNT && n < max_entries; ++sct) {
+            if (c->ctx->prof.count[sct] == 0) continue;
+            lc_profile_entry &e = out[n++];
+            std::snprintf(e.name, sizeof(e.name), "%s", prof_name(sct));
+            e.count = c->ctx->prof.count[sct];
+            e.total_ms = c->ctx->prof.ms[sct];
+            e.bytes = c->ctx->prof.bytes[sct];
+        }
+        *n_entries = n;
     });
 }
 

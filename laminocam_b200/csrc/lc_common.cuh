@@ -30,7 +30,16 @@ struct Error : std::runtime_error {
             throw ::lc::Error(3, std::string(#call) + ": " + cudaGetErrorString(e_));  \
     } while (0)
 
-#define LC_CHECK_LAUNCH() LC_CUDA(cudaGetLastError())
+// Kernel launches issued by this library (every launch site is followed by
+// LC_CHECK_LAUNCH(), which also counts it).
+long kernel_launch_count();
+void note_kernel_launch();
+
+#define LC_CHECK_LAUNCH()              \
+    do {                               \
+        ::lc::note_kernel_launch();    \
+        LC_CUDA(cudaGetLastError());   \
+    } while (0)
 
 #define LC_REQUIRE(cond, msg)                                                           \
     do {                                                                                \

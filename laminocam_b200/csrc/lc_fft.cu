@@ -31,8 +31,6 @@ __device__ __forceinline__ void st_elem(TO *p, cx<T> v) {
     }
 }
 
-__device__ __forceinline__ int fold(int k, int n) { return k <= n - k ? k : n - k; }
-
 struct KArgs {
     const void *in;
     void *out;
@@ -43,7 +41,6 @@ struct KArgs {
     double scale;
     const float *mid;
     long mid_ra;
-    int mid_p3h, mid_pmid;
     int C;
     long blocks_per_outer;
 };
@@ -144,10 +141,7 @@ __global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
             int f = idx / C;
             long o, c;
             if (!line_ok(cl, o, c)) continue;
-            long ci = c % a.mid_p3h;
-            long cm = c / a.mid_p3h;
-            long ridx = (long)fold(f, L) * a.mid_ra + (long)fold((int)cm, a.mid_pmid) * a.mid_p3h + ci;
-            buf[idx] = cscale(buf[idx], (T)__ldg(a.mid + ridx));
+            buf[idx] = cscale(buf[idx], (T)__ldg(a.mid + (long)f * a.mid_ra + c));
         }
         __syncthreads();
         buf = smem_fft<T>(buf, alt, C, pl, a.sign2);
@@ -265,8 +259,6 @@ void launch_axis_fft(Context &ctx, const AxisFFT &a) {
     ka.scale = a.scale;
     ka.mid = a.mid;
     ka.mid_ra = a.mid_ra;
-    ka.mid_p3h = a.mid_p3h;
-    ka.mid_pmid = a.mid_pmid;
     ka.C = C;
     long blocks;
     if (a.n_inner == 1) {
@@ -390,6 +382,9 @@ void dft_launch(Context &ctx, const DArgs &d, long blocks, int threads, size_t s
 
 void launch_axis_dft(Context &ctx, const AxisDFT &a) {
     LC_REQUIRE(a.n > 0, "DFT length must be positive");
+    const double lines = (double)a.n_outer * a.n_inner;
+    ProfScope ps(ctx, PS_DFT,
+                 lines * a.n * ((a.in_t == E_F32 ? 4.0 : 8.0) + (a.out_t == E_F32 ? 4.0 : 8.0)));
     LC_REQUIRE(a.in_t == E_F32 || a.in_t == E_C64, "DFT input must be float or float2");
     LC_REQUIRE(a.out_t == E_F32 || a.out_t == E_C64, "DFT output must be float or float2");
     if (a.n_outer <= 0 || a.n_inner <= 0) return;

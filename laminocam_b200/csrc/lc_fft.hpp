@@ -43,12 +43,9 @@ struct AxisFFT {
     const void *post = nullptr;     // real factor per output index j
     double scale = 1.0;
     // spectral multiply between a transform of `sign` and one of `sign2`:
-    // value at FFT index f of line (o, c) is multiplied by
-    // mid[fold(f, L)*mid_ra + fold(c / mid_p3h, mid_pmid)*mid_p3h + c % mid_p3h]
-    // with fold(k, n) = min(k, n - k).
+    // the value at FFT index f of line (o, c) is multiplied by mid[f*mid_ra + c]
     const float *mid = nullptr;
     long mid_ra = 0;
-    int mid_p3h = 1, mid_pmid = 1;
     int sign2 = +1;
     bool fp64 = false;  // compute precision
     int lines_per_cta = 0;  // 0 = choose automatically

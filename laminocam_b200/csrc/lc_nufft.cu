@@ -2,6 +2,7 @@
 // (type 2) on polar grids, plus the pruned fine-grid FFT passes.
 #include <algorithm>
 #include <cmath>
+#include <memory>
 #include <numeric>
 
 #include "lc_nufft.hpp"
@@ -578,6 +579,8 @@ void NufftPlan::sort_points(Context &ctx) {
 void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, PtMode mode) {
     GridCfg g = make_cfg(dim_, nf_, bs_, nb_, w_, beta_);
     const long gvol = (long)nf_[0] * nf_[1] * nf_[2];
+    // values read once, fine grid written once (plus the permutation)
+    ProfScope ps(ctx, PS_SPREAD, (double)nvol * (8.0 * pts_.M + 8.0 * gvol) + 4.0 * pts_.M);
     const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(float2);
     int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
     for (int v0 = 0; v0 < nvol; v0 += vchunk) {
@@ -599,6 +602,7 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
 void NufftPlan::interp(Context &ctx, const float2 *grid, int nvol, float2 *c, PtMode mode) {
     GridCfg g = make_cfg(dim_, nf_, bs_, nb_, w_, beta_);
     const long gvol = (long)nf_[0] * nf_[1] * nf_[2];
+    ProfScope ps(ctx, PS_INTERP, (double)nvol * (8.0 * pts_.M + 8.0 * gvol) + 4.0 * pts_.M);
     const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(float2);
     int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
     for (int v0 = 0; v0 < nvol; v0 += vchunk) {
@@ -626,6 +630,9 @@ void NufftPlan::type1_real(Context &ctx, const float2 *c, int nvol, float *out, 
     spread(ctx, c, nvol, grid_.get(), mode);
     const int n3 = modes_[0], n2 = modes_[1], n1 = modes_[2];
     const int fx = nf_[0], fy = nf_[1], fz = nf_[2];
+    ProfScope ps(ctx, PS_NUFFT_FFT,
+                 (double)nvol * 8.0 * ((double)gvol + 2.0 * fz * fy * n3 + 2.0 * fz * n2 * n3) +
+                     (double)nvol * 4.0 * n1 * n2 * n3);
     // x pass: fine rows -> n3 modes
     h1_.ensure((long)nvol * fz * fy * n3, st);
     {
@@ -713,6 +720,10 @@ void NufftPlan::type2_real(Context &ctx, const float *in, int nvol, float2 *c, P
     const long gvol = (long)fx * fy * fz;
     grid_.ensure(gvol * nvol, st);
     h1_.ensure((long)nvol * fz * fy * n3, st);
+    std::unique_ptr<ProfScope> ps(new ProfScope(
+        ctx, PS_NUFFT_FFT,
+        (double)nvol * 8.0 * ((double)gvol + 2.0 * fz * fy * n3 + 2.0 * fz * n2 * n3) +
+            (double)nvol * 4.0 * n1 * n2 * n3));
     if (dim_ == 2) {
         AxisFFT a;
         a.in = in;
@@ -787,6 +798,7 @@ void NufftPlan::type2_real(Context &ctx, const float *in, int nvol, float2 *c, P
         a.sign = -1;
         launch_axis_fft(ctx, a);
     }
+    ps.reset();
     interp(ctx, grid_.get(), nvol, c, mode);
 }
 

@@ -1,10 +1,15 @@
 // Host runtime: context, FFT plan cache and twiddle tables.
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 
 #include "lc_runtime.hpp"
 
 namespace lc {
+
+static std::atomic<long> g_launches{0};
+long kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
+void note_kernel_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 bool is_smooth23(long n) {
     if (n < 1) return false;
@@ -98,6 +103,71 @@ const float2 *PlanCache::dft_twiddles(int n, cudaStream_t s) {
     const float2 *p = b->get();
     dft_[n] = std::move(b);
     return p;
+}
+
+const char *prof_name(int s) {
+    static const char *names[PS_COUNT] = {
+        "toeplitz_x_fwd", "toeplitz_y_fwd", "toeplitz_z_mid", "toeplitz_y_inv", "toeplitz_x_inv",
+        "toeplitz_y_mid", "neg_laplacian", "nufft_spread", "nufft_interp", "nufft_fft",
+        "detector_dft", "psf_generate", "psf_fft", "cg_vector", "sb_vector"};
+    return (s >= 0 && s < PS_COUNT) ? names[s] : "?";
+}
+
+cudaEvent_t Profiler::take() {
+    if (!pool.empty()) {
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    LC_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void Profiler::collect() {
+    for (auto &r : recs) {
+        LC_CUDA(cudaEventSynchronize(r.b));
+        float t = 0;
+        LC_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+        ms[r.sec] += t;
+        bytes[r.sec] += r.bytes;
+        count[r.sec] += 1;
+        pool.push_back(r.a);
+        pool.push_back(r.b);
+    }
+    recs.clear();
+}
+
+void Profiler::reset() {
+    collect();
+    for (int i = 0; i < PS_COUNT; ++i) {
+        ms[i] = 0;
+        bytes[i] = 0;
+        count[i] = 0;
+    }
+}
+
+Profiler::~Profiler() {
+    for (auto &r : recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : pool) cudaEventDestroy(e);
+}
+
+ProfScope::ProfScope(Context &ctx, int sec, double bytes) : ctx_(&ctx) {
+    if (!ctx.prof.on) return;
+    // bound the number of live events: fold finished records into the totals
+    if (ctx.prof.recs.size() >= 50000) ctx.prof.collect();
+    Profiler::Rec r{sec, bytes, ctx.prof.take(), ctx.prof.take()};
+    LC_CUDA(cudaEventRecord(r.a, ctx.stream()));
+    ctx.prof.recs.push_back(r);
+    idx_ = (int)ctx.prof.recs.size() - 1;
+}
+
+ProfScope::~ProfScope() {
+    if (idx_ < 0) return;
+    cudaEventRecord(ctx_->prof.recs[idx_].b, ctx_->stream());
 }
 
 Context::Context(int device, cudaStream_t stream) : device_(device) {

@@ -102,6 +102,58 @@ class PlanCache {
     std::map<int, std::unique_ptr<DevBuf<float2>>> dft_;
 };
 
+// Optional per-section device timing: sections record a CUDA event pair on
+// the context stream; totals are read back (with one synchronisation) later.
+enum ProfSection {
+    PS_TOEP_X_FWD = 0,
+    PS_TOEP_Y_FWD,
+    PS_TOEP_Z_MID,
+    PS_TOEP_Y_INV,
+    PS_TOEP_X_INV,
+    PS_TOEP_Y_MID,
+    PS_NEG_LAP,
+    PS_SPREAD,
+    PS_INTERP,
+    PS_NUFFT_FFT,
+    PS_DFT,
+    PS_PSF_GEN,
+    PS_PSF_FFT,
+    PS_CG_VEC,
+    PS_SB_VEC,
+    PS_COUNT
+};
+const char *prof_name(int s);
+
+struct Profiler {
+    bool on = false;
+    struct Rec {
+        int sec;
+        double bytes;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    double ms[PS_COUNT] = {0};
+    double bytes[PS_COUNT] = {0};
+    long count[PS_COUNT] = {0};
+    cudaEvent_t take();
+    void collect();  // synchronises on the events, folds them into the totals
+    void reset();
+    ~Profiler();
+};
+
+class Context;
+
+class ProfScope {
+  public:
+    ProfScope(Context &ctx, int sec, double bytes);
+    ~ProfScope();
+
+  private:
+    Context *ctx_;
+    int idx_ = -1;
+};
+
 class Context {
   public:
     Context(int device, cudaStream_t stream);
@@ -114,6 +166,7 @@ class Context {
     size_t max_smem() const { return max_smem_; }
     std::string last_error;
     int verbose = 0;
+    Profiler prof;
 
   private:
     int device_;

@@ -2,6 +2,7 @@
 // CTA (deterministic fixed-order sum of per-CTA partials), and the
 // Split-Bregman stencil kernels (right-hand side, shrinkage + Bregman update).
 #include <algorithm>
+#include <memory>
 
 #include "lc_solver.hpp"
 #include "lc_toeplitz.hpp"
@@ -308,18 +309,23 @@ void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, i
     LC_CHECK_LAUNCH();
     for (int it = 0; it < iters; ++it) {
         A(p_.get(), ap_.get());
+        ProfScope ps(ctx, PS_CG_VEC, 4.0 * n_ * 10.0);
         if (fp32) {
             dot_pap_kernel<float><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
                                                              counter_.get(), st_.get());
+            LC_CHECK_LAUNCH();
             cg_update_kernel<float><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), n_,
                                                                part_.get(), counter_.get(),
                                                                st_.get(), tol, xtol);
+            LC_CHECK_LAUNCH();
         } else {
             dot_pap_kernel<double><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
                                                               counter_.get(), st_.get());
+            LC_CHECK_LAUNCH();
             cg_update_kernel<double><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), n_,
                                                                 part_.get(), counter_.get(),
                                                                 st_.get(), tol, xtol);
+            LC_CHECK_LAUNCH();
         }
         p_update_kernel<<<nblk_, kThreads, 0, s>>>(p_.get(), r_.get(), n_, st_.get());
         LC_CHECK_LAUNCH();
@@ -376,11 +382,14 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
     int total_cg = 0;
     int poll = p.xtol > 0 ? std::max(1, p.poll_every) : 0;
     for (int it = 0; it < p.max_iters; ++it) {
+        std::unique_ptr<ProfScope> ps1(new ProfScope(ctx, PS_SB_VEC, 4.0 * n_ * 8.0));
         sb_rhs_kernel<<<gsz, kThreads, 0, s>>>(yT, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(),
                                                 b_[1].get(), b_[2].get(), rhs_.get(), dm, mu, st_.get());
         LC_CHECK_LAUNCH();
+        ps1.reset();
         cg_run(ctx, Ap, rhs_.get(), x, p.inner_iters, p.tol, p.xtol, p.fp32_scalars, 0, true);
         total_cg += p.inner_iters;
+        ProfScope ps2(ctx, PS_SB_VEC, 4.0 * n_ * 16.0);
         sb_shrink_kernel<<<gsz, kThreads, 0, s>>>(x, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(),
                                                    b_[1].get(), b_[2].get(), dm, p.lambda / p.mu,
                                                    st_.get());

@@ -62,6 +62,22 @@ __global__ void psf3d_kernel(const double *__restrict__ rot, int ntheta, int nro
     }
 }
 
+// Zero the planes of mode -P/2 (index 0 in mode order) along every axis of even
+// length.  Their values are never reached by the cropped convolution
+// (|i - j| <= n - 1 < P/2), and without them the zero-centred kernel is
+// exactly point-symmetric, so its spectrum is real.
+__global__ void zero_unpaired_kernel(double *__restrict__ K, int P1, int P2, int P3) {
+    long total = (long)P1 * P2 * P3;
+    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long)gridDim.x * blockDim.x) {
+        int jz = (int)(idx / ((long)P2 * P3));
+        long r = idx - (long)jz * P2 * P3;
+        int jy = (int)(r / P3), jx = (int)(r - (long)jy * P3);
+        if ((P1 % 2 == 0 && jz == 0) || (P2 % 2 == 0 && jy == 0) || (P3 % 2 == 0 && jx == 0))
+            K[idx] = 0.0;
+    }
+}
+
 __global__ void d2f_kernel(const double *__restrict__ in, float *__restrict__ out, long n) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         out[i] = (float)in[i];
@@ -118,6 +134,7 @@ inline unsigned grid_for(long n, int threads, int sms) {
 
 void launch_neg_laplacian_axpy(Context &ctx, const float *x, float *y, const long dims[3], float mu) {
     long n = dims[0] * dims[1] * dims[2];
+    ProfScope ps(ctx, PS_NEG_LAP, 12.0 * n);
     neg_lap_axpy_kernel<<<grid_for(n, 256, ctx.num_sms()), 256, 0, ctx.stream()>>>(
         x, y, dims[0], dims[1], dims[2], mu);
     LC_CHECK_LAUNCH();
@@ -145,49 +162,21 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
     cudaStream_t st = ctx.stream();
     DevBuf<double> K;
     build_kernel(ctx, K);
-    // spectrum of the zero-centred kernel: FFT with the mode placement k -> k mod P,
-    // keeping the first P/2+1 outputs per axis; the result is real and even.
+    {
+        long total = (long)P_[0] * P_[1] * P_[2];
+        zero_unpaired_kernel<<<grid_for(total, 256, ctx.num_sms()), 256, 0, st>>>(K.get(), P_[0], P_[1],
+                                                                                  P_[2]);
+        LC_CHECK_LAUNCH();
+    }
+    // Spectrum of the zero-centred kernel: FFT with the mode placement k -> k mod P.
+    // It is real and point-symmetric; keep x in [0, P3/2] (the R2C half) and all
+    // of y and z, i.e. a real {P1, P2, P3/2+1} array.
+    ProfScope ps(ctx, PS_PSF_FFT, 0.0);
     DevBuf<double2> a, b;
-    DevBuf<double> Rd((long)Ph_[0] * Ph_[1] * Ph_[2], st);
-    if (!three_d) {
-        const int P = P_[2], Ph = Ph_[2];
-        a.alloc((long)P * Ph, st);
-        AxisFFT x;
-        x.in = K.get();
-        x.in_t = E_F64;
-        x.out = a.get();
-        x.out_t = E_C128;
-        x.fp64 = true;
-        x.n_outer = P;
-        x.n_inner = 1;
-        x.in_ostride = P;
-        x.out_ostride = Ph;
-        x.n_in = P;
-        x.in_map = IN_MODES;
-        x.L = P;
-        x.n_out = Ph;
-        x.sign = -1;
-        launch_axis_fft(ctx, x);
-        AxisFFT y;
-        y.in = a.get();
-        y.in_t = E_C128;
-        y.out = Rd.get();
-        y.out_t = E_F64;
-        y.fp64 = true;
-        y.n_outer = 1;
-        y.n_inner = Ph;
-        y.in_ostride = 0;
-        y.out_ostride = 0;
-        y.n_in = P;
-        y.in_map = IN_MODES;
-        y.L = P;
-        y.n_out = Ph;
-        y.sign = -1;
-        launch_axis_fft(ctx, y);
-    } else {
-        const int P1 = P_[0], P2 = P_[1], P3 = P_[2];
-        const int P1h = Ph_[0], P2h = Ph_[1], P3h = Ph_[2];
-        a.alloc((long)P1 * P2 * P3h, st);
+    DevBuf<double> Rd(spectrum_elems(), st);
+    const int P1 = P_[0], P2 = P_[1], P3 = P_[2], P3h = Ph_[2];
+    a.alloc((long)P1 * P2 * P3h, st);
+    {
         AxisFFT x;
         x.in = K.get();
         x.in_t = E_F64;
@@ -204,25 +193,34 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         x.n_out = P3h;
         x.sign = -1;
         launch_axis_fft(ctx, x);
-        K.release();
-        b.alloc((long)P1 * P2h * P3h, st);
+    }
+    K.release();
+    {
         AxisFFT y;
         y.in = a.get();
         y.in_t = E_C128;
-        y.out = b.get();
-        y.out_t = E_C128;
         y.fp64 = true;
         y.n_outer = P1;
         y.n_inner = P3h;
         y.in_ostride = (long)P2 * P3h;
-        y.out_ostride = (long)P2h * P3h;
+        y.out_ostride = (long)P2 * P3h;
         y.n_in = P2;
         y.in_map = IN_MODES;
         y.L = P2;
-        y.n_out = P2h;
+        y.n_out = P2;
         y.sign = -1;
+        if (three_d) {
+            b.alloc((long)P1 * P2 * P3h, st);
+            y.out = b.get();
+            y.out_t = E_C128;
+        } else {
+            y.out = Rd.get();
+            y.out_t = E_F64;
+        }
         launch_axis_fft(ctx, y);
-        a.release();
+    }
+    a.release();
+    if (three_d) {
         AxisFFT z;
         z.in = b.get();
         z.in_t = E_C128;
@@ -230,17 +228,17 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         z.out_t = E_F64;
         z.fp64 = true;
         z.n_outer = 1;
-        z.n_inner = (long)P2h * P3h;
+        z.n_inner = (long)P2 * P3h;
         z.in_ostride = 0;
         z.out_ostride = 0;
         z.n_in = P1;
         z.in_map = IN_MODES;
         z.L = P1;
-        z.n_out = P1h;
+        z.n_out = P1;
         z.sign = -1;
         launch_axis_fft(ctx, z);
     }
-    long nR = (long)Ph_[0] * Ph_[1] * Ph_[2];
+    long nR = spectrum_elems();
     R_.alloc(nR, st);
     d2f_kernel<<<grid_for(nR, 256, ctx.num_sms()), 256, 0, st>>>(Rd.get(), R_.get(), nR);
     LC_CHECK_LAUNCH();
@@ -256,6 +254,7 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
 
 void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
     cudaStream_t st = ctx.stream();
+    ProfScope ps(ctx, PS_PSF_GEN, 0.0);
     if (!three_d_) {
         const int P = P_[2];
         K.alloc((long)P * P, st);
@@ -292,9 +291,14 @@ double Toeplitz::algorithmic_bytes() const {
 void Toeplitz::apply(Context &ctx, const float *x, float *y) {
     const long n1 = n_[0], n2 = n_[1], n3 = n_[2];
     const int P1 = P_[0], P2 = P_[1], P3 = P_[2];
-    const int P2h = Ph_[1], P3h = Ph_[2];
+    const int P3h = Ph_[2];
+    const double N = (double)n1 * n2 * n3;
+    const double T1 = (double)n1 * n2 * P3h * 8.0;      // half-spectrum rows, complex
+    const double T2 = (double)n1 * P2 * P3h * 8.0;      // after the y transform
+    const double Rb = 4.0 * (double)spectrum_elems();
     // x rows: real -> half spectrum
     {
+        ProfScope ps(ctx, PS_TOEP_X_FWD, 4.0 * N + T1);
         AxisFFT a;
         a.in = x;
         a.in_t = E_F32;
@@ -311,6 +315,7 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
         launch_axis_fft(ctx, a);
     }
     if (!three_d_) {
+        ProfScope ps(ctx, PS_TOEP_Y_MID, 2.0 * T1 + Rb);
         AxisFFT a;
         a.in = t1_.get();
         a.in_t = E_C64;
@@ -328,12 +333,11 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
         a.sign = -1;
         a.mid = R_.get();
         a.mid_ra = P3h;
-        a.mid_p3h = P3h;
-        a.mid_pmid = 1;
         a.sign2 = +1;
         launch_axis_fft(ctx, a);
     } else {
         {
+            ProfScope ps(ctx, PS_TOEP_Y_FWD, T1 + T2);
             AxisFFT a;
             a.in = t1_.get();
             a.in_t = E_C64;
@@ -350,6 +354,7 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
             launch_axis_fft(ctx, a);
         }
         {
+            ProfScope ps(ctx, PS_TOEP_Z_MID, 2.0 * T2 + Rb);
             AxisFFT a;
             a.in = t2_.get();
             a.in_t = E_C64;
@@ -366,13 +371,12 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
             a.out_off = 0;
             a.sign = -1;
             a.mid = R_.get();
-            a.mid_ra = (long)P2h * P3h;
-            a.mid_p3h = P3h;
-            a.mid_pmid = P2;
+            a.mid_ra = (long)P2 * P3h;
             a.sign2 = +1;
             launch_axis_fft(ctx, a);
         }
         {
+            ProfScope ps(ctx, PS_TOEP_Y_INV, T1 + T2);
             AxisFFT a;
             a.in = t2_.get();
             a.in_t = E_C64;
@@ -392,6 +396,7 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
         }
     }
     {
+        ProfScope ps(ctx, PS_TOEP_X_INV, T1 + 4.0 * N);
         AxisFFT a;
         a.in = t1_.get();
         a.in_t = E_C64;

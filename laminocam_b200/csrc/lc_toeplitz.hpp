@@ -8,10 +8,12 @@
 //     sum_m exp(i u r_m) = sin(pi u) / sin(pi u / n),
 // so K is generated exactly, in FP64, as a sum over angles of products of
 // Dirichlet kernels (one factor in 2D, two in 3D) instead of a type-1 NUFFT of
-// ones.  K is real and even, so the spectrum of the zero-centred kernel K0 is
-// real and even too; only its first octant (quadrant in 2D) is kept, in FP32.
-// Convolving with K0 and cropping at offset 0 equals the reference's
-// convolution with the centred kernel cropped at P/2.
+// ones.  K(-k) = K(k).  After zeroing the unpaired planes k = -P/2 (never reached
+// by the cropped convolution) the zero-centred kernel K0 is point-symmetric, so
+// its spectrum is real; the R2C half {P1, P2, P3/2+1} is kept in FP32 (half the
+// bytes of the reference's complex half spectrum).  Convolving with K0 and
+// cropping at offset 0 equals the reference's convolution with the centred
+// kernel cropped at P/2.
 #pragma once
 
 #include "lc_nufft.hpp"
@@ -31,7 +33,7 @@ class Toeplitz {
     const int *P() const { return P_; }
     bool three_d() const { return three_d_; }
     long nvox() const { return n_[0] * n_[1] * n_[2]; }
-    long spectrum_elems() const { return (long)Ph_[0] * Ph_[1] * Ph_[2]; }
+    long spectrum_elems() const { return (long)P_[0] * P_[1] * Ph_[2]; }
     const float *spectrum() const { return R_.get(); }
     // FP64 PSF K on the P-grid in mode order (k = j - P/2), for tests
     void kernel_fp64(Context &ctx, double *host_out);

@@ -225,6 +225,29 @@ def ifftshift_axis(a, axis):
     return np.roll(a, -((n + 1) // 2), axis=axis)
 
 
+_FFT_WORKERS = None
+
+
+def set_fft_workers(n):
+    """Use scipy.fft with n threads for the Toeplitz FFTs (CPU baseline timing)."""
+    global _FFT_WORKERS
+    _FFT_WORKERS = n
+
+
+def _rfftn(a, axes):
+    if _FFT_WORKERS:
+        import scipy.fft
+        return scipy.fft.rfftn(a, axes=axes, workers=_FFT_WORKERS)
+    return np.fft.rfftn(a, axes=axes)
+
+
+def _irfftn(a, s, axes):
+    if _FFT_WORKERS:
+        import scipy.fft
+        return scipy.fft.irfftn(a, s=s, axes=axes, workers=_FFT_WORKERS)
+    return np.fft.irfftn(a, s=s, axes=axes)
+
+
 def fft_fwd(a, axes):
     """FFTW_FORWARD, unnormalised."""
     return np.fft.fftn(a, axes=axes)
@@ -304,8 +327,8 @@ def convolve2d(x, psf: PSF2D):
     P = psf.psf_n
     padded = np.zeros((ns, P, P))
     padded[:, :n2, :n3] = x
-    Xh = np.fft.rfft2(padded) * psf.kernel_hat[None]
-    res = np.fft.irfft2(Xh, s=(P, P)) * (P * P)   # FFTW C2R is unnormalised
+    Xh = _rfftn(padded, (1, 2)) * psf.kernel_hat[None]
+    res = _irfftn(Xh, (P, P), (1, 2)) * (P * P)   # FFTW C2R is unnormalised
     norm = float(P) * float(P) * float(n3)
     c = P // 2
     return res[:, c:c + n2, c:c + n3] / norm
@@ -397,7 +420,7 @@ def convolve3d(xv, psf: PSF3D):
     P1, P2, P3 = psf.dims
     padded = np.zeros((P1, P2, P3))
     padded[:n1, :n2, :n3] = xv
-    res = np.fft.irfftn(np.fft.rfftn(padded) * psf.kernel_hat, s=(P1, P2, P3)) * (P1 * P2 * P3)
+    res = _irfftn(_rfftn(padded, (0, 1, 2)) * psf.kernel_hat, (P1, P2, P3), (0, 1, 2)) * (P1 * P2 * P3)
     norm = float(P1 * P2 * P3) * float(n2 * n3)
     c1, c2, c3 = P1 // 2, P2 // 2, P3 // 2
     return res[c1:c1 + n1, c2:c2 + n2, c3:c3 + n3] / norm

@@ -19,6 +19,7 @@ sys.path.insert(0, ROOT)
 
 from oracle import oracle as O  # noqa: E402
 from oracle import refrun as R  # noqa: E402
+from laminocam_b200 import synthetic as S  # noqa: E402
 
 
 def check(name, a, b, tol=1e-10):
@@ -41,8 +42,15 @@ def case2d(tag, ns, n, nth, nr, seed, theta_kind="ref"):
     sm = O.sysmat2d_nufft(vol, theta, nr)
     psf = O.psf2d(theta, nr, n)
     tp = O.convolve2d(vol, psf)
-    cg = O.mbir2d(sino, theta, (ns, n, n), "cg", 10, 0.0, 0.0)
-    sb = O.mbir2d(sino, theta, (ns, n, n), "sb", 4, 0.0, 0.0, lam=0.05, mu=2.0, inner=2)
+    # solver inputs: a consistent phantom sinogram (1% noise) with enough angles
+    # for a well-posed system, normalised by its maximum (include/mbir2d_prep.h:61-62)
+    nth_s = int(np.ceil(1.6 * n))
+    theta_s = np.arange(nth_s) * np.pi / nth_s
+    ph = np.stack([S.ellipse_phantom(n, 6, 1000 + seed + i) for i in range(ns)]).astype(np.float64)
+    ys = S.add_noise(O.forward2d(ph, theta_s, nr), 0.01, 2000 + seed).astype(np.float64)
+    ys = (ys / ys.max()).astype(np.float32).astype(np.float64)
+    cg = O.mbir2d(ys, theta_s, (ns, n, n), "cg", 10, 0.0, 0.0)
+    sb = O.mbir2d(ys, theta_s, (ns, n, n), "sb", 4, 0.0, 0.0, lam=0.05, mu=2.0, inner=2)
     if R.available():
         check("forward2d", fw, R.forward2d(vol, theta, nr))
         check("backproj2d", bp, R.backproj2d(sino, theta, n))
@@ -50,12 +58,13 @@ def case2d(tag, ns, n, nth, nr, seed, theta_kind="ref"):
         check("psf2d.kernel_hat", psf.kernel_hat, kh)
         check("sysmat2d.toeplitz", tp, st)
         check("sysmat2d.nufft", sm, sn)
-        check("cg", cg, R.mbir2d(sino, theta, n, "cg", 10, 0.0, 0.0), 1e-6)
-        check("sb", sb, R.mbir2d(sino, theta, n, "sb", 4, 0.0, 0.0, lam=0.05, mu=2.0, inner=2), 1e-8)
+        check("cg", cg, R.mbir2d(ys, theta_s, n, "cg", 10, 0.0, 0.0), 1e-8)
+        check("sb", sb, R.mbir2d(ys, theta_s, n, "sb", 4, 0.0, 0.0, lam=0.05, mu=2.0, inner=2), 1e-8)
     np.savez_compressed(os.path.join(HERE, f"{tag}.npz"), theta=theta, vol=vol.astype(np.float32),
                         sino=sino.astype(np.float32), nr=nr, forward2d=fw, backproj2d=bp,
                         sysmat2d_nufft=sm, psf_kernel=psf.kernel, psf_kernel_hat=psf.kernel_hat,
-                        toeplitz=tp, cg10=cg, sb4=sb)
+                        toeplitz=tp, theta_solve=theta_s, sino_solve=ys.astype(np.float32),
+                        cg10=cg, sb4=sb)
     print(f"wrote {tag}.npz")
 
 
@@ -97,7 +106,9 @@ def mbir3d_case(tag, projs_dims, recon_dims, gamma, seed):
     rng = np.random.default_rng(seed)
     nth, nrows, ncols = projs_dims
     theta = np.arange(nth) * 2 * np.pi / nth
-    projs = rng.random(projs_dims).astype(np.float32)
+    vol = S.ellipsoid_phantom(recon_dims, 6, 3000 + seed).astype(np.float64)
+    grid = O.Grid3D(theta, np.full(nth, gamma), np.zeros(nth), nrows, ncols)
+    projs = S.add_noise(O.forward3d(vol, grid), 0.01, 4000 + seed)
     p64 = projs.astype(np.float64)
     lam, mu = float(np.float32(0.1)), float(np.float32(10.0))
     cg = O.mbir3d(p64, theta, gamma, 0.0, recon_dims, method="cg", max_iters=6, tol=0, xtol=0)
@@ -118,4 +129,4 @@ if __name__ == "__main__":
     case2d("golden2d_nr", ns=1, n=21, nth=12, nr=25, seed=13, theta_kind="uniform")
     case3d("golden3d_a", (5, 8, 9), nth=6, nrows=10, ncols=11, gamma=-0.4, beta=0.1, seed=21)
     case3d("golden3d_b", (3, 12, 12), nth=8, nrows=12, ncols=12, gamma=-np.pi / 6, beta=0.0, seed=22)
-    mbir3d_case("golden_mbir3d", (8, 9, 9), (3, 7, 7), -np.pi / 6, seed=31)
+    mbir3d_case("golden_mbir3d", (16, 9, 9), (5, 9, 9), -np.pi / 6, seed=31)

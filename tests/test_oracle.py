@@ -127,14 +127,38 @@ def test_dirichlet_closed_form_psf_matches_nudft():
     assert np.abs(K - K_exact).max() / np.abs(K_exact).max() < 1e-12
 
 
-def test_zero_centred_spectrum_is_real_even():
-    th = np.arange(9) * np.pi / 9
-    for n in (8, 9, 15):
-        psf = O.psf2d(th, n, n)
-        K0 = np.roll(np.roll(psf.kernel, -(psf.psf_n // 2), 0), -(psf.psf_n // 2), 1)
-        R0 = np.fft.fft2(K0)
-        assert np.abs(R0.imag).max() < 1e-9 * np.abs(R0.real).max()
-        assert np.abs(R0.real - np.roll(R0.real[::-1, ::-1], 1, (0, 1))).max() < 1e-9 * np.abs(R0).max()
+@pytest.mark.parametrize("three_d", [False, True])
+def test_zero_centred_spectrum_is_real_after_dropping_unpaired_planes(three_d):
+    """The CUDA PSF keeps Re(FFT(K0)) with K0 the zero-centred kernel whose -P/2
+    planes are zeroed: that spectrum is real for any angle set, and the cropped
+    convolution with it equals the reference's centred convolution."""
+    rng = np.random.default_rng(11)
+    if three_d:
+        th = np.sort(rng.uniform(0, 2 * np.pi, 5))
+        grid = O.Grid3D(th, np.full(5, -0.5), np.full(5, 0.2), 10, 11)
+        x = rng.random((4, 8, 9))
+        psf = O.psf3d(grid, x.shape)
+        K, ref = psf.kernel.copy(), O.convolve3d(x, psf)
+    else:
+        th = np.sort(rng.uniform(0, np.pi, 7))   # no mirror symmetry
+        x = rng.random((1, 12, 12))
+        psf = O.psf2d(th, 13, 12)
+        K, ref = psf.kernel.copy()[None], O.convolve2d(x, psf)[0][None]
+        x = x[0][None]
+    for ax, P in enumerate(K.shape):
+        if P % 2 == 0 and P > 1:
+            sl = [slice(None)] * 3
+            sl[ax] = 0
+            K[tuple(sl)] = 0
+    K0 = np.roll(K, [-(P // 2) for P in K.shape], axis=(0, 1, 2))
+    R = np.fft.fftn(K0)
+    assert np.abs(R.imag).max() < 1e-12 * np.abs(R.real).max()
+    Pd = K.shape
+    X = np.zeros(Pd)
+    X[:x.shape[0], :x.shape[1], :x.shape[2]] = x
+    y = np.fft.irfftn(np.fft.rfftn(X) * R.real[:, :, :Pd[2] // 2 + 1], s=Pd, axes=(0, 1, 2))
+    y = y[:x.shape[0], :x.shape[1], :x.shape[2]] / (x.shape[1] * x.shape[2] if three_d else x.shape[2])
+    assert O.rel_l2(y, ref) < 1e-12
 
 
 def test_finite_differences_are_antisymmetric():
