@@ -93,7 +93,9 @@ int lc_psf_create(lc_context ctx, lc_geometry g, int n1, int n2, int n3, lc_psf 
 int lc_psf_destroy(lc_psf psf);
 /* P[3]: PSF grid (P[0] = 1 for 2D); spectrum_elems: stored real spectrum size */
 int lc_psf_info(lc_psf psf, int *P, long *spectrum_elems);
-/* FP64 PSF K on the P grid in mode order (index k + P/2), host buffer */
+/* FP64 PSF K on the P grid in mode order (index k + P/2), host buffer; the
+ * planes of mode -P/2 along even axes are zero (the cropped convolution never
+ * reads them) */
 int lc_psf_kernel(lc_context ctx, lc_psf psf, double *host_out);
 /* real R2C half spectrum {P0, P1, P2/2+1} of the zero-centred PSF (its
  * unpaired -P/2 planes zeroed), host buffer */
@@ -180,6 +182,7 @@ int lc_profile_enable(lc_context ctx, int on);
 int lc_profile_read(lc_context ctx, lc_profile_entry *out, int max_entries, int *n_entries);
 /* number of kernels this library has launched in the process so far */
 long lc_kernel_launches(void);
+
 
 #ifdef __cplusplus
 }

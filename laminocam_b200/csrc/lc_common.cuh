@@ -103,14 +103,55 @@ template <typename V> __device__ __forceinline__ V cmul_i(V a, int sign) {
 // ---------------------------------------------------------------------------
 constexpr int kMaxStages = 16;
 
-// Device-side description of one FFT length: radix sequence and twiddle table
-// tw[m] = exp(-2*pi*i*m/L), m in [0, L), in the plan's precision.
+// Device-side description of one FFT length: radix sequence, the multiplier
+// that divides by Ns (the product of the earlier radices) at each stage, and
+// the twiddle table tw[m] = exp(-2*pi*i*m/L), m in [0, L), in the plan's
+// precision.
 struct FFTPlan {
     int L;
     int nst;
     int radix[kMaxStages];
+    unsigned long long ns_magic[kMaxStages];  // ceil(2^40 / Ns)
     const void *tw;
 };
+
+// floor(n / d) for n, d < 2^20 from magic = ceil(2^40 / d): the error term
+// n * (magic * d - 2^40) < n * d < 2^40 keeps the quotient exact.
+__host__ __device__ __forceinline__ unsigned fast_div(unsigned n, unsigned long long magic) {
+    return (unsigned)(((unsigned long long)n * magic) >> 40);
+}
+__host__ __device__ __forceinline__ unsigned long long fast_div_magic(unsigned d) {
+    return ((1ULL << 40) + d - 1) / d;
+}
+
+// Fills radices (8, 9, 4, 2, 3 preferred in that order) and division
+// multipliers; returns false unless L = 2^p 3^q fits in kMaxStages stages.
+inline bool fft_factorise(int L, FFTPlan &pl) {
+    pl.L = L;
+    pl.nst = 0;
+    int r = L;
+    auto push = [&](int R) {
+        if (pl.nst >= kMaxStages) return false;
+        pl.radix[pl.nst++] = R;
+        r /= R;
+        return true;
+    };
+    while (r % 8 == 0)
+        if (!push(8)) return false;
+    while (r % 9 == 0)
+        if (!push(9)) return false;
+    if (r % 4 == 0 && !push(4)) return false;
+    if (r % 2 == 0 && !push(2)) return false;
+    while (r % 3 == 0)
+        if (!push(3)) return false;
+    if (r != 1) return false;
+    unsigned ns = 1;
+    for (int s = 0; s < pl.nst; ++s) {
+        pl.ns_magic[s] = fast_div_magic(ns);
+        ns *= (unsigned)pl.radix[s];
+    }
+    return true;
+}
 
 template <typename V, int R>
 __device__ __forceinline__ void dft_small(V *v, int sign) {
@@ -138,6 +179,32 @@ __device__ __forceinline__ void dft_small(V *v, int sign) {
         v[2] = csub(t0, t2);
         v[1] = cadd(t1, t3);
         v[3] = csub(t1, t3);
+    } else if constexpr (R == 9) {
+        // 3 x 3: DFT3 over n1 for each n2, twiddle W9^(n2 k1), DFT3 over n2
+        const T c1 = T(0.76604444311897803520), s1 = T(0.64278760968653932632) * T(sign);
+        const T c2 = T(0.17364817766693034885), s2 = T(0.98480775301220805936) * T(sign);
+        const T c4 = T(-0.93969262078590838405), s4 = T(0.34202014332566873304) * T(sign);
+        V y[3][3];
+#pragma unroll
+        for (int n2 = 0; n2 < 3; ++n2) {
+            V t[3] = {v[n2], v[n2 + 3], v[n2 + 6]};
+            dft_small<V, 3>(t, sign);
+            y[n2][0] = t[0];
+            y[n2][1] = t[1];
+            y[n2][2] = t[2];
+        }
+        y[1][1] = cmul(y[1][1], mk<T>(c1, s1));  // W9^1
+        y[1][2] = cmul(y[1][2], mk<T>(c2, s2));  // W9^2
+        y[2][1] = cmul(y[2][1], mk<T>(c2, s2));  // W9^2
+        y[2][2] = cmul(y[2][2], mk<T>(c4, s4));  // W9^4
+#pragma unroll
+        for (int k1 = 0; k1 < 3; ++k1) {
+            V t[3] = {y[0][k1], y[1][k1], y[2][k1]};
+            dft_small<V, 3>(t, sign);
+            v[k1] = t[0];
+            v[k1 + 3] = t[1];
+            v[k1 + 6] = t[2];
+        }
     } else if constexpr (R == 8) {
         const T h = T(0.70710678118654752440);
         // radix-2 over even/odd, then radix-4 each
@@ -161,22 +228,25 @@ __device__ __forceinline__ void dft_small(V *v, int sign) {
 }
 
 // One Stockham stage of radix R over C lines of length L, out of place:
-// element (i, c) of line c lives at src[i*C + c] / dst[i*C + c].
+// element (i, c) of line c lives at src[i*C + c] / dst[i*C + c].  C is a power
+// of two (1 << logC); the division by Ns uses the plan's multiplier.
 template <typename T, int R>
 __device__ __forceinline__ void stockham_stage(const cx<T> *__restrict__ src, cx<T> *__restrict__ dst,
-                                               int L, int C, int Ns, const cx<T> *__restrict__ tw,
-                                               int sign) {
+                                               int L, int logC, int Ns, unsigned long long ns_magic,
+                                               const cx<T> *__restrict__ tw, int sign) {
     using V = cx<T>;
+    const int C = 1 << logC;
     const int nb = L / R;
-    const int items = nb * C;
+    const int items = nb << logC;
     const int tstride = L / (Ns * R);
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int c = it % C;
-        const int j = it / C;
-        const int k = j % Ns;
+        const int c = it & (C - 1);
+        const int j = it >> logC;
+        const int g = (int)fast_div((unsigned)j, ns_magic);
+        const int k = j - g * Ns;
         V v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * C + c];
+        for (int r = 0; r < R; ++r) v[r] = src[((j + r * nb) << logC) + c];
         if (Ns > 1) {
 #pragma unroll
             for (int r = 1; r < R; ++r) {
@@ -186,29 +256,31 @@ __device__ __forceinline__ void stockham_stage(const cx<T> *__restrict__ src, cx
             }
         }
         dft_small<V, R>(v, sign);
-        const int base = (j / Ns) * Ns * R + k;
+        const int base = g * Ns * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) dst[(base + r * Ns) * C + c] = v[r];
+        for (int r = 0; r < R; ++r) dst[((base + r * Ns) << logC) + c] = v[r];
     }
 }
 
-// Unnormalised DFT of C lines held in shared memory ([L][C] layout), natural
-// order in and out, ping-ponging between a and b.  Returns the buffer that
-// holds the result.  sign = -1: forward (e^{-i}); sign = +1: backward.
+// Unnormalised DFT of C = 1 << logC lines held in shared memory ([L][C]
+// layout), natural order in and out, ping-ponging between a and b.  Returns
+// the buffer that holds the result.  sign = -1: forward (e^{-i}); +1: backward.
 // The data must be complete in `a` (__syncthreads() before the call); the
 // result is complete when the call returns.
 template <typename T>
-__device__ cx<T> *smem_fft(cx<T> *a, cx<T> *b, int C, const FFTPlan &pl, int sign) {
+__device__ cx<T> *smem_fft(cx<T> *a, cx<T> *b, int logC, const FFTPlan &pl, int sign) {
     const cx<T> *tw = reinterpret_cast<const cx<T> *>(pl.tw);
     cx<T> *src = a, *dst = b;
     int Ns = 1;
     for (int s = 0; s < pl.nst; ++s) {
         const int R = pl.radix[s];
+        const unsigned long long mg = pl.ns_magic[s];
         switch (R) {
-            case 2: stockham_stage<T, 2>(src, dst, pl.L, C, Ns, tw, sign); break;
-            case 3: stockham_stage<T, 3>(src, dst, pl.L, C, Ns, tw, sign); break;
-            case 4: stockham_stage<T, 4>(src, dst, pl.L, C, Ns, tw, sign); break;
-            default: stockham_stage<T, 8>(src, dst, pl.L, C, Ns, tw, sign); break;
+            case 2: stockham_stage<T, 2>(src, dst, pl.L, logC, Ns, mg, tw, sign); break;
+            case 3: stockham_stage<T, 3>(src, dst, pl.L, logC, Ns, mg, tw, sign); break;
+            case 4: stockham_stage<T, 4>(src, dst, pl.L, logC, Ns, mg, tw, sign); break;
+            case 9: stockham_stage<T, 9>(src, dst, pl.L, logC, Ns, mg, tw, sign); break;
+            default: stockham_stage<T, 8>(src, dst, pl.L, logC, Ns, mg, tw, sign); break;
         }
         __syncthreads();
         cx<T> *t = src;

@@ -41,138 +41,166 @@ struct KArgs {
     double scale;
     const float *mid;
     long mid_ra;
-    int C;
+    int logC;
     long blocks_per_outer;
 };
 
+// One CTA transforms C = 1 << logC lines.  Rows (n_inner == 1) are C
+// consecutive lines, each contiguous in memory, walked line by line so that
+// consecutive threads touch consecutive addresses; otherwise the CTA takes C
+// adjacent inner indices c of one outer index o and consecutive threads walk c.
 template <typename T, typename TI, typename TO>
 __global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using V = cx<T>;
-    const int C = a.C;
+    const int logC = a.logC;
+    const int C = 1 << logC;
     const int L = a.L;
     V *buf = reinterpret_cast<V *>(smem_raw);
-    V *alt = buf + (long)L * C;
+    V *alt = buf + ((long)L << logC);
     const TI *in = reinterpret_cast<const TI *>(a.in);
     TO *out = reinterpret_cast<TO *>(a.out);
     const T *pre = reinterpret_cast<const T *>(a.pre);
     const T *linefac = reinterpret_cast<const T *>(a.linefac);
     const T *post = reinterpret_cast<const T *>(a.post);
-
-    // lines handled by this CTA
-    long o_base, c_base;
+    const int tid = threadIdx.x, nt = blockDim.x;
     const bool rows = (a.n_inner == 1);
+    long o_base, c_base;
     if (rows) {
-        o_base = (long)blockIdx.x * C;
+        o_base = (long)blockIdx.x << logC;
         c_base = 0;
     } else {
         o_base = (long)blockIdx.x / a.blocks_per_outer;
-        c_base = ((long)blockIdx.x % a.blocks_per_outer) * C;
+        c_base = ((long)blockIdx.x % a.blocks_per_outer) << logC;
     }
-    auto line_ok = [&](int cl, long &o, long &c) -> bool {
-        if (rows) {
-            o = o_base + cl;
-            c = 0;
-        } else {
-            o = o_base;
-            c = c_base + cl;
-        }
-        return o < a.n_outer && c < a.n_inner;
-    };
+    // lines of this CTA that exist
+    const int nlines = rows ? (int)min((long)C, a.n_outer - o_base) : (int)min((long)C, a.n_inner - c_base);
 
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int idx = tid; idx < L * C; idx += nt) buf[idx] = mk<T>(T(0), T(0));
-    __syncthreads();
+    // ---- zero padding (only the positions the load does not write) ----
+    int gap0 = 0, gap1 = 0;
+    if (a.in_map == IN_DIRECT) {
+        gap0 = a.n_in;
+        gap1 = L;
+    } else if (a.in_map == IN_MODES) {
+        gap0 = a.n_in - a.n_in / 2;
+        gap1 = L - a.n_in / 2;
+    }
+    const int gap = gap1 - gap0;
+    for (int idx = tid; idx < (gap << logC); idx += nt) {
+        const int cl = idx & (C - 1);
+        buf[((gap0 + (idx >> logC)) << logC) + cl] = mk<T>(T(0), T(0));
+    }
 
     // ---- load ----
-    if (a.in_map == IN_HERM) {
-        const int nh = L / 2 + 1;
-        for (int idx = tid; idx < L * C; idx += nt) {
-            int f, cl;
-            if (rows) {
-                f = idx % L;
-                cl = idx / L;
+    if (rows) {
+        for (int cl = 0; cl < nlines; ++cl) {
+            const TI *src = in + (o_base + cl) * a.in_ostride;
+            if (a.in_map == IN_HERM) {
+                const int nh = L / 2 + 1;
+                for (int f = tid; f < L; f += nt) {
+                    const int j = f < nh ? f : L - f;
+                    V v = ld_elem<T, TI>(src + j);
+                    if (f >= nh) v.y = -v.y;
+                    buf[(f << logC) + cl] = v;
+                }
             } else {
-                cl = idx % C;
-                f = idx / C;
+                const T lf = linefac ? linefac[0] : T(1);
+                for (int j = tid; j < a.n_in; j += nt) {
+                    V v = ld_elem<T, TI>(src + j);
+                    if (pre) v = cscale(v, pre[j] * lf);
+                    else if (linefac) v = cscale(v, lf);
+                    int f = j;
+                    if (a.in_map == IN_MODES) {
+                        f = j - a.n_in / 2;
+                        if (f < 0) f += L;
+                    }
+                    buf[(f << logC) + cl] = v;
+                }
             }
-            long o, c;
-            if (!line_ok(cl, o, c)) continue;
-            int j = f < nh ? f : L - f;
-            V v = ld_elem<T, TI>(in + o * a.in_ostride + (long)j * a.n_inner + c);
-            if (f >= nh) v.y = -v.y;
-            buf[f * C + cl] = v;
         }
     } else {
-        for (int idx = tid; idx < a.n_in * C; idx += nt) {
-            int j, cl;
-            if (rows) {
-                j = idx % a.n_in;
-                cl = idx / a.n_in;
-            } else {
-                cl = idx % C;
-                j = idx / C;
+        const TI *src = in + o_base * a.in_ostride + c_base;
+        if (a.in_map == IN_HERM) {
+            const int nh = L / 2 + 1;
+            for (int idx = tid; idx < (L << logC); idx += nt) {
+                const int cl = idx & (C - 1);
+                const int f = idx >> logC;
+                if (cl >= nlines) continue;
+                const int j = f < nh ? f : L - f;
+                V v = ld_elem<T, TI>(src + (long)j * a.n_inner + cl);
+                if (f >= nh) v.y = -v.y;
+                buf[idx] = v;
             }
-            long o, c;
-            if (!line_ok(cl, o, c)) continue;
-            V v = ld_elem<T, TI>(in + o * a.in_ostride + (long)j * a.n_inner + c);
-            T s = T(1);
-            if (pre) s *= pre[j];
-            if (linefac) s *= linefac[c];
-            if (pre || linefac) v = cscale(v, s);
-            int f;
-            if (a.in_map == IN_MODES) {
-                f = j - a.n_in / 2;
-                if (f < 0) f += L;
-            } else {
-                f = j;
+        } else {
+            for (int idx = tid; idx < (a.n_in << logC); idx += nt) {
+                const int cl = idx & (C - 1);
+                const int j = idx >> logC;
+                if (cl >= nlines) continue;
+                V v = ld_elem<T, TI>(src + (long)j * a.n_inner + cl);
+                if (pre || linefac) {
+                    T s = T(1);
+                    if (pre) s *= pre[j];
+                    if (linefac) s *= linefac[c_base + cl];
+                    v = cscale(v, s);
+                }
+                int f = j;
+                if (a.in_map == IN_MODES) {
+                    f = j - a.n_in / 2;
+                    if (f < 0) f += L;
+                }
+                buf[(f << logC) + cl] = v;
             }
-            buf[f * C + cl] = v;
         }
     }
     __syncthreads();
 
-    buf = smem_fft<T>(buf, alt, C, pl, a.sign);
-    alt = (buf == reinterpret_cast<V *>(smem_raw)) ? buf + (long)L * C : reinterpret_cast<V *>(smem_raw);
+    buf = smem_fft<T>(buf, alt, logC, pl, a.sign);
+    alt = (buf == reinterpret_cast<V *>(smem_raw)) ? buf + ((long)L << logC) : reinterpret_cast<V *>(smem_raw);
 
     if (a.mid) {
-        for (int idx = tid; idx < L * C; idx += nt) {
-            int cl = idx % C;
-            int f = idx / C;
-            long o, c;
-            if (!line_ok(cl, o, c)) continue;
-            buf[idx] = cscale(buf[idx], (T)__ldg(a.mid + (long)f * a.mid_ra + c));
+        // rows mode never carries a spectral multiply (lines are columns here)
+        const float *mrow = a.mid + c_base;
+        for (int idx = tid; idx < (L << logC); idx += nt) {
+            const int cl = idx & (C - 1);
+            const int f = idx >> logC;
+            if (cl >= nlines) continue;
+            buf[idx] = cscale(buf[idx], (T)__ldg(mrow + (long)f * a.mid_ra + cl));
         }
         __syncthreads();
-        buf = smem_fft<T>(buf, alt, C, pl, a.sign2);
+        buf = smem_fft<T>(buf, alt, logC, pl, a.sign2);
     }
 
     // ---- store ----
-    for (int idx = tid; idx < a.n_out * C; idx += nt) {
-        int j, cl;
-        if (rows) {
-            j = idx % a.n_out;
-            cl = idx / a.n_out;
-        } else {
-            cl = idx % C;
-            j = idx / C;
-        }
-        long o, c;
-        if (!line_ok(cl, o, c)) continue;
-        int f;
+    const T scale = (T)a.scale;
+    auto fidx = [&](int j) {
+        int f = j;
         if (a.out_map == OUT_MODES) {
             f = j - a.n_out / 2;
             if (f < 0) f += L;
         } else if (a.out_map == OUT_WINDOW) {
             f = j + a.out_off;
-        } else {
-            f = j;
         }
-        V v = buf[f * C + cl];
-        T s = (T)a.scale;
-        if (post) s *= post[j];
-        v = cscale(v, s);
-        st_elem<T, TO>(out + o * a.out_ostride + (long)j * a.n_inner + c, v);
+        return f;
+    };
+    if (rows) {
+        for (int cl = 0; cl < nlines; ++cl) {
+            TO *dst = out + (o_base + cl) * a.out_ostride;
+            for (int j = tid; j < a.n_out; j += nt) {
+                T s = scale;
+                if (post) s *= post[j];
+                st_elem<T, TO>(dst + j, cscale(buf[(fidx(j) << logC) + cl], s));
+            }
+        }
+    } else {
+        TO *dst = out + o_base * a.out_ostride + c_base;
+        for (int idx = tid; idx < (a.n_out << logC); idx += nt) {
+            const int cl = idx & (C - 1);
+            const int j = idx >> logC;
+            if (cl >= nlines) continue;
+            T s = scale;
+            if (post) s *= post[j];
+            st_elem<T, TO>(dst + (long)j * a.n_inner + cl, cscale(buf[(fidx(j) << logC) + cl], s));
+        }
     }
 }
 
@@ -208,6 +236,29 @@ void dispatch(Context &ctx, const AxisFFT &a, const KArgs &ka, const FFTPlan &pl
     else launch_t<T, Cx, Cx>(ctx, ka, pl, threads, smem, blocks);
 }
 
+// log2 of the lines per CTA (a power of two) and the CTA size: rows are
+// grouped so that a CTA moves >= 2048 elements, column groups take 16 adjacent
+// lines (128 contiguous bytes of float2) when the inner extent allows; both
+// ping-pong buffers must fit in shared memory.
+int choose_lines(const AxisFFT &a, size_t esz, size_t max_smem, int &threads) {
+    LC_REQUIRE(!a.mid || a.n_inner > 1, "axis FFT: a spectral multiply needs column lines");
+    const size_t smem_cap = std::min<size_t>(max_smem, 200 * 1024);
+    int logC = 0;
+    if (a.lines_per_cta > 0) {
+        while ((2 << logC) <= a.lines_per_cta) ++logC;
+    } else if (a.n_inner == 1) {
+        while ((a.L << (logC + 1)) <= 2048 && (1L << (logC + 1)) <= a.n_outer) ++logC;
+    } else {
+        logC = 4;
+        while (logC > 0 && (1L << logC) > a.n_inner * 2) --logC;
+    }
+    while (logC > 0 && 2 * ((size_t)a.L << logC) * esz > smem_cap) --logC;
+    LC_REQUIRE(2 * (size_t)a.L * esz <= max_smem, "axis FFT: line does not fit shared memory");
+    const long work = ((long)a.L << logC) / 2;
+    threads = work >= 4096 ? 512 : (work >= 1024 ? 256 : 128);
+    return logC;
+}
+
 }  // namespace
 
 void launch_axis_fft(Context &ctx, const AxisFFT &a) {
@@ -221,22 +272,9 @@ void launch_axis_fft(Context &ctx, const AxisFFT &a) {
 
     const FFTPlan &pl = ctx.plans().get(a.L, a.fp64, ctx.stream());
     const size_t esz = a.fp64 ? sizeof(double2) : sizeof(float2);
-    const size_t smem_cap = std::min<size_t>(ctx.max_smem(), 200 * 1024);
-
-    int C = a.lines_per_cta;
-    if (C <= 0) {
-        if (a.n_inner == 1) {
-            C = std::max(1, 2048 / a.L);
-        } else {
-            C = 16;
-            while (C > 1 && (long)C > a.n_inner * 2) C /= 2;
-        }
-    }
-    // two ping-pong buffers of L*C elements must fit in shared memory
-    while (C > 1 && 2 * (size_t)a.L * C * esz > smem_cap) --C;
-    LC_REQUIRE(2 * (size_t)a.L * C * esz <= ctx.max_smem(), "axis FFT: line does not fit shared memory");
-    long work = (long)a.L * C / 2;
-    int threads = work >= 4096 ? 512 : (work >= 1024 ? 256 : 128);
+    int threads = 0;
+    const int logC = choose_lines(a, esz, ctx.max_smem(), threads);
+    const int C = 1 << logC;
 
     KArgs ka{};
     ka.in = a.in;
@@ -259,7 +297,7 @@ void launch_axis_fft(Context &ctx, const AxisFFT &a) {
     ka.scale = a.scale;
     ka.mid = a.mid;
     ka.mid_ra = a.mid_ra;
-    ka.C = C;
+    ka.logC = logC;
     long blocks;
     if (a.n_inner == 1) {
         blocks = (a.n_outer + C - 1) / C;
@@ -272,6 +310,74 @@ void launch_axis_fft(Context &ctx, const AxisFFT &a) {
     size_t smem = 2 * (size_t)a.L * C * esz;
     if (a.fp64) dispatch<double>(ctx, a, ka, pl, threads, smem, blocks);
     else dispatch<float>(ctx, a, ka, pl, threads, smem, blocks);
+}
+
+void launch_axis_fft_f32_with_plan(cudaStream_t stream, size_t max_smem, const AxisFFT &a,
+                                   const FFTPlan &pl) {
+    LC_REQUIRE(!a.fp64, "explicit-plan axis FFT is FP32 only");
+    LC_REQUIRE(pl.L == a.L, "explicit-plan axis FFT: plan length mismatch");
+    if (a.in_map == IN_HERM) LC_REQUIRE(a.n_in == a.L / 2 + 1, "IN_HERM needs n_in = L/2+1");
+    else LC_REQUIRE(a.n_in <= a.L, "axis FFT: n_in > L");
+    if (a.out_map == OUT_WINDOW) LC_REQUIRE(a.out_off >= 0 && a.out_off + a.n_out <= a.L, "window");
+    else LC_REQUIRE(a.n_out <= a.L, "axis FFT: n_out > L");
+    if (a.n_outer <= 0 || a.n_inner <= 0 || a.n_out == 0) return;
+    const size_t esz = sizeof(float2);
+    int threads = 0;
+    const int logC = choose_lines(a, esz, max_smem, threads);
+    const int C = 1 << logC;
+    KArgs ka{};
+    ka.in = a.in;
+    ka.out = a.out;
+    ka.n_outer = a.n_outer;
+    ka.n_inner = a.n_inner;
+    ka.in_ostride = a.in_ostride;
+    ka.out_ostride = a.out_ostride;
+    ka.n_in = a.n_in;
+    ka.n_out = a.n_out;
+    ka.L = a.L;
+    ka.in_map = a.in_map;
+    ka.out_map = a.out_map;
+    ka.out_off = a.out_off;
+    ka.sign = a.sign;
+    ka.sign2 = a.sign2;
+    ka.pre = a.pre;
+    ka.linefac = a.linefac;
+    ka.post = a.post;
+    ka.scale = a.scale;
+    ka.mid = a.mid;
+    ka.mid_ra = a.mid_ra;
+    ka.logC = logC;
+    long blocks;
+    if (a.n_inner == 1) {
+        blocks = (a.n_outer + C - 1) / C;
+        ka.blocks_per_outer = 1;
+    } else {
+        ka.blocks_per_outer = (a.n_inner + C - 1) / C;
+        blocks = a.n_outer * ka.blocks_per_outer;
+    }
+    LC_REQUIRE(blocks < (1L << 31), "axis FFT: grid too large");
+    size_t smem = 2 * (size_t)a.L * C * esz;
+    bool in_real = a.in_t == E_F32, out_real = a.out_t == E_F32;
+    LC_REQUIRE((a.in_t == E_F32 || a.in_t == E_C64) && (a.out_t == E_F32 || a.out_t == E_C64),
+               "explicit-plan axis FFT: float or float2 elements only");
+    if (in_real && out_real) {
+        auto k = axis_fft_kernel<float, float, float>;
+        LC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+        k<<<(unsigned)blocks, threads, smem, stream>>>(ka, pl);
+    } else if (in_real) {
+        auto k = axis_fft_kernel<float, float, float2>;
+        LC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+        k<<<(unsigned)blocks, threads, smem, stream>>>(ka, pl);
+    } else if (out_real) {
+        auto k = axis_fft_kernel<float, float2, float>;
+        LC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+        k<<<(unsigned)blocks, threads, smem, stream>>>(ka, pl);
+    } else {
+        auto k = axis_fft_kernel<float, float2, float2>;
+        LC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+        k<<<(unsigned)blocks, threads, smem, stream>>>(ka, pl);
+    }
+    LC_CHECK_LAUNCH();
 }
 
 // ---------------------------------------------------------------------------

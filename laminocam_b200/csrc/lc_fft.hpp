@@ -53,6 +53,11 @@ struct AxisFFT {
 
 void launch_axis_fft(Context &ctx, const AxisFFT &a);
 
+// Same transform with a caller-supplied FP32 plan (radices and twiddle table)
+// on an explicit stream; touches no context, plan cache or allocator.
+void launch_axis_fft_f32_with_plan(cudaStream_t stream, size_t max_smem, const AxisFFT &a,
+                                   const FFTPlan &pl);
+
 struct AxisDFT {
     const void *in = nullptr;
     Elem in_t = E_C64;

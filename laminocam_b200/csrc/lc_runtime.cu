@@ -30,26 +30,7 @@ long next_smooth23(long n) {
 }
 
 static void factorise(int L, FFTPlan &pl) {
-    pl.L = L;
-    pl.nst = 0;
-    int r = L;
-    while (r % 8 == 0) {
-        pl.radix[pl.nst++] = 8;
-        r /= 8;
-    }
-    if (r % 4 == 0) {
-        pl.radix[pl.nst++] = 4;
-        r /= 4;
-    }
-    if (r % 2 == 0) {
-        pl.radix[pl.nst++] = 2;
-        r /= 2;
-    }
-    while (r % 3 == 0) {
-        pl.radix[pl.nst++] = 3;
-        r /= 3;
-    }
-    LC_REQUIRE(r == 1 && pl.nst <= kMaxStages, "FFT length must be 2^p*3^q");
+    LC_REQUIRE(L >= 1 && L < (1 << 20) && fft_factorise(L, pl), "FFT length must be 2^p*3^q");
 }
 
 const FFTPlan &PlanCache::get(int L, bool fp64, cudaStream_t s) {

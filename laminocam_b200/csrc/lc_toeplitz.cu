@@ -20,45 +20,106 @@ __device__ __forceinline__ double dirichlet(double u, int n) {
     return sinpi(u) / sv;
 }
 
-// K[ky][kx] over modes k = j - P/2, 2D polar grid: sum_theta D_nr(kx c + ky s)
-__global__ void psf2d_kernel(const double2 *__restrict__ cs, int ntheta, int nr, int P2, int P3,
-                             double *__restrict__ K) {
-    long total = (long)P2 * P3;
-    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (long)gridDim.x * blockDim.x) {
-        int jy = (int)(idx / P3), jx = (int)(idx - (long)jy * P3);
-        double kx = (double)(jx - P3 / 2), ky = (double)(jy - P2 / 2);
-        double s = 0.0;
-        for (int i = 0; i < ntheta; ++i) {
-            double2 t = cs[i];
-            s += dirichlet(kx * t.x + ky * t.y, nr);
-        }
-        K[idx] = s;
-    }
+// Per-angle coefficients of the fast PSF generator: uX = a . k, uY = b . k
+// (k = (kx, ky, kz)), and the phasors exp(i pi a0), exp(i pi a0 / nx),
+// exp(i pi b0), exp(i pi b0 / ny) that advance sin(pi uX), sin(pi uX / nx), ...
+// by one step in kx.
+struct PsfAngle {
+    double a[3], b[3];
+    double2 stepA, stepB, stepC, stepD;
+};
+
+__device__ __forceinline__ double2 crot(double2 p, double2 s) {
+    return make_double2(p.x * s.x - p.y * s.y, p.x * s.y + p.y * s.x);
 }
 
-// K[kz][ky][kx], 3D rotated detector lattice:
-// sum_theta D_ncols(uX) D_nrows(uY), uX = R00 kx + R10 ky + R20 kz, uY = R01 kx + R11 ky + R21 kz
-__global__ void psf3d_kernel(const double *__restrict__ rot, int ntheta, int nrows, int ncols,
-                             int P1, int P2, int P3, double *__restrict__ K) {
-    extern __shared__ double srot[];
-    for (int i = threadIdx.x; i < 6 * ntheta; i += blockDim.x) srot[i] = rot[i];
+__device__ __forceinline__ int mirror_index(int j, int P) {
+    // index of -k for mode index j (k = j - P/2); -1 when -k is outside the grid
+    if (P % 2 == 0) return j == 0 ? -1 : P - j;
+    return P - 1 - j;
+}
+
+// Rows of K (all kx of one (kz, ky)) in segments of S values of kx.  The sum over
+// angles uses the Dirichlet closed form, with sin(pi u) and sin(pi u / n)
+// advanced along kx by complex rotations (FP64; rounding grows by ~1e-16 per
+// step over S steps) and evaluated directly whenever the denominator is small.
+// Only the half space kz <= 0 (2D: ky <= 0) is summed; K(-k) = K(k) fills the
+// rest.
+template <int DIM, int S>
+__global__ void __launch_bounds__(128) psf_rows_kernel(const PsfAngle *__restrict__ angles, int ntheta,
+                                                      int nx, int ny, int P1, int P2, int P3,
+                                                      double *__restrict__ K) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PsfAngle *ang = reinterpret_cast<PsfAngle *>(smem_raw);
+    for (int i = threadIdx.x; i < ntheta; i += blockDim.x) ang[i] = angles[i];
     __syncthreads();
-    long total = (long)P1 * P2 * P3;
-    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (long)gridDim.x * blockDim.x) {
-        int jz = (int)(idx / ((long)P2 * P3));
-        long r = idx - (long)jz * P2 * P3;
-        int jy = (int)(r / P3), jx = (int)(r - (long)jy * P3);
-        double kx = (double)(jx - P3 / 2), ky = (double)(jy - P2 / 2), kz = (double)(jz - P1 / 2);
-        double s = 0.0;
-        for (int i = 0; i < ntheta; ++i) {
-            const double *R = srot + 6 * i;
-            double uX = R[0] * kx + R[2] * ky + R[4] * kz;
-            double uY = R[1] * kx + R[3] * ky + R[5] * kz;
-            s += dirichlet(uX, ncols) * dirichlet(uY, nrows);
+    const int nseg = (P3 + S - 1) / S;
+    // rows of the half space: 3D (jz <= P1/2, all jy); 2D (jy <= P2/2)
+    const long nrows_half = DIM == 3 ? (long)(P1 / 2 + 1) * P2 : (long)(P2 / 2 + 1);
+    const long items = nrows_half * nseg;
+    const double inv_nx = 1.0 / (double)nx, inv_ny = 1.0 / (double)ny;
+    for (long it = (long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
+         it += (long)gridDim.x * blockDim.x) {
+        const long row = it / nseg;
+        const int seg = (int)(it - row * nseg);
+        int jz = 0, jy;
+        if (DIM == 3) {
+            jz = (int)(row / P2);
+            jy = (int)(row - (long)jz * P2);
+        } else {
+            jy = (int)row;
         }
-        K[idx] = s;
+        const int jx0 = seg * S;
+        const double kx0 = (double)(jx0 - P3 / 2);
+        const double ky = (double)(jy - P2 / 2);
+        const double kz = DIM == 3 ? (double)(jz - P1 / 2) : 0.0;
+        double acc[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) acc[s] = 0.0;
+        for (int i = 0; i < ntheta; ++i) {
+            const PsfAngle &A = ang[i];
+            const double uX0 = A.a[0] * kx0 + A.a[1] * ky + A.a[2] * kz;
+            double2 pA, pB, pC = make_double2(1.0, 0.0), pD = make_double2(1.0, 0.0);
+            sincospi(uX0, &pA.y, &pA.x);
+            sincospi(uX0 * inv_nx, &pB.y, &pB.x);
+            double uY0 = 0.0;
+            if (DIM == 3) {
+                uY0 = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
+                sincospi(uY0, &pC.y, &pC.x);
+                sincospi(uY0 * inv_ny, &pD.y, &pD.x);
+            }
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                double dX, dY = 1.0;
+                if (fabs(pB.y) > 1e-6) dX = pA.y / pB.y;
+                else dX = dirichlet(uX0 + (double)s * A.a[0], nx);
+                if (DIM == 3) {
+                    if (fabs(pD.y) > 1e-6) dY = pC.y / pD.y;
+                    else dY = dirichlet(uY0 + (double)s * A.b[0], ny);
+                }
+                acc[s] += dX * dY;
+                pA = crot(pA, A.stepA);
+                pB = crot(pB, A.stepB);
+                if (DIM == 3) {
+                    pC = crot(pC, A.stepC);
+                    pD = crot(pD, A.stepD);
+                }
+            }
+        }
+        const long plane = (long)P2 * P3;
+        const int mz = DIM == 3 ? mirror_index(jz, P1) : 0;
+        const int my = mirror_index(jy, P2);
+        const bool self_plane = DIM == 3 ? (mz == jz) : (my == jy);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const int jx = jx0 + s;
+            if (jx >= P3) break;
+            K[(long)jz * plane + (long)jy * P3 + jx] = acc[s];
+            if (self_plane) continue;  // its mirror is summed by another row of the half space
+            const int mx = mirror_index(jx, P3);
+            if ((DIM == 3 && mz < 0) || my < 0 || mx < 0) continue;
+            K[(long)mz * plane + (long)my * P3 + mx] = acc[s];
+        }
     }
 }
 
@@ -161,13 +222,7 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
     }
     cudaStream_t st = ctx.stream();
     DevBuf<double> K;
-    build_kernel(ctx, K);
-    {
-        long total = (long)P_[0] * P_[1] * P_[2];
-        zero_unpaired_kernel<<<grid_for(total, 256, ctx.num_sms()), 256, 0, st>>>(K.get(), P_[0], P_[1],
-                                                                                  P_[2]);
-        LC_CHECK_LAUNCH();
-    }
+    build_kernel(ctx, K);  // unpaired -P/2 planes already zeroed
     // Spectrum of the zero-centred kernel: FFT with the mode placement k -> k mod P.
     // It is real and point-symmetric; keep x in [0, P3/2] (the R2C half) and all
     // of y and z, i.e. a real {P1, P2, P3/2+1} array.
@@ -255,23 +310,69 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
 void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
     cudaStream_t st = ctx.stream();
     ProfScope ps(ctx, PS_PSF_GEN, 0.0);
-    if (!three_d_) {
-        const int P = P_[2];
-        K.alloc((long)P * P, st);
-        long total = (long)P * P;
-        psf2d_kernel<<<grid_for(total, 128, ctx.num_sms()), 128, 0, st>>>(
-            g_->pts.cs, g_->pts.ntheta, g_->pts.nr, P, P, K.get());
+    const int nth = g_->pts.ntheta;
+    const double pi = 3.14159265358979323846;
+    std::vector<PsfAngle> tab(nth);
+    int nx, ny;
+    for (int i = 0; i < nth; ++i) {
+        PsfAngle &A = tab[i];
+        if (three_d_) {
+            // columns of transpose(Rx(theta) Ry(beta) Rz(gamma)) (include/rotation.h:28-56):
+            // uX = (R00, R10, R20) . k, uY = (R01, R11, R21) . k
+            double ct = std::cos(g_->theta[i]), st_ = std::sin(g_->theta[i]);
+            double cb = std::cos(g_->beta[i]), sb = std::sin(g_->beta[i]);
+            double cg = std::cos(g_->gamma[i]), sg = std::sin(g_->gamma[i]);
+            A.a[0] = cb * cg;
+            A.a[1] = -cb * sg;
+            A.a[2] = sb;
+            A.b[0] = ct * sg + st_ * sb * cg;
+            A.b[1] = ct * cg - st_ * sb * sg;
+            A.b[2] = -st_ * cb;
+        } else {
+            A.a[0] = std::cos(g_->theta[i]);
+            A.a[1] = std::sin(g_->theta[i]);
+            A.a[2] = 0.0;
+            A.b[0] = A.b[1] = A.b[2] = 0.0;
+        }
+    }
+    if (three_d_) {
+        nx = g_->pts.ncols;
+        ny = g_->pts.nrows;
     } else {
-        long total = (long)P_[0] * P_[1] * P_[2];
-        K.alloc(total, st);
-        size_t smem = 6 * sizeof(double) * g_->pts.ntheta;
-        LC_REQUIRE(smem <= 200 * 1024, "Toeplitz3D: too many angles for one PSF launch");
-        auto kern = psf3d_kernel;
+        nx = g_->pts.nr;
+        ny = 1;
+    }
+    for (auto &A : tab) {
+        A.stepA = make_double2(std::cos(pi * A.a[0]), std::sin(pi * A.a[0]));
+        A.stepB = make_double2(std::cos(pi * A.a[0] / nx), std::sin(pi * A.a[0] / nx));
+        A.stepC = make_double2(std::cos(pi * A.b[0]), std::sin(pi * A.b[0]));
+        A.stepD = make_double2(std::cos(pi * A.b[0] / ny), std::sin(pi * A.b[0] / ny));
+    }
+    DevBuf<PsfAngle> dtab;
+    dtab.upload(tab.data(), tab.size(), st);
+    const int P1 = P_[0], P2 = P_[1], P3 = P_[2];
+    long total = (long)P1 * P2 * P3;
+    K.alloc(total, st);
+    constexpr int S = 16;
+    const long nseg = (P3 + S - 1) / S;
+    const long items = (three_d_ ? (long)(P1 / 2 + 1) * P2 : (long)(P2 / 2 + 1)) * nseg;
+    size_t smem = sizeof(PsfAngle) * nth;
+    LC_REQUIRE(smem <= 220 * 1024, "Toeplitz: too many angles for one PSF launch");
+    unsigned blocks = (unsigned)std::max<long>(1, std::min<long>((items + 127) / 128, (long)ctx.num_sms() * 16));
+    if (three_d_) {
+        auto kern = psf_rows_kernel<3, S>;
         LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<grid_for(total, 128, ctx.num_sms()), 128, smem, st>>>(
-            g_->pts.rot, g_->pts.ntheta, g_->pts.nrows, g_->pts.ncols, P_[0], P_[1], P_[2], K.get());
+        kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, nx, ny, P1, P2, P3, K.get());
+    } else {
+        auto kern = psf_rows_kernel<2, S>;
+        LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, nx, ny, P1, P2, P3, K.get());
     }
     LC_CHECK_LAUNCH();
+    // planes of mode -P/2 have no mirror inside the grid; they are not needed
+    zero_unpaired_kernel<<<grid_for(total, 256, ctx.num_sms()), 256, 0, st>>>(K.get(), P1, P2, P3);
+    LC_CHECK_LAUNCH();
+    LC_CUDA(cudaStreamSynchronize(st));  // the angle table is released on return
 }
 
 void Toeplitz::kernel_fp64(Context &ctx, double *host_out) {
