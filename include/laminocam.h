@@ -32,6 +32,7 @@ extern "C" {
 #define LC_ERR_NOMEM 2    /* device allocation failed / over the memory budget */
 #define LC_ERR_CUDA 3     /* CUDA runtime error */
 #define LC_ERR_INTERNAL 4 /* anything else */
+#define LC_ERR_TOO_LARGE 5 /* sizes beyond a fixed maximum (lc_sysmat2d_toeplitz_noalloc) */
 
 typedef struct lc_context_s *lc_context;
 typedef struct lc_geometry_s *lc_geometry;
@@ -183,6 +184,28 @@ int lc_profile_read(lc_context ctx, lc_profile_entry *out, int max_entries, int 
 /* number of kernels this library has launched in the process so far */
 long lc_kernel_launches(void);
 
+/* ---- allocation-free Toeplitz apply --------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory while running (for example a reconstruction inside a detector's
+ * acquisition loop that reserves all device memory up front, or a host that
+ * forbids cudaMalloc/cudaFree after start-up because they can synchronise the
+ * device): y = A^T A x for nslices slices of n x n, like lc_sysmat_toeplitz on
+ * a 2D PSF, without any allocation.  The intermediate spectrum lives in a
+ * 16 MiB array compiled into the library (held by every GPU that loads it
+ * until the process exits).
+ *   stream:   cudaStream_t the work is issued on (NULL = legacy default stream)
+ *   spectrum: device, the PSF's real half spectrum {P, P/2+1}, as returned by
+ *             lc_psf_spectrum for a 2D PSF of image size n
+ *   P:        the PSF grid, next 2^p 3^q >= 2n-1 (lc_psf_info)
+ *   x, y:     device {nslices, n, n}
+ * Limits: P <= 4096 and nslices * n * (P/2+1) <= 2^21; larger sizes return
+ * LC_ERR_TOO_LARGE.  The first call on a device looks up the array's device
+ * address; make that first call before any stream capture.  All calls share
+ * the array and its contents are left over from the previous call: calls that
+ * overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller. */
+int lc_sysmat2d_toeplitz_noalloc(void *stream, const float *spectrum, int P, const float *x,
+                                 float *y, int nslices, int n);
 
 #ifdef __cplusplus
 }

@@ -70,6 +70,7 @@ SIGNATURES = {
                                C.POINTER(ReconParamsC), vp, C.POINTER(SolverStats)]),
     "lc_profile_enable": (i32, [vp, i32]),
     "lc_kernel_launches": (C.c_long, []),
+    "lc_sysmat2d_toeplitz_noalloc": (i32, [vp, vp, i32, vp, vp, i32, i32]),
     "lc_profile_read": (i32, [vp, C.POINTER(ProfileEntry), i32, C.POINTER(C.c_int)]),
 }
 
