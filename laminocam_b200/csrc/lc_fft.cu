@@ -2,6 +2,9 @@
 // global loads and stores are arranged so that consecutive threads touch
 // consecutive addresses (along i for contiguous lines, along c otherwise).
 #include <algorithm>
+#include <cmath>
+#include <memory>
+#include <vector>
 
 #include "lc_fft.hpp"
 
@@ -486,6 +489,197 @@ void dft_launch(Context &ctx, const DArgs &d, long blocks, int threads, size_t s
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Bluestein (chirp-z) DFT of arbitrary length on the Stockham core:
+//   X[k] = sum_m x[m] e^{s 2 pi i m k / n} = a[k] sum_m (x[m] a[m]) conj(a[k-m]),
+//   a[j] = e^{s i pi j^2 / n},
+// a cyclic convolution of length L = next 2^p 3^q >= 2n - 1 done as
+// FFT -> multiply by V = FFT(conj a, wrapped) / L -> inverse FFT.
+// ---------------------------------------------------------------------------
+struct BArgs {
+    const void *in;
+    void *out;
+    long n_outer, n_inner, in_ostride, out_ostride;
+    int n, L, d_pre, d_post, logC;
+    float scale;
+    long blocks_per_outer;
+    const float2 *chirp, *V;
+};
+
+template <typename TI, typename TO>
+__global__ void bluestein_kernel(BArgs a, FFTPlan pl) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int logC = a.logC, C = 1 << logC, L = a.L, n = a.n;
+    float2 *buf = reinterpret_cast<float2 *>(smem_raw);
+    float2 *alt = buf + ((long)L << logC);
+    const TI *in = reinterpret_cast<const TI *>(a.in);
+    TO *out = reinterpret_cast<TO *>(a.out);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const bool rows = (a.n_inner == 1);
+    long o_base, c_base;
+    if (rows) {
+        o_base = (long)blockIdx.x << logC;
+        c_base = 0;
+    } else {
+        o_base = (long)blockIdx.x / a.blocks_per_outer;
+        c_base = ((long)blockIdx.x % a.blocks_per_outer) << logC;
+    }
+    const int nlines = rows ? (int)min((long)C, a.n_outer - o_base) : (int)min((long)C, a.n_inner - c_base);
+    for (int idx = tid; idx < ((L - n) << logC); idx += nt)
+        buf[((n + (idx >> logC)) << logC) + (idx & (C - 1))] = make_float2(0.f, 0.f);
+    // load with the pre-roll: line value m is in[(m + d_pre) % n], times chirp[m]
+    if (rows) {
+        for (int cl = 0; cl < nlines; ++cl) {
+            const TI *src = in + (o_base + cl) * a.in_ostride;
+            for (int m = tid; m < n; m += nt) {
+                int s = m + a.d_pre;
+                if (s >= n) s -= n;
+                buf[(m << logC) + cl] = cmul(ld_elem<float, TI>(src + s), a.chirp[m]);
+            }
+        }
+    } else {
+        const TI *src = in + o_base * a.in_ostride + c_base;
+        for (int idx = tid; idx < (n << logC); idx += nt) {
+            const int cl = idx & (C - 1), m = idx >> logC;
+            if (cl >= nlines) continue;
+            int s = m + a.d_pre;
+            if (s >= n) s -= n;
+            buf[idx] = cmul(ld_elem<float, TI>(src + (long)s * a.n_inner + cl), a.chirp[m]);
+        }
+    }
+    __syncthreads();
+    float2 *res = smem_fft<float>(buf, alt, logC, pl, -1);
+    float2 *oth = (res == buf) ? alt : buf;
+    for (int idx = tid; idx < (L << logC); idx += nt) res[idx] = cmul(res[idx], a.V[idx >> logC]);
+    __syncthreads();
+    res = smem_fft<float>(res, oth, logC, pl, +1);
+    // store with the post-roll: out[k] = X[(k + d_post) % n], X[q] = a[q] * conv[q]
+    if (rows) {
+        for (int cl = 0; cl < nlines; ++cl) {
+            TO *dst = out + (o_base + cl) * a.out_ostride;
+            for (int k = tid; k < n; k += nt) {
+                int q = k + a.d_post;
+                if (q >= n) q -= n;
+                st_elem<float, TO>(dst + k, cscale(cmul(res[(q << logC) + cl], a.chirp[q]), a.scale));
+            }
+        }
+    } else {
+        TO *dst = out + o_base * a.out_ostride + c_base;
+        for (int idx = tid; idx < (n << logC); idx += nt) {
+            const int cl = idx & (C - 1), k = idx >> logC;
+            if (cl >= nlines) continue;
+            int q = k + a.d_post;
+            if (q >= n) q -= n;
+            st_elem<float, TO>(dst + (long)k * a.n_inner + cl,
+                               cscale(cmul(res[(q << logC) + cl], a.chirp[q]), a.scale));
+        }
+    }
+}
+
+__global__ void c128_to_c64_kernel(const double2 *in, float2 *out, int n, double scale) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = make_float2((float)(in[i].x * scale), (float)(in[i].y * scale));
+}
+
+const BluesteinEntry &bluestein_tables(Context &ctx, int n, int sign) {
+    if (BluesteinEntry *e = ctx.plans().find_bluestein(n, sign)) return *e;
+    cudaStream_t st = ctx.stream();
+    auto e = std::make_unique<BluesteinEntry>();
+    e->n = n;
+    e->sign = sign;
+    e->L = (int)next_smooth23(2L * n - 1);
+    const int L = e->L;
+    const double pi = 3.14159265358979323846;
+    std::vector<double2> a(n), v(L, make_double2(0.0, 0.0));
+    for (int j = 0; j < n; ++j) {
+        long t = ((long)j * j) % (2L * n);  // exact j^2 mod 2n
+        double ang = sign * pi * (double)t / (double)n;
+        a[j] = make_double2(std::cos(ang), std::sin(ang));
+    }
+    for (int j = 0; j < n; ++j) {
+        double2 c = make_double2(a[j].x, -a[j].y);
+        v[j] = c;
+        if (j > 0) v[L - j] = c;
+    }
+    std::vector<float2> af(n);
+    for (int j = 0; j < n; ++j) af[j] = make_float2((float)a[j].x, (float)a[j].y);
+    e->chirp.upload(af.data(), n, st);
+    DevBuf<double2> dv, dV;
+    dv.upload(v.data(), L, st);
+    dV.alloc(L, st);
+    AxisFFT f;
+    f.in = dv.get();
+    f.in_t = E_C128;
+    f.out = dV.get();
+    f.out_t = E_C128;
+    f.fp64 = true;
+    f.n_outer = 1;
+    f.n_inner = 1;
+    f.in_ostride = L;
+    f.out_ostride = L;
+    f.n_in = L;
+    f.L = L;
+    f.n_out = L;
+    f.sign = -1;
+    launch_axis_fft(ctx, f);
+    e->V.alloc(L, st);
+    c128_to_c64_kernel<<<(L + 255) / 256, 256, 0, st>>>(dV.get(), e->V.get(), L, 1.0 / (double)L);
+    LC_CHECK_LAUNCH();
+    LC_CUDA(cudaStreamSynchronize(st));  // host vectors and dv/dV die on return
+    return *ctx.plans().store_bluestein(std::move(e));
+}
+
+template <typename TI, typename TO>
+void bluestein_launch(Context &ctx, const BArgs &b, const FFTPlan &pl, long blocks, int threads,
+                      size_t smem) {
+    auto kern = bluestein_kernel<TI, TO>;
+    LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx.max_smem()));
+    kern<<<(unsigned)blocks, threads, smem, ctx.stream()>>>(b, pl);
+    LC_CHECK_LAUNCH();
+}
+
+void launch_bluestein(Context &ctx, const AxisDFT &a) {
+    const BluesteinEntry &e = bluestein_tables(ctx, a.n, a.sign);
+    const FFTPlan &pl = ctx.plans().get(e.L, false, ctx.stream());
+    AxisFFT shape;  // only to pick the line grouping
+    shape.L = e.L;
+    shape.n_inner = a.n_inner;
+    shape.n_outer = a.n_outer;
+    int threads = 0;
+    const int logC = choose_lines(shape, sizeof(float2), ctx.max_smem(), threads);
+    const int C = 1 << logC;
+    BArgs b{};
+    b.in = a.in;
+    b.out = a.out;
+    b.n_outer = a.n_outer;
+    b.n_inner = a.n_inner;
+    b.in_ostride = a.in_ostride;
+    b.out_ostride = a.out_ostride;
+    b.n = a.n;
+    b.L = e.L;
+    b.d_pre = ((a.d_pre % a.n) + a.n) % a.n;
+    b.d_post = ((a.d_post % a.n) + a.n) % a.n;
+    b.logC = logC;
+    b.scale = a.scale;
+    b.chirp = e.chirp.get();
+    b.V = e.V.get();
+    long blocks;
+    if (a.n_inner == 1) {
+        blocks = (a.n_outer + C - 1) / C;
+        b.blocks_per_outer = 1;
+    } else {
+        b.blocks_per_outer = (a.n_inner + C - 1) / C;
+        blocks = a.n_outer * b.blocks_per_outer;
+    }
+    LC_REQUIRE(blocks < (1L << 31), "DFT: grid too large");
+    size_t smem = 2 * ((size_t)e.L << logC) * sizeof(float2);
+    bool in_real = a.in_t == E_F32, out_real = a.out_t == E_F32;
+    if (in_real && out_real) bluestein_launch<float, float>(ctx, b, pl, blocks, threads, smem);
+    else if (in_real) bluestein_launch<float, float2>(ctx, b, pl, blocks, threads, smem);
+    else if (out_real) bluestein_launch<float2, float>(ctx, b, pl, blocks, threads, smem);
+    else bluestein_launch<float2, float2>(ctx, b, pl, blocks, threads, smem);
+}
+
 void launch_axis_dft(Context &ctx, const AxisDFT &a) {
     LC_REQUIRE(a.n > 0, "DFT length must be positive");
     const double lines = (double)a.n_outer * a.n_inner;
@@ -494,6 +688,10 @@ void launch_axis_dft(Context &ctx, const AxisDFT &a) {
     LC_REQUIRE(a.in_t == E_F32 || a.in_t == E_C64, "DFT input must be float or float2");
     LC_REQUIRE(a.out_t == E_F32 || a.out_t == E_C64, "DFT output must be float or float2");
     if (a.n_outer <= 0 || a.n_inner <= 0) return;
+    if (a.n >= 16 && next_smooth23(2L * a.n - 1) <= 8192) {
+        launch_bluestein(ctx, a);
+        return;
+    }
     DArgs d{};
     d.in = a.in;
     d.out = a.out;

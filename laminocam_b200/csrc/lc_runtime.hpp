@@ -82,6 +82,13 @@ struct PlanEntry {
 bool is_smooth23(long n);
 long next_smooth23(long n);  // smallest 2^p 3^q >= n
 
+// Bluestein (chirp-z) tables for a DFT of arbitrary length n and sign s:
+// chirp[j] = exp(s i pi j^2 / n) (j < n) and V = FFT_L(conj chirp, wrapped) / L.
+struct BluesteinEntry {
+    int n = 0, L = 0, sign = 0;
+    DevBuf<float2> chirp, V;
+};
+
 class Context;
 
 // Per-device cache of FFT plans and twiddle tables.
@@ -90,16 +97,31 @@ class PlanCache {
     const FFTPlan &get(int L, bool fp64, cudaStream_t s);
     // twiddle table exp(-2*pi*i*m/n) for a direct DFT of arbitrary n (float2)
     const float2 *dft_twiddles(int n, cudaStream_t s);
+    // cached Bluestein tables (built by the caller on a miss)
+    BluesteinEntry *find_bluestein(int n, int sign) {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = blue_.find(std::make_pair(n, sign));
+        return it == blue_.end() ? nullptr : it->second.get();
+    }
+    BluesteinEntry *store_bluestein(std::unique_ptr<BluesteinEntry> e) {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto key = std::make_pair(e->n, e->sign);
+        auto &slot = blue_[key];
+        if (!slot) slot = std::move(e);
+        return slot.get();
+    }
     void clear() {
         std::lock_guard<std::mutex> lk(mu_);
         plans_.clear();
         dft_.clear();
+        blue_.clear();
     }
 
   private:
     std::mutex mu_;
     std::map<std::pair<int, bool>, std::unique_ptr<PlanEntry>> plans_;
     std::map<int, std::unique_ptr<DevBuf<float2>>> dft_;
+    std::map<std::pair<int, int>, std::unique_ptr<BluesteinEntry>> blue_;
 };
 
 // Optional per-section device timing: sections record a CUDA event pair on

@@ -134,6 +134,23 @@ def test_projection_ops_3d_golden(lc, f):
     assert O.rel_l2(to_np(lc.sysmat(vol, pg)), g["sysmat3d_nufft"]) < PROJ_TOL
 
 
+def test_projection_ops_3d_bluestein_detector(lc):
+    """Detector lines of 33 and 40 samples take the Bluestein (chirp-z) DFT path."""
+    rng = np.random.default_rng(31)
+    nth = 12
+    th = np.arange(nth) * 2 * np.pi / nth
+    ga, be = np.full(nth, -0.45), np.full(nth, 0.05)
+    vol = rng.random((5, 24, 24)).astype(np.float32)
+    proj = rng.random((nth, 33, 40)).astype(np.float32)
+    sh = rng.normal(scale=2.0, size=(nth, 2)).astype(np.float32)
+    grid = O.Grid3D(th, ga, be, 33, 40)
+    pg = lc.PolarGrid(th, ga, be, 33, 40, shifts=sh)
+    v64, p64 = vol.astype(np.float64), proj.astype(np.float64)
+    assert O.rel_l2(to_np(lc.forward(vol, pg)), O.forward3d(v64, grid)) < PROJ_TOL
+    assert O.rel_l2(to_np(lc.backproj(proj, pg, vol.shape, shifts=True)),
+                    O.backproj3d(p64, grid, vol.shape, sh.astype(np.float64))) < PROJ_TOL
+
+
 @pytest.mark.parametrize("f", ["golden3d_a.npz", "golden3d_b.npz"])
 def test_toeplitz_3d_golden(lc, f):
     g = load(f)
