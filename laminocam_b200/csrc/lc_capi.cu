@@ -7,31 +7,16 @@
 #include <memory>
 #include <tuple>
 
-#include "../../include/laminocam.h"
-#include "lc_nufft.hpp"
-#include "lc_solver.hpp"
-#include "lc_toeplitz.hpp"
+#include "lc_internal.hpp"
 
 using namespace lc;
 
-struct lc_context_s {
-    std::unique_ptr<Context> ctx;
-    std::string err;
-};
-
-struct lc_geometry_s {
-    lc_context owner = nullptr;
-    PolarGeometry g;
-    std::map<std::tuple<int, int, int, int>, std::unique_ptr<NufftPlan>> plans;
-    DevBuf<float2> work;
-};
-
-struct lc_psf_s {
-    lc_context owner = nullptr;
-    lc_geometry geom = nullptr;
-    std::unique_ptr<Toeplitz> T;
-    std::unique_ptr<Solver> solver;
-};
+namespace lc {
+long odd_pad(long n, float factor) {
+    long v = (long)((float)n * factor);
+    return v % 2 == 0 ? v - 1 : v;
+}
+}  // namespace lc
 
 namespace {
 
@@ -130,11 +115,6 @@ __global__ void crop_kernel(const float *__restrict__ in, long N1, long N2, long
 unsigned grid_for(long n, int threads, int sms) {
     long b = (n + threads - 1) / threads;
     return (unsigned)std::max<long>(1, std::min<long>(b, (long)sms * 32));
-}
-
-long odd_pad(long n, float factor) {
-    long v = (long)((float)n * factor);
-    return v % 2 == 0 ? v - 1 : v;
 }
 
 // --- operator implementations shared by the API and the drivers ----------
@@ -566,47 +546,79 @@ int lc_split_bregman(lc_context c, lc_psf p, const float *rhs, float *x,
     });
 }
 
+}  // extern "C"
+
+namespace lc {
+
+static std::shared_ptr<Toeplitz> make_psf(Context &ctx, const PolarGeometry &g, const long dims[3],
+                                          bool three_d, const PsfProvider *psf, bool *hit) {
+    if (hit) *hit = false;
+    if (psf && *psf) return (*psf)(ctx, g, dims, three_d, hit);
+    return std::make_shared<Toeplitz>(ctx, g, dims, three_d);
+}
+
+void mbir2d_core(lc_context c, const float *dsino, int ns, int ntheta, int nradial,
+                 const double *theta, const int *recon_dims, const lc_recon_params *p,
+                 float *drecon, lc_solver_stats *stats, const PsfProvider *psfp, bool *psf_hit) {
+    LC_REQUIRE(dsino && theta && recon_dims && p && drecon, "NULL argument");
+    LC_REQUIRE(ns > 0 && ntheta > 0 && nradial > 0, "sizes must be positive");
+    LC_REQUIRE(recon_dims[0] == ns, "recon_dims[0] must equal the number of sinogram slices");
+    LC_REQUIRE(recon_dims[1] == recon_dims[2] && recon_dims[1] > 0, "recon_dims must be square in-plane");
+    LC_REQUIRE(p->method == 0 || p->method == 1, "method must be 0 (CG) or 1 (Split-Bregman)");
+    check_solver_params(&p->solver);
+    Context &ctx = *c->ctx;
+    cudaStream_t s = ctx.stream();
+    const int n = recon_dims[1];
+    const long nv = (long)ns * n * n;
+    lc_geometry g = nullptr;
+    int rc = lc_geometry2d_create(c, theta, ntheta, nradial, &g);
+    if (rc) throw Error(rc == LC_ERR_INVALID ? 1 : 3, c->err);
+    std::unique_ptr<lc_geometry_s> gown(g);
+    DevBuf<float> rhs(nv, s);
+    do_backproj2d(g, dsino, ns, n, n, rhs.get(), eff_tol(p->nufft_tol));
+    g->work.release();
+    g->plans.clear();
+    lc_psf_s psf;
+    psf.owner = c;
+    psf.geom = g;
+    long dims[3] = {ns, n, n};
+    psf.T = make_psf(ctx, g->g, dims, false, psfp, psf_hit);
+    LC_CUDA(cudaMemsetAsync(drecon, 0, nv * sizeof(float), s));
+    run_solver(&psf, p->method, rhs.get(), drecon, &p->solver, stats);
+}
+
+}  // namespace lc
+
+extern "C" {
+
 int lc_mbir2d(lc_context c, const float *sino, int ns, int ntheta, int nradial,
               const double *theta, const int *recon_dims, const lc_recon_params *p, float *recon,
               lc_solver_stats *stats) {
     return guarded(c, [&] {
         LC_REQUIRE(sino && theta && recon_dims && p && recon, "NULL argument");
         LC_REQUIRE(ns > 0 && ntheta > 0 && nradial > 0, "sizes must be positive");
-        LC_REQUIRE(recon_dims[0] == ns, "recon_dims[0] must equal the number of sinogram slices");
-        LC_REQUIRE(recon_dims[1] == recon_dims[2] && recon_dims[1] > 0,
-                   "recon_dims must be square in-plane");
-        LC_REQUIRE(p->method == 0 || p->method == 1, "method must be 0 (CG) or 1 (Split-Bregman)");
-        check_solver_params(&p->solver);
         Context &ctx = *c->ctx;
         cudaStream_t s = ctx.stream();
-        const int n = recon_dims[1];
-        const long nv = (long)ns * n * n;
         const long nsino = (long)ns * ntheta * nradial;
-        DevBuf<float> dsino;
+        const long nv = (long)ns * recon_dims[1] * recon_dims[2];
+        LC_REQUIRE(nv > 0, "recon_dims must be positive");
+        DevBuf<float> dsino, x(nv, s);
         dsino.upload(sino, nsino, s);
-        lc_geometry g = nullptr;
-        int rc = lc_geometry2d_create(c, theta, ntheta, nradial, &g);
-        if (rc) throw Error(rc == LC_ERR_INVALID ? 1 : 3, c->err);
-        std::unique_ptr<lc_geometry_s> gown(g);
-        DevBuf<float> rhs(nv, s), x(nv, s);
-        do_backproj2d(g, dsino.get(), ns, n, n, rhs.get(), eff_tol(p->nufft_tol));
-        dsino.release();
-        lc_psf_s psf;
-        psf.owner = c;
-        psf.geom = g;
-        long dims[3] = {ns, n, n};
-        psf.T = std::make_unique<Toeplitz>(ctx, g->g, dims, false);
-        x.zero(s);
-        run_solver(&psf, p->method, rhs.get(), x.get(), &p->solver, stats);
+        mbir2d_core(c, dsino.get(), ns, ntheta, nradial, theta, recon_dims, p, x.get(), stats, nullptr,
+                    nullptr);
         LC_CUDA(cudaMemcpyAsync(recon, x.get(), nv * sizeof(float), cudaMemcpyDeviceToHost, s));
         LC_CUDA(cudaStreamSynchronize(s));
     });
 }
 
-static void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nrows, int ncols,
-                        const double *theta, const double *gamma, const double *beta,
-                        const float *shifts, const int *recon_dims, const lc_recon_params *p,
-                        float *dout, lc_solver_stats *stats) {
+}  // extern "C"
+
+namespace lc {
+
+void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nrows, int ncols,
+                 const double *theta, const double *gamma, const double *beta, const float *shifts,
+                 const int *recon_dims, const lc_recon_params *p, float *dout,
+                 lc_solver_stats *stats, const PsfProvider *psfp, bool *psf_hit) {
     LC_REQUIRE(theta && gamma && beta && recon_dims && p, "NULL argument");
     LC_REQUIRE(ntheta > 0 && nrows > 0 && ncols > 0, "sizes must be positive");
     LC_REQUIRE(recon_dims[0] > 0 && recon_dims[1] > 0 && recon_dims[2] > 0,
@@ -653,7 +665,7 @@ static void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nr
     lc_psf_s psf;
     psf.owner = c;
     psf.geom = g;
-    psf.T = std::make_unique<Toeplitz>(ctx, g->g, N, true);
+    psf.T = make_psf(ctx, g->g, N, true, psfp, psf_hit);
     x.zero(s);
     run_solver(&psf, p->method, yT.get(), x.get(), &p->solver, stats);
     const long nv = (long)recon_dims[0] * recon_dims[1] * recon_dims[2];
@@ -662,6 +674,10 @@ static void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nr
         (N[0] - recon_dims[0]) / 2, (N[1] - recon_dims[1]) / 2, (N[2] - recon_dims[2]) / 2);
     LC_CHECK_LAUNCH();
 }
+
+}  // namespace lc
+
+extern "C" {
 
 int lc_mbir3d(lc_context c, const float *projs, int ntheta, int nrows, int ncols,
               const double *theta, const double *gamma, const double *beta, const float *shifts,
@@ -679,7 +695,7 @@ int lc_mbir3d(lc_context c, const float *projs, int ntheta, int nrows, int ncols
         LC_REQUIRE(nv > 0, "recon_dims must be positive");
         DevBuf<float> out(nv, s);
         mbir3d_core(c, draw.get(), ntheta, nrows, ncols, theta, gamma, beta, shifts, recon_dims, p,
-                    out.get(), stats);
+                    out.get(), stats, nullptr, nullptr);
         LC_CUDA(cudaMemcpyAsync(recon, out.get(), nv * sizeof(float), cudaMemcpyDeviceToHost, s));
         LC_CUDA(cudaStreamSynchronize(s));
     });
@@ -692,7 +708,7 @@ int lc_mbir3d_device(lc_context c, const float *projs, int ntheta, int nrows, in
     return guarded(c, [&] {
         LC_REQUIRE(projs && recon, "NULL argument");
         mbir3d_core(c, projs, ntheta, nrows, ncols, theta, gamma, beta, shifts, recon_dims, p,
-                    recon, stats);
+                    recon, stats, nullptr, nullptr);
     });
 }
 

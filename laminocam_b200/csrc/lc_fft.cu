@@ -95,64 +95,85 @@ __global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
     }
 
     // ---- load ----
+    // Each thread issues kBatch independent global loads before it writes any
+    // of them to shared memory, so that several loads per thread are in flight.
+    constexpr int kBatch = 4;
+    const int nh = L / 2 + 1;
     if (rows) {
-        for (int cl = 0; cl < nlines; ++cl) {
-            const TI *src = in + (o_base + cl) * a.in_ostride;
-            if (a.in_map == IN_HERM) {
-                const int nh = L / 2 + 1;
-                for (int f = tid; f < L; f += nt) {
-                    const int j = f < nh ? f : L - f;
-                    V v = ld_elem<T, TI>(src + j);
-                    if (f >= nh) v.y = -v.y;
-                    buf[(f << logC) + cl] = v;
-                }
-            } else {
-                const T lf = linefac ? linefac[0] : T(1);
-                for (int j = tid; j < a.n_in; j += nt) {
-                    V v = ld_elem<T, TI>(src + j);
-                    if (pre) v = cscale(v, pre[j] * lf);
-                    else if (linefac) v = cscale(v, lf);
-                    int f = j;
+        const T lf = linefac ? linefac[0] : T(1);
+        const int per = a.in_map == IN_HERM ? L : a.n_in;
+        const int total = per * nlines;
+        const unsigned long long per_magic = fast_div_magic((unsigned)max(per, 1));
+        for (int base = tid; base < total; base += kBatch * nt) {
+            V v[kBatch];
+            int dst[kBatch];
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u) {
+                const int idx = base + u * nt;
+                dst[u] = -1;
+                if (idx >= total) continue;
+                const int cl = (int)fast_div((unsigned)idx, per_magic);
+                const int e = idx - cl * per;
+                const TI *src = in + (o_base + cl) * a.in_ostride;
+                if (a.in_map == IN_HERM) {
+                    const int j = e < nh ? e : L - e;
+                    v[u] = ld_elem<T, TI>(src + j);
+                    if (e >= nh) v[u].y = -v[u].y;
+                    dst[u] = (e << logC) + cl;
+                } else {
+                    v[u] = ld_elem<T, TI>(src + e);
+                    if (pre) v[u] = cscale(v[u], pre[e] * lf);
+                    else if (linefac) v[u] = cscale(v[u], lf);
+                    int f = e;
                     if (a.in_map == IN_MODES) {
-                        f = j - a.n_in / 2;
+                        f = e - a.n_in / 2;
                         if (f < 0) f += L;
                     }
-                    buf[(f << logC) + cl] = v;
+                    dst[u] = (f << logC) + cl;
                 }
             }
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u)
+                if (dst[u] >= 0) buf[dst[u]] = v[u];
         }
     } else {
         const TI *src = in + o_base * a.in_ostride + c_base;
-        if (a.in_map == IN_HERM) {
-            const int nh = L / 2 + 1;
-            for (int idx = tid; idx < (L << logC); idx += nt) {
+        const int total = (a.in_map == IN_HERM ? L : a.n_in) << logC;
+        for (int base = tid; base < total; base += kBatch * nt) {
+            V v[kBatch];
+            int dst[kBatch];
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u) {
+                const int idx = base + u * nt;
+                dst[u] = -1;
+                if (idx >= total) continue;
                 const int cl = idx & (C - 1);
-                const int f = idx >> logC;
                 if (cl >= nlines) continue;
-                const int j = f < nh ? f : L - f;
-                V v = ld_elem<T, TI>(src + (long)j * a.n_inner + cl);
-                if (f >= nh) v.y = -v.y;
-                buf[idx] = v;
-            }
-        } else {
-            for (int idx = tid; idx < (a.n_in << logC); idx += nt) {
-                const int cl = idx & (C - 1);
-                const int j = idx >> logC;
-                if (cl >= nlines) continue;
-                V v = ld_elem<T, TI>(src + (long)j * a.n_inner + cl);
-                if (pre || linefac) {
-                    T s = T(1);
-                    if (pre) s *= pre[j];
-                    if (linefac) s *= linefac[c_base + cl];
-                    v = cscale(v, s);
+                const int e = idx >> logC;
+                if (a.in_map == IN_HERM) {
+                    const int j = e < nh ? e : L - e;
+                    v[u] = ld_elem<T, TI>(src + (long)j * a.n_inner + cl);
+                    if (e >= nh) v[u].y = -v[u].y;
+                    dst[u] = idx;
+                } else {
+                    v[u] = ld_elem<T, TI>(src + (long)e * a.n_inner + cl);
+                    if (pre || linefac) {
+                        T s = T(1);
+                        if (pre) s *= pre[e];
+                        if (linefac) s *= linefac[c_base + cl];
+                        v[u] = cscale(v[u], s);
+                    }
+                    int f = e;
+                    if (a.in_map == IN_MODES) {
+                        f = e - a.n_in / 2;
+                        if (f < 0) f += L;
+                    }
+                    dst[u] = (f << logC) + cl;
                 }
-                int f = j;
-                if (a.in_map == IN_MODES) {
-                    f = j - a.n_in / 2;
-                    if (f < 0) f += L;
-                }
-                buf[(f << logC) + cl] = v;
             }
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u)
+                if (dst[u] >= 0) buf[dst[u]] = v[u];
         }
     }
     __syncthreads();

@@ -1,0 +1,58 @@
+// Definitions shared by the C ABI (lc_capi.cu) and the job server
+// (lc_server.cu): the handle structs and the reconstruction drivers on
+// device buffers.
+#pragma once
+
+#include <functional>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+
+#include "../../include/laminocam.h"
+#include "lc_nufft.hpp"
+#include "lc_solver.hpp"
+#include "lc_toeplitz.hpp"
+
+struct lc_context_s {
+    std::unique_ptr<lc::Context> ctx;
+    std::string err;
+};
+
+struct lc_geometry_s {
+    lc_context owner = nullptr;
+    lc::PolarGeometry g;
+    std::map<std::tuple<int, int, int, int>, std::unique_ptr<lc::NufftPlan>> plans;
+    lc::DevBuf<float2> work;
+};
+
+struct lc_psf_s {
+    lc_context owner = nullptr;
+    lc_geometry geom = nullptr;
+    std::shared_ptr<lc::Toeplitz> T;
+    std::unique_ptr<lc::Solver> solver;
+};
+
+namespace lc {
+
+// Supplies the Toeplitz operator of a reconstruction: either a new one or one
+// that shares a cached spectrum.  `hit` is set when the spectrum was reused.
+using PsfProvider = std::function<std::shared_ptr<Toeplitz>(Context &ctx, const PolarGeometry &g,
+                                                            const long dims[3], bool three_d,
+                                                            bool *hit)>;
+
+// gpu::MBIR2D on a device sinogram {ns, ntheta, nradial}; drecon {ns, n, n}
+void mbir2d_core(lc_context c, const float *dsino, int ns, int ntheta, int nradial,
+                 const double *theta, const int *recon_dims, const lc_recon_params *p,
+                 float *drecon, lc_solver_stats *stats, const PsfProvider *psf, bool *psf_hit);
+
+// gpu::MBIR on device projections {ntheta, nrows, ncols}; drecon = recon_dims
+void mbir3d_core(lc_context c, const float *dprojs, int ntheta, int nrows, int ncols,
+                 const double *theta, const double *gamma, const double *beta, const float *shifts,
+                 const int *recon_dims, const lc_recon_params *p, float *drecon,
+                 lc_solver_stats *stats, const PsfProvider *psf, bool *psf_hit);
+
+// padded size of the reference: int(n * factor) in float, forced odd
+long odd_pad(long n, float factor);
+
+}  // namespace lc

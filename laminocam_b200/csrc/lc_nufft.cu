@@ -345,6 +345,159 @@ __global__ void __launch_bounds__(256) spread_kernel(PolarPts pts, GridCfg g,
     }
 }
 
+// ---- warp-cooperative spreading -------------------------------------------
+// One warp spreads one point at a time: lane (r, c) = (lane / 8, lane % 8)
+// owns kernel rows r and r + 4 and column c of the W x W footprint (W <= 8),
+// and the warp walks z.  The tile is planar (real and imaginary parts in
+// separate arrays) with a row stride txs = 8 (mod 32), so the 28 cells one
+// atomic instruction touches (4 rows x 7 columns for W = 7) fall in distinct
+// shared-memory banks.  Each lane first computes the placement and value of
+// one of 32 points; the warp then broadcasts them one by one with shuffles.
+template <int DIM, int W>
+__global__ void __launch_bounds__(256) spread_warp_kernel(PolarPts pts, GridCfg g, int txs,
+                                                          const float2 *__restrict__ c, long cstride,
+                                                          int nvol, const int *__restrict__ perm,
+                                                          const int4 *__restrict__ subs,
+                                                          float2 *__restrict__ grid, long gstride,
+                                                          int mode, const float2 *__restrict__ shifts) {
+    static_assert(W <= 8, "warp spreading covers at most 8 x 8 footprint columns");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int4 sp = subs[blockIdx.x];
+    int bcoord[3] = {0, 0, 0};
+    {
+        int rr = sp.x;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            bcoord[d] = rr % g.nb[d];
+            rr /= g.nb[d];
+        }
+    }
+    int S[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) S[d] = bcoord[d] * g.bs[d] - g.hw[d];
+    const int ty = g.td[1], tz = DIM == 3 ? g.td[2] : 1;
+    const int plane = ty * txs;
+    const int tsize = tz * plane;  // padded cells per slice
+    float *tre = reinterpret_cast<float *>(smem_raw);
+    float *tim = tre + (long)nvol * tsize;
+    for (int idx = threadIdx.x; idx < 2 * nvol * tsize; idx += blockDim.x) tre[idx] = 0.f;
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int r = lane >> 3, cx = lane & 7;
+    const float inv_hw = 2.0f / (float)W;
+    for (int pbase = warp * 32; pbase < sp.z; pbase += nwarps * 32) {
+        // this lane's point
+        int ok = 0, lo0 = 0, lo1 = 0, lo2 = 0, jj = 0;
+        float of0 = 0.f, of1 = 0.f, of2 = 0.f;
+        float2 v = make_float2(0.f, 0.f), mult = make_float2(1.f, 0.f);
+        if (pbase + lane < sp.z) {
+            jj = perm[sp.y + pbase + lane];
+            PointInfo pi;
+            point_at(pts, jj, pi);
+            ok = (mode == PT_PLAIN) || in_band(pi);
+            if (ok && mode == PT_SHIFT) {
+                float2 sh = shifts[pi.angle];
+                double ph = pi.qX * (double)sh.x + pi.qY * (double)sh.y;
+                double sn, cs;
+                sincos(ph, &sn, &cs);
+                mult = make_float2((float)cs, (float)-sn);
+            }
+            int cell, l0;
+            place(pi.c[0], g.nf[0], W, cell, l0, of0);
+            lo0 = l0 - S[0];
+            place(pi.c[1], g.nf[1], W, cell, l0, of1);
+            lo1 = l0 - S[1];
+            if (DIM == 3) {
+                place(pi.c[2], g.nf[2], W, cell, l0, of2);
+                lo2 = l0 - S[2];
+            }
+            if (ok && nvol == 1) v = cmul(c[jj], mult);
+        }
+        const int npts = min(32, sp.z - pbase);
+        for (int q = 0; q < npts; ++q) {
+            if (!__shfl_sync(0xffffffffu, ok, q)) continue;
+            const int q0 = __shfl_sync(0xffffffffu, lo0, q);
+            const int q1 = __shfl_sync(0xffffffffu, lo1, q);
+            const float f0 = __shfl_sync(0xffffffffu, of0, q);
+            const float f1 = __shfl_sync(0xffffffffu, of1, q);
+            const float wx = cx < W ? es_evalf(((float)cx - f0) * inv_hw, g.beta) : 0.f;
+            const float wy0 = es_evalf(((float)r - f1) * inv_hw, g.beta);
+            const float wy1 = (r + 4 < W) ? es_evalf(((float)(r + 4) - f1) * inv_hw, g.beta) : 0.f;
+            int q2 = 0;
+            float wzl = 0.f;
+            if (DIM == 3) {
+                q2 = __shfl_sync(0xffffffffu, lo2, q);
+                const float f2 = __shfl_sync(0xffffffffu, of2, q);
+                wzl = lane < W ? es_evalf(((float)lane - f2) * inv_hw, g.beta) : 0.f;
+            }
+            for (int s = 0; s < nvol; ++s) {
+                float2 val;
+                if (nvol == 1) {
+                    val.x = __shfl_sync(0xffffffffu, v.x, q);
+                    val.y = __shfl_sync(0xffffffffu, v.y, q);
+                } else {
+                    const int jq = __shfl_sync(0xffffffffu, jj, q);
+                    float2 mq;
+                    mq.x = __shfl_sync(0xffffffffu, mult.x, q);
+                    mq.y = __shfl_sync(0xffffffffu, mult.y, q);
+                    val = cmul(c[(long)s * cstride + jq], mq);
+                }
+                float *re = tre + (long)s * tsize;
+                float *im = tim + (long)s * tsize;
+                const int col = q0 + cx;
+                const int row0 = (q1 + r) * txs + col;
+                const int row1 = (q1 + r + 4) * txs + col;
+                if (DIM == 2) {
+                    if (cx < W) {
+                        const float w0 = wx * wy0;
+                        atomicAdd(re + row0, val.x * w0);
+                        atomicAdd(im + row0, val.y * w0);
+                        if (r + 4 < W) {
+                            const float w1 = wx * wy1;
+                            atomicAdd(re + row1, val.x * w1);
+                            atomicAdd(im + row1, val.y * w1);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int dz = 0; dz < W; ++dz) {
+                        const float wz = __shfl_sync(0xffffffffu, wzl, dz);
+                        const int zoff = (q2 + dz) * plane;
+                        if (cx < W) {
+                            const float w0 = wx * wy0 * wz;
+                            atomicAdd(re + zoff + row0, val.x * w0);
+                            atomicAdd(im + zoff + row0, val.y * w0);
+                            if (r + 4 < W) {
+                                const float w1 = wx * wy1 * wz;
+                                atomicAdd(re + zoff + row1, val.x * w1);
+                                atomicAdd(im + zoff + row1, val.y * w1);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // flush the tile (halos overlap neighbouring bins, so accumulate atomically)
+    const int tx = g.td[0];
+    for (int idx = threadIdx.x; idx < nvol * tsize; idx += blockDim.x) {
+        const int s = idx / tsize;
+        const int rr = idx - s * tsize;
+        const int ix = rr % txs;
+        if (ix >= tx) continue;
+        const float a = tre[idx], b = tim[idx];
+        if (a == 0.f && b == 0.f) continue;
+        const int iy = (rr / txs) % ty;
+        const int iz = rr / plane;
+        long gi = (long)wrap(S[0] + ix, g.nf[0]) + (long)wrap(S[1] + iy, g.nf[1]) * g.nf[0];
+        if (DIM == 3) gi += (long)wrap(S[2] + iz, g.nf[2]) * g.nf[0] * g.nf[1];
+        float2 *dst = grid + (long)s * gstride + gi;
+        atomicAdd(dst, make_float2(a, b));
+    }
+}
+
 // ---- interpolation --------------------------------------------------------
 template <int DIM, int W>
 __global__ void __launch_bounds__(256) interp_kernel(PolarPts pts, GridCfg g,
@@ -461,6 +614,17 @@ void launch_spread_w(dim3 grid, int threads, size_t smem, cudaStream_t st, const
 }
 
 template <int DIM, int W>
+void launch_spread_warp_w(dim3 grid, size_t smem, cudaStream_t st, const PolarPts &pts,
+                          const GridCfg &g, int txs, const float2 *c, long cstride, int nvol,
+                          const int *perm, const int4 *subs, float2 *out, long gstride, int mode,
+                          const float2 *shifts) {
+    auto kern = spread_warp_kernel<DIM, W>;
+    LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, 256, smem, st>>>(pts, g, txs, c, cstride, nvol, perm, subs, out, gstride, mode, shifts);
+    LC_CHECK_LAUNCH();
+}
+
+template <int DIM, int W>
 void launch_interp_w(dim3 grid, int threads, size_t smem, cudaStream_t st, const PolarPts &pts,
                      const GridCfg &g, const float2 *gr, long gstride, int nvol, const int *perm,
                      const int4 *subs, float2 *c, long cstride, int mode) {
@@ -515,7 +679,8 @@ NufftPlan::NufftPlan(Context &ctx, const PolarGeometry &g, const int modes[3], d
         nf_[d] = d < dim_ ? (int)next_smooth23(std::max(2 * modes_[d], 2 * w_)) : 1;
     }
     const int bs2[3] = {32, 32, 1};
-    const int bs3[3] = {16, 16, 8};
+    // bin x-extents of 32 give tile rows of 32 + 2*ceil(w/2) = 40 cells (= 8 mod 32)
+    const int bs3[3] = {32, 8, 8};
     for (int d = 0; d < 3; ++d) {
         bs_[d] = std::min(dim_ == 2 ? bs2[d] : bs3[d], nf_[d]);
         nb_[d] = (nf_[d] + bs_[d] - 1) / bs_[d];
@@ -581,6 +746,30 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
     const long gvol = (long)nf_[0] * nf_[1] * nf_[2];
     // values read once, fine grid written once (plus the permutation)
     ProfScope ps(ctx, PS_SPREAD, (double)nvol * (8.0 * pts_.M + 8.0 * gvol) + 4.0 * pts_.M);
+    if (w_ <= 8) {
+        // warp-cooperative path: planar tile, row stride = 8 (mod 32)
+        const int tx = g.td[0];
+        const int txs = tx + (((8 - tx) % 32) + 32) % 32;
+        const size_t tile_bytes = (size_t)txs * g.td[1] * g.td[2] * 2 * sizeof(float);
+        int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
+        for (int v0 = 0; v0 < nvol; v0 += vchunk) {
+            int nv = std::min(vchunk, nvol - v0);
+            size_t smem = tile_bytes * nv;
+            const float2 *cv = c + (long)v0 * pts_.M;
+            float2 *gv = grid + (long)v0 * gvol;
+            dim3 gd(nsub_);
+            if (dim_ == 2) {
+                LC_W_SWITCH(w_, (launch_spread_warp_w<2, (WW <= 8 ? WW : 8)>(
+                                    gd, smem, ctx.stream(), pts_, g, txs, cv, pts_.M, nv, perm_.get(),
+                                    subs_.get(), gv, gvol, mode, shifts_)));
+            } else {
+                LC_W_SWITCH(w_, (launch_spread_warp_w<3, (WW <= 8 ? WW : 8)>(
+                                    gd, smem, ctx.stream(), pts_, g, txs, cv, pts_.M, nv, perm_.get(),
+                                    subs_.get(), gv, gvol, mode, shifts_)));
+            }
+        }
+        return;
+    }
     const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(float2);
     int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
     for (int v0 = 0; v0 < nvol; v0 += vchunk) {

@@ -90,14 +90,17 @@ __global__ void __launch_bounds__(128) psf_rows_kernel(const PsfAngle *__restric
             }
 #pragma unroll
             for (int s = 0; s < S; ++s) {
-                double dX, dY = 1.0;
-                if (fabs(pB.y) > 1e-6) dX = pA.y / pB.y;
-                else dX = dirichlet(uX0 + (double)s * A.a[0], nx);
-                if (DIM == 3) {
-                    if (fabs(pD.y) > 1e-6) dY = pC.y / pD.y;
-                    else dY = dirichlet(uY0 + (double)s * A.b[0], ny);
+                const bool okX = fabs(pB.y) > 1e-6;
+                const bool okY = DIM != 3 || fabs(pD.y) > 1e-6;
+                if (okX && okY) {
+                    // one division: D_X D_Y = (sin(pi uX) sin(pi uY)) / (sin(pi uX/nx) sin(pi uY/ny))
+                    acc[s] += DIM == 3 ? (pA.y * pC.y) / (pB.y * pD.y) : pA.y / pB.y;
+                } else {
+                    double dX = okX ? pA.y / pB.y : dirichlet(uX0 + (double)s * A.a[0], nx);
+                    double dY = 1.0;
+                    if (DIM == 3) dY = okY ? pC.y / pD.y : dirichlet(uY0 + (double)s * A.b[0], ny);
+                    acc[s] += dX * dY;
                 }
-                acc[s] += dX * dY;
                 pA = crot(pA, A.stepA);
                 pB = crot(pB, A.stepB);
                 if (DIM == 3) {
@@ -294,8 +297,8 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         launch_axis_fft(ctx, z);
     }
     long nR = spectrum_elems();
-    R_.alloc(nR, st);
-    d2f_kernel<<<grid_for(nR, 256, ctx.num_sms()), 256, 0, st>>>(Rd.get(), R_.get(), nR);
+    R_ = std::make_shared<DevBuf<float>>(nR, st);
+    d2f_kernel<<<grid_for(nR, 256, ctx.num_sms()), 256, 0, st>>>(Rd.get(), R_->get(), nR);
     LC_CHECK_LAUNCH();
     LC_CUDA(cudaStreamSynchronize(st));
     // work buffers
@@ -305,6 +308,18 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
     } else {
         t1_.alloc(n_[0] * n_[1] * Ph_[2], st);
     }
+}
+
+Toeplitz::Toeplitz(Context &ctx, const Toeplitz &src)
+    : three_d_(src.three_d_), g_(nullptr), R_(src.R_), scale_(src.scale_) {
+    for (int d = 0; d < 3; ++d) {
+        n_[d] = src.n_[d];
+        P_[d] = src.P_[d];
+        Ph_[d] = src.Ph_[d];
+    }
+    cudaStream_t st = ctx.stream();
+    t1_.alloc(n_[0] * n_[1] * Ph_[2], st);
+    if (three_d_) t2_.alloc(n_[0] * (long)P_[1] * Ph_[2], st);
 }
 
 void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
@@ -376,6 +391,7 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
 }
 
 void Toeplitz::kernel_fp64(Context &ctx, double *host_out) {
+    LC_REQUIRE(g_ != nullptr, "PSF kernel export needs the PSF's own geometry");
     DevBuf<double> K;
     build_kernel(ctx, K);
     long total = three_d_ ? (long)P_[0] * P_[1] * P_[2] : (long)P_[2] * P_[2];
@@ -432,7 +448,7 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
         a.out_map = OUT_WINDOW;
         a.out_off = 0;
         a.sign = -1;
-        a.mid = R_.get();
+        a.mid = R_->get();
         a.mid_ra = P3h;
         a.sign2 = +1;
         launch_axis_fft(ctx, a);
@@ -471,7 +487,7 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
             a.out_map = OUT_WINDOW;
             a.out_off = 0;
             a.sign = -1;
-            a.mid = R_.get();
+            a.mid = R_->get();
             a.mid_ra = (long)P2 * P3h;
             a.sign2 = +1;
             launch_axis_fft(ctx, a);

@@ -25,6 +25,9 @@ class Toeplitz {
     // dims = {n1, n2, n3}: volume (3D) or stack of n1 independent n2 x n3
     // slices (2D, n2 == n3 required by the reference API).
     Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], bool three_d);
+    // shares src's spectrum (read-only) and owns fresh work buffers on ctx's
+    // stream: concurrent jobs on one geometry use one spectrum
+    Toeplitz(Context &ctx, const Toeplitz &src);
     void apply(Context &ctx, const float *x, float *y);
     // y = A^T A x + mu * (-laplacian(x))
     void apply_reg(Context &ctx, const float *x, float *y, float mu);
@@ -34,7 +37,10 @@ class Toeplitz {
     bool three_d() const { return three_d_; }
     long nvox() const { return n_[0] * n_[1] * n_[2]; }
     long spectrum_elems() const { return (long)P_[0] * P_[1] * Ph_[2]; }
-    const float *spectrum() const { return R_.get(); }
+    const float *spectrum() const { return R_->get(); }
+    size_t device_bytes() const {
+        return R_->size() * sizeof(float) + (t1_.size() + t2_.size()) * sizeof(float2);
+    }
     // FP64 PSF K on the P-grid in mode order (k = j - P/2), for tests
     void kernel_fp64(Context &ctx, double *host_out);
     // bytes the apply must move at minimum (algorithmic traffic)
@@ -47,7 +53,7 @@ class Toeplitz {
     int P_[3];
     int Ph_[3];
     const PolarGeometry *g_;
-    DevBuf<float> R_;
+    std::shared_ptr<DevBuf<float>> R_;
     DevBuf<float2> t1_, t2_;
     double scale_;
 };
