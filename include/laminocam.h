@@ -115,6 +115,8 @@ typedef struct {
     float mu;         /* Bregman penalty */
     int fp32_scalars; /* 1: float dot products as the reference GPU path */
     int poll_every;   /* iterations between host checks of the stop flag */
+    int use_graph;    /* 1: replay iterations as CUDA graphs (CG: a chunk of iterations,
+                         Split-Bregman: one outer iteration); ignored while profiling */
 } lc_solver_params;
 
 typedef struct {

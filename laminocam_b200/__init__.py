@@ -356,13 +356,15 @@ class SolveInfo:
     elapsed_ms: float
 
 
-def _solver_params(max_iters, inner, tol, xtol, lam, mu, fp32_scalars=False, poll_every=8):
+def _solver_params(max_iters, inner, tol, xtol, lam, mu, fp32_scalars=False, poll_every=8,
+                   use_graph=False):
     p = SolverParams()
     _lib.load().lc_solver_params_default(C.byref(p))
     p.max_iters, p.inner_iters = int(max_iters), int(inner)
     p.tol, p.xtol, p.lambda_, p.mu = float(tol), float(xtol), float(lam), float(mu)
     p.fp32_scalars = int(bool(fp32_scalars))
     p.poll_every = int(poll_every)
+    p.use_graph = int(bool(use_graph))
     return p
 
 
@@ -371,25 +373,25 @@ def _info(st: SolverStats) -> SolveInfo:
 
 
 def cgsolver(A: _PSFBase, y, x0, max_iter: int, tol: float, xtol: float, fp32_scalars=False,
-             return_info=False):
+             return_info=False, use_graph=False):
     """opt::cgsolver (src/conjgrad.cpp:33-76) with the Toeplitz operator A."""
     A.ctx.sync_stream()
     yv = _dev(y, device=A.ctx.device)
     x = _dev(x0, device=A.ctx.device).clone()
     st = SolverStats()
-    p = _solver_params(max_iter, 1, tol, xtol, 0.1, 10.0, fp32_scalars)
+    p = _solver_params(max_iter, 1, tol, xtol, 0.1, 10.0, fp32_scalars, use_graph=use_graph)
     _check(A.ctx.lib.lc_cgsolver(A.ctx.handle, A.handle, _ptr(yv), _ptr(x), C.byref(p), C.byref(st)), A.ctx)
     return (x, _info(st)) if return_info else x
 
 
 def split_bregman(A: _PSFBase, yT, x0, lam: float, mu: float, outer_max: int, inner_max: int,
-                  tol: float, xtol: float, fp32_scalars=False, return_info=False):
+                  tol: float, xtol: float, fp32_scalars=False, return_info=False, use_graph=False):
     """opt::split_bregman (src/bregman.cpp:36-94) with the Toeplitz operator A."""
     A.ctx.sync_stream()
     yv = _dev(yT, device=A.ctx.device)
     x = _dev(x0, device=A.ctx.device).clone()
     st = SolverStats()
-    p = _solver_params(outer_max, inner_max, tol, xtol, lam, mu, fp32_scalars)
+    p = _solver_params(outer_max, inner_max, tol, xtol, lam, mu, fp32_scalars, use_graph=use_graph)
     _check(A.ctx.lib.lc_split_bregman(A.ctx.handle, A.handle, _ptr(yv), _ptr(x), C.byref(p), C.byref(st)),
            A.ctx)
     return (x, _info(st)) if return_info else x
@@ -409,13 +411,15 @@ class ReconParams:
     pad_factor: float = 1.4142
     nufft_tol: float = DEFAULT_TOL
     fp32_scalars: bool = False
+    poll_every: int = 8
+    use_graph: bool = False
 
     def to_c(self) -> ReconParamsC:
         r = ReconParamsC()
         _lib.load().lc_recon_params_default(C.byref(r))
         r.method = 1 if self.regularizer == "split_bregman" else 0
         r.solver = _solver_params(self.max_iters, self.inner_iters, self.tol, self.xtol, self.lam,
-                                  self.mu, self.fp32_scalars)
+                                  self.mu, self.fp32_scalars, self.poll_every, self.use_graph)
         r.nufft_tol = float(self.nufft_tol)
         r.pad_factor = float(self.pad_factor)
         return r

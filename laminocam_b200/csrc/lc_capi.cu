@@ -268,6 +268,7 @@ SolverParams to_sp(const lc_solver_params *p) {
     s.mu = p->mu;
     s.fp32_scalars = p->fp32_scalars;
     s.poll_every = p->poll_every;
+    s.use_graph = p->use_graph;
     return s;
 }
 
@@ -321,6 +322,7 @@ void lc_solver_params_default(lc_solver_params *p) {
     p->mu = 10.0f;
     p->fp32_scalars = 0;
     p->poll_every = 8;
+    p->use_graph = 0;
 }
 
 void lc_recon_params_default(lc_recon_params *p) {

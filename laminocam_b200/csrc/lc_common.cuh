@@ -245,20 +245,44 @@ __device__ __forceinline__ void stockham_stage(const cx<T> *__restrict__ src, cx
         const int g = (int)fast_div((unsigned)j, ns_magic);
         const int k = j - g * Ns;
         V v[R];
+        const V *s0 = src + (j << logC) + c;
+        const int sstep = nb << logC;
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = src[((j + r * nb) << logC) + c];
+        for (int r = 0; r < R; ++r) v[r] = s0[r * sstep];
         if (Ns > 1) {
+            // twiddles w^r from w = tw[k * tstride], with w^2 also taken from
+            // the table for radices above 4 (halves the recurrence depth)
+            V w1 = tw[k * tstride];
+            if (sign > 0) w1.y = -w1.y;
+            v[1] = cmul(v[1], w1);
+            if (R > 2) {
+                V w2;
+                if (R > 4) {
+                    w2 = tw[2 * k * tstride];
+                    if (sign > 0) w2.y = -w2.y;
+                } else {
+                    w2 = cmul(w1, w1);
+                }
+                v[2] = cmul(v[2], w2);
+                V wo = w1, we = w2;
 #pragma unroll
-            for (int r = 1; r < R; ++r) {
-                V w = tw[r * k * tstride];
-                if (sign > 0) w.y = -w.y;
-                v[r] = cmul(v[r], w);
+                for (int r = 3; r < R; ++r) {
+                    if (r & 1) {
+                        wo = cmul(wo, w2);
+                        v[r] = cmul(v[r], wo);
+                    } else {
+                        we = cmul(we, w2);
+                        v[r] = cmul(v[r], we);
+                    }
+                }
             }
         }
         dft_small<V, R>(v, sign);
         const int base = g * Ns * R + k;
+        V *d0 = dst + (base << logC) + c;
+        const int dstep = Ns << logC;
 #pragma unroll
-        for (int r = 0; r < R; ++r) dst[((base + r * Ns) << logC) + c] = v[r];
+        for (int r = 0; r < R; ++r) d0[r * dstep] = v[r];
     }
 }
 

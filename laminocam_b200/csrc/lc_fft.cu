@@ -3,7 +3,11 @@
 // consecutive addresses (along i for contiguous lines, along c otherwise).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "lc_fft.hpp"
@@ -260,6 +264,51 @@ void dispatch(Context &ctx, const AxisFFT &a, const KArgs &ka, const FFTPlan &pl
     else launch_t<T, Cx, Cx>(ctx, ka, pl, threads, smem, blocks);
 }
 
+KArgs make_kargs(const AxisFFT &a, int logC, long &blocks) {
+    const int C = 1 << logC;
+    KArgs ka{};
+    ka.in = a.in;
+    ka.out = a.out;
+    ka.n_outer = a.n_outer;
+    ka.n_inner = a.n_inner;
+    ka.in_ostride = a.in_ostride;
+    ka.out_ostride = a.out_ostride;
+    ka.n_in = a.n_in;
+    ka.n_out = a.n_out;
+    ka.L = a.L;
+    ka.in_map = a.in_map;
+    ka.out_map = a.out_map;
+    ka.out_off = a.out_off;
+    ka.sign = a.sign;
+    ka.sign2 = a.sign2;
+    ka.pre = a.pre;
+    ka.linefac = a.linefac;
+    ka.post = a.post;
+    ka.scale = a.scale;
+    ka.mid = a.mid;
+    ka.mid_ra = a.mid_ra;
+    ka.logC = logC;
+    if (a.n_inner == 1) {
+        blocks = (a.n_outer + C - 1) / C;
+        ka.blocks_per_outer = 1;
+    } else {
+        ka.blocks_per_outer = (a.n_inner + C - 1) / C;
+        blocks = a.n_outer * ka.blocks_per_outer;
+    }
+    LC_REQUIRE(blocks < (1L << 31), "axis FFT: grid too large");
+    return ka;
+}
+
+// one launch of the transform with C = 1 << logC lines per CTA
+void run_axis(Context &ctx, const AxisFFT &a, const FFTPlan &pl, int logC, int threads) {
+    const size_t esz = a.fp64 ? sizeof(double2) : sizeof(float2);
+    long blocks = 0;
+    const KArgs ka = make_kargs(a, logC, blocks);
+    const size_t smem = 2 * ((size_t)a.L << logC) * esz;
+    if (a.fp64) dispatch<double>(ctx, a, ka, pl, threads, smem, blocks);
+    else dispatch<float>(ctx, a, ka, pl, threads, smem, blocks);
+}
+
 // log2 of the lines per CTA (a power of two) and the CTA size: rows are
 // grouped so that a CTA moves >= 2048 elements, column groups take 16 adjacent
 // lines (128 contiguous bytes of float2) when the inner extent allows; both
@@ -283,6 +332,108 @@ int choose_lines(const AxisFFT &a, size_t esz, size_t max_smem, int &threads) {
     return logC;
 }
 
+// ---- launch autotuner -------------------------------------------------------
+// The lines per CTA and the CTA size of an FP32 transform are chosen per
+// transform shape by timing the candidates once (CUDA events on the launching
+// stream) and kept per device for the life of the process.  Column candidates
+// keep groups of >= 4 lines (whole 32-byte sectors of float2).  A trial of a
+// transform whose output overwrites its input writes to a scratch buffer.
+// Tuning is skipped while the stream is being captured into a graph (the
+// heuristic of choose_lines is used), and LC_FFT_AUTOTUNE=0 turns it off.
+struct TuneKey {
+    int dev, L, n_in, n_out, in_map, out_map, in_t, out_t, mid, pre, post, linefac;
+    long n_outer, n_inner, in_ostride, out_ostride;
+    auto tie() const {
+        return std::tie(dev, L, n_in, n_out, in_map, out_map, in_t, out_t, mid, pre, post, linefac,
+                        n_outer, n_inner, in_ostride, out_ostride);
+    }
+    bool operator<(const TuneKey &o) const { return tie() < o.tie(); }
+};
+
+struct TuneVal {
+    int logC, threads;
+    float ms;
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+
+bool autotune_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("LC_FFT_AUTOTUNE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+TuneKey tune_key(int dev, const AxisFFT &a) {
+    return TuneKey{dev, a.L, a.n_in, a.n_out, (int)a.in_map, (int)a.out_map, (int)a.in_t,
+                   (int)a.out_t, a.mid != nullptr, a.pre != nullptr, a.post != nullptr,
+                   a.linefac != nullptr, a.n_outer, a.n_inner, a.in_ostride, a.out_ostride};
+}
+
+// elements spanned by the output lines
+long out_extent(const AxisFFT &a) {
+    if (a.n_inner == 1) return (a.n_outer - 1) * a.out_ostride + a.n_out;
+    return (a.n_outer - 1) * a.out_ostride + (long)(a.n_out - 1) * a.n_inner + a.n_inner;
+}
+
+TuneVal autotune(Context &ctx, const AxisFFT &a0, const FFTPlan &pl) {
+    cudaStream_t st = ctx.stream();
+    const size_t esz = sizeof(float2);
+    const size_t cap = std::min<size_t>(ctx.max_smem(), 200 * 1024);
+    int base_threads = 0;
+    const int base_logC = choose_lines(a0, esz, ctx.max_smem(), base_threads);
+    std::vector<std::pair<int, int>> cands{{base_logC, base_threads}};
+    const bool rows = a0.n_inner == 1;
+    for (int logC = rows ? 0 : 2; logC <= (rows ? 6 : 5); ++logC) {
+        if (rows && (((long)a0.L << logC) > 8192 || (1L << logC) > std::max<long>(1, a0.n_outer)))
+            break;
+        if (!rows && (1L << logC) > 2 * a0.n_inner) break;
+        if (2 * ((size_t)a0.L << logC) * esz > cap) break;
+        for (int th : {128, 256, 512}) {
+            if (((long)a0.L << logC) < th) continue;
+            if (logC == base_logC && th == base_threads) continue;
+            cands.emplace_back(logC, th);
+        }
+    }
+    AxisFFT a = a0;
+    DevBuf<char> scratch;
+    if (a0.out == a0.in) {
+        const size_t oesz = (a0.out_t == E_F32) ? sizeof(float) : sizeof(float2);
+        scratch.alloc(out_extent(a0) * oesz, st);
+        a.out = scratch.get();
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TuneVal best{base_logC, base_threads, 1e30f};
+    try {
+        LC_CUDA(cudaEventCreate(&e0));
+        LC_CUDA(cudaEventCreate(&e1));
+        for (auto [logC, th] : cands) {
+            run_axis(ctx, a, pl, logC, th);  // warm
+            float tbest = 1e30f;
+            for (int rep = 0; rep < 2; ++rep) {
+                LC_CUDA(cudaEventRecord(e0, st));
+                run_axis(ctx, a, pl, logC, th);
+                LC_CUDA(cudaEventRecord(e1, st));
+                LC_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                LC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                tbest = std::min(tbest, ms);
+            }
+            if (tbest < best.ms) best = TuneVal{logC, th, tbest};
+        }
+        LC_CUDA(cudaStreamSynchronize(st));  // the scratch buffer is released on return
+    } catch (...) {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
 }  // namespace
 
 void launch_axis_fft(Context &ctx, const AxisFFT &a) {
@@ -297,43 +448,30 @@ void launch_axis_fft(Context &ctx, const AxisFFT &a) {
     const FFTPlan &pl = ctx.plans().get(a.L, a.fp64, ctx.stream());
     const size_t esz = a.fp64 ? sizeof(double2) : sizeof(float2);
     int threads = 0;
-    const int logC = choose_lines(a, esz, ctx.max_smem(), threads);
-    const int C = 1 << logC;
-
-    KArgs ka{};
-    ka.in = a.in;
-    ka.out = a.out;
-    ka.n_outer = a.n_outer;
-    ka.n_inner = a.n_inner;
-    ka.in_ostride = a.in_ostride;
-    ka.out_ostride = a.out_ostride;
-    ka.n_in = a.n_in;
-    ka.n_out = a.n_out;
-    ka.L = a.L;
-    ka.in_map = a.in_map;
-    ka.out_map = a.out_map;
-    ka.out_off = a.out_off;
-    ka.sign = a.sign;
-    ka.sign2 = a.sign2;
-    ka.pre = a.pre;
-    ka.linefac = a.linefac;
-    ka.post = a.post;
-    ka.scale = a.scale;
-    ka.mid = a.mid;
-    ka.mid_ra = a.mid_ra;
-    ka.logC = logC;
-    long blocks;
-    if (a.n_inner == 1) {
-        blocks = (a.n_outer + C - 1) / C;
-        ka.blocks_per_outer = 1;
-    } else {
-        ka.blocks_per_outer = (a.n_inner + C - 1) / C;
-        blocks = a.n_outer * ka.blocks_per_outer;
+    int logC = choose_lines(a, esz, ctx.max_smem(), threads);
+    if (!a.fp64 && a.lines_per_cta == 0 && autotune_enabled()) {
+        const TuneKey key = tune_key(ctx.device(), a);
+        bool found = false;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto it = g_tune.find(key);
+            if (it != g_tune.end()) {
+                logC = it->second.logC;
+                threads = it->second.threads;
+                found = true;
+            }
+        }
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        LC_CUDA(cudaStreamIsCapturing(ctx.stream(), &cs));
+        if (!found && cs == cudaStreamCaptureStatusNone) {
+            const TuneVal v = autotune(ctx, a, pl);
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune.emplace(key, v);
+            logC = v.logC;
+            threads = v.threads;
+        }
     }
-    LC_REQUIRE(blocks < (1L << 31), "axis FFT: grid too large");
-    size_t smem = 2 * (size_t)a.L * C * esz;
-    if (a.fp64) dispatch<double>(ctx, a, ka, pl, threads, smem, blocks);
-    else dispatch<float>(ctx, a, ka, pl, threads, smem, blocks);
+    run_axis(ctx, a, pl, logC, threads);
 }
 
 void launch_axis_fft_f32_with_plan(cudaStream_t stream, size_t max_smem, const AxisFFT &a,

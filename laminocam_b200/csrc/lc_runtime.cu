@@ -8,8 +8,60 @@
 namespace lc {
 
 static std::atomic<long> g_launches{0};
+// launches recorded while this thread captures a graph run only on replay
+static thread_local bool t_capturing = false;
 long kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
-void note_kernel_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_kernel_launch() {
+    if (!t_capturing) g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void CapturedGraph::reset() {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    exec_ = nullptr;
+    kernels_ = 0;
+}
+
+void CapturedGraph::capture(cudaStream_t s, const std::function<void()> &body) {
+    reset();
+    LC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    t_capturing = true;
+    cudaGraph_t g = nullptr;
+    try {
+        body();
+    } catch (...) {
+        t_capturing = false;
+        cudaStreamEndCapture(s, &g);  // leaves the stream usable again
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+    }
+    t_capturing = false;
+    LC_CUDA(cudaStreamEndCapture(s, &g));
+    size_t nn = 0;
+    cudaError_t e = cudaGraphGetNodes(g, nullptr, &nn);
+    if (e == cudaSuccess && nn) {
+        std::vector<cudaGraphNode_t> nodes(nn);
+        e = cudaGraphGetNodes(g, nodes.data(), &nn);
+        for (size_t i = 0; e == cudaSuccess && i < nn; ++i) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+                ++kernels_;
+        }
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiateWithFlags(&exec_, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        exec_ = nullptr;
+        kernels_ = 0;
+        LC_CUDA(e);
+    }
+}
+
+void CapturedGraph::launch(cudaStream_t s) {
+    LC_REQUIRE(exec_ != nullptr, "graph launched before capture");
+    LC_CUDA(cudaGraphLaunch(exec_, s));
+    g_launches.fetch_add(kernels_, std::memory_order_relaxed);
+}
 
 bool is_smooth23(long n) {
     if (n < 1) return false;

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -183,6 +184,9 @@ class Context {
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }
     void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+    // the context's private stream: graphs are captured there (the caller's
+    // stream may be the legacy default stream, which cannot capture)
+    cudaStream_t capture_stream() const { return own_stream_; }
     PlanCache &plans() { return plans_; }
     int num_sms() const { return num_sms_; }
     size_t max_smem() const { return max_smem_; }
@@ -197,6 +201,27 @@ class Context {
     PlanCache plans_;
     int num_sms_ = 148;
     size_t max_smem_ = 227 * 1024;
+};
+
+// A fixed launch sequence captured once from one stream into a CUDA graph and
+// replayed.  Launches issued while capturing are not counted; each replay
+// counts the graph's kernel nodes instead.  The body must not allocate, copy
+// to the host or synchronise.
+class CapturedGraph {
+  public:
+    CapturedGraph() = default;
+    CapturedGraph(const CapturedGraph &) = delete;
+    CapturedGraph &operator=(const CapturedGraph &) = delete;
+    ~CapturedGraph() { reset(); }
+    void capture(cudaStream_t s, const std::function<void()> &body);
+    void launch(cudaStream_t s);
+    bool ready() const { return exec_ != nullptr; }
+    long kernels() const { return kernels_; }
+    void reset();
+
+  private:
+    cudaGraphExec_t exec_ = nullptr;
+    long kernels_ = 0;
 };
 
 // Makes `dev` current for the lifetime of the guard.

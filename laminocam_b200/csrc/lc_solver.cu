@@ -294,8 +294,54 @@ Solver::Solver(Context &ctx, long n) : n_(n) {
     LC_CUDA(cudaMallocHost((void **)&host_st_, sizeof(CGState)));
 }
 
+Solver::~Solver() {
+    graph_.reset();
+    if (host_st_) cudaFreeHost(host_st_);
+}
+
+void Solver::capture(Context &ctx, const std::function<void()> &body) {
+    // Capturing records the launches without running them.  It happens on the
+    // context's private stream (the caller's stream may be the legacy default
+    // stream, which cannot capture); the replays go to the caller's stream.
+    const cudaStream_t user = ctx.stream();
+    const cudaStream_t side = ctx.capture_stream();
+    ctx.set_stream(side);
+    try {
+        graph_.capture(side, body);
+    } catch (...) {
+        ctx.set_stream(user);
+        throw;
+    }
+    ctx.set_stream(user);
+}
+
+void Solver::cg_iter(Context &ctx, const Operator &A, float *x, float tol, float xtol, int fp32) {
+    cudaStream_t s = ctx.stream();
+    A(p_.get(), ap_.get());
+    ProfScope ps(ctx, PS_CG_VEC, 4.0 * n_ * 10.0);
+    if (fp32) {
+        dot_pap_kernel<float><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
+                                                         counter_.get(), st_.get());
+        LC_CHECK_LAUNCH();
+        cg_update_kernel<float><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), n_,
+                                                           part_.get(), counter_.get(), st_.get(),
+                                                           tol, xtol);
+        LC_CHECK_LAUNCH();
+    } else {
+        dot_pap_kernel<double><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
+                                                          counter_.get(), st_.get());
+        LC_CHECK_LAUNCH();
+        cg_update_kernel<double><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), n_,
+                                                            part_.get(), counter_.get(), st_.get(),
+                                                            tol, xtol);
+        LC_CHECK_LAUNCH();
+    }
+    p_update_kernel<<<nblk_, kThreads, 0, s>>>(p_.get(), r_.get(), n_, st_.get());
+    LC_CHECK_LAUNCH();
+}
+
 void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, int iters,
-                    float tol, float xtol, int fp32, int poll_every, bool in_sb) {
+                    float tol, float xtol, int fp32, int poll_every, bool in_sb, bool graph) {
     cudaStream_t s = ctx.stream();
     A(x, ap_.get());
     // r <- A x0 (moved), then r = y - r, p = r
@@ -307,29 +353,28 @@ void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, i
         cg_init_kernel<double><<<nblk_, kThreads, 0, s>>>(y, r_.get(), p_.get(), n_, part_.get(),
                                                           counter_.get(), st_.get());
     LC_CHECK_LAUNCH();
-    for (int it = 0; it < iters; ++it) {
-        A(p_.get(), ap_.get());
-        ProfScope ps(ctx, PS_CG_VEC, 4.0 * n_ * 10.0);
-        if (fp32) {
-            dot_pap_kernel<float><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
-                                                             counter_.get(), st_.get());
-            LC_CHECK_LAUNCH();
-            cg_update_kernel<float><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), n_,
-                                                               part_.get(), counter_.get(),
-                                                               st_.get(), tol, xtol);
-            LC_CHECK_LAUNCH();
+    const bool poll = !in_sb && poll_every > 0;
+    // With graphs one replay covers `chunk` iterations (the polling interval
+    // when the host polls); a remainder runs as ordinary launches.  Iterations
+    // after the stop flag are no-ops on the device either way.
+    int chunk = 0;
+    if (graph && iters > 1) {
+        chunk = poll ? std::min(poll_every, iters) : std::min(iters, 8);
+        capture(ctx, [&] {
+            for (int k = 0; k < chunk; ++k) cg_iter(ctx, A, x, tol, xtol, fp32);
+        });
+    }
+    int it = 0;
+    while (it < iters) {
+        if (chunk > 0 && iters - it >= chunk) {
+            graph_.launch(s);
+            it += chunk;
         } else {
-            dot_pap_kernel<double><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
-                                                              counter_.get(), st_.get());
-            LC_CHECK_LAUNCH();
-            cg_update_kernel<double><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), n_,
-                                                                part_.get(), counter_.get(),
-                                                                st_.get(), tol, xtol);
-            LC_CHECK_LAUNCH();
+            cg_iter(ctx, A, x, tol, xtol, fp32);
+            it += 1;
         }
-        p_update_kernel<<<nblk_, kThreads, 0, s>>>(p_.get(), r_.get(), n_, st_.get());
-        LC_CHECK_LAUNCH();
-        if (!in_sb && poll_every > 0 && (it + 1) % poll_every == 0 && it + 1 < iters) {
+        const bool boundary = chunk > 0 || it % std::max(poll_every, 1) == 0;
+        if (poll && boundary && it < iters) {
             LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
             LC_CUDA(cudaStreamSynchronize(s));
             if (host_st_->done) break;
@@ -343,7 +388,9 @@ void Solver::cg(Context &ctx, const Operator &A, const float *y, float *x, const
     reset_state_kernel<<<1, 1, 0, s>>>(st_.get());
     LC_CHECK_LAUNCH();
     int poll = (p.tol > 0 || p.xtol > 0) ? p.poll_every : 0;
-    cg_run(ctx, A, y, x, p.max_iters, p.tol, p.xtol, p.fp32_scalars, poll, false);
+    const bool graph = p.use_graph != 0 && !ctx.prof.on;
+    cg_run(ctx, A, y, x, p.max_iters, p.tol, p.xtol, p.fp32_scalars, poll, false, graph);
+    graph_.reset();
     LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
     LC_CUDA(cudaStreamSynchronize(s));
     if (stats) {
@@ -379,39 +426,58 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
     Dims dm{dims[0], dims[1], dims[2]};
     unsigned gsz = (unsigned)std::max<long>(1, std::min<long>((n_ + kThreads - 1) / kThreads,
                                                              (long)ctx.num_sms() * 16));
-    int total_cg = 0;
-    int poll = p.xtol > 0 ? std::max(1, p.poll_every) : 0;
-    for (int it = 0; it < p.max_iters; ++it) {
-        std::unique_ptr<ProfScope> ps1(new ProfScope(ctx, PS_SB_VEC, 4.0 * n_ * 8.0));
-        sb_rhs_kernel<<<gsz, kThreads, 0, s>>>(yT, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(),
-                                                b_[1].get(), b_[2].get(), rhs_.get(), dm, mu, st_.get());
-        LC_CHECK_LAUNCH();
-        ps1.reset();
-        cg_run(ctx, Ap, rhs_.get(), x, p.inner_iters, p.tol, p.xtol, p.fp32_scalars, 0, true);
-        total_cg += p.inner_iters;
+    // one outer iteration: rhs, inner CG (warm start), shrinkage, change test.
+    // Launches go to ctx.stream() as it is when the lambda runs (the capture
+    // stream while a graph is recorded).
+    auto outer = [&] {
+        const cudaStream_t os = ctx.stream();
+        {
+            ProfScope ps1(ctx, PS_SB_VEC, 4.0 * n_ * 8.0);
+            sb_rhs_kernel<<<gsz, kThreads, 0, os>>>(yT, d_[0].get(), d_[1].get(), d_[2].get(),
+                                                     b_[0].get(), b_[1].get(), b_[2].get(),
+                                                     rhs_.get(), dm, mu, st_.get());
+            LC_CHECK_LAUNCH();
+        }
+        cg_run(ctx, Ap, rhs_.get(), x, p.inner_iters, p.tol, p.xtol, p.fp32_scalars, 0, true, false);
         ProfScope ps2(ctx, PS_SB_VEC, 4.0 * n_ * 16.0);
-        sb_shrink_kernel<<<gsz, kThreads, 0, s>>>(x, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(),
-                                                   b_[1].get(), b_[2].get(), dm, p.lambda / p.mu,
-                                                   st_.get());
+        sb_shrink_kernel<<<gsz, kThreads, 0, os>>>(x, d_[0].get(), d_[1].get(), d_[2].get(),
+                                                    b_[0].get(), b_[1].get(), b_[2].get(), dm,
+                                                    p.lambda / p.mu, st_.get());
         LC_CHECK_LAUNCH();
         if (p.fp32_scalars)
-            sb_diff_kernel<float><<<nblk_, kThreads, 0, s>>>(x, xold_.get(), n_, part_.get(),
-                                                             counter_.get(), st_.get(), p.xtol);
-        else
-            sb_diff_kernel<double><<<nblk_, kThreads, 0, s>>>(x, xold_.get(), n_, part_.get(),
+            sb_diff_kernel<float><<<nblk_, kThreads, 0, os>>>(x, xold_.get(), n_, part_.get(),
                                                               counter_.get(), st_.get(), p.xtol);
+        else
+            sb_diff_kernel<double><<<nblk_, kThreads, 0, os>>>(x, xold_.get(), n_, part_.get(),
+                                                               counter_.get(), st_.get(), p.xtol);
         LC_CHECK_LAUNCH();
+    };
+    const bool graph = p.use_graph != 0 && !ctx.prof.on && p.max_iters > 1;
+    if (graph && p.max_iters > 0) {
+        // the first outer iteration runs eagerly (it also fills the plan and
+        // launch-tuner caches the recorded launches rely on); the rest replay it
+        outer();
+        capture(ctx, outer);
+    }
+    const int poll = p.xtol > 0 ? std::max(1, p.poll_every) : 0;
+    for (int it = graph ? 1 : 0; it < p.max_iters; ++it) {
+        if (graph)
+            graph_.launch(s);
+        else
+            outer();
         if (poll > 0 && (it + 1) % poll == 0 && it + 1 < p.max_iters) {
             LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
             LC_CUDA(cudaStreamSynchronize(s));
             if (host_st_->sb_done) break;
         }
     }
+    graph_.reset();
     LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
     LC_CUDA(cudaStreamSynchronize(s));
     if (stats) {
         stats->iters = host_st_->sb_iters;
-        stats->cg_iters_total = total_cg;
+        // outer iterations after the stop flag run no CG work
+        stats->cg_iters_total = host_st_->sb_iters * p.inner_iters;
         stats->residual = host_st_->res;
         stats->dx = host_st_->sb_rel;
         stats->stop_reason = host_st_->sb_done ? 2 : 0;

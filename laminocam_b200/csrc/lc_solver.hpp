@@ -23,6 +23,7 @@ struct SolverParams {
     float mu = 10.0f;
     int fp32_scalars = 0;  // 1: float accumulation of dots (the reference GPU path)
     int poll_every = 8;    // iterations between host checks of the stop flag (0: never)
+    int use_graph = 0;     // 1: replay CG iterations (Split-Bregman: outer iterations) as CUDA graphs
 };
 
 struct SolverStats {
@@ -49,6 +50,9 @@ using Operator = std::function<void(const float *in, float *out)>;
 class Solver {
   public:
     Solver(Context &ctx, long n);
+    ~Solver();
+    Solver(const Solver &) = delete;
+    Solver &operator=(const Solver &) = delete;
     // x (in: x0, out: solution); y = right-hand side
     void cg(Context &ctx, const Operator &A, const float *y, float *x, const SolverParams &p,
             SolverStats *stats);
@@ -58,7 +62,12 @@ class Solver {
 
   private:
     void cg_run(Context &ctx, const Operator &A, const float *y, float *x, int iters, float tol,
-                float xtol, int fp32, int poll_every, bool in_sb);
+                float xtol, int fp32, int poll_every, bool in_sb, bool graph);
+    // one CG iteration: Ap = A p, the fused scalar/vector updates, p = r + beta p
+    void cg_iter(Context &ctx, const Operator &A, float *x, float tol, float xtol, int fp32);
+    // records body into graph_ on the context's private stream
+    void capture(Context &ctx, const std::function<void()> &body);
+    CapturedGraph graph_;
     long n_;
     int nblk_;
     DevBuf<float> r_, p_, ap_, xold_;
