@@ -32,7 +32,8 @@ extern "C" {
 #define LC_ERR_NOMEM 2    /* device allocation failed / over the memory budget */
 #define LC_ERR_CUDA 3     /* CUDA runtime error */
 #define LC_ERR_INTERNAL 4 /* anything else */
-#define LC_ERR_TOO_LARGE 5 /* sizes beyond a fixed maximum (lc_sysmat2d_toeplitz_noalloc) */
+#define LC_ERR_TOO_LARGE 5 /* sizes beyond a fixed maximum or above a server's HBM budget */
+#define LC_ERR_TIMEOUT 6   /* lc_server_wait gave up before the job ended */
 
 typedef struct lc_context_s *lc_context;
 typedef struct lc_geometry_s *lc_geometry;
@@ -208,6 +209,73 @@ long lc_kernel_launches(void);
  * serialised by the caller. */
 int lc_sysmat2d_toeplitz_noalloc(void *stream, const float *spectrum, int P, const float *x,
                                  float *y, int nslices, int n);
+
+/* ---- reconstruction server ----------------------------------------------
+ * Replaces running one recon_tomo / recon_lamino process per reconstruction
+ * (src/recon.cpp:40-118, src/mbir2d.cpp:66-100) with a long-lived server on
+ * one GPU.  Jobs submitted from any thread queue in FIFO order; a fixed set of
+ * workers (one context and stream each) starts the head job once its
+ * estimated device footprint fits the HBM budget next to the running jobs, so
+ * jobs that arrive while others run overlap with them on the device.  Toeplitz
+ * spectra are kept in a geometry-keyed cache (key: the exact angles, the
+ * detector size and the padded dims); a job whose geometry is cached skips
+ * the PSF construction.  A job computes what lc_mbir2d / lc_mbir3d compute for
+ * the same arguments.  Its input and output host buffers must stay valid
+ * until lc_server_wait has returned for it; angle arrays are copied at
+ * submission. */
+typedef struct lc_server_s *lc_server;
+
+typedef struct {
+    int device;
+    int workers;             /* concurrent jobs (one context and stream each), 1..64 */
+    double hbm_budget_bytes; /* admission budget; 0: 85% of the free memory at creation */
+    double psf_cache_bytes;  /* cap of the Toeplitz spectrum cache; 0: 16 GiB */
+    int psf_cache;           /* 0 disables the cache */
+} lc_server_params;
+
+typedef struct {
+    double queue_ms;     /* submission to start */
+    double run_ms;       /* start to result in host memory */
+    double latency_ms;   /* submission to result */
+    int psf_hit;         /* 1 if the Toeplitz spectrum came from the cache */
+    int worker;
+    double device_bytes; /* the footprint admission charged for the job */
+    char error[160];     /* message of a failed job */
+} lc_job_info;
+
+typedef struct {
+    long completed, failed, queued, running, peak_running;
+    double p50_ms, p99_ms, mean_ms; /* latency of completed jobs (nearest rank) */
+    double span_s;                  /* first submission to last completion */
+    double recons_per_s;            /* completed / span_s */
+    double hbm_budget_bytes, peak_admitted_bytes;
+    long psf_hits, psf_misses, psf_cache_entries;
+    double psf_cache_bytes;
+} lc_server_stats;
+
+void lc_server_params_default(lc_server_params *p);
+int lc_server_create(const lc_server_params *p, lc_server *out);
+/* runs the jobs still queued, then releases everything */
+int lc_server_destroy(lc_server server);
+/* gpu::MBIR2D as a job, with the arguments of lc_mbir2d; LC_ERR_TOO_LARGE if
+ * the job alone would exceed the HBM budget */
+int lc_server_submit2d(lc_server server, const float *sino, int ns, int ntheta, int nradial,
+                       const double *theta, const int *recon_dims, const lc_recon_params *p,
+                       float *recon, long long *job_id);
+/* gpu::MBIR as a job, with the arguments of lc_mbir3d */
+int lc_server_submit3d(lc_server server, const float *projs, int ntheta, int nrows, int ncols,
+                       const double *theta, const double *gamma, const double *beta,
+                       const float *shifts, const int *recon_dims, const lc_recon_params *p,
+                       float *recon, long long *job_id);
+/* Blocks until the job ends (timeout_ms <= 0: no limit) and returns the job's
+ * status, LC_OK or its error; LC_ERR_TIMEOUT leaves the job registered. */
+int lc_server_wait(lc_server server, long long job_id, double timeout_ms, lc_solver_stats *stats,
+                   lc_job_info *info);
+int lc_server_get_stats(lc_server server, lc_server_stats *out);
+/* clears the latency record and the counters (the PSF cache stays) */
+int lc_server_reset_stats(lc_server server);
+/* message of the last failed submit / wait on the server */
+const char *lc_server_last_error(lc_server server);
 
 #ifdef __cplusplus
 }

@@ -25,7 +25,7 @@ __all__ = [
     "Context", "PolarGrid2D", "PolarGrid", "PointSpreadFunction2D", "PointSpreadFunction",
     "forward2d", "backproj2d", "sysmat2d", "forward", "backproj", "sysmat", "cgsolver",
     "split_bregman", "MBIR2D", "MBIR", "ReconParams", "Dataset", "LaminocamError",
-    "next_fast_dim", "make_odd", "pad_size",
+    "next_fast_dim", "make_odd", "pad_size", "Server", "JobResult",
 ]
 
 DEFAULT_TOL = 1e-6
@@ -486,3 +486,132 @@ def MBIR(datasets: Sequence[Dataset], params: ReconParams, ctx: Optional[Context
     _check(ctx.lib.lc_mbir3d(ctx.handle, pp, nth, nr, nc, tp, gp, bp, shp, rd, C.byref(rp),
                              out.ctypes.data_as(C.POINTER(C.c_float)), C.byref(st)), ctx)
     return (out, _info(st)) if return_info else out
+
+
+@dataclass
+class JobResult:
+    """Outcome of one server job: the reconstruction and its timings."""
+    recon: np.ndarray
+    info: SolveInfo
+    queue_ms: float
+    run_ms: float
+    latency_ms: float
+    psf_hit: bool
+    worker: int
+    device_bytes: float
+
+
+class Server:
+    """Reconstruction server on one GPU (lc_server_* in include/laminocam.h).
+
+    Jobs are gpu::MBIR2D / gpu::MBIR reconstructions with the arguments of
+    MBIR2D and MBIR.  They queue in FIFO order, and up to `workers` of them run
+    at once when their device footprint fits the HBM budget.  Toeplitz spectra
+    are cached per geometry.  `submit2d` / `submit3d` return a job id; `wait`
+    returns a JobResult or raises LaminocamError with the job's message.
+    """
+
+    def __init__(self, device: int = 0, workers: int = 4, hbm_budget_bytes: float = 0.0,
+                 psf_cache_bytes: float = 0.0, psf_cache: bool = True):
+        self.lib = _lib.load()
+        p = _lib.ServerParams()
+        self.lib.lc_server_params_default(C.byref(p))
+        p.device, p.workers = int(device), int(workers)
+        p.hbm_budget_bytes, p.psf_cache_bytes = float(hbm_budget_bytes), float(psf_cache_bytes)
+        p.psf_cache = int(bool(psf_cache))
+        h = C.c_void_p()
+        rc = self.lib.lc_server_create(C.byref(p), C.byref(h))
+        if rc != 0:
+            raise LaminocamError(f"lc_server_create failed with code {rc}")
+        self.handle = h
+        self._pending = {}
+
+    def _fail(self, rc, what):
+        msg = self.lib.lc_server_last_error(self.handle)
+        raise LaminocamError(f"{what} failed (code {rc}): {msg.decode() if msg else ''}")
+
+    def submit2d(self, sinogram, theta, params: ReconParams) -> int:
+        s = np.ascontiguousarray(sinogram, dtype=np.float32)
+        if s.ndim == 2:
+            s = np.ascontiguousarray(s[None])
+        ns, nth, nr = s.shape
+        _, tp = _dptr(theta)
+        rd = (C.c_int * 3)(*[int(d) for d in params.recon_dims])
+        out = np.empty(tuple(int(d) for d in params.recon_dims), dtype=np.float32)
+        rp = params.to_c()
+        jid = C.c_longlong()
+        rc = self.lib.lc_server_submit2d(self.handle, s.ctypes.data, ns, nth, nr, tp, rd, C.byref(rp),
+                                         out.ctypes.data, C.byref(jid))
+        if rc != 0:
+            self._fail(rc, "submit2d")
+        self._pending[jid.value] = (s, out)
+        return jid.value
+
+    def submit3d(self, datasets: Sequence[Dataset], params: ReconParams) -> int:
+        projs = np.ascontiguousarray(np.concatenate(
+            [np.asarray(d.projs, dtype=np.float32) for d in datasets], axis=0))
+        theta = np.concatenate([np.asarray(d.angles, dtype=np.float64) for d in datasets])
+        gamma = np.concatenate([np.full(len(d.angles), d.gamma, dtype=np.float64) for d in datasets])
+        beta = np.concatenate([np.full(len(d.angles), d.beta, dtype=np.float64) for d in datasets])
+        sh, shp = None, None
+        if any(d.shifts is not None for d in datasets):
+            sh = np.ascontiguousarray(np.concatenate(
+                [np.zeros((len(d.angles), 2), np.float32) if d.shifts is None
+                 else np.asarray(d.shifts, np.float32).reshape(-1, 2) for d in datasets]))
+            shp = sh.ctypes.data
+        _, tp = _dptr(theta)
+        _, gp = _dptr(gamma)
+        _, bp = _dptr(beta)
+        rd = (C.c_int * 3)(*[int(d) for d in params.recon_dims])
+        out = np.empty(tuple(int(d) for d in params.recon_dims), dtype=np.float32)
+        rp = params.to_c()
+        nth, nr, nc = projs.shape
+        jid = C.c_longlong()
+        rc = self.lib.lc_server_submit3d(self.handle, projs.ctypes.data, nth, nr, nc, tp, gp, bp, shp,
+                                         rd, C.byref(rp), out.ctypes.data, C.byref(jid))
+        if rc != 0:
+            self._fail(rc, "submit3d")
+        self._pending[jid.value] = (projs, out, sh)
+        return jid.value
+
+    def wait(self, job: int, timeout_s: float = 0.0) -> JobResult:
+        """Blocks until the job ends (timeout_s <= 0: no limit)."""
+        st = SolverStats()
+        info = _lib.JobInfo()
+        rc = self.lib.lc_server_wait(self.handle, int(job), float(timeout_s) * 1e3, C.byref(st),
+                                     C.byref(info))
+        if rc == 6:
+            self._fail(rc, f"wait for job {job}")
+        bufs = self._pending.pop(int(job), None)
+        if rc != 0:
+            raise LaminocamError(f"job {job} failed (code {rc}): {info.error.decode()}")
+        return JobResult(bufs[1], _info(st), info.queue_ms, info.run_ms, info.latency_ms,
+                         bool(info.psf_hit), info.worker, info.device_bytes)
+
+    def stats(self) -> dict:
+        s = _lib.ServerStats()
+        rc = self.lib.lc_server_get_stats(self.handle, C.byref(s))
+        if rc != 0:
+            self._fail(rc, "stats")
+        return {name: getattr(s, name) for name, _ in s._fields_}
+
+    def reset_stats(self):
+        self.lib.lc_server_reset_stats(self.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.lc_server_destroy(self.handle)
+            self.handle = None
+            self._pending.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -29,6 +29,27 @@ class ProfileEntry(C.Structure):
                 ("bytes", C.c_double)]
 
 
+class ServerParams(C.Structure):
+    _fields_ = [("device", C.c_int), ("workers", C.c_int), ("hbm_budget_bytes", C.c_double),
+                ("psf_cache_bytes", C.c_double), ("psf_cache", C.c_int)]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double),
+                ("psf_hit", C.c_int), ("worker", C.c_int), ("device_bytes", C.c_double),
+                ("error", C.c_char * 160)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_long), ("failed", C.c_long), ("queued", C.c_long),
+                ("running", C.c_long), ("peak_running", C.c_long), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("span_s", C.c_double),
+                ("recons_per_s", C.c_double), ("hbm_budget_bytes", C.c_double),
+                ("peak_admitted_bytes", C.c_double), ("psf_hits", C.c_long),
+                ("psf_misses", C.c_long), ("psf_cache_entries", C.c_long),
+                ("psf_cache_bytes", C.c_double)]
+
+
 vp = C.c_void_p
 i32 = C.c_int
 f64 = C.c_double
@@ -72,6 +93,17 @@ SIGNATURES = {
     "lc_kernel_launches": (C.c_long, []),
     "lc_sysmat2d_toeplitz_noalloc": (i32, [vp, vp, i32, vp, vp, i32, i32]),
     "lc_profile_read": (i32, [vp, C.POINTER(ProfileEntry), i32, C.POINTER(C.c_int)]),
+    "lc_server_params_default": (None, [C.POINTER(ServerParams)]),
+    "lc_server_create": (i32, [C.POINTER(ServerParams), C.POINTER(vp)]),
+    "lc_server_destroy": (i32, [vp]),
+    "lc_server_submit2d": (i32, [vp, vp, i32, i32, i32, dptr, C.POINTER(C.c_int),
+                                 C.POINTER(ReconParamsC), vp, C.POINTER(C.c_longlong)]),
+    "lc_server_submit3d": (i32, [vp, vp, i32, i32, i32, dptr, dptr, dptr, vp, C.POINTER(C.c_int),
+                                 C.POINTER(ReconParamsC), vp, C.POINTER(C.c_longlong)]),
+    "lc_server_wait": (i32, [vp, C.c_longlong, f64, C.POINTER(SolverStats), C.POINTER(JobInfo)]),
+    "lc_server_get_stats": (i32, [vp, C.POINTER(ServerStats)]),
+    "lc_server_reset_stats": (i32, [vp]),
+    "lc_server_last_error": (C.c_char_p, [vp]),
 }
 
 _lib = None

@@ -25,26 +25,6 @@ int fail(lc_context c, int code, const char *msg) {
     return code;
 }
 
-template <typename F>
-int guarded(lc_context c, F &&f) {
-    if (!c) return LC_ERR_INVALID;
-    try {
-        DeviceGuard dg(c->ctx->device());
-        f();
-        return LC_OK;
-    } catch (const Error &e) {
-        c->err = e.what();
-        if (std::string(e.what()).find("out of memory") != std::string::npos) return LC_ERR_NOMEM;
-        return e.code == 1 ? LC_ERR_INVALID : (e.code == 3 ? LC_ERR_CUDA : LC_ERR_INTERNAL);
-    } catch (const std::bad_alloc &) {
-        c->err = "host allocation failed";
-        return LC_ERR_NOMEM;
-    } catch (const std::exception &e) {
-        c->err = e.what();
-        return LC_ERR_INTERNAL;
-    }
-}
-
 double eff_tol(double tol) { return tol > 0 ? tol : 1e-6; }
 
 NufftPlan &plan_for(lc_geometry g, int n3, int n2, int n1, double tol) {

@@ -55,4 +55,34 @@ void mbir3d_core(lc_context c, const float *dprojs, int ntheta, int nrows, int n
 // padded size of the reference: int(n * factor) in float, forced odd
 long odd_pad(long n, float factor);
 
+// Runs f and maps an exception to its C status code; the message goes to err.
+template <typename F>
+int run_guarded(std::string &err, F &&f) {
+    try {
+        f();
+        return LC_OK;
+    } catch (const Error &e) {
+        err = e.what();
+        if (err.find("out of memory") != std::string::npos) return LC_ERR_NOMEM;
+        if (e.code == LC_ERR_TOO_LARGE) return LC_ERR_TOO_LARGE;
+        return e.code == 1 ? LC_ERR_INVALID : (e.code == 3 ? LC_ERR_CUDA : LC_ERR_INTERNAL);
+    } catch (const std::bad_alloc &) {
+        err = "host allocation failed";
+        return LC_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        err = e.what();
+        return LC_ERR_INTERNAL;
+    }
+}
+
+// run_guarded on the context's device, recording the message in the context
+template <typename F>
+int guarded(lc_context c, F &&f) {
+    if (!c) return LC_ERR_INVALID;
+    return run_guarded(c->err, [&] {
+        DeviceGuard dg(c->ctx->device());
+        f();
+    });
+}
+
 }  // namespace lc

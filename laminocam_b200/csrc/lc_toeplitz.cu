@@ -310,13 +310,41 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
     }
 }
 
-Toeplitz::Toeplitz(Context &ctx, const Toeplitz &src)
+static void psf_sizes(const long dims[3], bool three_d, long P[3], long Ph[3]) {
+    if (three_d) {
+        for (int d = 0; d < 3; ++d) P[d] = next_smooth23(2 * dims[d] - 1);
+    } else {
+        P[0] = 1;
+        P[1] = P[2] = next_smooth23(2 * dims[2] - 1);
+    }
+    for (int d = 0; d < 3; ++d) Ph[d] = (three_d || d > 0) ? P[d] / 2 + 1 : 1;
+}
+
+size_t Toeplitz::work_bytes(const long dims[3], bool three_d) {
+    long P[3], Ph[3];
+    psf_sizes(dims, three_d, P, Ph);
+    const size_t t1 = (size_t)dims[0] * dims[1] * Ph[2];
+    const size_t t2 = three_d ? (size_t)dims[0] * P[1] * Ph[2] : 0;
+    return (t1 + t2) * sizeof(float2);
+}
+
+size_t Toeplitz::build_peak_bytes(const long dims[3], bool three_d) {
+    long P[3], Ph[3];
+    psf_sizes(dims, three_d, P, Ph);
+    // FP64 kernel, two complex FP64 FFT buffers, FP64 and FP32 real spectra
+    const size_t full = (size_t)P[0] * P[1] * P[2];
+    const size_t half = (size_t)P[0] * P[1] * Ph[2];
+    return full * sizeof(double) + 2 * half * sizeof(double2) + half * (sizeof(double) + sizeof(float));
+}
+
+Toeplitz::Toeplitz(Context &ctx, const Toeplitz &src, bool work)
     : three_d_(src.three_d_), g_(nullptr), R_(src.R_), scale_(src.scale_) {
     for (int d = 0; d < 3; ++d) {
         n_[d] = src.n_[d];
         P_[d] = src.P_[d];
         Ph_[d] = src.Ph_[d];
     }
+    if (!work) return;
     cudaStream_t st = ctx.stream();
     t1_.alloc(n_[0] * n_[1] * Ph_[2], st);
     if (three_d_) t2_.alloc(n_[0] * (long)P_[1] * Ph_[2], st);

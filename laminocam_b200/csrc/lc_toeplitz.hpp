@@ -25,9 +25,11 @@ class Toeplitz {
     // dims = {n1, n2, n3}: volume (3D) or stack of n1 independent n2 x n3
     // slices (2D, n2 == n3 required by the reference API).
     Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], bool three_d);
-    // shares src's spectrum (read-only) and owns fresh work buffers on ctx's
-    // stream: concurrent jobs on one geometry use one spectrum
-    Toeplitz(Context &ctx, const Toeplitz &src);
+    // shares src's spectrum (read-only) and, with `work`, owns fresh work
+    // buffers on ctx's stream: concurrent jobs on one geometry use one
+    // spectrum.  Without work buffers the copy only holds the spectrum (a
+    // cache entry) and cannot be applied.
+    Toeplitz(Context &ctx, const Toeplitz &src, bool work = true);
     void apply(Context &ctx, const float *x, float *y);
     // y = A^T A x + mu * (-laplacian(x))
     void apply_reg(Context &ctx, const float *x, float *y, float mu);
@@ -39,8 +41,13 @@ class Toeplitz {
     long spectrum_elems() const { return (long)P_[0] * P_[1] * Ph_[2]; }
     const float *spectrum() const { return R_->get(); }
     size_t device_bytes() const {
-        return R_->size() * sizeof(float) + (t1_.size() + t2_.size()) * sizeof(float2);
+        return spectrum_bytes() + (t1_.size() + t2_.size()) * sizeof(float2);
     }
+    size_t spectrum_bytes() const { return R_->size() * sizeof(float); }
+    // device bytes, for given dims, of the work buffers of one apply and of
+    // the peak of a spectrum construction
+    static size_t work_bytes(const long dims[3], bool three_d);
+    static size_t build_peak_bytes(const long dims[3], bool three_d);
     // FP64 PSF K on the P-grid in mode order (k = j - P/2), for tests
     void kernel_fp64(Context &ctx, double *host_out);
     // bytes the apply must move at minimum (algorithmic traffic)

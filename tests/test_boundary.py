@@ -53,6 +53,25 @@ def test_context_create_without_gpu_fails_cleanly(lib):
     assert rc != 0 and not h.value
 
 
+def test_server_rejects_bad_parameters_and_missing_gpu(lib):
+    from laminocam_b200 import _lib
+    L = _lib.load()
+    p = _lib.ServerParams()
+    L.lc_server_params_default(ctypes.byref(p))
+    assert p.workers == 4 and p.psf_cache == 1 and p.hbm_budget_bytes == 0
+    h = ctypes.c_void_p()
+    bad = _lib.ServerParams()
+    ctypes.memmove(ctypes.byref(bad), ctypes.byref(p), ctypes.sizeof(p))
+    bad.workers = 0
+    assert L.lc_server_create(ctypes.byref(bad), ctypes.byref(h)) == 1 and not h.value
+    import torch
+    if not torch.cuda.is_available():
+        # no device: creation fails with a CUDA status and leaves no handle
+        assert L.lc_server_create(ctypes.byref(p), ctypes.byref(h)) == 3 and not h.value
+    assert L.lc_server_destroy(None) == 1
+    assert L.lc_server_wait(None, 1, 0.0, None, None) == 1
+
+
 def test_python_api_refuses_to_run_without_gpu():
     import torch
     if torch.cuda.is_available():

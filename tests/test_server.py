@@ -1,0 +1,151 @@
+"""The reconstruction server (lc_server_*) and CUDA-graph replay of the solvers.
+
+Every result the server computes, alone or among concurrent jobs, must equal
+what the one-job drivers (lc_mbir2d / lc_mbir3d) return for the same
+arguments within 1e-5 relative L2 (the spreading accumulates with float
+atomics, whose order varies from run to run); graph replay must equal eager
+launches within the same bound; a failing job must leave the other jobs and
+the server intact.  Every wait has a time limit, so a stuck job fails the test
+instead of stalling the run.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SAME_TOL = 1e-5
+RECON_TOL = 1e-4
+WAIT_S = 300.0
+
+
+@pytest.fixture(scope="module")
+def lc(cuda):
+    import laminocam_b200 as lc
+    return lc
+
+
+def sino2d(lc, n, nth, seed):
+    from laminocam_b200.synthetic import add_noise, ellipse_phantom
+    th = np.arange(nth) * np.pi / nth
+    img = ellipse_phantom(n, 8, seed)
+    s = lc.forward2d(img[None], lc.PolarGrid2D(th, n)).cpu().numpy()
+    s = add_noise(s, 0.01, seed + 1000)
+    return (s / s.max()).astype(np.float32), th
+
+
+def lamino(lc, dims, nth, gamma_deg, seed):
+    from laminocam_b200.synthetic import add_noise, ellipsoid_phantom
+    th = np.arange(nth) * 2 * np.pi / nth
+    vol = ellipsoid_phantom(dims, 6, seed)
+    n = dims[1]
+    g = -np.deg2rad(gamma_deg)
+    pg = lc.PolarGrid(th, np.full(nth, g), np.zeros(nth), n, n)
+    p = lc.forward(vol, pg).cpu().numpy()
+    p = add_noise(p, 0.01, seed + 1000)
+    return p.astype(np.float32), th, g
+
+
+def params2d(lc, n, method, iters, graph=False):
+    return lc.ReconParams(regularizer=method, recon_dims=(1, n, n), max_iters=iters, tol=0.0,
+                          xtol=0.0, use_graph=graph)
+
+
+def test_graph_replay_matches_eager(lc):
+    s, th = sino2d(lc, 95, 90, 11)
+    for method, iters in (("unconstrained", 12), ("split_bregman", 5)):
+        a = lc.MBIR2D(s, th, params2d(lc, 95, method, iters, graph=False))
+        b, info = lc.MBIR2D(s, th, params2d(lc, 95, method, iters, graph=True), return_info=True)
+        assert info.iters == iters
+        assert O.rel_l2(b, a) < SAME_TOL
+
+
+def test_graph_replay_with_tolerance_stop(lc):
+    s, th = sino2d(lc, 63, 60, 12)
+    res = []
+    for graph in (True, False):
+        p = params2d(lc, 63, "unconstrained", 200, graph=graph)
+        p.tol, p.poll_every = 1e-3, 4
+        res.append(lc.MBIR2D(s, th, p, return_info=True))
+    (x, info), (y, jnfo) = res
+    assert info.stop_reason == 1 and jnfo.stop_reason == 1
+    assert info.iters == jnfo.iters < 200
+    assert O.rel_l2(x, y) < SAME_TOL
+
+
+def test_server_results_match_single_jobs(lc):
+    jobs2d = [(63, 60, 1, "unconstrained", 10), (95, 120, 2, "split_bregman", 4),
+              (127, 90, 3, "unconstrained", 8), (63, 60, 4, "split_bregman", 3)]
+    data = [sino2d(lc, n, nth, seed) for n, nth, seed, _, _ in jobs2d]
+    ref = [lc.MBIR2D(s, th, params2d(lc, n, m, it))
+           for (n, _, _, m, it), (s, th) in zip(jobs2d, data)]
+    p3, th3, g3 = lamino(lc, (7, 31, 31), 40, 30.0, 5)
+    rp3 = lc.ReconParams(regularizer="split_bregman", recon_dims=(7, 31, 31), max_iters=3, tol=0,
+                         xtol=0)
+    ds = [lc.Dataset(p3, th3, g3, 0.0)]
+    ref3 = lc.MBIR(ds, rp3)
+    with lc.Server(workers=3) as sv:
+        ids = []
+        for rep in range(2):  # the second round finds every PSF in the cache
+            for (n, _, _, m, it), (s, th) in zip(jobs2d, data):
+                ids.append(sv.submit2d(s, th, params2d(lc, n, m, it, graph=rep == 1)))
+            ids.append(sv.submit3d(ds, rp3))
+        res = [sv.wait(j, WAIT_S) for j in ids]
+        st = sv.stats()
+    for r, e in zip(res, (ref + [ref3]) * 2):
+        assert O.rel_l2(r.recon, e) < SAME_TOL
+    assert st["completed"] == len(ids) and st["failed"] == 0
+    assert st["psf_hits"] >= 5 and all(r.psf_hit for r in res[5:])
+    assert st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_server_result_matches_oracle(lc):
+    s, th = sino2d(lc, 63, 60, 21)
+    with lc.Server(workers=2) as sv:
+        r = sv.wait(sv.submit2d(s, th, params2d(lc, 63, "unconstrained", 5)), WAIT_S)
+    xo = O.mbir2d(s.astype(np.float64), th, (1, 63, 63), method="cg", max_iters=5, tol=0, xtol=0)
+    assert O.rel_l2(r.recon, xo) < RECON_TOL
+
+
+def test_server_isolates_failing_job(lc):
+    s, th = sino2d(lc, 63, 60, 31)
+    good = params2d(lc, 63, "unconstrained", 6)
+    bad = lc.ReconParams(regularizer="unconstrained", recon_dims=(2, 63, 63), max_iters=6)
+    ref = lc.MBIR2D(s, th, good)
+    with lc.Server(workers=2) as sv:
+        a = sv.submit2d(s, th, good)
+        b = sv.submit2d(s, th, bad)  # recon_dims[0] != number of slices: fails when it runs
+        c = sv.submit2d(s, th, good)
+        ra = sv.wait(a, WAIT_S)
+        with pytest.raises(lc.LaminocamError, match="recon_dims"):
+            sv.wait(b, WAIT_S)
+        rc = sv.wait(c, WAIT_S)
+        st = sv.stats()
+        rd = sv.wait(sv.submit2d(s, th, good), WAIT_S)  # still serving after the failure
+    for r in (ra, rc, rd):
+        assert O.rel_l2(r.recon, ref) < SAME_TOL
+    assert st["failed"] == 1 and st["completed"] == 2
+
+
+def test_server_rejects_job_over_budget(lc):
+    s, th = sino2d(lc, 63, 60, 41)
+    with lc.Server(workers=1, hbm_budget_bytes=1 << 20) as sv:
+        with pytest.raises(lc.LaminocamError, match="code 5"):
+            sv.submit2d(s, th, params2d(lc, 63, "unconstrained", 3))
+
+
+def test_server_admission_respects_budget(lc):
+    """With a budget for two jobs, no more than two run at once."""
+    s, th = sino2d(lc, 127, 90, 51)
+    p = params2d(lc, 127, "split_bregman", 3)
+    with lc.Server(workers=1) as probe:
+        one = probe.wait(probe.submit2d(s, th, p), WAIT_S).device_bytes
+    with lc.Server(workers=4, hbm_budget_bytes=2.5 * one) as sv:
+        ids = [sv.submit2d(s, th, p) for _ in range(6)]
+        res = [sv.wait(j, WAIT_S) for j in ids]
+        st = sv.stats()
+    assert st["peak_admitted_bytes"] <= 2.5 * one
+    assert 1 <= st["peak_running"] <= 2
+    for r in res[1:]:
+        assert O.rel_l2(r.recon, res[0].recon) < SAME_TOL
