@@ -80,28 +80,60 @@ def make_projections(lc):
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples the SM clock and the clock-event (throttle) reasons every 0.2 s
+    during the timed region: read-only NVML queries in this process, or
+    nvidia-smi when NVML cannot be loaded."""
+
+    REASONS = [("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap")]
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
+        self.samples = []  # (sm_mhz, sm_max_mhz, [active reasons])
+        self.source = None
         self._stop = threading.Event()
         self._t = threading.Thread(target=self._run, daemon=True)
 
-    def _run(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+    def _nvml(self):
+        import pynvml as N
+        N.nvmlInit()
+        h = N.nvmlDeviceGetHandleByIndex(self.index)
+        mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+        get = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons",
+                      getattr(N, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
+        masks = [(name, getattr(N, attr, 0)) for name, attr in self.REASONS]
+        self.source = "nvml"
+        while not self._stop.is_set():
+            sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+            bits = get(h) if get else 0
+            self.samples.append((float(sm), float(mx), [n for n, m in masks if m and bits & m]))
+            self._stop.wait(0.2)
+
+    def _smi(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
+        self.source = "nvidia-smi"
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
                                       "--format=csv,noheader,nounits"], capture_output=True,
                                      text=True, timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([v.strip() for v in out.split(",")])
+                v = [x.strip() for x in out.split(",")]
+                if len(v) >= 6:
+                    act = [self.REASONS[i][0] for i in range(4) if v[2 + i].lower() == "active"]
+                    self.samples.append((float(v[0]), float(v[1]), act))
             except Exception:
                 pass
             self._stop.wait(0.2)
+
+    def _run(self):
+        try:
+            self._nvml()
+        except Exception:
+            self._smi()
 
     def __enter__(self):
         self._t.start()
@@ -113,14 +145,11 @@ class ClockSampler:
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4)
-                          if len(s) > 3 + i and s[3 + i].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock samples"]}
+        sm = [s[0] for s in self.samples]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": sorted({r for s in self.samples for r in s[2]}),
+                "samples": len(self.samples), "source": self.source}
 
 
 def measured_peak():
@@ -155,6 +184,102 @@ def cpu_baseline(sample_outer: int = 1):
                       f"extrapolated to 100 outer iterations; backprojection and PSF setup excluded"}
 
 
+MIX_JOBS = 64
+MIX_ITERS = 50
+
+
+def mix_jobs(lc, count=MIX_JOBS, seed=3000):
+    """Uneven 2D slices: n = odd(round(exp(U[ln 128, ln 1024]))), ntheta ~ U{90..720}
+    over [0, pi), 10 ellipses each, forward-projected on the GPU, 1% noise,
+    normalised by the maximum."""
+    import torch
+    from laminocam_b200 import synthetic as S
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(128), np.log(1024)))))
+        n -= (n % 2 == 0)
+        nth = int(rng.integers(90, 721))
+        th = np.arange(nth) * np.pi / nth
+        img = S.ellipse_phantom(n, 10, 1000 + k)
+        s = lc.forward2d(torch.as_tensor(img[None], device="cuda"), lc.PolarGrid2D(th, n))
+        s = S.add_noise(s.cpu().numpy(), NOISE, 2000 + k)
+        jobs.append((np.ascontiguousarray(s / s.max(), dtype=np.float32), th, n))
+    torch.cuda.synchronize()
+    return jobs
+
+
+def serving_mix(lc, workers=4):
+    """The same 64 uneven 2D CG jobs (50 iterations each) solved (a) one at a time
+    the plain way -- float scalars, a host check of the solver state after every
+    iteration, no graphs, a PSF built per job -- and (b) submitted together to
+    the server: concurrent jobs on 4 streams, CUDA-graph iterations, FP64
+    scalars, geometry-keyed PSF cache.  Wall-clock times, host buffers in and
+    out.  The error of both forms against the FP64 oracle is measured on one
+    small job (n = 63, 60 angles) of the same kind."""
+    from oracle import oracle as O
+    jobs = mix_jobs(lc)
+
+    def prm(n, plain, iters=MIX_ITERS):
+        # plain: tol 1e-30 keeps the per-iteration host check without ever stopping
+        return lc.ReconParams(regularizer="unconstrained", recon_dims=(1, n, n), max_iters=iters,
+                              tol=1e-30 if plain else 0.0, xtol=0.0, fp32_scalars=plain,
+                              poll_every=1 if plain else 8, use_graph=not plain)
+
+    # untimed pass over every job shape (one CG iteration each): fills the FFT
+    # launch-tuner cache that both forms share, so neither pays for tuning
+    for s, th, n in jobs:
+        lc.MBIR2D(s, th, prm(n, True, 1))
+    t0 = time.perf_counter()
+    plain_out, plain_ms = [], []
+    for s, th, n in jobs:
+        a = time.perf_counter()
+        plain_out.append(lc.MBIR2D(s, th, prm(n, True)))
+        plain_ms.append((time.perf_counter() - a) * 1e3)
+    t_plain = time.perf_counter() - t0
+
+    with lc.Server(workers=workers) as sv:
+        small = min(jobs, key=lambda j: j[2])
+        sv.wait(sv.submit2d(small[0], small[1], prm(small[2], False)), 600)
+        sv.reset_stats()
+        t0 = time.perf_counter()
+        ids = [sv.submit2d(s, th, prm(n, False)) for s, th, n in jobs]
+        res = [sv.wait(j, 600) for j in ids]
+        t_served = time.perf_counter() - t0
+        st = sv.stats()
+        # the FP64 oracle on one small job of the same kind
+        from laminocam_b200 import synthetic as S
+        th1 = np.arange(60) * np.pi / 60
+        s1 = lc.forward2d(S.ellipse_phantom(63, 10, 4000)[None], lc.PolarGrid2D(th1, 63)).cpu().numpy()
+        s1 = np.ascontiguousarray(S.add_noise(s1, NOISE, 4001), dtype=np.float32)
+        s1 /= s1.max()
+        x_served = sv.wait(sv.submit2d(s1, th1, prm(63, False)), 600).recon
+    x_plain = lc.MBIR2D(s1, th1, prm(63, True))
+    xo = O.mbir2d(s1.astype(np.float64), th1, (1, 63, 63), method="cg", max_iters=MIX_ITERS, tol=0,
+                  xtol=0)
+    sizes = [j[2] for j in jobs]
+    return {
+        "workload": f"{MIX_JOBS} uneven 2D slices, n odd log-uniform in [127, 1023], ntheta U{{90..720}} "
+                    f"over [0,180), 10 ellipses, 1% noise, CG {MIX_ITERS} iterations (fixed count)",
+        "n_range": [min(sizes), max(sizes)],
+        "plain": {"recons_per_s": MIX_JOBS / t_plain, "seconds": t_plain,
+                  "job_ms_p50": float(np.percentile(plain_ms, 50)),
+                  "job_ms_p99": float(np.percentile(plain_ms, 99)),
+                  "form": "one job at a time, float scalars, host check every iteration, no graphs, "
+                          "PSF built per job"},
+        "served": {"recons_per_s": MIX_JOBS / t_served, "seconds": t_served,
+                   "latency_ms_p50": st["p50_ms"], "latency_ms_p99": st["p99_ms"],
+                   "workers": workers, "peak_running": st["peak_running"],
+                   "psf_hits": st["psf_hits"], "psf_misses": st["psf_misses"],
+                   "form": "all 64 submitted at once; concurrent streams, CUDA-graph CG iterations, "
+                           "FP64 scalars, geometry-keyed PSF cache"},
+        "speedup": t_plain / t_served,
+        "max_rel_l2_served_vs_plain": max(O.rel_l2(r.recon, p) for r, p in zip(res, plain_out)),
+        "rel_l2_vs_fp64_oracle_n63": {"served": O.rel_l2(x_served, xo), "plain": O.rel_l2(x_plain, xo)},
+        "timing": "wall clock, host buffers in and out",
+    }
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -183,6 +308,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mix", action="store_true",
+                    help="skip the served-vs-plain 64-job 2D mix")
     ap.add_argument("--small", action="store_true",
                     help="reduced case for profiler captures: recon_dims [15,255,255], 180 angles, "
                          "255x255 detector, 5 outer iterations (not a benchmark line)")
@@ -194,6 +321,7 @@ def main():
                        "recon_dims": list(RECON_DIMS), "padded_dims": [21, 359, 359],
                        "angles": NANGLES, "detector": list(DET), "outer_iters": OUTER})
         args.no_cpu_baseline = True
+        args.no_mix = True
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -316,13 +444,31 @@ def main():
                      "bytes_per_launch": e.bytes / max(e.count, 1)})
     prof.sort(key=lambda d: -d["total_ms"])
     peak, peak_kind = measured_peak()
-    dom = next((p for p in prof if p["bytes_per_launch"] > 0), prof[0] if prof else None)
+    # The Toeplitz apply (A^T A, the per-iteration hot spot) is one unit of five
+    # line-FFT launches; it competes with the single sections for "dominant".
+    toep = [p for p in prof if p["name"].startswith("toeplitz_")]
+    units = [p for p in prof if not p["name"].startswith("toeplitz_") and p["bytes_per_launch"] > 0]
+    if toep:
+        applies = max(p["launches"] for p in toep)
+        tot_ms = sum(p["total_ms"] for p in toep)
+        tot_b = sum(p["bytes_per_launch"] * p["launches"] for p in toep)
+        units.append({"name": "toeplitz_apply (" + "+".join(p["name"][9:] for p in toep) + ")",
+                      "launches": applies, "total_ms": tot_ms, "avg_ms": tot_ms / applies,
+                      "gbs": tot_b / tot_ms / 1e6, "bytes_per_launch": tot_b / applies})
+    dom = max(units, key=lambda d: d["total_ms"]) if units else None
     roof = None
     if dom:
         roof = {"bound": "hbm", "kernel": dom["name"], "achieved": dom["gbs"], "peak": peak,
                 "unit": "GB/s", "frac": dom["gbs"] / peak, "peak_source": peak_kind,
                 "bytes_per_launch": dom["bytes_per_launch"], "avg_launch_ms": dom["avg_ms"],
                 "traffic": None}
+
+    serving = None
+    if rank == 0 and world == 1 and not args.no_mix:
+        try:
+            serving = serving_mix(lc)
+        except Exception as ex:  # reported, not fatal
+            serving = {"error": repr(ex)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -339,11 +485,12 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 PSF and solver scalars)",
         "data": "synthetic", "config": CONFIG,
         "latency_ms": {"p50": float(np.percentile(lats_sorted, 50)),
-                       "p99": float(np.percentile(lats_sorted, 99))},
+                       "p99": float(np.percentile(lats_sorted, 99)),
+                       "steps": [round(v, 2) for v in lats]},
         "e2e": {"value": e2e_value, "unit": "recons/s",
                 "h2d_bytes_per_step": int(host_proj.numel() * 4),
                 "d2h_bytes_per_step": int(host_recon.numel() * 4)},
-        "roofline": roof, "kernels": prof[:8], "clocks": clk.summary(),
+        "roofline": roof, "kernels": prof[:8], "clocks": clk.summary(), "serving": serving,
         "gpu_launches": int(launches), "cpu_baseline": cpu,
         "solver": {"outer_iters": stats.iters, "cg_iters": stats.cg_iters_total, "dx": stats.dx},
     }

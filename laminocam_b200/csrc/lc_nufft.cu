@@ -234,134 +234,24 @@ __global__ void bin_scatter_kernel(PolarPts pts, GridCfg g, int W, int *cursor, 
 }
 
 // ---- spreading ----------------------------------------------------------
-template <int DIM, int W>
-__global__ void __launch_bounds__(256) spread_kernel(PolarPts pts, GridCfg g,
-                                                     const float2 *__restrict__ c, long cstride,
-                                                     int nvol, const int *__restrict__ perm,
-                                                     const int4 *__restrict__ subs,
-                                                     float2 *__restrict__ grid, long gstride,
-                                                     int mode, const float2 *__restrict__ shifts) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2 *tile = reinterpret_cast<float2 *>(smem_raw);
-    const int4 sp = subs[blockIdx.x];
-    const int bin = sp.x;
-    int bcoord[3] = {0, 0, 0};
-    {
-        int r = bin;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            bcoord[d] = r % g.nb[d];
-            r /= g.nb[d];
-        }
-    }
-    int S[3] = {0, 0, 0};
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) S[d] = bcoord[d] * g.bs[d] - g.hw[d];
-    const int tx = g.td[0], ty = g.td[1], tz = DIM == 3 ? g.td[2] : 1;
-    const int tsize = tx * ty * tz;
-    for (int idx = threadIdx.x; idx < nvol * tsize; idx += blockDim.x) tile[idx] = make_float2(0.f, 0.f);
-    __syncthreads();
+// One thread spreads one point over its W^DIM footprint with shared-memory
+// atomics into a planar tile (real and imaginary parts in separate arrays).
+// All lanes of a warp issue each atomic instruction at the same footprint
+// offset, so their addresses differ by the differences of their footprint
+// corners.  The points of a subproblem are therefore first bucketed by the
+// shared-memory bank of their corner (corner index mod 32), and in round r
+// lane i spreads the r-th point of bank i: the 32 addresses of every atomic
+// instruction fall in 32 distinct banks.
+constexpr int kSpreadThreads = 256;
 
-    const float inv_hw = 2.0f / (float)W;
-    for (int p = threadIdx.x; p < sp.z; p += blockDim.x) {
-        const int j = perm[sp.y + p];
-        PointInfo pi;
-        point_at(pts, j, pi);
-        float2 mult = make_float2(1.f, 0.f);
-        if (mode != PT_PLAIN) {
-            if (!in_band(pi)) continue;
-            if (mode == PT_SHIFT) {
-                float2 sh = shifts[pi.angle];
-                double ph = pi.qX * (double)sh.x + pi.qY * (double)sh.y;
-                double sn, cs;
-                sincos(ph, &sn, &cs);
-                mult = make_float2((float)cs, (float)-sn);
-            }
-        }
-        float wk[2][W];
-        int lo[3] = {0, 0, 0};
-        float offz = 0.f;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            int cell, l0;
-            float off;
-            place(pi.c[d], g.nf[d], W, cell, l0, off);
-            lo[d] = l0 - S[d];
-            if (d < 2) {
-#pragma unroll
-                for (int m = 0; m < W; ++m) wk[d][m] = es_evalf(((float)m - off) * inv_hw, g.beta);
-            } else {
-                offz = off;
-            }
-        }
-        for (int s = 0; s < nvol; ++s) {
-            float2 v = c[(long)s * cstride + j];
-            if (mode == PT_SHIFT) v = cmul(v, mult);
-            float2 *ts = tile + (long)s * tsize;
-            if constexpr (DIM == 2) {
-#pragma unroll
-                for (int dy = 0; dy < W; ++dy) {
-                    float2 vy = make_float2(v.x * wk[1][dy], v.y * wk[1][dy]);
-                    float2 *row = ts + (lo[1] + dy) * tx + lo[0];
-#pragma unroll
-                    for (int dx = 0; dx < W; ++dx) {
-                        atomicAdd(&row[dx].x, vy.x * wk[0][dx]);
-                        atomicAdd(&row[dx].y, vy.y * wk[0][dx]);
-                    }
-                }
-            } else {
-                for (int dz = 0; dz < W; ++dz) {
-                    const float wz = es_evalf(((float)dz - offz) * inv_hw, g.beta);
-                    float2 vz = make_float2(v.x * wz, v.y * wz);
-#pragma unroll
-                    for (int dy = 0; dy < W; ++dy) {
-                        float2 vy = make_float2(vz.x * wk[1][dy], vz.y * wk[1][dy]);
-                        float2 *row = ts + ((lo[2] + dz) * ty + (lo[1] + dy)) * tx + lo[0];
-#pragma unroll
-                        for (int dx = 0; dx < W; ++dx) {
-                            atomicAdd(&row[dx].x, vy.x * wk[0][dx]);
-                            atomicAdd(&row[dx].y, vy.y * wk[0][dx]);
-                        }
-                    }
-                }
-            }
-        }
-    }
-    __syncthreads();
-    // flush: halos overlap neighbouring bins, so accumulate atomically
-    for (int idx = threadIdx.x; idx < nvol * tsize; idx += blockDim.x) {
-        float2 v = tile[idx];
-        if (v.x == 0.f && v.y == 0.f) continue;
-        int s = idx / tsize;
-        int r = idx - s * tsize;
-        int ix = r % tx;
-        int iy = (r / tx) % ty;
-        int iz = r / (tx * ty);
-        long gi = (long)wrap(S[0] + ix, g.nf[0]) + (long)wrap(S[1] + iy, g.nf[1]) * g.nf[0];
-        if (DIM == 3) gi += (long)wrap(S[2] + iz, g.nf[2]) * g.nf[0] * g.nf[1];
-        float2 *dst = grid + (long)s * gstride + gi;
-        atomicAdd(&dst->x, v.x);
-        atomicAdd(&dst->y, v.y);
-    }
-}
-
-// ---- warp-cooperative spreading -------------------------------------------
-// One warp spreads one point at a time: lane (r, c) = (lane / 8, lane % 8)
-// owns kernel rows r and r + 4 and column c of the W x W footprint (W <= 8),
-// and the warp walks z.  The tile is planar (real and imaginary parts in
-// separate arrays) with a row stride txs = 8 (mod 32), so the 28 cells one
-// atomic instruction touches (4 rows x 7 columns for W = 7) fall in distinct
-// shared-memory banks.  Each lane first computes the placement and value of
-// one of 32 points; the warp then broadcasts them one by one with shuffles.
 template <int DIM, int W>
-__global__ void __launch_bounds__(256) spread_warp_kernel(PolarPts pts, GridCfg g, int txs,
-                                                          const float2 *__restrict__ c, long cstride,
-                                                          int nvol, const int *__restrict__ perm,
-                                                          const int4 *__restrict__ subs,
-                                                          float2 *__restrict__ grid, long gstride,
-                                                          int mode, const float2 *__restrict__ shifts) {
-    static_assert(W <= 8, "warp spreading covers at most 8 x 8 footprint columns");
+__global__ void __launch_bounds__(kSpreadThreads, 2)
+    spread_kernel(PolarPts pts, GridCfg g, const float2 *__restrict__ c, long cstride, int nvol,
+                  const int *__restrict__ perm, const int4 *__restrict__ subs,
+                  float2 *__restrict__ grid, long gstride, int mode,
+                  const float2 *__restrict__ shifts, int maxpts) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int cnt[32], start[32], maxcnt;
     const int4 sp = subs[blockIdx.x];
     int bcoord[3] = {0, 0, 0};
     {
@@ -375,104 +265,124 @@ __global__ void __launch_bounds__(256) spread_warp_kernel(PolarPts pts, GridCfg 
     int S[3] = {0, 0, 0};
 #pragma unroll
     for (int d = 0; d < DIM; ++d) S[d] = bcoord[d] * g.bs[d] - g.hw[d];
-    const int ty = g.td[1], tz = DIM == 3 ? g.td[2] : 1;
-    const int plane = ty * txs;
-    const int tsize = tz * plane;  // padded cells per slice
+    const int tx = g.td[0], ty = g.td[1], tz = DIM == 3 ? g.td[2] : 1;
+    const int plane = tx * ty;
+    const int tsize = plane * tz;
     float *tre = reinterpret_cast<float *>(smem_raw);
     float *tim = tre + (long)nvol * tsize;
-    for (int idx = threadIdx.x; idx < 2 * nvol * tsize; idx += blockDim.x) tre[idx] = 0.f;
+    int *order = reinterpret_cast<int *>(tim + (long)nvol * tsize);
+    int *key = order + maxpts;
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < 2 * nvol * tsize; idx += blockDim.x) tre[idx] = 0.f;
+    if (tid < 32) cnt[tid] = 0;
     __syncthreads();
 
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int r = lane >> 3, cx = lane & 7;
-    const float inv_hw = 2.0f / (float)W;
-    for (int pbase = warp * 32; pbase < sp.z; pbase += nwarps * 32) {
-        // this lane's point
-        int ok = 0, lo0 = 0, lo1 = 0, lo2 = 0, jj = 0;
-        float of0 = 0.f, of1 = 0.f, of2 = 0.f;
-        float2 v = make_float2(0.f, 0.f), mult = make_float2(1.f, 0.f);
-        if (pbase + lane < sp.z) {
-            jj = perm[sp.y + pbase + lane];
-            PointInfo pi;
-            point_at(pts, jj, pi);
-            ok = (mode == PT_PLAIN) || in_band(pi);
-            if (ok && mode == PT_SHIFT) {
-                float2 sh = shifts[pi.angle];
-                double ph = pi.qX * (double)sh.x + pi.qY * (double)sh.y;
-                double sn, cs;
-                sincos(ph, &sn, &cs);
-                mult = make_float2((float)cs, (float)-sn);
-            }
-            int cell, l0;
-            place(pi.c[0], g.nf[0], W, cell, l0, of0);
-            lo0 = l0 - S[0];
-            place(pi.c[1], g.nf[1], W, cell, l0, of1);
-            lo1 = l0 - S[1];
-            if (DIM == 3) {
-                place(pi.c[2], g.nf[2], W, cell, l0, of2);
-                lo2 = l0 - S[2];
-            }
-            if (ok && nvol == 1) v = cmul(c[jj], mult);
-        }
-        const int npts = min(32, sp.z - pbase);
-        for (int q = 0; q < npts; ++q) {
-            if (!__shfl_sync(0xffffffffu, ok, q)) continue;
-            const int q0 = __shfl_sync(0xffffffffu, lo0, q);
-            const int q1 = __shfl_sync(0xffffffffu, lo1, q);
-            const float f0 = __shfl_sync(0xffffffffu, of0, q);
-            const float f1 = __shfl_sync(0xffffffffu, of1, q);
-            const float wx = cx < W ? es_evalf(((float)cx - f0) * inv_hw, g.beta) : 0.f;
-            const float wy0 = es_evalf(((float)r - f1) * inv_hw, g.beta);
-            const float wy1 = (r + 4 < W) ? es_evalf(((float)(r + 4) - f1) * inv_hw, g.beta) : 0.f;
-            int q2 = 0;
-            float wzl = 0.f;
-            if (DIM == 3) {
-                q2 = __shfl_sync(0xffffffffu, lo2, q);
-                const float f2 = __shfl_sync(0xffffffffu, of2, q);
-                wzl = lane < W ? es_evalf(((float)lane - f2) * inv_hw, g.beta) : 0.f;
-            }
-            for (int s = 0; s < nvol; ++s) {
-                float2 val;
-                if (nvol == 1) {
-                    val.x = __shfl_sync(0xffffffffu, v.x, q);
-                    val.y = __shfl_sync(0xffffffffu, v.y, q);
-                } else {
-                    const int jq = __shfl_sync(0xffffffffu, jj, q);
-                    float2 mq;
-                    mq.x = __shfl_sync(0xffffffffu, mult.x, q);
-                    mq.y = __shfl_sync(0xffffffffu, mult.y, q);
-                    val = cmul(c[(long)s * cstride + jq], mq);
-                }
-                float *re = tre + (long)s * tsize;
-                float *im = tim + (long)s * tsize;
-                const int col = q0 + cx;
-                const int row0 = (q1 + r) * txs + col;
-                const int row1 = (q1 + r + 4) * txs + col;
-                if (DIM == 2) {
-                    if (cx < W) {
-                        const float w0 = wx * wy0;
-                        atomicAdd(re + row0, val.x * w0);
-                        atomicAdd(im + row0, val.y * w0);
-                        if (r + 4 < W) {
-                            const float w1 = wx * wy1;
-                            atomicAdd(re + row1, val.x * w1);
-                            atomicAdd(im + row1, val.y * w1);
-                        }
-                    }
-                } else {
+    // ---- bucket the points by the bank of their footprint corner ----
+    for (int p = tid; p < sp.z; p += blockDim.x) {
+        const int j = perm[sp.y + p];
+        PointInfo pi;
+        point_at(pts, j, pi);
+        int k = -1;
+        if (mode == PT_PLAIN || in_band(pi)) {
+            const int stride[3] = {1, tx, plane};
+            int corner = 0;
 #pragma unroll
-                    for (int dz = 0; dz < W; ++dz) {
-                        const float wz = __shfl_sync(0xffffffffu, wzl, dz);
-                        const int zoff = (q2 + dz) * plane;
-                        if (cx < W) {
-                            const float w0 = wx * wy0 * wz;
-                            atomicAdd(re + zoff + row0, val.x * w0);
-                            atomicAdd(im + zoff + row0, val.y * w0);
-                            if (r + 4 < W) {
-                                const float w1 = wx * wy1 * wz;
-                                atomicAdd(re + zoff + row1, val.x * w1);
-                                atomicAdd(im + zoff + row1, val.y * w1);
-                            }
+            for (int d = 0; d < DIM; ++d) {
+                int cell, l0;
+                float off;
+                place(pi.c[d], g.nf[d], W, cell, l0, off);
+                corner += (l0 - S[d]) * stride[d];
+            }
+            const int b = corner & 31;
+            k = (b << 16) | atomicAdd(&cnt[b], 1);
+        }
+        key[p] = k;
+    }
+    __syncthreads();
+    if (tid < 32) {
+        const int v = cnt[tid];
+        int incl = v, m = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (tid >= o) incl += t;
+            m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        }
+        start[tid] = incl - v;
+        if (tid == 0) maxcnt = m;
+    }
+    __syncthreads();
+    for (int p = tid; p < sp.z; p += blockDim.x) {
+        const int k = key[p];
+        if (k >= 0) order[start[k >> 16] + (k & 0xffff)] = p;
+    }
+    __syncthreads();
+
+    // ---- spread: in round r, lane i takes the r-th point of bank i ----
+    const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const float inv_hw = 2.0f / (float)W;
+    const int mycnt = cnt[lane], mystart = start[lane];
+    for (int r = warp; r < maxcnt; r += nwarps) {
+        if (r >= mycnt) continue;
+        const int j = perm[sp.y + order[mystart + r]];
+        PointInfo pi;
+        point_at(pts, j, pi);
+        float2 mult = make_float2(1.f, 0.f);
+        if (mode == PT_SHIFT) {
+            const float2 sh = shifts[pi.angle];
+            const double ph = pi.qX * (double)sh.x + pi.qY * (double)sh.y;
+            double sn, cs;
+            sincos(ph, &sn, &cs);
+            mult = make_float2((float)cs, (float)-sn);
+        }
+        float wk[DIM][W];
+        int corner = 0;
+        {
+            const int stride[3] = {1, tx, plane};
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                int cell, l0;
+                float off;
+                place(pi.c[d], g.nf[d], W, cell, l0, off);
+                corner += (l0 - S[d]) * stride[d];
+#pragma unroll
+                for (int m = 0; m < W; ++m) wk[d][m] = es_evalf(((float)m - off) * inv_hw, g.beta);
+            }
+        }
+        for (int s = 0; s < nvol; ++s) {
+            float2 v = c[(long)s * cstride + j];
+            if (mode == PT_SHIFT) v = cmul(v, mult);
+            float *re = tre + (long)s * tsize + corner;
+            float *im = tim + (long)s * tsize + corner;
+            if constexpr (DIM == 2) {
+#pragma unroll
+                for (int dy = 0; dy < W; ++dy) {
+                    const float vr = v.x * wk[1][dy], vi = v.y * wk[1][dy];
+                    const int row = dy * tx;
+#pragma unroll
+                    for (int dx = 0; dx < W; ++dx) {
+                        atomicAdd(re + row + dx, vr * wk[0][dx]);
+                        atomicAdd(im + row + dx, vi * wk[0][dx]);
+                    }
+                }
+            } else {
+#pragma unroll 1
+                for (int dz = 0; dz < W; ++dz) {
+                    float wz = wk[2][0];
+#pragma unroll
+                    for (int m = 1; m < W; ++m)
+                        if (dz == m) wz = wk[2][m];
+                    const float zr = v.x * wz, zi = v.y * wz;
+                    float *rez = re + dz * plane;
+                    float *imz = im + dz * plane;
+#pragma unroll
+                    for (int dy = 0; dy < W; ++dy) {
+                        const float vr = zr * wk[1][dy], vi = zi * wk[1][dy];
+                        const int row = dy * tx;
+#pragma unroll
+                        for (int dx = 0; dx < W; ++dx) {
+                            atomicAdd(rez + row + dx, vr * wk[0][dx]);
+                            atomicAdd(imz + row + dx, vi * wk[0][dx]);
                         }
                     }
                 }
@@ -481,20 +391,17 @@ __global__ void __launch_bounds__(256) spread_warp_kernel(PolarPts pts, GridCfg 
     }
     __syncthreads();
     // flush the tile (halos overlap neighbouring bins, so accumulate atomically)
-    const int tx = g.td[0];
-    for (int idx = threadIdx.x; idx < nvol * tsize; idx += blockDim.x) {
-        const int s = idx / tsize;
-        const int rr = idx - s * tsize;
-        const int ix = rr % txs;
-        if (ix >= tx) continue;
+    for (int idx = tid; idx < nvol * tsize; idx += blockDim.x) {
         const float a = tre[idx], b = tim[idx];
         if (a == 0.f && b == 0.f) continue;
-        const int iy = (rr / txs) % ty;
+        const int s = idx / tsize;
+        const int rr = idx - s * tsize;
+        const int ix = rr % tx;
+        const int iy = (rr / tx) % ty;
         const int iz = rr / plane;
         long gi = (long)wrap(S[0] + ix, g.nf[0]) + (long)wrap(S[1] + iy, g.nf[1]) * g.nf[0];
         if (DIM == 3) gi += (long)wrap(S[2] + iz, g.nf[2]) * g.nf[0] * g.nf[1];
-        float2 *dst = grid + (long)s * gstride + gi;
-        atomicAdd(dst, make_float2(a, b));
+        atomicAdd(grid + (long)s * gstride + gi, make_float2(a, b));
     }
 }
 
@@ -603,24 +510,14 @@ __global__ void __launch_bounds__(256) interp_kernel(PolarPts pts, GridCfg g,
 }
 
 template <int DIM, int W>
-void launch_spread_w(dim3 grid, int threads, size_t smem, cudaStream_t st, const PolarPts &pts,
+void launch_spread_w(dim3 grid, size_t smem, cudaStream_t st, const PolarPts &pts,
                      const GridCfg &g, const float2 *c, long cstride, int nvol, const int *perm,
-                     const int4 *subs, float2 *out, long gstride, int mode, const float2 *shifts) {
+                     const int4 *subs, float2 *out, long gstride, int mode, const float2 *shifts,
+                     int maxpts) {
     auto kern = spread_kernel<DIM, W>;
     LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<grid, threads, smem, st>>>(pts, g, c, cstride, nvol, perm, subs, out, gstride, mode,
-                                      shifts);
-    LC_CHECK_LAUNCH();
-}
-
-template <int DIM, int W>
-void launch_spread_warp_w(dim3 grid, size_t smem, cudaStream_t st, const PolarPts &pts,
-                          const GridCfg &g, int txs, const float2 *c, long cstride, int nvol,
-                          const int *perm, const int4 *subs, float2 *out, long gstride, int mode,
-                          const float2 *shifts) {
-    auto kern = spread_warp_kernel<DIM, W>;
-    LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<grid, 256, smem, st>>>(pts, g, txs, c, cstride, nvol, perm, subs, out, gstride, mode, shifts);
+    kern<<<grid, kSpreadThreads, smem, st>>>(pts, g, c, cstride, nvol, perm, subs, out, gstride,
+                                             mode, shifts, maxpts);
     LC_CHECK_LAUNCH();
 }
 
@@ -679,8 +576,8 @@ NufftPlan::NufftPlan(Context &ctx, const PolarGeometry &g, const int modes[3], d
         nf_[d] = d < dim_ ? (int)next_smooth23(std::max(2 * modes_[d], 2 * w_)) : 1;
     }
     const int bs2[3] = {32, 32, 1};
-    // bin x-extents of 32 give tile rows of 32 + 2*ceil(w/2) = 40 cells (= 8 mod 32)
     const int bs3[3] = {32, 8, 8};
+    maxsub_ = dim_ == 2 ? 1024 : 2048;
     for (int d = 0; d < 3; ++d) {
         bs_[d] = std::min(dim_ == 2 ? bs2[d] : bs3[d], nf_[d]);
         nb_[d] = (nf_[d] + bs_[d] - 1) / bs_[d];
@@ -720,7 +617,7 @@ void NufftPlan::sort_points(Context &ctx) {
     LC_CUDA(cudaStreamSynchronize(st));
     std::vector<int> off(nbins);
     long acc = 0;
-    const int maxsub = dim_ == 2 ? 1024 : 2048;
+    const int maxsub = maxsub_;
     std::vector<int4> subs;
     for (long b = 0; b < nbins; ++b) {
         off[b] = (int)acc;
@@ -746,44 +643,24 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
     const long gvol = (long)nf_[0] * nf_[1] * nf_[2];
     // values read once, fine grid written once (plus the permutation)
     ProfScope ps(ctx, PS_SPREAD, (double)nvol * (8.0 * pts_.M + 8.0 * gvol) + 4.0 * pts_.M);
-    if (w_ <= 8) {
-        // warp-cooperative path: planar tile, row stride = 8 (mod 32)
-        const int tx = g.td[0];
-        const int txs = tx + (((8 - tx) % 32) + 32) % 32;
-        const size_t tile_bytes = (size_t)txs * g.td[1] * g.td[2] * 2 * sizeof(float);
-        int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
-        for (int v0 = 0; v0 < nvol; v0 += vchunk) {
-            int nv = std::min(vchunk, nvol - v0);
-            size_t smem = tile_bytes * nv;
-            const float2 *cv = c + (long)v0 * pts_.M;
-            float2 *gv = grid + (long)v0 * gvol;
-            dim3 gd(nsub_);
-            if (dim_ == 2) {
-                LC_W_SWITCH(w_, (launch_spread_warp_w<2, (WW <= 8 ? WW : 8)>(
-                                    gd, smem, ctx.stream(), pts_, g, txs, cv, pts_.M, nv, perm_.get(),
-                                    subs_.get(), gv, gvol, mode, shifts_)));
-            } else {
-                LC_W_SWITCH(w_, (launch_spread_warp_w<3, (WW <= 8 ? WW : 8)>(
-                                    gd, smem, ctx.stream(), pts_, g, txs, cv, pts_.M, nv, perm_.get(),
-                                    subs_.get(), gv, gvol, mode, shifts_)));
-            }
-        }
-        return;
-    }
-    const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(float2);
-    int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
+    const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * 2 * sizeof(float);
+    const size_t bucket_bytes = (size_t)2 * maxsub_ * sizeof(int);
+    const int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
     for (int v0 = 0; v0 < nvol; v0 += vchunk) {
-        int nv = std::min(vchunk, nvol - v0);
-        size_t smem = tile_bytes * nv;
+        const int nv = std::min(vchunk, nvol - v0);
+        const size_t smem = tile_bytes * nv + bucket_bytes;
+        LC_REQUIRE(smem <= ctx.max_smem(), "NUFFT spread: tile does not fit shared memory");
         const float2 *cv = c + (long)v0 * pts_.M;
         float2 *gv = grid + (long)v0 * gvol;
         dim3 gd(nsub_);
         if (dim_ == 2) {
-            LC_W_SWITCH(w_, (launch_spread_w<2, WW>(gd, 256, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
-                                                   perm_.get(), subs_.get(), gv, gvol, mode, shifts_)));
+            LC_W_SWITCH(w_, (launch_spread_w<2, WW>(gd, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
+                                                   perm_.get(), subs_.get(), gv, gvol, mode, shifts_,
+                                                   maxsub_)));
         } else {
-            LC_W_SWITCH(w_, (launch_spread_w<3, WW>(gd, 256, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
-                                                   perm_.get(), subs_.get(), gv, gvol, mode, shifts_)));
+            LC_W_SWITCH(w_, (launch_spread_w<3, WW>(gd, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
+                                                   perm_.get(), subs_.get(), gv, gvol, mode, shifts_,
+                                                   maxsub_)));
         }
     }
 }

@@ -92,6 +92,7 @@ class NufftPlan {
     DevBuf<int> perm_;
     DevBuf<int4> subs_;
     int nsub_ = 0;
+    int maxsub_ = 1024;  // most points of one spreading subproblem
     DevBuf<float2> grid_, h1_, h2_;
 };
 
