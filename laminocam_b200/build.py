@@ -65,9 +65,43 @@ def build(verbose: bool = False, extra=()) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_drivers()
     if verbose:
         print(LIB)
     return LIB
+
+
+DRIVERS = os.path.join(HERE, "drivers")
+BIN = os.path.join(HERE, "bin")
+DRIVER_COMMON = ["lc_toml.cpp", "lc_io.cpp", "lc_config.cpp"]
+EXECUTABLES = {"recon_lamino": DRIVER_COMMON + ["recon_lamino.cpp"],
+               "recon_tomo": DRIVER_COMMON + ["recon_tomo.cpp"],
+               "lc_convert": ["lc_io.cpp", "lc_convert.cpp"]}
+
+
+def host_cxx() -> str:
+    for cand in (os.environ.get("HOSTCXX"), shutil.which("g++"), "/usr/bin/g++"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("g++ not found")
+
+
+def build_drivers() -> None:
+    """Builds the host-side drivers (plain C++17 over the C ABI) into bin/."""
+    os.makedirs(BIN, exist_ok=True)
+    deps = [os.path.join(DRIVERS, f) for f in os.listdir(DRIVERS)] + [os.path.join(ROOT, "include", "laminocam.h")]
+    newest = max(os.path.getmtime(d) for d in deps)
+    for exe, srcs in EXECUTABLES.items():
+        out = os.path.join(BIN, exe)
+        if os.path.exists(out) and os.path.getmtime(out) >= max(newest, os.path.getmtime(LIB)):
+            continue
+        cmd = [host_cxx(), "-std=c++17", "-O2", "-Wall", "-o", out,
+               *[os.path.join(DRIVERS, s) for s in srcs]]
+        if exe != "lc_convert":
+            cmd += ["-L", HERE, "-llaminocam_b200", "-Wl,-rpath,$ORIGIN/.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"building {exe} failed:\n{r.stdout}\n{r.stderr}")
 
 
 if __name__ == "__main__":
