@@ -299,7 +299,7 @@ void lc_server_s::worker_loop(int w) {
 namespace {
 
 int submit(lc_server sv, const std::shared_ptr<Job> &j, long long *job_id) {
-    return run_guarded(sv->err, [&] {
+    const int rc = run_guarded(sv->err, [&] {
         LC_REQUIRE(job_id, "NULL job id");
         LC_REQUIRE(j->in && j->out, "NULL input or output buffer");
         LC_REQUIRE(j->d0 > 0 && j->d1 > 0 && j->d2 > 0, "sizes must be positive");
@@ -324,6 +324,9 @@ int submit(lc_server sv, const std::shared_ptr<Job> &j, long long *job_id) {
         sv->queue.push_back(j);
         *job_id = j->id;
     });
+    // wake an idle worker: the new job may be the head of the queue
+    if (rc == LC_OK) sv->cv_work.notify_all();
+    return rc;
 }
 
 // nearest-rank percentile
