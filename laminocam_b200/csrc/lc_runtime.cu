@@ -2,6 +2,9 @@
 #include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
+
+#include <nvtx3/nvToolsExt.h>
 
 #include "lc_runtime.hpp"
 
@@ -188,7 +191,21 @@ Profiler::~Profiler() {
     for (auto e : pool) cudaEventDestroy(e);
 }
 
+// LC_NVTX=1 names every profiler section with an NVTX range (for example to
+// select one section's kernels in a profiler with --nvtx-include)
+static bool nvtx_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("LC_NVTX");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
 ProfScope::ProfScope(Context &ctx, int sec, double bytes) : ctx_(&ctx) {
+    if (nvtx_enabled()) {
+        nvtxRangePushA(prof_name(sec));
+        nvtx_ = true;
+    }
     if (!ctx.prof.on) return;
     // bound the number of live events: fold finished records into the totals
     if (ctx.prof.recs.size() >= 50000) ctx.prof.collect();
@@ -199,6 +216,7 @@ ProfScope::ProfScope(Context &ctx, int sec, double bytes) : ctx_(&ctx) {
 }
 
 ProfScope::~ProfScope() {
+    if (nvtx_) nvtxRangePop();
     if (idx_ < 0) return;
     cudaEventRecord(ctx_->prof.recs[idx_].b, ctx_->stream());
 }

@@ -175,6 +175,7 @@ class ProfScope {
   private:
     Context *ctx_;
     int idx_ = -1;
+    bool nvtx_ = false;
 };
 
 class Context {

@@ -97,7 +97,9 @@ def test_graph_replay_with_tolerance_stop(lc):
     th = np.arange(nth) * np.pi / nth
     A = lc.PointSpreadFunction2D(lc.PolarGrid2D(th, n), n, 1)
     rng = np.random.default_rng(6)
-    y = torch.as_tensor(rng.standard_normal((1, n, n)).astype(np.float32), device="cuda")
+    # a right-hand side in the range of the operator, so that CG converges
+    xt = torch.as_tensor(rng.standard_normal((1, n, n)).astype(np.float32), device="cuda")
+    y = A.convolve(xt)
     x0 = torch.zeros_like(y)
     a, ia = lc.cgsolver(A, y, x0, 200, 1e-2, 0.0, return_info=True)
     b, ib = lc.cgsolver(A, y, x0, 200, 1e-2, 0.0, return_info=True, use_graph=True)
