@@ -53,6 +53,14 @@ struct AxisFFT {
 
 void launch_axis_fft(Context &ctx, const AxisFFT &a);
 
+// The Toeplitz z stage in place on `data` (n_inner columns, rows of n_inner
+// complex values): zero-pad n_in rows to L, FFT, multiply row f by the real
+// spec[f * n_inner + column], inverse FFT, keep n_out rows.  Register-resident
+// kernels for L in {16, 24, 32, 36, 48, 64, 72, 96, 128}; returns false for
+// other lengths (the caller then uses launch_axis_fft).
+bool launch_zconv(cudaStream_t st, float2 *data, long n_inner, int L, int n_in, int n_out,
+                  const float *spec);
+
 // Same transform with a caller-supplied FP32 plan (radices and twiddle table)
 // on an explicit stream; touches no context, plan cache or allocator.
 void launch_axis_fft_f32_with_plan(cudaStream_t stream, size_t max_smem, const AxisFFT &a,

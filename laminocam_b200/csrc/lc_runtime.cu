@@ -1,4 +1,5 @@
 // Host runtime: context, FFT plan cache and twiddle tables.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -237,9 +238,23 @@ Context::Context(int device, cudaStream_t stream) : device_(device) {
     }
 }
 
+void *Context::pinned_scratch(size_t bytes) {
+    if (bytes > pinned_bytes_) {
+        // pinned allocation and release synchronise the whole device, so the
+        // buffer is grown rarely and kept for the context's lifetime
+        if (pinned_) cudaFreeHost(pinned_);
+        pinned_ = nullptr;
+        pinned_bytes_ = 0;
+        LC_CUDA(cudaMallocHost(&pinned_, std::max<size_t>(bytes, 4096)));
+        pinned_bytes_ = std::max<size_t>(bytes, 4096);
+    }
+    return pinned_;
+}
+
 Context::~Context() {
     cudaSetDevice(device_);
     plans_.clear();
+    if (pinned_) cudaFreeHost(pinned_);
     if (own_stream_) {
         cudaStreamSynchronize(own_stream_);
         cudaStreamDestroy(own_stream_);

@@ -188,6 +188,10 @@ class Context {
     // the context's private stream: graphs are captured there (the caller's
     // stream may be the legacy default stream, which cannot capture)
     cudaStream_t capture_stream() const { return own_stream_; }
+    // A pinned host buffer of at least `bytes`, owned by the context and
+    // reused by its solvers for device-to-host copies of small state.  The
+    // pointer stays valid until a larger request or the context's end.
+    void *pinned_scratch(size_t bytes);
     PlanCache &plans() { return plans_; }
     int num_sms() const { return num_sms_; }
     size_t max_smem() const { return max_smem_; }
@@ -200,6 +204,8 @@ class Context {
     cudaStream_t stream_;
     cudaStream_t own_stream_ = nullptr;
     PlanCache plans_;
+    void *pinned_ = nullptr;
+    size_t pinned_bytes_ = 0;
     int num_sms_ = 148;
     size_t max_smem_ = 227 * 1024;
 };

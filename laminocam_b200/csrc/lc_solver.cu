@@ -291,13 +291,9 @@ Solver::Solver(Context &ctx, long n) : n_(n) {
     counter_.alloc(1, s);
     counter_.zero(s);
     st_.alloc(1, s);
-    LC_CUDA(cudaMallocHost((void **)&host_st_, sizeof(CGState)));
 }
 
-Solver::~Solver() {
-    graph_.reset();
-    if (host_st_) cudaFreeHost(host_st_);
-}
+Solver::~Solver() { graph_.reset(); }
 
 void Solver::capture(Context &ctx, const std::function<void()> &body) {
     // Capturing records the launches without running them.  It happens on the
@@ -385,6 +381,7 @@ void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, i
 void Solver::cg(Context &ctx, const Operator &A, const float *y, float *x, const SolverParams &p,
                 SolverStats *stats) {
     cudaStream_t s = ctx.stream();
+    host_st_ = static_cast<CGState *>(ctx.pinned_scratch(sizeof(CGState)));
     reset_state_kernel<<<1, 1, 0, s>>>(st_.get());
     LC_CHECK_LAUNCH();
     int poll = (p.tol > 0 || p.xtol > 0) ? p.poll_every : 0;
@@ -406,6 +403,7 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
                            float *x, const SolverParams &p, SolverStats *stats) {
     cudaStream_t s = ctx.stream();
     LC_REQUIRE(dims[0] * dims[1] * dims[2] == n_, "split_bregman: dims do not match the solver size");
+    host_st_ = static_cast<CGState *>(ctx.pinned_scratch(sizeof(CGState)));
     for (int a = 0; a < 3; ++a) {
         d_[a].ensure(n_, s);
         b_[a].ensure(n_, s);

@@ -75,7 +75,7 @@ class Solver {
     DevBuf<double> part_;
     DevBuf<unsigned> counter_;
     DevBuf<CGState> st_;
-    CGState *host_st_ = nullptr;
+    CGState *host_st_ = nullptr;  // the context's pinned scratch, set per solve
 };
 
 }  // namespace lc

@@ -1,0 +1,176 @@
+// The z stage of the 3D Toeplitz apply as one register-resident kernel.
+//
+// For every column (ky, kx) of the half spectrum, the stage takes the n1
+// values along z, zero-pads them to L = P1, transforms, multiplies by the real
+// spectrum column, transforms back and keeps the first n1 values (the cropped
+// circular convolution of include/toeplitz.h:95-129 along z).  L is small for
+// laminography volumes (P1 <= 128), so a line is split as L = A * B over
+// max(A, B) threads: each thread keeps A (then B) elements in registers and
+// does its radix-A (radix-B) DFTs there, and the line crosses shared memory
+// once per transform.  The generic shared-memory Stockham kernel instead
+// passes through shared memory and a barrier at every radix stage, and spends
+// about 280 instructions per element at L = 48.
+//
+// Decomposition (n = b + B a, k = k1 + A k2, w = exp(-2 pi i / L)):
+//   Y_b[k1]        = sum_a x[b + B a] w^(B a k1)            (DFT_A in thread b)
+//   X[k1 + A k2]   = sum_b (Y_b[k1] w^(b k1)) w^(A b k2)    (DFT_B in thread k1)
+// and the inverse runs the same steps backwards with conjugate roots.
+#include "lc_fft.hpp"
+
+namespace lc {
+namespace {
+
+// exp(sign * 2 pi i m / N) for the composite radices 6, 12 and 16
+template <int N>
+__device__ __forceinline__ float2 unit_root(int m, int sign) {
+    const float h = 0.70710678118654752440f, c30 = 0.86602540378443864676f;
+    const float c22 = 0.92387953251128675613f, s22 = 0.38268343236508977173f;
+    float c = 1.f, s = 0.f;
+    if constexpr (N == 6) {
+        const float cs[6] = {1.f, 0.5f, -0.5f, -1.f, -0.5f, 0.5f};
+        const float sn[6] = {0.f, c30, c30, 0.f, -c30, -c30};
+        c = cs[m];
+        s = sn[m];
+    } else if constexpr (N == 12) {
+        const float cs[12] = {1.f, c30, 0.5f, 0.f, -0.5f, -c30, -1.f, -c30, -0.5f, 0.f, 0.5f, c30};
+        const float sn[12] = {0.f, 0.5f, c30, 1.f, c30, 0.5f, 0.f, -0.5f, -c30, -1.f, -c30, -0.5f};
+        c = cs[m];
+        s = sn[m];
+    } else if constexpr (N == 16) {
+        const float cs[16] = {1.f, c22, h, s22, 0.f, -s22, -h, -c22, -1.f, -c22, -h, -s22, 0.f, s22, h, c22};
+        const float sn[16] = {0.f, s22, h, c22, 1.f, c22, h, s22, 0.f, -s22, -h, -c22, -1.f, -c22, -h, -s22};
+        c = cs[m];
+        s = sn[m];
+    }
+    return make_float2(c, sign * s);
+}
+
+// N = R1 * R2 from two small DFTs (same decomposition as the kernel)
+template <int R1, int R2>
+__device__ __forceinline__ void dft_composite(float2 *v, int sign) {
+    constexpr int N = R1 * R2;
+    float2 y[R2][R1];
+#pragma unroll
+    for (int b = 0; b < R2; ++b) {
+        float2 t[R1];
+#pragma unroll
+        for (int a = 0; a < R1; ++a) t[a] = v[b + R2 * a];
+        dft_small<float2, R1>(t, sign);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) y[b][k1] = (b * k1 == 0) ? t[k1] : cmul(t[k1], unit_root<N>(b * k1, sign));
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+        float2 t[R2];
+#pragma unroll
+        for (int b = 0; b < R2; ++b) t[b] = y[b][k1];
+        dft_small<float2, R2>(t, sign);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = t[k2];
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void dft_reg(float2 *v, int sign) {
+    if constexpr (N == 6) dft_composite<3, 2>(v, sign);
+    else if constexpr (N == 12) dft_composite<3, 4>(v, sign);
+    else if constexpr (N == 16) dft_composite<4, 4>(v, sign);
+    else dft_small<float2, N>(v, sign);
+}
+
+template <int A, int B, int C>
+__global__ void __launch_bounds__(C *(A > B ? A : B))
+    zconv_kernel(float2 *data, long n_inner, int n_in, int n_out, const float *__restrict__ spec) {
+    constexpr int L = A * B;
+    constexpr int TPL = A > B ? A : B;
+    __shared__ float2 sm[L * C];
+    __shared__ float2 tw[L];  // exp(-2 pi i m / L)
+    for (int m = threadIdx.x; m < L; m += blockDim.x) {
+        float s, c;
+        sincospif(2.0f * (float)m / (float)L, &s, &c);
+        tw[m] = make_float2(c, -s);
+    }
+    const int cl = threadIdx.x % C, j = threadIdx.x / C;
+    const long col = (long)blockIdx.x * C + cl;
+    const bool valid = col < n_inner;
+    float2 v[TPL];
+    // forward, radix A in thread b = j: x[b + B a] -> Y_b[k1] w^(b k1)
+    if (j < B) {
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+            const int n = j + B * a;
+            v[a] = (valid && n < n_in) ? data[(long)n * n_inner + col] : make_float2(0.f, 0.f);
+        }
+    }
+    __syncthreads();  // twiddle table ready
+    if (j < B) {
+        dft_reg<A>(v, -1);
+#pragma unroll
+        for (int k1 = 1; k1 < A; ++k1) v[k1] = cmul(v[k1], tw[(j * k1) % L]);
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) sm[(k1 * B + j) * C + cl] = v[k1];
+    }
+    __syncthreads();
+    // radix B in thread k1 = j, spectral multiply, inverse radix B
+    if (j < A) {
+#pragma unroll
+        for (int b = 0; b < B; ++b) v[b] = sm[(j * B + b) * C + cl];
+        dft_reg<B>(v, -1);
+#pragma unroll
+        for (int k2 = 0; k2 < B; ++k2) {
+            const float r = valid ? __ldg(spec + (long)(j + A * k2) * n_inner + col) : 0.f;
+            v[k2] = make_float2(v[k2].x * r, v[k2].y * r);
+        }
+        dft_reg<B>(v, +1);
+#pragma unroll
+        for (int b = 1; b < B; ++b) {
+            const float2 w = tw[(j * b) % L];
+            v[b] = cmul(v[b], make_float2(w.x, -w.y));
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) sm[(j * B + b) * C + cl] = v[b];
+    }
+    __syncthreads();
+    // inverse radix A in thread b = j, keep the first n_out rows
+    if (j < B) {
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) v[k1] = sm[(k1 * B + j) * C + cl];
+        dft_reg<A>(v, +1);
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+            const int n = j + B * a;
+            if (valid && n < n_out) data[(long)n * n_inner + col] = v[a];
+        }
+    }
+}
+
+template <int A, int B, int C>
+void launch_z(cudaStream_t st, float2 *data, long n_inner, int n_in, int n_out, const float *spec) {
+    constexpr int TPL = A > B ? A : B;
+    const long blocks = (n_inner + C - 1) / C;
+    LC_REQUIRE(blocks < (1L << 31), "z convolution: grid too large");
+    zconv_kernel<A, B, C><<<(unsigned)blocks, C * TPL, 0, st>>>(data, n_inner, n_in, n_out, spec);
+    LC_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+bool launch_zconv(cudaStream_t st, float2 *data, long n_inner, int L, int n_in, int n_out,
+                  const float *spec) {
+    LC_REQUIRE(n_in >= 0 && n_in <= L && n_out >= 0 && n_out <= L, "z convolution: bad lengths");
+    if (n_inner <= 0 || n_out == 0) return true;
+    switch (L) {
+        case 16: launch_z<4, 4, 32>(st, data, n_inner, n_in, n_out, spec); return true;
+        case 24: launch_z<8, 3, 32>(st, data, n_inner, n_in, n_out, spec); return true;
+        case 32: launch_z<8, 4, 32>(st, data, n_inner, n_in, n_out, spec); return true;
+        case 36: launch_z<6, 6, 32>(st, data, n_inner, n_in, n_out, spec); return true;
+        case 48: launch_z<8, 6, 32>(st, data, n_inner, n_in, n_out, spec); return true;
+        case 64: launch_z<8, 8, 32>(st, data, n_inner, n_in, n_out, spec); return true;
+        case 72: launch_z<8, 9, 16>(st, data, n_inner, n_in, n_out, spec); return true;
+        case 96: launch_z<8, 12, 16>(st, data, n_inner, n_in, n_out, spec); return true;
+        case 128: launch_z<8, 16, 16>(st, data, n_inner, n_in, n_out, spec); return true;
+        default: return false;
+    }
+}
+
+}  // namespace lc

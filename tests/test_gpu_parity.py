@@ -212,6 +212,22 @@ def test_toeplitz_matches_nufft_normal_operator_gpu(lc):
     assert O.rel_l2(b, a) < 5e-5
 
 
+@pytest.mark.parametrize("n1", [5, 8, 11, 15, 17, 21, 29, 33, 43, 63])
+def test_toeplitz3d_matches_nufft_normal_operator_gpu(lc, n1):
+    """3D A^T A by the Toeplitz apply against the NUFFT normal operator for
+    thicknesses whose P1 (9, 16, 24, 32, 36, 48, 64, 72, 96, 128) cover every
+    register-resident z kernel and, with P1 = 9, the generic fallback."""
+    rng = np.random.default_rng(9 + n1)
+    n, nth = 15, 24
+    th = np.arange(nth) * 2 * np.pi / nth
+    g = -np.deg2rad(25.0)
+    pg = lc.PolarGrid(th, np.full(nth, g), np.zeros(nth), n, n)
+    x = rng.random((n1, n, n)).astype(np.float32)
+    a = to_np(lc.sysmat(x, pg))
+    b = to_np(lc.PointSpreadFunction(pg, (n1, n, n)).convolve(x))
+    assert O.rel_l2(b, a) < 5e-5
+
+
 def test_toeplitz_slice_independence(lc):
     """tests/test_sysmat_toeplitz2d.cpp:98-137: batched slices equal single-slice runs."""
     rng = np.random.default_rng(8)
