@@ -11,7 +11,8 @@ tolerance 1e-6.
 
 A step is one complete reconstruction: normalisation and padding of the
 projections, geometry and bin sort, backprojection (type-1 NUFFT), FP64 PSF
-generation (no cache), 100 Split-Bregman outer iterations and the final crop.
+generation (no cache), 100 Split-Bregman outer iterations (the first one eager,
+the other 99 replayed as a CUDA graph) and the final crop.
 `value` is measured with the projections resident in HBM (lc_mbir3d_device);
 `e2e` through the host-buffer API (lc_mbir3d) with a pinned host copy in and
 the reconstruction copied back out every step.
@@ -80,17 +81,18 @@ def make_projections(lc):
 
 
 class ClockSampler:
-    """Samples the SM clock and the clock-event (throttle) reasons every 0.2 s
-    during the timed region: read-only NVML queries in this process, or
-    nvidia-smi when NVML cannot be loaded."""
+    """Samples the SM clock and the clock-event (throttle) reasons during the
+    timed region (every `interval` seconds): read-only NVML queries in this
+    process, or nvidia-smi when NVML cannot be loaded."""
 
     REASONS = [("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
                ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
                ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
                ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap")]
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, interval: float = 1.0):
         self.index = index
+        self.interval = interval
         self.samples = []  # (sm_mhz, sm_max_mhz, [active reasons])
         self.source = None
         self._stop = threading.Event()
@@ -109,7 +111,7 @@ class ClockSampler:
             sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
             bits = get(h) if get else 0
             self.samples.append((float(sm), float(mx), [n for n, m in masks if m and bits & m]))
-            self._stop.wait(0.2)
+            self._stop.wait(self.interval)
 
     def _smi(self):
         q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
@@ -127,7 +129,7 @@ class ClockSampler:
                     self.samples.append((float(v[0]), float(v[1]), act))
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(self.interval)
 
     def _run(self):
         try:
@@ -308,6 +310,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clock-interval", type=float, default=1.0,
+                    help="seconds between clock samples during the timed region")
     ap.add_argument("--no-mix", action="store_true",
                     help="skip the served-vs-plain 64-job 2D mix")
     ap.add_argument("--small", action="store_true",
@@ -351,8 +355,9 @@ def main():
     nth, nr, nc = dproj.shape
     gam = np.full(nth, gamma)
     bet = np.zeros(nth)
+    # the outer iterations replay as a CUDA graph (the first one runs eagerly)
     params = lc.ReconParams(regularizer="split_bregman", recon_dims=RECON_DIMS, max_iters=OUTER,
-                            inner_iters=1, lam=LAM, mu=MU, tol=1e-5, xtol=0.0).to_c()
+                            inner_iters=1, lam=LAM, mu=MU, tol=1e-5, xtol=0.0, use_graph=True).to_c()
     rd = (C.c_int * 3)(*RECON_DIMS)
     _, tp = lc._dptr(theta)
     _, gp = lc._dptr(gam)
@@ -414,7 +419,7 @@ def main():
         step_device()
     torch.cuda.synchronize()
 
-    with ClockSampler(local) as clk:
+    with ClockSampler(local, args.clock_interval) as clk:
         launches0 = lib.lc_kernel_launches()
         total_ms, lats = timed(step_device, args.steps)
         launches = lib.lc_kernel_launches() - launches0

@@ -245,7 +245,7 @@ __global__ void bin_scatter_kernel(PolarPts pts, GridCfg g, int W, int *cursor, 
 constexpr int kSpreadThreads = 256;
 
 template <int DIM, int W>
-__global__ void __launch_bounds__(kSpreadThreads, 2)
+__global__ void __launch_bounds__(kSpreadThreads, 4)
     spread_kernel(PolarPts pts, GridCfg g, const float2 *__restrict__ c, long cstride, int nvol,
                   const int *__restrict__ perm, const int4 *__restrict__ subs,
                   float2 *__restrict__ grid, long gstride, int mode,
@@ -271,14 +271,19 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
     float *tre = reinterpret_cast<float *>(smem_raw);
     float *tim = tre + (long)nvol * tsize;
     int *order = reinterpret_cast<int *>(tim + (long)nvol * tsize);
-    int *key = order + maxpts;
+    constexpr int kKeys = 8;  // points per thread in the bucketing pass (maxpts <= 8 * threads)
+    int key[kKeys];
     const int tid = threadIdx.x;
     for (int idx = tid; idx < 2 * nvol * tsize; idx += blockDim.x) tre[idx] = 0.f;
     if (tid < 32) cnt[tid] = 0;
     __syncthreads();
 
     // ---- bucket the points by the bank of their footprint corner ----
-    for (int p = tid; p < sp.z; p += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < kKeys; ++q) {
+        const int p = tid + q * (int)blockDim.x;
+        key[q] = -1;
+        if (p >= sp.z) continue;
         const int j = perm[sp.y + p];
         PointInfo pi;
         point_at(pts, j, pi);
@@ -296,7 +301,7 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
             const int b = corner & 31;
             k = (b << 16) | atomicAdd(&cnt[b], 1);
         }
-        key[p] = k;
+        key[q] = k;
     }
     __syncthreads();
     if (tid < 32) {
@@ -312,9 +317,10 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
         if (tid == 0) maxcnt = m;
     }
     __syncthreads();
-    for (int p = tid; p < sp.z; p += blockDim.x) {
-        const int k = key[p];
-        if (k >= 0) order[start[k >> 16] + (k & 0xffff)] = p;
+#pragma unroll
+    for (int q = 0; q < kKeys; ++q) {
+        const int k = key[q];
+        if (k >= 0) order[start[k >> 16] + (k & 0xffff)] = tid + q * (int)blockDim.x;
     }
     __syncthreads();
 
@@ -547,13 +553,16 @@ void launch_interp_w(dim3 grid, int threads, size_t smem, cudaStream_t st, const
 
 GridCfg make_cfg(int dim, const int nf[3], const int bs[3], const int nb[3], int w, double beta) {
     GridCfg g{};
-    int hw = (w + 1) / 2;
+    // A point in cell c covers cells [c - floor(w/2), c + ceil(w/2)] (first
+    // covered cell ceil(u - w/2) for u in [c, c+1)), so a bin of bs cells
+    // needs a tile of bs + w cells starting floor(w/2) cells before it.
+    const int lo = w / 2;
     for (int d = 0; d < 3; ++d) {
         g.nf[d] = nf[d];
         g.bs[d] = bs[d];
         g.nb[d] = nb[d];
-        g.hw[d] = d < dim ? hw : 0;
-        g.td[d] = d < dim ? bs[d] + 2 * hw : 1;
+        g.hw[d] = d < dim ? lo : 0;
+        g.td[d] = d < dim ? bs[d] + w : 1;
     }
     g.beta = (float)beta;
     return g;
@@ -576,7 +585,7 @@ NufftPlan::NufftPlan(Context &ctx, const PolarGeometry &g, const int modes[3], d
         nf_[d] = d < dim_ ? (int)next_smooth23(std::max(2 * modes_[d], 2 * w_)) : 1;
     }
     const int bs2[3] = {32, 32, 1};
-    const int bs3[3] = {32, 8, 8};
+    const int bs3[3] = {16, 8, 8};
     maxsub_ = dim_ == 2 ? 1024 : 2048;
     for (int d = 0; d < 3; ++d) {
         bs_[d] = std::min(dim_ == 2 ? bs2[d] : bs3[d], nf_[d]);
@@ -644,7 +653,8 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
     // values read once, fine grid written once (plus the permutation)
     ProfScope ps(ctx, PS_SPREAD, (double)nvol * (8.0 * pts_.M + 8.0 * gvol) + 4.0 * pts_.M);
     const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * 2 * sizeof(float);
-    const size_t bucket_bytes = (size_t)2 * maxsub_ * sizeof(int);
+    const size_t bucket_bytes = (size_t)maxsub_ * sizeof(int);
+    LC_REQUIRE(maxsub_ <= 8 * kSpreadThreads, "NUFFT spread: subproblem larger than the bucketing pass");
     const int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
     for (int v0 = 0; v0 < nvol; v0 += vchunk) {
         const int nv = std::min(vchunk, nvol - v0);

@@ -185,66 +185,60 @@ __global__ void __launch_bounds__(kThreads) p_update_kernel(float *p, const floa
 }
 
 struct Dims {
-    long n1, n2, n3;
+    int n1, n2, n3;
 };
 
-__device__ __forceinline__ float at(const float *f, long i, long j, long k, const Dims &d) {
-    return (i >= 0 && j >= 0 && k >= 0 && i < d.n1 && j < d.n2 && k < d.n3)
-               ? f[(i * d.n2 + j) * d.n3 + k]
-               : 0.f;
-}
+// The stencil kernels run one thread per voxel on a (32 x 8) x n1 grid of
+// CTAs: k and j come from the CTA and thread indices and i = blockIdx.z, so
+// no index is divided; offsets are 32-bit (the host checks the size).
+#define LC_VOXEL_INDEX(dm)                                  \
+    const int k = blockIdx.x * 32 + threadIdx.x;            \
+    const int j = blockIdx.y * 8 + threadIdx.y;             \
+    const int i = blockIdx.z;                               \
+    if (k >= (dm).n3 || j >= (dm).n2) return;               \
+    const int sj = (dm).n3, si = (dm).n2 * (dm).n3;         \
+    const int idx = i * si + j * sj + k
 
 // rhs = yT - mu * div(d - b); div = D_n3(v0) + D_n2(v1) + D_n1(v2), zero padded
-__global__ void __launch_bounds__(kThreads) sb_rhs_kernel(const float *__restrict__ yT,
-                                                         const float *d0, const float *d1,
-                                                         const float *d2, const float *b0,
-                                                         const float *b1, const float *b2,
-                                                         float *rhs, Dims dm, float mu,
-                                                         const CGState *st) {
+__global__ void __launch_bounds__(256) sb_rhs_kernel(const float *__restrict__ yT,
+                                                     const float *__restrict__ d0,
+                                                     const float *__restrict__ d1,
+                                                     const float *__restrict__ d2,
+                                                     const float *__restrict__ b0,
+                                                     const float *__restrict__ b1,
+                                                     const float *__restrict__ b2, float *rhs,
+                                                     Dims dm, float mu, const CGState *st) {
     if (st->sb_done) return;
-    long total_n = dm.n1 * dm.n2 * dm.n3;
-    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total_n;
-         idx += (long)gridDim.x * blockDim.x) {
-        long i = idx / (dm.n2 * dm.n3);
-        long rr = idx - i * dm.n2 * dm.n3;
-        long j = rr / dm.n3, k = rr - j * dm.n3;
-        float dv = 0.5f * ((at(d0, i, j, k + 1, dm) - at(b0, i, j, k + 1, dm)) -
-                           (at(d0, i, j, k - 1, dm) - at(b0, i, j, k - 1, dm))) +
-                   0.5f * ((at(d1, i, j + 1, k, dm) - at(b1, i, j + 1, k, dm)) -
-                           (at(d1, i, j - 1, k, dm) - at(b1, i, j - 1, k, dm))) +
-                   0.5f * ((at(d2, i + 1, j, k, dm) - at(b2, i + 1, j, k, dm)) -
-                           (at(d2, i - 1, j, k, dm) - at(b2, i - 1, j, k, dm)));
-        rhs[idx] = fmaf(-mu, dv, yT[idx]);
-    }
+    LC_VOXEL_INDEX(dm);
+    auto v = [&](const float *d, const float *b, int o) { return d[idx + o] - b[idx + o]; };
+    const float dk = (k + 1 < dm.n3 ? v(d0, b0, 1) : 0.f) - (k >= 1 ? v(d0, b0, -1) : 0.f);
+    const float dj = (j + 1 < dm.n2 ? v(d1, b1, sj) : 0.f) - (j >= 1 ? v(d1, b1, -sj) : 0.f);
+    const float di = (i + 1 < dm.n1 ? v(d2, b2, si) : 0.f) - (i >= 1 ? v(d2, b2, -si) : 0.f);
+    rhs[idx] = fmaf(-mu, 0.5f * dk + 0.5f * dj + 0.5f * di, yT[idx]);
 }
 
 // g = grad x; t = g + b; s = |t|; d = max(0, s - lam/mu) t / (s + 1e-8); b += g - d
-__global__ void __launch_bounds__(kThreads) sb_shrink_kernel(const float *__restrict__ x, float *d0,
-                                                            float *d1, float *d2, float *b0,
-                                                            float *b1, float *b2, Dims dm,
-                                                            float thresh, const CGState *st) {
+__global__ void __launch_bounds__(256) sb_shrink_kernel(const float *__restrict__ x, float *d0,
+                                                        float *d1, float *d2, float *b0, float *b1,
+                                                        float *b2, Dims dm, float thresh,
+                                                        const CGState *st) {
     if (st->sb_done) return;
-    long total_n = dm.n1 * dm.n2 * dm.n3;
-    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total_n;
-         idx += (long)gridDim.x * blockDim.x) {
-        long i = idx / (dm.n2 * dm.n3);
-        long rr = idx - i * dm.n2 * dm.n3;
-        long j = rr / dm.n3, k = rr - j * dm.n3;
-        float g0 = 0.5f * (at(x, i, j, k + 1, dm) - at(x, i, j, k - 1, dm));
-        float g1 = 0.5f * (at(x, i, j + 1, k, dm) - at(x, i, j - 1, k, dm));
-        float g2 = 0.5f * (at(x, i + 1, j, k, dm) - at(x, i - 1, j, k, dm));
-        float t0 = g0 + b0[idx], t1 = g1 + b1[idx], t2 = g2 + b2[idx];
-        float s = sqrtf(t0 * t0 + t1 * t1 + t2 * t2);
-        float m = fmaxf(0.f, s - thresh);
-        float inv = 1.0f / (s + 1e-8f);
-        float e0 = m * (t0 * inv), e1 = m * (t1 * inv), e2 = m * (t2 * inv);
-        d0[idx] = e0;
-        d1[idx] = e1;
-        d2[idx] = e2;
-        b0[idx] = b0[idx] + (g0 - e0);
-        b1[idx] = b1[idx] + (g1 - e1);
-        b2[idx] = b2[idx] + (g2 - e2);
-    }
+    LC_VOXEL_INDEX(dm);
+    const float g0 = 0.5f * ((k + 1 < dm.n3 ? x[idx + 1] : 0.f) - (k >= 1 ? x[idx - 1] : 0.f));
+    const float g1 = 0.5f * ((j + 1 < dm.n2 ? x[idx + sj] : 0.f) - (j >= 1 ? x[idx - sj] : 0.f));
+    const float g2 = 0.5f * ((i + 1 < dm.n1 ? x[idx + si] : 0.f) - (i >= 1 ? x[idx - si] : 0.f));
+    const float c0 = b0[idx], c1 = b1[idx], c2 = b2[idx];
+    const float t0 = g0 + c0, t1 = g1 + c1, t2 = g2 + c2;
+    const float s = sqrtf(t0 * t0 + t1 * t1 + t2 * t2);
+    const float m = fmaxf(0.f, s - thresh);
+    const float inv = 1.0f / (s + 1e-8f);
+    const float e0 = m * (t0 * inv), e1 = m * (t1 * inv), e2 = m * (t2 * inv);
+    d0[idx] = e0;
+    d1[idx] = e1;
+    d2[idx] = e2;
+    b0[idx] = c0 + (g0 - e0);
+    b1[idx] = c1 + (g1 - e1);
+    b2[idx] = c2 + (g2 - e2);
 }
 
 template <typename A>
@@ -421,9 +415,11 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
         AtA(in, out);
         launch_neg_laplacian_axpy(ctx, in, out, dcopy, mu);
     };
-    Dims dm{dims[0], dims[1], dims[2]};
-    unsigned gsz = (unsigned)std::max<long>(1, std::min<long>((n_ + kThreads - 1) / kThreads,
-                                                             (long)ctx.num_sms() * 16));
+    LC_REQUIRE(n_ < (1L << 31) && dims[0] < 65536 && dims[1] < 65536 * 8,
+               "split_bregman: volume too large for 32-bit indexing");
+    const Dims dm{(int)dims[0], (int)dims[1], (int)dims[2]};
+    const dim3 vblock(32, 8, 1);
+    const dim3 vgrid((unsigned)((dims[2] + 31) / 32), (unsigned)((dims[1] + 7) / 8), (unsigned)dims[0]);
     // one outer iteration: rhs, inner CG (warm start), shrinkage, change test.
     // Launches go to ctx.stream() as it is when the lambda runs (the capture
     // stream while a graph is recorded).
@@ -431,14 +427,14 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
         const cudaStream_t os = ctx.stream();
         {
             ProfScope ps1(ctx, PS_SB_VEC, 4.0 * n_ * 8.0);
-            sb_rhs_kernel<<<gsz, kThreads, 0, os>>>(yT, d_[0].get(), d_[1].get(), d_[2].get(),
+            sb_rhs_kernel<<<vgrid, vblock, 0, os>>>(yT, d_[0].get(), d_[1].get(), d_[2].get(),
                                                      b_[0].get(), b_[1].get(), b_[2].get(),
                                                      rhs_.get(), dm, mu, st_.get());
             LC_CHECK_LAUNCH();
         }
         cg_run(ctx, Ap, rhs_.get(), x, p.inner_iters, p.tol, p.xtol, p.fp32_scalars, 0, true, false);
         ProfScope ps2(ctx, PS_SB_VEC, 4.0 * n_ * 16.0);
-        sb_shrink_kernel<<<gsz, kThreads, 0, os>>>(x, d_[0].get(), d_[1].get(), d_[2].get(),
+        sb_shrink_kernel<<<vgrid, vblock, 0, os>>>(x, d_[0].get(), d_[1].get(), d_[2].get(),
                                                     b_[0].get(), b_[1].get(), b_[2].get(), dm,
                                                     p.lambda / p.mu, st_.get());
         LC_CHECK_LAUNCH();

@@ -151,42 +151,43 @@ __global__ void d2f_kernel(const double *__restrict__ in, float *__restrict__ ou
 // divergence of the reference GPU build (src/gpu/finitediff.cu:28-222):
 // per axis  lap_a(x)[i] = 0.5*(g[i+1] - g[i-1]),  g[k] = 0.5*(x[k+1] - x[k-1]),
 // g = 0 outside the volume and x = 0 outside the volume.
-__global__ void neg_lap_axpy_kernel(const float *__restrict__ x, float *__restrict__ y, long n1,
-                                    long n2, long n3, float mu) {
-    long total = n1 * n2 * n3;
-    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (long)gridDim.x * blockDim.x) {
-        long i = idx / (n2 * n3);
-        long r = idx - i * n2 * n3;
-        long j = r / n3, k = r - j * n3;
-        float c = x[idx];
-        float lap = 0.f;
-        // axis k (n3), stride 1
-        {
-            float p2 = (k + 2 < n3) ? x[idx + 2] : 0.f;
-            float m2 = (k - 2 >= 0) ? x[idx - 2] : 0.f;
-            float gp = (k + 1 < n3) ? 0.5f * (p2 - c) : 0.f;
-            float gm = (k - 1 >= 0) ? 0.5f * (c - m2) : 0.f;
-            lap += 0.5f * (gp - gm);
-        }
-        {
-            long s = n3;
-            float p2 = (j + 2 < n2) ? x[idx + 2 * s] : 0.f;
-            float m2 = (j - 2 >= 0) ? x[idx - 2 * s] : 0.f;
-            float gp = (j + 1 < n2) ? 0.5f * (p2 - c) : 0.f;
-            float gm = (j - 1 >= 0) ? 0.5f * (c - m2) : 0.f;
-            lap += 0.5f * (gp - gm);
-        }
-        {
-            long s = n2 * n3;
-            float p2 = (i + 2 < n1) ? x[idx + 2 * s] : 0.f;
-            float m2 = (i - 2 >= 0) ? x[idx - 2 * s] : 0.f;
-            float gp = (i + 1 < n1) ? 0.5f * (p2 - c) : 0.f;
-            float gm = (i - 1 >= 0) ? 0.5f * (c - m2) : 0.f;
-            lap += 0.5f * (gp - gm);
-        }
-        y[idx] = fmaf(-mu, lap, y[idx]);
+// One thread per voxel on a (32 x 8) x n1 grid of CTAs: (k, j) from the CTA
+// and thread indices, i = blockIdx.z, so no index division; 32-bit offsets
+// (the launcher checks n1 n2 n3 < 2^31).
+__global__ void __launch_bounds__(256) neg_lap_axpy_kernel(const float *__restrict__ x,
+                                                           float *__restrict__ y, int n1, int n2,
+                                                           int n3, float mu) {
+    const int k = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * 8 + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= n3 || j >= n2) return;
+    const int idx = (i * n2 + j) * n3 + k;
+    const float c = x[idx];
+    float lap = 0.f;
+    {  // axis k (n3), stride 1
+        const float p2 = (k + 2 < n3) ? x[idx + 2] : 0.f;
+        const float m2 = (k >= 2) ? x[idx - 2] : 0.f;
+        const float gp = (k + 1 < n3) ? 0.5f * (p2 - c) : 0.f;
+        const float gm = (k >= 1) ? 0.5f * (c - m2) : 0.f;
+        lap += 0.5f * (gp - gm);
     }
+    {  // axis j (n2)
+        const int s = n3;
+        const float p2 = (j + 2 < n2) ? x[idx + 2 * s] : 0.f;
+        const float m2 = (j >= 2) ? x[idx - 2 * s] : 0.f;
+        const float gp = (j + 1 < n2) ? 0.5f * (p2 - c) : 0.f;
+        const float gm = (j >= 1) ? 0.5f * (c - m2) : 0.f;
+        lap += 0.5f * (gp - gm);
+    }
+    {  // axis i (n1)
+        const int s = n2 * n3;
+        const float p2 = (i + 2 < n1) ? x[idx + 2 * s] : 0.f;
+        const float m2 = (i >= 2) ? x[idx - 2 * s] : 0.f;
+        const float gp = (i + 1 < n1) ? 0.5f * (p2 - c) : 0.f;
+        const float gm = (i >= 1) ? 0.5f * (c - m2) : 0.f;
+        lap += 0.5f * (gp - gm);
+    }
+    y[idx] = fmaf(-mu, lap, y[idx]);
 }
 
 inline unsigned grid_for(long n, int threads, int sms) {
@@ -199,8 +200,12 @@ inline unsigned grid_for(long n, int threads, int sms) {
 void launch_neg_laplacian_axpy(Context &ctx, const float *x, float *y, const long dims[3], float mu) {
     long n = dims[0] * dims[1] * dims[2];
     ProfScope ps(ctx, PS_NEG_LAP, 12.0 * n);
-    neg_lap_axpy_kernel<<<grid_for(n, 256, ctx.num_sms()), 256, 0, ctx.stream()>>>(
-        x, y, dims[0], dims[1], dims[2], mu);
+    LC_REQUIRE(n < (1L << 31) && dims[0] < 65536 && dims[1] < 65536 * 8,
+               "negative Laplacian: volume too large for 32-bit indexing");
+    const dim3 block(32, 8, 1);
+    const dim3 grid((unsigned)((dims[2] + 31) / 32), (unsigned)((dims[1] + 7) / 8), (unsigned)dims[0]);
+    neg_lap_axpy_kernel<<<grid, block, 0, ctx.stream()>>>(x, y, (int)dims[0], (int)dims[1],
+                                                          (int)dims[2], mu);
     LC_CHECK_LAUNCH();
 }
 
