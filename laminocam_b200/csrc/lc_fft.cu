@@ -91,6 +91,9 @@ __global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
     } else if (a.in_map == IN_MODES) {
         gap0 = a.n_in - a.n_in / 2;
         gap1 = L - a.n_in / 2;
+    } else if (a.in_map == IN_REAL_PACKED) {
+        gap0 = (a.n_in + 1) / 2;
+        gap1 = L;
     }
     const int gap = gap1 - gap0;
     for (int idx = tid; idx < (gap << logC); idx += nt) {
@@ -105,7 +108,9 @@ __global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
     const int nh = L / 2 + 1;
     if (rows) {
         const T lf = linefac ? linefac[0] : T(1);
-        const int per = a.in_map == IN_HERM ? L : a.n_in;
+        const int per = (a.in_map == IN_HERM || a.in_map == IN_C2R_PACK)
+                            ? L
+                            : (a.in_map == IN_REAL_PACKED ? (a.n_in + 1) / 2 : a.n_in);
         const int total = per * nlines;
         const unsigned long long per_magic = fast_div_magic((unsigned)max(per, 1));
         for (int base = tid; base < total; base += kBatch * nt) {
@@ -123,6 +128,24 @@ __global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
                     const int j = e < nh ? e : L - e;
                     v[u] = ld_elem<T, TI>(src + j);
                     if (e >= nh) v[u].y = -v[u].y;
+                    dst[u] = (e << logC) + cl;
+                } else if (a.in_map == IN_REAL_PACKED) {
+                    // z[e] = x[2e] + i x[2e+1]
+                    const T re = ld_elem<T, TI>(src + 2 * e).x;
+                    const T im = 2 * e + 1 < a.n_in ? ld_elem<T, TI>(src + 2 * e + 1).x : T(0);
+                    v[u] = mk<T>(re, im);
+                    dst[u] = (e << logC) + cl;
+                } else if (a.in_map == IN_C2R_PACK) {
+                    // Z[k] = (X[k] + conj X[L-k]) + i exp(i pi k / L) (X[k] - conj X[L-k])
+                    const V xa = ld_elem<T, TI>(src + e);
+                    const V xb = ld_elem<T, TI>(src + (L - e));
+                    const V sm = mk<T>(xa.x + xb.x, xa.y - xb.y);
+                    const V df = mk<T>(xa.x - xb.x, xa.y + xb.y);
+                    T sn, cs;
+                    if constexpr (std::is_same_v<T, double>) sincospi((double)e / (double)L, &sn, &cs);
+                    else sincospif((float)e / (float)L, &sn, &cs);
+                    const V wd = cmul(mk<T>(cs, sn), df);
+                    v[u] = mk<T>(sm.x - wd.y, sm.y + wd.x);
                     dst[u] = (e << logC) + cl;
                 } else {
                     v[u] = ld_elem<T, TI>(src + e);
@@ -210,7 +233,37 @@ __global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
         }
         return f;
     };
-    if (rows) {
+    if (rows && a.out_map == OUT_R2C_UNPACK) {
+        // X[k] = (Z[k] + conj Z[L-k]) / 2 - (i/2) exp(-i pi k / L) (Z[k] - conj Z[L-k])
+        for (int cl = 0; cl < nlines; ++cl) {
+            TO *dst = out + (o_base + cl) * a.out_ostride;
+            for (int k = tid; k < a.n_out; k += nt) {
+                const int k1 = k == L ? 0 : k;
+                const int k2 = k == 0 ? 0 : L - k;
+                const V za = buf[(k1 << logC) + cl];
+                const V zb = buf[(k2 << logC) + cl];
+                const V sm = mk<T>(T(0.5) * (za.x + zb.x), T(0.5) * (za.y - zb.y));
+                const V df = mk<T>(T(0.5) * (za.x - zb.x), T(0.5) * (za.y + zb.y));
+                T sn, cs;
+                if constexpr (std::is_same_v<T, double>) sincospi((double)k / (double)L, &sn, &cs);
+                else sincospif((float)k / (float)L, &sn, &cs);
+                const V wd = cmul(mk<T>(cs, -sn), df);  // exp(-i pi k / L) (Z[k] - conj Z[L-k]) / 2
+                T s = scale;
+                if (post) s *= post[k];
+                st_elem<T, TO>(dst + k, cscale(mk<T>(sm.x + wd.y, sm.y - wd.x), s));
+            }
+        }
+    } else if (rows && a.out_map == OUT_REAL_UNPACK) {
+        for (int cl = 0; cl < nlines; ++cl) {
+            TO *dst = out + (o_base + cl) * a.out_ostride;
+            for (int j = tid; j < a.n_out; j += nt) {
+                const V z = buf[((j >> 1) << logC) + cl];
+                T s = scale;
+                if (post) s *= post[j];
+                st_elem<T, TO>(dst + j, mk<T>(((j & 1) ? z.y : z.x) * s, T(0)));
+            }
+        }
+    } else if (rows) {
         for (int cl = 0; cl < nlines; ++cl) {
             TO *dst = out + (o_base + cl) * a.out_ostride;
             for (int j = tid; j < a.n_out; j += nt) {
@@ -439,9 +492,16 @@ TuneVal autotune(Context &ctx, const AxisFFT &a0, const FFTPlan &pl) {
 void launch_axis_fft(Context &ctx, const AxisFFT &a) {
     LC_REQUIRE(is_smooth23(a.L), "axis FFT length must be 2^p*3^q");
     LC_REQUIRE(a.n_in >= 0 && a.n_out >= 0, "axis FFT: bad lengths");
+    const bool packed_in = a.in_map == IN_REAL_PACKED || a.in_map == IN_C2R_PACK;
+    const bool packed_out = a.out_map == OUT_R2C_UNPACK || a.out_map == OUT_REAL_UNPACK;
+    LC_REQUIRE(!(packed_in || packed_out) || a.n_inner == 1, "axis FFT: packed real maps need rows");
     if (a.in_map == IN_HERM) LC_REQUIRE(a.n_in == a.L / 2 + 1, "IN_HERM needs n_in = L/2+1");
+    else if (a.in_map == IN_REAL_PACKED) LC_REQUIRE(a.n_in <= 2 * a.L, "axis FFT: n_in > 2L");
+    else if (a.in_map == IN_C2R_PACK) LC_REQUIRE(a.n_in == a.L + 1, "IN_C2R_PACK needs n_in = L+1");
     else LC_REQUIRE(a.n_in <= a.L, "axis FFT: n_in > L");
     if (a.out_map == OUT_WINDOW) LC_REQUIRE(a.out_off >= 0 && a.out_off + a.n_out <= a.L, "window");
+    else if (a.out_map == OUT_R2C_UNPACK) LC_REQUIRE(a.n_out <= a.L + 1, "axis FFT: n_out > L+1");
+    else if (a.out_map == OUT_REAL_UNPACK) LC_REQUIRE(a.n_out <= 2 * a.L, "axis FFT: n_out > 2L");
     else LC_REQUIRE(a.n_out <= a.L, "axis FFT: n_out > L");
     if (a.n_outer <= 0 || a.n_inner <= 0 || a.n_out == 0) return;
 

@@ -13,8 +13,8 @@
 namespace lc {
 
 enum Elem { E_F32 = 0, E_C64 = 1, E_F64 = 2, E_C128 = 3 };  // float, float2, double, double2
-enum InMap { IN_DIRECT = 0, IN_MODES = 1, IN_HERM = 2 };
-enum OutMap { OUT_DIRECT = 0, OUT_MODES = 1, OUT_WINDOW = 2 };
+enum InMap { IN_DIRECT = 0, IN_MODES = 1, IN_HERM = 2, IN_REAL_PACKED = 3, IN_C2R_PACK = 4 };
+enum OutMap { OUT_DIRECT = 0, OUT_MODES = 1, OUT_WINDOW = 2, OUT_R2C_UNPACK = 3, OUT_REAL_UNPACK = 4 };
 
 // Lines are indexed by (o, c), o in [0, n_outer), c in [0, n_inner); element i
 // of line (o, c) is at  o*ostride + i*n_inner + c  (input and output alike).
@@ -26,6 +26,17 @@ enum OutMap { OUT_DIRECT = 0, OUT_MODES = 1, OUT_WINDOW = 2 };
 //              (n_in = L/2 + 1, half spectrum of a real line)
 // Output maps (output element j <- FFT index f):
 //   OUT_DIRECT f = j; OUT_MODES f = (j - n_out/2) mod L; OUT_WINDOW f = j + out_off
+//
+// Real lines of even length N = 2L as complex transforms of length L (rows
+// only; the usual even/odd packing):
+//   IN_REAL_PACKED  z[e] = x[2e] + i x[2e+1] (real input of n_in <= 2L samples)
+//   OUT_R2C_UNPACK  X[k] = E[k] + exp(-i pi k / L) O[k], k < n_out <= L+1, with
+//                   E = (Z[k] + conj Z[L-k]) / 2 and O = (Z[k] - conj Z[L-k]) / 2i:
+//                   the half spectrum of the length-N real DFT
+//   IN_C2R_PACK     Z[k] = (X[k] + conj X[L-k]) + i exp(+i pi k / L) (X[k] - conj X[L-k])
+//                   from a half spectrum of n_in = L+1 values
+//   OUT_REAL_UNPACK out[j] = Re z[j/2] (j even) or Im z[j/2] (j odd), j < n_out <= 2L:
+//                   with sign +1 the unnormalised length-N inverse real DFT
 struct AxisFFT {
     const void *in = nullptr;
     Elem in_t = E_C64;

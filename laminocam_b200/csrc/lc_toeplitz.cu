@@ -462,6 +462,12 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
         a.L = P3;
         a.n_out = P3h;
         a.sign = -1;
+        if (P3 % 2 == 0) {
+            // real rows as half-length complex transforms (even/odd packing)
+            a.L = P3 / 2;
+            a.in_map = IN_REAL_PACKED;
+            a.out_map = OUT_R2C_UNPACK;
+        }
         launch_axis_fft(ctx, a);
     }
     if (!three_d_) {
@@ -564,6 +570,11 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
         a.out_off = 0;
         a.sign = +1;
         a.scale = scale_;
+        if (P3 % 2 == 0) {
+            a.L = P3 / 2;
+            a.in_map = IN_C2R_PACK;
+            a.out_map = OUT_REAL_UNPACK;
+        }
         launch_axis_fft(ctx, a);
     }
 }
