@@ -1,5 +1,6 @@
 // PSF generation (closed form, FP64) and the fused-FFT Toeplitz apply.
 #include <algorithm>
+#include <tuple>
 
 #include "lc_toeplitz.hpp"
 
@@ -47,11 +48,14 @@ __device__ __forceinline__ int mirror_index(int j, int P) {
 // rest.
 template <int DIM, int S>
 __global__ void __launch_bounds__(128) psf_rows_kernel(const PsfAngle *__restrict__ angles, int ntheta,
+                                                      const int *__restrict__ groups, int ngroups,
                                                       int nx, int ny, int P1, int P2, int P3,
                                                       double *__restrict__ K) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PsfAngle *ang = reinterpret_cast<PsfAngle *>(smem_raw);
+    int *gst = reinterpret_cast<int *>(ang + ntheta);
     for (int i = threadIdx.x; i < ntheta; i += blockDim.x) ang[i] = angles[i];
+    for (int i = threadIdx.x; i <= ngroups; i += blockDim.x) gst[i] = groups[i];
     __syncthreads();
     const int nseg = (P3 + S - 1) / S;
     // rows of the half space: 3D (jz <= P1/2, all jy); 2D (jy <= P2/2)
@@ -76,7 +80,45 @@ __global__ void __launch_bounds__(128) psf_rows_kernel(const PsfAngle *__restric
         double acc[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) acc[s] = 0.0;
-        for (int i = 0; i < ntheta; ++i) {
+        if constexpr (DIM == 3) {
+            // uX = a . k does not depend on theta (a is the first column of
+            // transpose(Rx(theta) Ry(beta) Rz(gamma)), which Rx leaves alone), so
+            // within a group of angles of equal (beta, gamma) the sum factors:
+            // K = sum_groups D_nx(uX) * sum_{theta in group} D_ny(uY)
+            for (int gi = 0; gi < ngroups; ++gi) {
+                const int i0 = gst[gi], i1 = gst[gi + 1];
+                double ay[S];
+#pragma unroll
+                for (int s = 0; s < S; ++s) ay[s] = 0.0;
+                for (int i = i0; i < i1; ++i) {
+                    const PsfAngle &A = ang[i];
+                    const double uY0 = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
+                    double2 pC, pD;
+                    sincospi(uY0, &pC.y, &pC.x);
+                    sincospi(uY0 * inv_ny, &pD.y, &pD.x);
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        ay[s] += fabs(pD.y) > 1e-6 ? pC.y / pD.y : dirichlet(uY0 + (double)s * A.b[0], ny);
+                        pC = crot(pC, A.stepC);
+                        pD = crot(pD, A.stepD);
+                    }
+                }
+                const PsfAngle &A = ang[i0];
+                const double uX0 = A.a[0] * kx0 + A.a[1] * ky + A.a[2] * kz;
+                double2 pA, pB;
+                sincospi(uX0, &pA.y, &pA.x);
+                sincospi(uX0 * inv_nx, &pB.y, &pB.x);
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    const double dX =
+                        fabs(pB.y) > 1e-6 ? pA.y / pB.y : dirichlet(uX0 + (double)s * A.a[0], nx);
+                    acc[s] = fma(dX, ay[s], acc[s]);
+                    pA = crot(pA, A.stepA);
+                    pB = crot(pB, A.stepB);
+                }
+            }
+        }
+        for (int i = 0; DIM == 2 && i < ntheta; ++i) {
             const PsfAngle &A = ang[i];
             const double uX0 = A.a[0] * kx0 + A.a[1] * ky + A.a[2] * kz;
             double2 pA, pB, pC = make_double2(1.0, 0.0), pD = make_double2(1.0, 0.0);
@@ -396,25 +438,47 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
         A.stepC = make_double2(std::cos(pi * A.b[0]), std::sin(pi * A.b[0]));
         A.stepD = make_double2(std::cos(pi * A.b[0] / ny), std::sin(pi * A.b[0] / ny));
     }
+    // group the angles by their theta-independent vector a (equal beta and gamma)
+    std::vector<int> order(nth);
+    for (int i = 0; i < nth; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int p, int q) {
+        const PsfAngle &x = tab[p], &y = tab[q];
+        return std::tie(x.a[0], x.a[1], x.a[2]) < std::tie(y.a[0], y.a[1], y.a[2]);
+    });
+    std::vector<PsfAngle> sorted(nth);
+    std::vector<int> groups{0};
+    for (int r = 0; r < nth; ++r) {
+        sorted[r] = tab[order[r]];
+        if (r > 0) {
+            const PsfAngle &x = sorted[r - 1], &y = sorted[r];
+            if (x.a[0] != y.a[0] || x.a[1] != y.a[1] || x.a[2] != y.a[2]) groups.push_back(r);
+        }
+    }
+    groups.push_back(nth);
+    const int ngroups = three_d_ ? (int)groups.size() - 1 : 0;
+    if (!three_d_) groups.assign(1, 0);
     DevBuf<PsfAngle> dtab;
-    dtab.upload(tab.data(), tab.size(), st);
+    dtab.upload(three_d_ ? sorted.data() : tab.data(), tab.size(), st);
+    DevBuf<int> dgroups;
+    dgroups.upload(groups.data(), groups.size(), st);
     const int P1 = P_[0], P2 = P_[1], P3 = P_[2];
     long total = (long)P1 * P2 * P3;
     K.alloc(total, st);
     constexpr int S = 16;
     const long nseg = (P3 + S - 1) / S;
     const long items = (three_d_ ? (long)(P1 / 2 + 1) * P2 : (long)(P2 / 2 + 1)) * nseg;
-    size_t smem = sizeof(PsfAngle) * nth;
+    size_t smem = sizeof(PsfAngle) * nth + sizeof(int) * groups.size();
     LC_REQUIRE(smem <= 220 * 1024, "Toeplitz: too many angles for one PSF launch");
     unsigned blocks = (unsigned)std::max<long>(1, std::min<long>((items + 127) / 128, (long)ctx.num_sms() * 16));
     if (three_d_) {
         auto kern = psf_rows_kernel<3, S>;
         LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, nx, ny, P1, P2, P3, K.get());
+        kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), ngroups, nx, ny, P1, P2, P3,
+                                        K.get());
     } else {
         auto kern = psf_rows_kernel<2, S>;
         LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, nx, ny, P1, P2, P3, K.get());
+        kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), 0, nx, ny, P1, P2, P3, K.get());
     }
     LC_CHECK_LAUNCH();
     // planes of mode -P/2 have no mirror inside the grid; they are not needed

@@ -125,6 +125,7 @@ int run(int argc, char **argv) {
     rp.solver.xtol = params.xtol;
     rp.solver.lambda = params.lambda;
     rp.solver.mu = params.mu;
+    rp.solver.use_graph = 1;  // replay the iterations as CUDA graphs
     io::Volume recon;
     recon.n1 = rd[0];
     recon.n2 = rd[1];
