@@ -165,7 +165,8 @@ int lc_mbir3d(lc_context ctx, const float *projs, int ntheta, int nrows, int nco
               lc_solver_stats *stats);
 
 /* As lc_mbir3d with device pointers: projs {ntheta, nrows, ncols} and recon
- * {n1, n2, n3} stay in device memory (the DeviceArray overload of gpu::MBIR). */
+ * {n1, n2, n3} stay in device memory (the DeviceArray overload of gpu::MBIR).
+ * Returns when the reconstruction is complete. */
 int lc_mbir3d_device(lc_context ctx, const float *projs, int ntheta, int nrows, int ncols,
                      const double *theta, const double *gamma, const double *beta,
                      const float *shifts, const int *recon_dims, const lc_recon_params *p,

@@ -691,6 +691,8 @@ int lc_mbir3d_device(lc_context c, const float *projs, int ntheta, int nrows, in
         LC_REQUIRE(projs && recon, "NULL argument");
         mbir3d_core(c, projs, ntheta, nrows, ncols, theta, gamma, beta, shifts, recon_dims, p,
                     recon, stats, nullptr, nullptr);
+        // the reconstruction is complete on return, as with lc_mbir3d
+        LC_CUDA(cudaStreamSynchronize(c->ctx->stream()));
     });
 }
 
