@@ -495,7 +495,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": "recons/s",
                 "h2d_bytes_per_step": int(host_proj.numel() * 4),
                 "d2h_bytes_per_step": int(host_recon.numel() * 4)},
-        "roofline": roof, "kernels": prof[:8], "clocks": clk.summary(), "serving": serving,
+        "roofline": roof, "kernels": prof[:12], "clocks": clk.summary(), "serving": serving,
         "gpu_launches": int(launches), "cpu_baseline": cpu,
         "solver": {"outer_iters": stats.iters, "cg_iters": stats.cg_iters_total, "dx": stats.dx},
     }

@@ -489,6 +489,16 @@ TuneVal autotune(Context &ctx, const AxisFFT &a0, const FFTPlan &pl) {
 
 }  // namespace
 
+// LC_LINE_KERNELS=0 routes every transform through the generic kernel (for
+// A/B timing of the register-plan line kernels).
+bool line_kernels_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("LC_LINE_KERNELS");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 void launch_axis_fft(Context &ctx, const AxisFFT &a) {
     LC_REQUIRE(is_smooth23(a.L), "axis FFT length must be 2^p*3^q");
     LC_REQUIRE(a.n_in >= 0 && a.n_out >= 0, "axis FFT: bad lengths");
@@ -504,6 +514,7 @@ void launch_axis_fft(Context &ctx, const AxisFFT &a) {
     else if (a.out_map == OUT_REAL_UNPACK) LC_REQUIRE(a.n_out <= 2 * a.L, "axis FFT: n_out > 2L");
     else LC_REQUIRE(a.n_out <= a.L, "axis FFT: n_out > L");
     if (a.n_outer <= 0 || a.n_inner <= 0 || a.n_out == 0) return;
+    if (line_kernels_enabled() && (launch_col_fft(ctx.stream(), a) || launch_row_fft(ctx.stream(), a))) return;
 
     const FFTPlan &pl = ctx.plans().get(a.L, a.fp64, ctx.stream());
     const size_t esz = a.fp64 ? sizeof(double2) : sizeof(float2);

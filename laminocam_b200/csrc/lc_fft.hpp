@@ -72,6 +72,23 @@ void launch_axis_fft(Context &ctx, const AxisFFT &a);
 bool launch_zconv(cudaStream_t st, float2 *data, long n_inner, int L, int n_in, int n_out,
                   const float *spec);
 
+// Column transforms (n_inner > 1) without index maps, per-index factors or
+// scale, in FP32 complex, as register-resident kernels with compile-time
+// radix plans; even lengths whose input or output fits in half the line run
+// as two half-length transforms.  Returns false for shapes without a plan
+// (the caller then uses the generic kernel).  launch_axis_fft tries it first.
+bool launch_col_fft(cudaStream_t st, const AxisFFT &a);
+
+// Real row passes (n_inner == 1) in the packed forms IN_REAL_PACKED ->
+// OUT_R2C_UNPACK (sign -1) and IN_C2R_PACK -> OUT_REAL_UNPACK (sign +1),
+// optionally scaled, as register-resident kernels for lengths with a plan.
+// Returns false otherwise.  launch_axis_fft tries it first.
+bool launch_row_fft(cudaStream_t st, const AxisFFT &a);
+
+// false when LC_LINE_KERNELS=0: every transform then takes the generic
+// shared-memory kernel (A/B timing of the register-plan kernels)
+bool line_kernels_enabled();
+
 // Same transform with a caller-supplied FP32 plan (radices and twiddle table)
 // on an explicit stream; touches no context, plan cache or allocator.
 void launch_axis_fft_f32_with_plan(cudaStream_t stream, size_t max_smem, const AxisFFT &a,

@@ -1,0 +1,193 @@
+// Real row passes of the axis FFT (the x passes of the Toeplitz apply) as
+// register-resident Stockham FFTs with compile-time radix plans.
+//
+// A real line of N = 2M samples is transformed as one complex line of M
+// points (the even/odd packing that the generic kernel implements with
+// IN_REAL_PACKED / OUT_R2C_UNPACK and IN_C2R_PACK / OUT_REAL_UNPACK):
+//   forward  z[e] = x[2e] + i x[2e+1];  Z = DFT_M(z);
+//            X[k] = (Z[k] + conj Z[M-k]) / 2 - (i/2) h(k) (Z[k] - conj Z[M-k]),
+//            k = 0..M, h(k) = exp(-i pi k / M)
+//   inverse  Z[k] = (X[k] + conj X[M-k]) + i conj h(k) (X[k] - conj X[M-k]),
+//            z = DFT_M^+(Z);  x[2e] = Re z[e], x[2e+1] = Im z[e]
+// A CTA transforms kRowLines lines of M points on M / min(R) threads each;
+// consecutive threads walk consecutive samples of a line, so the loads and
+// stores are contiguous.  The line crosses shared memory twice in the
+// transform, and once more in the forward unpack (which pairs k with M - k).
+#include <atomic>
+
+#include "lc_fft.hpp"
+#include "lc_regfft.cuh"
+
+namespace lc {
+namespace {
+
+constexpr int kRowLines = 4;
+
+enum RowMode { RM_R2C = 0, RM_C2R = 1 };
+
+struct RowArgs {
+    const void *in;
+    void *out;
+    long n_lines, in_stride, out_stride;
+    int n_in, n_out;
+    float scale;
+};
+
+template <int R0, int R1, int R2>
+constexpr size_t row_smem() {
+    constexpr int M = RegPlan<R0, R1, R2>::M;
+    return ((size_t)M * kRowLines + 2 * (size_t)M) * sizeof(float2);
+}
+
+template <int R0, int R1, int R2, int MODE>
+__global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_kernel(RowArgs a) {
+    using P = RegPlan<R0, R1, R2>;
+    constexpr int M = P::M, RM = P::RM, NT = P::NT;
+    extern __shared__ __align__(16) float2 row_sm[];
+    float2 *tw = row_sm + M * kRowLines;  // exp(-2 pi i m / M)
+    float2 *th = tw + M;                  // h(m) = exp(-pi i m / M)
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        float s, co;
+        sincospif(2.0f * (float)m / (float)M, &s, &co);
+        tw[m] = make_float2(co, -s);
+        sincospif((float)m / (float)M, &s, &co);
+        th[m] = make_float2(co, -s);
+    }
+    const int t = threadIdx.x % NT, c = threadIdx.x / NT;
+    const long line = (long)blockIdx.x * kRowLines + c;
+    const bool valid = line < a.n_lines;
+    float2 *buf = row_sm + c * M;
+    const auto at = [&](int, int i) -> float2 & { return buf[i]; };
+    constexpr int NA = M / R0;
+    float2 v[1][RM];
+    if constexpr (MODE == RM_R2C) {
+        const float *in = static_cast<const float *>(a.in) + (valid ? line : 0) * a.in_stride;
+        if (t < NA) {
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int e = t + r * NA;
+                const float re = (valid && 2 * e < a.n_in) ? in[2 * e] : 0.f;
+                const float im = (valid && 2 * e + 1 < a.n_in) ? in[2 * e + 1] : 0.f;
+                v[0][r] = make_float2(re, im);
+            }
+        }
+        __syncthreads();  // twiddle tables ready
+        xform3<M, R0, R1, R2>(v, at, t, tw, -1);
+        constexpr int NC = M / R2;
+        __syncthreads();  // the last stage's reads are done
+        if (t < NC) {
+#pragma unroll
+            for (int r = 0; r < R2; ++r) buf[t + r * NC] = v[0][r];
+        }
+        __syncthreads();
+        if (valid) {
+            float2 *out = static_cast<float2 *>(a.out) + line * a.out_stride;
+            for (int k = t; k < a.n_out; k += NT) {
+                const float2 za = buf[k == M ? 0 : k];
+                const float2 zb = buf[k == 0 ? 0 : M - k];
+                const float2 sm = make_float2(0.5f * (za.x + zb.x), 0.5f * (za.y - zb.y));
+                const float2 df = make_float2(0.5f * (za.x - zb.x), 0.5f * (za.y + zb.y));
+                const float2 wd = cmul(k == M ? make_float2(-1.f, 0.f) : th[k], df);
+                out[k] = make_float2(a.scale * (sm.x + wd.y), a.scale * (sm.y - wd.x));
+            }
+        }
+    } else {
+        const float2 *in = static_cast<const float2 *>(a.in) + (valid ? line : 0) * a.in_stride;
+        float2 xb[RM];
+        if (t < NA) {
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int k = t + r * NA;
+                v[0][r] = valid ? in[k] : make_float2(0.f, 0.f);
+                xb[r] = valid ? in[M - k] : make_float2(0.f, 0.f);
+            }
+        }
+        __syncthreads();  // twiddle tables ready
+        if (t < NA) {
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int k = t + r * NA;
+                const float2 xa = v[0][r];
+                const float2 sm = make_float2(xa.x + xb[r].x, xa.y - xb[r].y);
+                const float2 df = make_float2(xa.x - xb[r].x, xa.y + xb[r].y);
+                const float2 h = th[k];
+                const float2 wd = cmul(make_float2(h.x, -h.y), df);
+                v[0][r] = make_float2(sm.x - wd.y, sm.y + wd.x);
+            }
+        }
+        xform3<M, R0, R1, R2>(v, at, t, tw, +1);
+        constexpr int NC = M / R2;
+        if (t < NC && valid) {
+            float *out = static_cast<float *>(a.out) + line * a.out_stride;
+#pragma unroll
+            for (int r = 0; r < R2; ++r) {
+                const int e = t + r * NC;
+                if (2 * e < a.n_out) out[2 * e] = a.scale * v[0][r].x;
+                if (2 * e + 1 < a.n_out) out[2 * e + 1] = a.scale * v[0][r].y;
+            }
+        }
+    }
+}
+
+template <int R0, int R1, int R2, int MODE>
+void launch_row_mode(cudaStream_t st, const RowArgs &a, long blocks) {
+    constexpr size_t smem = row_smem<R0, R1, R2>();
+    auto kern = row_fft_kernel<R0, R1, R2, MODE>;
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    LC_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(configured.load() & bit)) {
+        LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured.fetch_or(bit);
+    }
+    kern<<<(unsigned)blocks, RegPlan<R0, R1, R2>::NT * kRowLines, smem, st>>>(a);
+    LC_CHECK_LAUNCH();
+}
+
+bool launch_row_plan(cudaStream_t st, int M, int mode, const RowArgs &a, long blocks) {
+    switch (M) {
+#define LC_ROW_CASE(m, r0, r1, r2)                                                    \
+    case m:                                                                           \
+        if (mode == RM_R2C) launch_row_mode<r0, r1, r2, RM_R2C>(st, a, blocks);       \
+        else launch_row_mode<r0, r1, r2, RM_C2R>(st, a, blocks);                      \
+        return true;
+        LC_LINE_PLANS(LC_ROW_CASE)
+#undef LC_ROW_CASE
+        default: return false;
+    }
+}
+
+}  // namespace
+
+bool launch_row_fft(cudaStream_t st, const AxisFFT &a) {
+    if (a.fp64 || a.n_inner != 1 || a.lines_per_cta > 0) return false;
+    if (a.pre || a.linefac || a.post) return false;
+    const int M = a.L;
+    int mode;
+    if (a.in_map == IN_REAL_PACKED && a.out_map == OUT_R2C_UNPACK && a.in_t == E_F32 && a.out_t == E_C64 &&
+        a.sign < 0 && a.n_in <= 2 * M && a.n_out <= M + 1) {
+        mode = RM_R2C;
+    } else if (a.in_map == IN_C2R_PACK && a.out_map == OUT_REAL_UNPACK && a.in_t == E_C64 &&
+               a.out_t == E_F32 && a.sign > 0 && a.n_in == M + 1 && a.n_out <= 2 * M) {
+        mode = RM_C2R;
+    } else {
+        return false;
+    }
+    if (!line_plan_exists(M)) return false;
+    if (a.n_outer <= 0 || a.n_out == 0) return true;
+    RowArgs ra;
+    ra.in = a.in;
+    ra.out = a.out;
+    ra.n_lines = a.n_outer;
+    ra.in_stride = a.in_ostride;
+    ra.out_stride = a.out_ostride;
+    ra.n_in = a.n_in;
+    ra.n_out = a.n_out;
+    ra.scale = (float)a.scale;
+    const long blocks = (a.n_outer + kRowLines - 1) / kRowLines;
+    LC_REQUIRE(blocks < (1L << 31), "row FFT: grid too large");
+    return launch_row_plan(st, M, mode, ra, blocks);
+}
+
+}  // namespace lc

@@ -574,7 +574,8 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
             launch_axis_fft(ctx, a);
         }
         if (ProfScope ps(ctx, PS_TOEP_Z_MID, 2.0 * T2 + Rb);
-            !launch_zconv(ctx.stream(), t2_.get(), (long)P2 * P3h, P1, (int)n1, (int)n1, R_->get())) {
+            !(line_kernels_enabled() &&
+              launch_zconv(ctx.stream(), t2_.get(), (long)P2 * P3h, P1, (int)n1, (int)n1, R_->get()))) {
             AxisFFT a;
             a.in = t2_.get();
             a.in_t = E_C64;

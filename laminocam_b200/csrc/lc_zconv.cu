@@ -16,67 +16,10 @@
 //   X[k1 + A k2]   = sum_b (Y_b[k1] w^(b k1)) w^(A b k2)    (DFT_B in thread k1)
 // and the inverse runs the same steps backwards with conjugate roots.
 #include "lc_fft.hpp"
+#include "lc_regfft.cuh"
 
 namespace lc {
 namespace {
-
-// exp(sign * 2 pi i m / N) for the composite radices 6, 12 and 16
-template <int N>
-__device__ __forceinline__ float2 unit_root(int m, int sign) {
-    const float h = 0.70710678118654752440f, c30 = 0.86602540378443864676f;
-    const float c22 = 0.92387953251128675613f, s22 = 0.38268343236508977173f;
-    float c = 1.f, s = 0.f;
-    if constexpr (N == 6) {
-        const float cs[6] = {1.f, 0.5f, -0.5f, -1.f, -0.5f, 0.5f};
-        const float sn[6] = {0.f, c30, c30, 0.f, -c30, -c30};
-        c = cs[m];
-        s = sn[m];
-    } else if constexpr (N == 12) {
-        const float cs[12] = {1.f, c30, 0.5f, 0.f, -0.5f, -c30, -1.f, -c30, -0.5f, 0.f, 0.5f, c30};
-        const float sn[12] = {0.f, 0.5f, c30, 1.f, c30, 0.5f, 0.f, -0.5f, -c30, -1.f, -c30, -0.5f};
-        c = cs[m];
-        s = sn[m];
-    } else if constexpr (N == 16) {
-        const float cs[16] = {1.f, c22, h, s22, 0.f, -s22, -h, -c22, -1.f, -c22, -h, -s22, 0.f, s22, h, c22};
-        const float sn[16] = {0.f, s22, h, c22, 1.f, c22, h, s22, 0.f, -s22, -h, -c22, -1.f, -c22, -h, -s22};
-        c = cs[m];
-        s = sn[m];
-    }
-    return make_float2(c, sign * s);
-}
-
-// N = R1 * R2 from two small DFTs (same decomposition as the kernel)
-template <int R1, int R2>
-__device__ __forceinline__ void dft_composite(float2 *v, int sign) {
-    constexpr int N = R1 * R2;
-    float2 y[R2][R1];
-#pragma unroll
-    for (int b = 0; b < R2; ++b) {
-        float2 t[R1];
-#pragma unroll
-        for (int a = 0; a < R1; ++a) t[a] = v[b + R2 * a];
-        dft_small<float2, R1>(t, sign);
-#pragma unroll
-        for (int k1 = 0; k1 < R1; ++k1) y[b][k1] = (b * k1 == 0) ? t[k1] : cmul(t[k1], unit_root<N>(b * k1, sign));
-    }
-#pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) {
-        float2 t[R2];
-#pragma unroll
-        for (int b = 0; b < R2; ++b) t[b] = y[b][k1];
-        dft_small<float2, R2>(t, sign);
-#pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = t[k2];
-    }
-}
-
-template <int N>
-__device__ __forceinline__ void dft_reg(float2 *v, int sign) {
-    if constexpr (N == 6) dft_composite<3, 2>(v, sign);
-    else if constexpr (N == 12) dft_composite<3, 4>(v, sign);
-    else if constexpr (N == 16) dft_composite<4, 4>(v, sign);
-    else dft_small<float2, N>(v, sign);
-}
 
 template <int A, int B, int C>
 __global__ void __launch_bounds__(C *(A > B ? A : B))
