@@ -118,6 +118,11 @@ typedef struct {
     int poll_every;   /* iterations between host checks of the stop flag */
     int use_graph;    /* 1: replay iterations as CUDA graphs (CG: a chunk of iterations,
                          Split-Bregman: one outer iteration); ignored while profiling */
+    int residual_refresh; /* Split-Bregman: recompute the operator product A x of the
+                             warm-started CG residual every this many outer iterations
+                             (1, the default: every one); in between it is carried by
+                             the CG updates (ax += alpha A p), equal up to rounding, which
+                             saves one operator application per outer iteration */
 } lc_solver_params;
 
 typedef struct {

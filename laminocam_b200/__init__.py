@@ -357,7 +357,7 @@ class SolveInfo:
 
 
 def _solver_params(max_iters, inner, tol, xtol, lam, mu, fp32_scalars=False, poll_every=8,
-                   use_graph=False):
+                   use_graph=False, residual_refresh=1):
     p = SolverParams()
     _lib.load().lc_solver_params_default(C.byref(p))
     p.max_iters, p.inner_iters = int(max_iters), int(inner)
@@ -365,6 +365,7 @@ def _solver_params(max_iters, inner, tol, xtol, lam, mu, fp32_scalars=False, pol
     p.fp32_scalars = int(bool(fp32_scalars))
     p.poll_every = int(poll_every)
     p.use_graph = int(bool(use_graph))
+    p.residual_refresh = int(residual_refresh)
     return p
 
 
@@ -385,13 +386,19 @@ def cgsolver(A: _PSFBase, y, x0, max_iter: int, tol: float, xtol: float, fp32_sc
 
 
 def split_bregman(A: _PSFBase, yT, x0, lam: float, mu: float, outer_max: int, inner_max: int,
-                  tol: float, xtol: float, fp32_scalars=False, return_info=False, use_graph=False):
-    """opt::split_bregman (src/bregman.cpp:36-94) with the Toeplitz operator A."""
+                  tol: float, xtol: float, fp32_scalars=False, return_info=False, use_graph=False,
+                  residual_refresh=1):
+    """opt::split_bregman (src/bregman.cpp:36-94) with the Toeplitz operator A.
+
+    residual_refresh: the operator product A x of each outer iteration's
+    warm-started residual is computed exactly every this many outer iterations
+    and carried by the CG updates in between (1: every outer iteration)."""
     A.ctx.sync_stream()
     yv = _dev(yT, device=A.ctx.device)
     x = _dev(x0, device=A.ctx.device).clone()
     st = SolverStats()
-    p = _solver_params(outer_max, inner_max, tol, xtol, lam, mu, fp32_scalars, use_graph=use_graph)
+    p = _solver_params(outer_max, inner_max, tol, xtol, lam, mu, fp32_scalars, use_graph=use_graph,
+                       residual_refresh=residual_refresh)
     _check(A.ctx.lib.lc_split_bregman(A.ctx.handle, A.handle, _ptr(yv), _ptr(x), C.byref(p), C.byref(st)),
            A.ctx)
     return (x, _info(st)) if return_info else x
@@ -413,13 +420,15 @@ class ReconParams:
     fp32_scalars: bool = False
     poll_every: int = 8
     use_graph: bool = False
+    residual_refresh: int = 1
 
     def to_c(self) -> ReconParamsC:
         r = ReconParamsC()
         _lib.load().lc_recon_params_default(C.byref(r))
         r.method = 1 if self.regularizer == "split_bregman" else 0
         r.solver = _solver_params(self.max_iters, self.inner_iters, self.tol, self.xtol, self.lam,
-                                  self.mu, self.fp32_scalars, self.poll_every, self.use_graph)
+                                  self.mu, self.fp32_scalars, self.poll_every, self.use_graph,
+                                  self.residual_refresh)
         r.nufft_tol = float(self.nufft_tol)
         r.pad_factor = float(self.pad_factor)
         return r

@@ -11,7 +11,8 @@ LIB_PATH = os.path.join(HERE, "liblaminocam_b200.so")
 class SolverParams(C.Structure):
     _fields_ = [("max_iters", C.c_int), ("inner_iters", C.c_int), ("tol", C.c_float),
                 ("xtol", C.c_float), ("lambda_", C.c_float), ("mu", C.c_float),
-                ("fp32_scalars", C.c_int), ("poll_every", C.c_int), ("use_graph", C.c_int)]
+                ("fp32_scalars", C.c_int), ("poll_every", C.c_int), ("use_graph", C.c_int),
+                ("residual_refresh", C.c_int)]
 
 
 class SolverStats(C.Structure):

@@ -249,6 +249,7 @@ SolverParams to_sp(const lc_solver_params *p) {
     s.fp32_scalars = p->fp32_scalars;
     s.poll_every = p->poll_every;
     s.use_graph = p->use_graph;
+    s.residual_refresh = p->residual_refresh;
     return s;
 }
 
@@ -286,6 +287,23 @@ void run_solver(lc_psf psf, int method, const float *rhs, float *x, const lc_sol
 
 }  // namespace
 
+// Destroys a geometry or PSF without touching its owner handle, which may
+// already be gone; the shared lc::Context keeps the streams alive meanwhile.
+template <typename H>
+static int destroy_child(H *h) {
+    if (!h) return LC_ERR_INVALID;
+    const std::shared_ptr<Context> keep = h->keep;
+    int rc = LC_OK;
+    try {
+        DeviceGuard dg(keep->device());
+        if (cudaStreamSynchronize(keep->stream()) != cudaSuccess) rc = LC_ERR_CUDA;
+        delete h;
+    } catch (...) {
+        rc = LC_ERR_CUDA;
+    }
+    return rc;
+}
+
 extern "C" {
 
 int lc_version(void) { return 100; }
@@ -303,6 +321,7 @@ void lc_solver_params_default(lc_solver_params *p) {
     p->fp32_scalars = 0;
     p->poll_every = 8;
     p->use_graph = 0;
+    p->residual_refresh = 1;
 }
 
 void lc_recon_params_default(lc_recon_params *p) {
@@ -358,6 +377,7 @@ int lc_geometry2d_create(lc_context c, const double *theta, int ntheta, int nrad
         LC_REQUIRE(theta != nullptr, "theta is NULL");
         for (int i = 0; i < ntheta; ++i) LC_REQUIRE(std::isfinite(theta[i]), "theta must be finite");
         auto g = std::make_unique<lc_geometry_s>();
+        g->keep = c->ctx;
         g->owner = c;
         geometry_init_2d(*c->ctx, g->g, theta, ntheta, nradial);
         *out = g.release();
@@ -375,20 +395,14 @@ int lc_geometry3d_create(lc_context c, const double *theta, const double *gamma,
             LC_REQUIRE(std::isfinite(theta[i]) && std::isfinite(gamma[i]) && std::isfinite(beta[i]),
                        "angles must be finite");
         auto g = std::make_unique<lc_geometry_s>();
+        g->keep = c->ctx;
         g->owner = c;
         geometry_init_3d(*c->ctx, g->g, theta, gamma, beta, shifts, ntheta, nrows, ncols);
         *out = g.release();
     });
 }
 
-int lc_geometry_destroy(lc_geometry g) {
-    if (!g) return LC_ERR_INVALID;
-    lc_context c = g->owner;
-    return guarded(c, [&] {
-        LC_CUDA(cudaStreamSynchronize(c->ctx->stream()));
-        delete g;
-    });
-}
+int lc_geometry_destroy(lc_geometry g) { return destroy_child(g); }
 
 int lc_forward2d(lc_context c, lc_geometry g, const float *volume, int ns, int n2, int n3,
                  float *sino, double tol) {
@@ -465,6 +479,7 @@ int lc_psf_create(lc_context c, lc_geometry g, int n1, int n2, int n3, lc_psf *o
         if (!three) LC_REQUIRE(n2 == n3, "2D PSF needs square slices (n2 == n3)");
         long dims[3] = {n1, n2, n3};
         auto p = std::make_unique<lc_psf_s>();
+        p->keep = c->ctx;
         p->owner = c;
         p->geom = g;
         p->T = std::make_unique<Toeplitz>(*c->ctx, g->g, dims, three);
@@ -472,14 +487,7 @@ int lc_psf_create(lc_context c, lc_geometry g, int n1, int n2, int n3, lc_psf *o
     });
 }
 
-int lc_psf_destroy(lc_psf p) {
-    if (!p) return LC_ERR_INVALID;
-    lc_context c = p->owner;
-    return guarded(c, [&] {
-        LC_CUDA(cudaStreamSynchronize(c->ctx->stream()));
-        delete p;
-    });
-}
+int lc_psf_destroy(lc_psf p) { return destroy_child(p); }
 
 int lc_psf_info(lc_psf p, int *P, long *spectrum_elems) {
     if (!p) return LC_ERR_INVALID;

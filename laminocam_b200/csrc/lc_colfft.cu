@@ -45,7 +45,7 @@ constexpr int col_nv() { return MODE >= CM_SPLIT_IN ? 2 : 1; }
 template <int R0, int R1, int R2, int MODE>
 constexpr size_t col_smem() {
     constexpr int M = RegPlan<R0, R1, R2>::M;
-    return ((size_t)col_nv<MODE>() * M * kCols + (size_t)M * (col_nv<MODE>() == 2 ? 2 : 1)) * sizeof(float2);
+    return ((size_t)col_nv<MODE>() * M * kCols + 2 * (size_t)M) * sizeof(float2);
 }
 
 template <int R0, int R1, int R2, int MODE>
@@ -56,16 +56,8 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kCols, 3) col_fft_ker
     constexpr int NV = col_nv<MODE>();
     extern __shared__ __align__(16) float2 col_sm[];
     float2 *tw = col_sm + NV * M * C;  // exp(-2 pi i m / M)
-    float2 *th = tw + M;               // exp(-pi i m / M), split modes
-    for (int m = threadIdx.x; m < M; m += blockDim.x) {
-        float s, co;
-        sincospif(2.0f * (float)m / (float)M, &s, &co);
-        tw[m] = make_float2(co, -s);
-        if constexpr (SPLIT) {
-            sincospif((float)m / (float)M, &s, &co);
-            th[m] = make_float2(co, -s);
-        }
-    }
+    float2 *th = tw + M;               // exp(-pi i m / M)
+    load_line_twiddles<M>(tw);
     const int c = threadIdx.x % C, t = threadIdx.x / C;
     const long o = (long)blockIdx.x / a.bpo;
     const long col = ((long)blockIdx.x - o * a.bpo) * C + c;

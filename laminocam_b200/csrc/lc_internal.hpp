@@ -14,12 +14,16 @@
 #include "lc_solver.hpp"
 #include "lc_toeplitz.hpp"
 
+// A context handle shares its lc::Context with the geometries and PSFs made
+// from it, so that those can still be destroyed (their device memory freed on
+// the context's streams) after the context handle itself was destroyed.
 struct lc_context_s {
-    std::unique_ptr<lc::Context> ctx;
+    std::shared_ptr<lc::Context> ctx;
     std::string err;
 };
 
 struct lc_geometry_s {
+    std::shared_ptr<lc::Context> keep;  // first member: released after the rest
     lc_context owner = nullptr;
     lc::PolarGeometry g;
     std::map<std::tuple<int, int, int, int>, std::unique_ptr<lc::NufftPlan>> plans;
@@ -27,6 +31,7 @@ struct lc_geometry_s {
 };
 
 struct lc_psf_s {
+    std::shared_ptr<lc::Context> keep;  // first member: released after the rest
     lc_context owner = nullptr;
     lc_geometry geom = nullptr;
     std::shared_ptr<lc::Toeplitz> T;

@@ -83,17 +83,18 @@ __device__ __forceinline__ void dft_reg(float2 *v, int sign) {
     else dft_small<float2, N>(v, sign);
 }
 
-// Stage twiddles: element r of butterfly j times w_M^(r k TS), k = j mod NS,
-// TS = M / (NS R); tw[m] = exp(-2 pi i m / M).  w and w^2 come from the
-// table, the higher powers from products of them.
-template <int M, int R, int NS>
-__device__ __forceinline__ void stage_twiddle(float2 *v, int j, const float2 *tw, int sign) {
+// Stage twiddles of NV lines at once: element r of butterfly j of every line
+// times w_M^(r k TS), k = j mod NS, TS = M / (NS R); tw[m] = exp(-2 pi i m / M).
+// w and w^2 come from the table, the higher powers from products of them.
+template <int M, int R, int NS, int NV, int RM>
+__device__ __forceinline__ void stage_twiddle(float2 (&v)[NV][RM], int j, const float2 *tw, int sign) {
     if constexpr (NS > 1 && R > 1) {
         constexpr int TS = M / (NS * R);
         const int k = j % NS;
         float2 w1 = tw[k * TS];
         if (sign > 0) w1.y = -w1.y;
-        v[1] = cmul(v[1], w1);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) v[q][1] = cmul(v[q][1], w1);
         if constexpr (R > 2) {
             float2 w2;
             if constexpr (R > 4) {
@@ -102,20 +103,78 @@ __device__ __forceinline__ void stage_twiddle(float2 *v, int j, const float2 *tw
             } else {
                 w2 = cmul(w1, w1);
             }
-            v[2] = cmul(v[2], w2);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) v[q][2] = cmul(v[q][2], w2);
             float2 wo = w1, we = w2;
 #pragma unroll
             for (int r = 3; r < R; ++r) {
+                float2 w;
                 if (r & 1) {
                     wo = cmul(wo, w2);
-                    v[r] = cmul(v[r], wo);
+                    w = wo;
                 } else {
                     we = cmul(we, w2);
-                    v[r] = cmul(v[r], we);
+                    w = we;
                 }
+#pragma unroll
+                for (int q = 0; q < NV; ++q) v[q][r] = cmul(v[q][r], w);
             }
         }
     }
+}
+
+// ---- compile-time twiddle tables -------------------------------------------
+// sin and cos of 2 pi num / den: the angle is reduced exactly (in integers) to
+// within 1/16 turn of a multiple of 1/8 turn, the remainder x (|x| <= pi/8)
+// goes through the Taylor series of sin and cos (12 terms: the truncation
+// error is far below double rounding), and the result is rotated by the
+// octant.  Used only to build constant tables at compile time.
+constexpr void ct_sincos(long num, long den, double &s, double &c) {
+    num %= den;
+    if (num < 0) num += den;
+    const long o8 = 8 * num;
+    const long oct = (o8 + den / 2) / den;
+    const double x = 2.0 * 3.14159265358979323846 * (double)(o8 - oct * den) / (8.0 * (double)den);
+    const double x2 = x * x;
+    double ts = x, ss = x, tc = 1.0, cc = 1.0;
+    for (int k = 1; k < 12; ++k) {
+        ts *= -x2 / ((2.0 * k) * (2.0 * k + 1.0));
+        ss += ts;
+        tc *= -x2 / ((2.0 * k - 1.0) * (2.0 * k));
+        cc += tc;
+    }
+    const double h = 0.70710678118654752440;
+    const double co[8] = {1, h, 0, -h, -1, -h, 0, h};
+    const double so[8] = {0, h, 1, h, 0, -h, -1, -h};
+    const int q = (int)(oct % 8);
+    s = ss * co[q] + cc * so[q];
+    c = cc * co[q] - ss * so[q];
+}
+
+// v[m] = exp(-2 pi i m / M) and v[M + m] = exp(-pi i m / M), m < M
+template <int M>
+struct LineTwiddles {
+    alignas(16) float2 v[2 * M];
+    constexpr LineTwiddles() : v() {
+        for (int m = 0; m < M; ++m) {
+            double s = 0.0, c = 0.0;
+            ct_sincos(m, M, s, c);
+            v[m] = float2{(float)c, (float)-s};
+            ct_sincos(m, 2 * M, s, c);
+            v[M + m] = float2{(float)c, (float)-s};
+        }
+    }
+};
+
+template <int M>
+__device__ const LineTwiddles<M> g_line_twiddles = LineTwiddles<M>();
+
+// copy the 2M table entries into shared memory (all threads of the CTA)
+template <int M>
+__device__ __forceinline__ void load_line_twiddles(float2 *dst) {
+    const float4 *src = reinterpret_cast<const float4 *>(g_line_twiddles<M>.v);
+    float4 *d4 = reinterpret_cast<float4 *>(dst);
+    for (int i = threadIdx.x; i < M; i += blockDim.x) d4[i] = __ldg(src + i);
 }
 
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
@@ -171,9 +230,10 @@ __device__ __forceinline__ void xform3(float2 (&v)[NV][RM], const At &at, int t,
         for (int q = 0; q < NV; ++q) {
 #pragma unroll
             for (int r = 0; r < RB; ++r) v[q][r] = at(q, t + r * NB);
-            stage_twiddle<M, RB, RA>(v[q], t, tw, sign);
-            dft_reg<RB>(v[q], sign);
         }
+        stage_twiddle<M, RB, RA>(v, t, tw, sign);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) dft_reg<RB>(v[q], sign);
     }
     __syncthreads();
     if (t < NB) {
@@ -189,9 +249,10 @@ __device__ __forceinline__ void xform3(float2 (&v)[NV][RM], const At &at, int t,
         for (int q = 0; q < NV; ++q) {
 #pragma unroll
             for (int r = 0; r < RC; ++r) v[q][r] = at(q, t + r * NC);
-            stage_twiddle<M, RC, RA * RB>(v[q], t, tw, sign);
-            dft_reg<RC>(v[q], sign);
         }
+        stage_twiddle<M, RC, RA * RB>(v, t, tw, sign);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) dft_reg<RC>(v[q], sign);
     }
 }
 

@@ -46,13 +46,7 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
     extern __shared__ __align__(16) float2 row_sm[];
     float2 *tw = row_sm + M * kRowLines;  // exp(-2 pi i m / M)
     float2 *th = tw + M;                  // h(m) = exp(-pi i m / M)
-    for (int m = threadIdx.x; m < M; m += blockDim.x) {
-        float s, co;
-        sincospif(2.0f * (float)m / (float)M, &s, &co);
-        tw[m] = make_float2(co, -s);
-        sincospif((float)m / (float)M, &s, &co);
-        th[m] = make_float2(co, -s);
-    }
+    load_line_twiddles<M>(tw);
     const int t = threadIdx.x % NT, c = threadIdx.x / NT;
     const long line = (long)blockIdx.x * kRowLines + c;
     const bool valid = line < a.n_lines;

@@ -76,8 +76,8 @@ __device__ double total(const double *part, int k, int nblk) {
 
 // r = y - r(=A x0);  p = r;  partials y.y, r.r
 template <typename A>
-__global__ void __launch_bounds__(kThreads) cg_init_kernel(const float *__restrict__ y, float *r,
-                                                          float *p, long n, double *part,
+__global__ void __launch_bounds__(kThreads) cg_init_kernel(const float *__restrict__ y, float *__restrict__ r,
+                                                          float *__restrict__ p, long n, double *part,
                                                           unsigned *counter, CGState *st) {
     if (st->sb_done) {
         if (blockIdx.x == 0 && threadIdx.x == 0) st->done = 1;
@@ -132,22 +132,29 @@ __global__ void __launch_bounds__(kThreads) dot_pap_kernel(const float *__restri
     }
 }
 
-// x += a p; r -= a Ap; partials r.r, |a p|^2, x.x; then beta, stopping tests
-template <typename A>
-__global__ void __launch_bounds__(kThreads) cg_update_kernel(float *x, float *r,
-                                                            const float *__restrict__ p,
-                                                            const float *__restrict__ ap, long n,
-                                                            double *part, unsigned *counter,
-                                                            CGState *st, float tol, float xtol) {
+// x += a p; r -= a Ap; partials r.r, |a p|^2, x.x; then beta, stopping tests.
+// AX: also carry the operator product, ax += a Ap (Split-Bregman keeps A x up
+// to date this way between exact recomputations).  STORE_R: false when no
+// later kernel reads r (one CG iteration per outer iteration, where p and r
+// may then share a buffer: both are only read then, which the restrict
+// qualifiers allow).
+template <typename A, bool AX = false, bool STORE_R = true>
+__global__ void __launch_bounds__(kThreads)
+    cg_update_kernel(float *__restrict__ x, float *__restrict__ r, const float *__restrict__ p,
+                     const float *__restrict__ ap, float *__restrict__ ax, long n, double *part,
+                     unsigned *counter, CGState *st, float tol, float xtol) {
     if (st->done) return;
     const float a = (float)st->alpha;
     A v[3] = {A(0), A(0), A(0)};
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        float step = a * p[i];
-        float xi = x[i] + step;
-        float ri = fmaf(-a, ap[i], r[i]);
+        const float api = ap[i], pi = p[i], xo = x[i], ro = r[i];
+        const float axo = AX ? ax[i] : 0.f;
+        float step = a * pi;
+        float xi = xo + step;
+        float ri = fmaf(-a, api, ro);
         x[i] = xi;
-        r[i] = ri;
+        if constexpr (STORE_R) r[i] = ri;
+        if constexpr (AX) ax[i] = fmaf(a, api, axo);
         v[0] += (A)ri * (A)ri;
         v[1] += (A)step * (A)step;
         v[2] += (A)xi * (A)xi;
@@ -176,7 +183,7 @@ __global__ void __launch_bounds__(kThreads) cg_update_kernel(float *x, float *r,
     }
 }
 
-__global__ void __launch_bounds__(kThreads) p_update_kernel(float *p, const float *__restrict__ r,
+__global__ void __launch_bounds__(kThreads) p_update_kernel(float *__restrict__ p, const float *__restrict__ r,
                                                            long n, const CGState *st) {
     if (st->done) return;
     const float b = (float)st->beta;
@@ -188,77 +195,202 @@ struct Dims {
     int n1, n2, n3;
 };
 
-// The stencil kernels run one thread per voxel on a (32 x 8) x n1 grid of
-// CTAs: k and j come from the CTA and thread indices and i = blockIdx.z, so
-// no index is divided; offsets are 32-bit (the host checks the size).
-#define LC_VOXEL_INDEX(dm)                                  \
-    const int k = blockIdx.x * 32 + threadIdx.x;            \
-    const int j = blockIdx.y * 8 + threadIdx.y;             \
-    const int i = blockIdx.z;                               \
-    if (k >= (dm).n3 || j >= (dm).n2) return;               \
-    const int sj = (dm).n3, si = (dm).n2 * (dm).n3;         \
-    const int idx = i * si + j * sj + k
+// The stencil kernels walk the volume in tiles of 32 (along n3) x kTileRows
+// (along n2) voxels of one plane, each thread taking kTileRows / 8 voxels 8
+// rows apart (two per thread measured slower than one: more registers, fewer
+// CTAs); a persistent grid of CTAs strides over the tiles, so one partial sum per CTA feeds the fused reductions.  The stride
+// (the grid size) is pre-split into whole planes, tile rows and tiles, so a
+// CTA steps from tile to tile without dividing.  Offsets are 32-bit (the host
+// checks the size).
+constexpr int kTileRows = 8;
 
-// rhs = yT - mu * div(d - b); div = D_n3(v0) + D_n2(v1) + D_n1(v2), zero padded
-__global__ void __launch_bounds__(256) sb_rhs_kernel(const float *__restrict__ yT,
-                                                     const float *__restrict__ d0,
-                                                     const float *__restrict__ d1,
-                                                     const float *__restrict__ d2,
-                                                     const float *__restrict__ b0,
-                                                     const float *__restrict__ b1,
-                                                     const float *__restrict__ b2, float *rhs,
-                                                     Dims dm, float mu, const CGState *st) {
-    if (st->sb_done) return;
-    LC_VOXEL_INDEX(dm);
-    auto v = [&](const float *d, const float *b, int o) { return d[idx + o] - b[idx + o]; };
-    const float dk = (k + 1 < dm.n3 ? v(d0, b0, 1) : 0.f) - (k >= 1 ? v(d0, b0, -1) : 0.f);
-    const float dj = (j + 1 < dm.n2 ? v(d1, b1, sj) : 0.f) - (j >= 1 ? v(d1, b1, -sj) : 0.f);
-    const float di = (i + 1 < dm.n1 ? v(d2, b2, si) : 0.f) - (i >= 1 ? v(d2, b2, -si) : 0.f);
-    rhs[idx] = fmaf(-mu, 0.5f * dk + 0.5f * dj + 0.5f * di, yT[idx]);
+struct Tiles {
+    int tk, tj;      // tiles along n3 and n2
+    int count;       // tk * tj * n1
+    int qi, qj, qk;  // grid size = qi (tk tj) + qj tk + qk
+};
+
+// body(i, j, k) for every voxel of this thread's tiles
+template <typename F>
+__device__ __forceinline__ void for_voxels(const Tiles &tl, const Dims &dm, F &&body) {
+    const int per = tl.tk * tl.tj;
+    int t = (int)blockIdx.x;
+    int i = t / per;
+    int jb = (t - i * per) / tl.tk;
+    int kb = t - i * per - jb * tl.tk;
+    const int ty = (int)(threadIdx.x >> 5), tx = (int)(threadIdx.x & 31);
+    for (; t < tl.count; t += (int)gridDim.x) {
+        const int k = kb * 32 + tx;
+        if (k < dm.n3) {
+#pragma unroll
+            for (int u = 0; u < kTileRows / 8; ++u) {
+                const int j = jb * kTileRows + ty + 8 * u;
+                if (j < dm.n2) body(i, j, k);
+            }
+        }
+        kb += tl.qk;
+        if (kb >= tl.tk) {
+            kb -= tl.tk;
+            ++jb;
+        }
+        jb += tl.qj;
+        if (jb >= tl.tj) {
+            jb -= tl.tj;
+            ++i;
+        }
+        i += tl.qi;
+    }
 }
 
-// g = grad x; t = g + b; s = |t|; d = max(0, s - lam/mu) t / (s + 1e-8); b += g - d
-__global__ void __launch_bounds__(256) sb_shrink_kernel(const float *__restrict__ x, float *d0,
-                                                        float *d1, float *d2, float *b0, float *b1,
-                                                        float *b2, Dims dm, float thresh,
-                                                        const CGState *st) {
-    if (st->sb_done) return;
-    LC_VOXEL_INDEX(dm);
-    const float g0 = 0.5f * ((k + 1 < dm.n3 ? x[idx + 1] : 0.f) - (k >= 1 ? x[idx - 1] : 0.f));
-    const float g1 = 0.5f * ((j + 1 < dm.n2 ? x[idx + sj] : 0.f) - (j >= 1 ? x[idx - sj] : 0.f));
-    const float g2 = 0.5f * ((i + 1 < dm.n1 ? x[idx + si] : 0.f) - (i >= 1 ? x[idx - si] : 0.f));
-    const float c0 = b0[idx], c1 = b1[idx], c2 = b2[idx];
-    const float t0 = g0 + c0, t1 = g1 + c1, t2 = g2 + c2;
-    const float s = sqrtf(t0 * t0 + t1 * t1 + t2 * t2);
-    const float m = fmaxf(0.f, s - thresh);
-    const float inv = 1.0f / (s + 1e-8f);
-    const float e0 = m * (t0 * inv), e1 = m * (t1 * inv), e2 = m * (t2 * inv);
-    d0[idx] = e0;
-    d1[idx] = e1;
-    d2[idx] = e2;
-    b0[idx] = c0 + (g0 - e0);
-    b1[idx] = c1 + (g1 - e1);
-    b2[idx] = c2 + (g2 - e2);
+// per-axis term of the negative-Laplacian stencil (src/gpu/finitediff.cu:28-222):
+// 0.5 (g[i+1] - g[i-1]) with g[k] = 0.5 (x[k+1] - x[k-1]) and x = g = 0 outside
+__device__ __forceinline__ float lap_term(const float *__restrict__ x, int idx, int pos, int n, int s,
+                                          float c) {
+    const float p2 = (pos + 2 < n) ? x[idx + 2 * s] : 0.f;
+    const float m2 = (pos >= 2) ? x[idx - 2 * s] : 0.f;
+    const float gp = (pos + 1 < n) ? 0.5f * (p2 - c) : 0.f;
+    const float gm = (pos >= 1) ? 0.5f * (c - m2) : 0.f;
+    return 0.5f * (gp - gm);
 }
 
+__device__ __forceinline__ float lap_at(const float *__restrict__ x, int idx, int i, int j, int k,
+                                        const Dims &dm) {
+    const float c = x[idx];
+    float lap = 0.f;
+    lap += lap_term(x, idx, k, dm.n3, 1, c);
+    lap += lap_term(x, idx, j, dm.n2, dm.n3, c);
+    lap += lap_term(x, idx, i, dm.n1, dm.n2 * dm.n3, c);
+    return lap;
+}
+
+// Start of a Split-Bregman outer iteration (src/bregman.cpp:36-94):
+//   rhs = yT - mu div(d - b)   (div = sum over axes of the zero-padded
+//                               central difference; rhs is not stored)
+//   ax  = tx - mu lap(x)       when tx (= A^T A x) is given, else the carried ax
+//   r = rhs - ax,  p = r (when p is given);  partials rhs.rhs, r.r
+// i.e. the warm-started CG initialisation of src/conjgrad.cpp:33-76.
 template <typename A>
-__global__ void __launch_bounds__(kThreads) sb_diff_kernel(const float *__restrict__ x, float *xold,
-                                                          long n, double *part, unsigned *counter,
-                                                          CGState *st, float xtol) {
+__global__ void __launch_bounds__(kThreads)
+    sb_begin_kernel(const float *__restrict__ yT, const float *__restrict__ d0, const float *__restrict__ d1,
+                    const float *__restrict__ d2, const float *__restrict__ b0, const float *__restrict__ b1,
+                    const float *__restrict__ b2, const float *__restrict__ tx, const float *__restrict__ x,
+                    float *__restrict__ ax, float *__restrict__ r, float *__restrict__ p, Dims dm, Tiles tl,
+                    float mu, double *part, unsigned *counter, CGState *st) {
+    if (st->sb_done) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->done = 1;
+        return;
+    }
+    A v[2] = {A(0), A(0)};
+    const int sj = dm.n3, si = dm.n2 * dm.n3;
+    for_voxels(tl, dm, [&](int i, int j, int k) {
+        const int idx = i * si + j * sj + k;
+        auto dv = [&](const float *d, const float *b, int o) { return d[idx + o] - b[idx + o]; };
+        const float dk = (k + 1 < dm.n3 ? dv(d0, b0, 1) : 0.f) - (k >= 1 ? dv(d0, b0, -1) : 0.f);
+        const float dj = (j + 1 < dm.n2 ? dv(d1, b1, sj) : 0.f) - (j >= 1 ? dv(d1, b1, -sj) : 0.f);
+        const float di = (i + 1 < dm.n1 ? dv(d2, b2, si) : 0.f) - (i >= 1 ? dv(d2, b2, -si) : 0.f);
+        const float rhs = fmaf(-mu, 0.5f * dk + 0.5f * dj + 0.5f * di, yT[idx]);
+        float a;
+        if (tx) {
+            a = fmaf(-mu, lap_at(x, idx, i, j, k, dm), tx[idx]);
+            ax[idx] = a;
+        } else {
+            a = ax[idx];
+        }
+        const float ri = rhs - a;
+        r[idx] = ri;
+        if (p) p[idx] = ri;
+        v[0] += (A)rhs * (A)rhs;
+        v[1] += (A)ri * (A)ri;
+    });
+    if (block_partials<A, 2>(v, part, counter)) {
+        double y2 = total<A>(part, 0, gridDim.x);
+        double r2 = total<A>(part, 1, gridDim.x);
+        if (threadIdx.x == 0) {
+            st->y2 = y2;
+            st->rs_old = r2;
+            st->iters = 0;
+            st->done = 0;
+            st->reason = 0;
+            st->res = 0;
+            st->dx = 0;
+            *counter = 0;
+        }
+    }
+}
+
+// ap = tp - mu lap(p) in place (tp = A^T A p on entry), then p.Ap and alpha:
+// the operator (A^T A + mu (-lap)) of the Split-Bregman CG and its dot product
+// in one pass
+template <typename A>
+__global__ void __launch_bounds__(kThreads) lap_dot_kernel(const float *__restrict__ p, float *__restrict__ ap, Dims dm,
+                                                          Tiles tl, float mu, double *part,
+                                                          unsigned *counter, CGState *st) {
+    if (st->done) return;
+    A v[1] = {A(0)};
+    const int sj = dm.n3, si = dm.n2 * dm.n3;
+    for_voxels(tl, dm, [&](int i, int j, int k) {
+        const int idx = i * si + j * sj + k;
+        const float a = fmaf(-mu, lap_at(p, idx, i, j, k, dm), ap[idx]);
+        const float pc = p[idx];
+        ap[idx] = a;
+        v[0] += (A)pc * (A)a;
+    });
+    if (block_partials<A, 1>(v, part, counter)) {
+        double pap = total<A>(part, 0, gridDim.x);
+        if (threadIdx.x == 0) {
+            st->pAp = pap;
+            if (fabs(pap) < 1e-10) {
+                st->done = 1;
+                st->reason = 3;
+            } else {
+                st->alpha = (double)((A)st->rs_old / (A)pap);
+            }
+            *counter = 0;
+        }
+    }
+}
+
+// End of an outer iteration: g = grad x; t = g + b; s = |t|;
+// d = max(0, s - lam/mu) t / (s + 1e-8); b += g - d; then the relative change
+// |x - xold| / |xold| (partials) and xold = x
+template <typename A>
+__global__ void __launch_bounds__(kThreads)
+    sb_shrink_diff_kernel(const float *__restrict__ x, float *__restrict__ xold, float *__restrict__ d0,
+                          float *__restrict__ d1, float *__restrict__ d2, float *__restrict__ b0,
+                          float *__restrict__ b1, float *__restrict__ b2, Dims dm, Tiles tl, float thresh,
+                          double *part, unsigned *counter, CGState *st, float xtol) {
     if (st->sb_done) return;
     A v[2] = {A(0), A(0)};
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        float xi = x[i], xo = xold[i];
-        float df = xi - xo;
+    const int sj = dm.n3, si = dm.n2 * dm.n3;
+    for_voxels(tl, dm, [&](int i, int j, int k) {
+        const int idx = i * si + j * sj + k;
+        // every load first (the buffers are distinct), then the stores
+        const float xi = x[idx], xo = xold[idx];
+        const float c0 = b0[idx], c1 = b1[idx], c2 = b2[idx];
+        const float g0 = 0.5f * ((k + 1 < dm.n3 ? x[idx + 1] : 0.f) - (k >= 1 ? x[idx - 1] : 0.f));
+        const float g1 = 0.5f * ((j + 1 < dm.n2 ? x[idx + sj] : 0.f) - (j >= 1 ? x[idx - sj] : 0.f));
+        const float g2 = 0.5f * ((i + 1 < dm.n1 ? x[idx + si] : 0.f) - (i >= 1 ? x[idx - si] : 0.f));
+        const float t0 = g0 + c0, t1 = g1 + c1, t2 = g2 + c2;
+        const float s = sqrtf(t0 * t0 + t1 * t1 + t2 * t2);
+        const float m = fmaxf(0.f, s - thresh);
+        const float inv = 1.0f / (s + 1e-8f);
+        const float e0 = m * (t0 * inv), e1 = m * (t1 * inv), e2 = m * (t2 * inv);
+        d0[idx] = e0;
+        d1[idx] = e1;
+        d2[idx] = e2;
+        b0[idx] = c0 + (g0 - e0);
+        b1[idx] = c1 + (g1 - e1);
+        b2[idx] = c2 + (g2 - e2);
+        const float df = xi - xo;
         v[0] += (A)df * (A)df;
         v[1] += (A)xo * (A)xo;
-        xold[i] = xi;
-    }
+        xold[idx] = xi;
+    });
     if (block_partials<A, 2>(v, part, counter)) {
-        double d2 = total<A>(part, 0, gridDim.x);
+        double d2s = total<A>(part, 0, gridDim.x);
         double o2 = total<A>(part, 1, gridDim.x);
         if (threadIdx.x == 0) {
-            double rel = sqrt(d2) / (sqrt(o2) + 1e-8);
+            double rel = sqrt(d2s) / (sqrt(o2) + 1e-8);
             st->sb_rel = rel;
             st->sb_iters += 1;
             if (rel < (double)xtol) st->sb_done = 1;
@@ -313,17 +445,17 @@ void Solver::cg_iter(Context &ctx, const Operator &A, float *x, float tol, float
         dot_pap_kernel<float><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
                                                          counter_.get(), st_.get());
         LC_CHECK_LAUNCH();
-        cg_update_kernel<float><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), n_,
-                                                           part_.get(), counter_.get(), st_.get(),
-                                                           tol, xtol);
+        cg_update_kernel<float><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), nullptr,
+                                                           n_, part_.get(), counter_.get(),
+                                                           st_.get(), tol, xtol);
         LC_CHECK_LAUNCH();
     } else {
         dot_pap_kernel<double><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
                                                           counter_.get(), st_.get());
         LC_CHECK_LAUNCH();
-        cg_update_kernel<double><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), n_,
-                                                            part_.get(), counter_.get(), st_.get(),
-                                                            tol, xtol);
+        cg_update_kernel<double><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), nullptr,
+                                                            n_, part_.get(), counter_.get(),
+                                                            st_.get(), tol, xtol);
         LC_CHECK_LAUNCH();
     }
     p_update_kernel<<<nblk_, kThreads, 0, s>>>(p_.get(), r_.get(), n_, st_.get());
@@ -331,7 +463,7 @@ void Solver::cg_iter(Context &ctx, const Operator &A, float *x, float tol, float
 }
 
 void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, int iters,
-                    float tol, float xtol, int fp32, int poll_every, bool in_sb, bool graph) {
+                    float tol, float xtol, int fp32, int poll_every, bool graph) {
     cudaStream_t s = ctx.stream();
     A(x, ap_.get());
     // r <- A x0 (moved), then r = y - r, p = r
@@ -343,7 +475,7 @@ void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, i
         cg_init_kernel<double><<<nblk_, kThreads, 0, s>>>(y, r_.get(), p_.get(), n_, part_.get(),
                                                           counter_.get(), st_.get());
     LC_CHECK_LAUNCH();
-    const bool poll = !in_sb && poll_every > 0;
+    const bool poll = poll_every > 0;
     // With graphs one replay covers `chunk` iterations (the polling interval
     // when the host polls); a remainder runs as ordinary launches.  Iterations
     // after the stop flag are no-ops on the device either way.
@@ -380,7 +512,7 @@ void Solver::cg(Context &ctx, const Operator &A, const float *y, float *x, const
     LC_CHECK_LAUNCH();
     int poll = (p.tol > 0 || p.xtol > 0) ? p.poll_every : 0;
     const bool graph = p.use_graph != 0 && !ctx.prof.on;
-    cg_run(ctx, A, y, x, p.max_iters, p.tol, p.xtol, p.fp32_scalars, poll, false, graph);
+    cg_run(ctx, A, y, x, p.max_iters, p.tol, p.xtol, p.fp32_scalars, poll, graph);
     graph_.reset();
     LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
     LC_CUDA(cudaStreamSynchronize(s));
@@ -397,68 +529,144 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
                            float *x, const SolverParams &p, SolverStats *stats) {
     cudaStream_t s = ctx.stream();
     LC_REQUIRE(dims[0] * dims[1] * dims[2] == n_, "split_bregman: dims do not match the solver size");
+    LC_REQUIRE(n_ < (1L << 31) && dims[1] < (1L << 24) && dims[2] < (1L << 24),
+               "split_bregman: volume too large for 32-bit indexing");
     host_st_ = static_cast<CGState *>(ctx.pinned_scratch(sizeof(CGState)));
+    const int inner = std::max(0, p.inner_iters);
     for (int a = 0; a < 3; ++a) {
         d_[a].ensure(n_, s);
         b_[a].ensure(n_, s);
         d_[a].zero(s);
         b_[a].zero(s);
     }
-    rhs_.ensure(n_, s);
+    ax_.ensure(n_, s);
     xold_.ensure(n_, s);
     LC_CUDA(cudaMemcpyAsync(xold_.get(), x, n_ * sizeof(float), cudaMemcpyDeviceToDevice, s));
     reset_state_kernel<<<1, 1, 0, s>>>(st_.get());
     LC_CHECK_LAUNCH();
     const float mu = p.mu;
-    long dcopy[3] = {dims[0], dims[1], dims[2]};
-    Operator Ap = [&](const float *in, float *out) {
-        AtA(in, out);
-        launch_neg_laplacian_axpy(ctx, in, out, dcopy, mu);
-    };
-    LC_REQUIRE(n_ < (1L << 31) && dims[0] < 65536 && dims[1] < 65536 * 8,
-               "split_bregman: volume too large for 32-bit indexing");
     const Dims dm{(int)dims[0], (int)dims[1], (int)dims[2]};
-    const dim3 vblock(32, 8, 1);
-    const dim3 vgrid((unsigned)((dims[2] + 31) / 32), (unsigned)((dims[1] + 7) / 8), (unsigned)dims[0]);
-    // one outer iteration: rhs, inner CG (warm start), shrinkage, change test.
-    // Launches go to ctx.stream() as it is when the lambda runs (the capture
-    // stream while a graph is recorded).
-    auto outer = [&] {
+    Tiles tl;
+    tl.tk = (int)((dims[2] + 31) / 32);
+    tl.tj = (int)((dims[1] + kTileRows - 1) / kTileRows);
+    const long ntiles = (long)tl.tk * tl.tj * dims[0];
+    LC_REQUIRE(ntiles < (1L << 31), "split_bregman: too many tiles");
+    tl.count = (int)ntiles;
+    // one full wave: the persistent grid is as large as the fewest CTAs of the
+    // three stencil kernels that fit on the device at once (a partial second
+    // wave would repeat a whole CTA's share of tiles on a few SMs)
+    int per_sm = 8;
+    {
+        int b = 0;
+        auto fit = [&](const void *k) {
+            LC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kThreads, 0));
+            per_sm = std::min(per_sm, std::max(b, 1));
+        };
+        if (p.fp32_scalars) {
+            fit((const void *)sb_begin_kernel<float>);
+            fit((const void *)lap_dot_kernel<float>);
+            fit((const void *)sb_shrink_diff_kernel<float>);
+        } else {
+            fit((const void *)sb_begin_kernel<double>);
+            fit((const void *)lap_dot_kernel<double>);
+            fit((const void *)sb_shrink_diff_kernel<double>);
+        }
+    }
+    const int sblk = (int)std::max<long>(1, std::min<long>(ntiles, (long)ctx.num_sms() * per_sm));
+    tl.qi = sblk / (tl.tk * tl.tj);
+    tl.qj = (sblk - tl.qi * tl.tk * tl.tj) / tl.tk;
+    tl.qk = sblk - tl.qi * tl.tk * tl.tj - tl.qj * tl.tk;
+    part_.ensure((long)std::max(sblk, nblk_) * kParts, s);
+    // With one CG iteration per outer iteration its direction is the residual
+    // itself, so p and r share a buffer and r is not stored after the update.
+    float *pp = inner > 1 ? p_.get() : r_.get();
+    const bool fp32 = p.fp32_scalars != 0;
+    // One outer iteration: rhs and the warm-started residual, `inner` CG
+    // iterations, shrinkage and the change test.  The operator product A x of
+    // the warm start is recomputed when `exact` is set and otherwise carried
+    // from the previous iteration's CG updates (ax += alpha A p), which equals
+    // it up to rounding.  Launches go to ctx.stream() as it is when the lambda
+    // runs (the capture stream while a graph is recorded).
+    auto outer = [&](bool exact) {
         const cudaStream_t os = ctx.stream();
+        if (exact) AtA(x, ap_.get());
         {
-            ProfScope ps1(ctx, PS_SB_VEC, 4.0 * n_ * 8.0);
-            sb_rhs_kernel<<<vgrid, vblock, 0, os>>>(yT, d_[0].get(), d_[1].get(), d_[2].get(),
-                                                     b_[0].get(), b_[1].get(), b_[2].get(),
-                                                     rhs_.get(), dm, mu, st_.get());
+            ProfScope ps(ctx, PS_SB_VEC, 4.0 * n_ * (exact ? 11.0 : 9.0) + (inner > 1 ? 4.0 * n_ : 0.0));
+            const float *tx = exact ? ap_.get() : nullptr;
+            float *pinit = inner > 1 ? p_.get() : nullptr;
+            if (fp32)
+                sb_begin_kernel<float><<<sblk, kThreads, 0, os>>>(
+                    yT, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), tx, x,
+                    ax_.get(), r_.get(), pinit, dm, tl, mu, part_.get(), counter_.get(), st_.get());
+            else
+                sb_begin_kernel<double><<<sblk, kThreads, 0, os>>>(
+                    yT, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), tx, x,
+                    ax_.get(), r_.get(), pinit, dm, tl, mu, part_.get(), counter_.get(), st_.get());
             LC_CHECK_LAUNCH();
         }
-        cg_run(ctx, Ap, rhs_.get(), x, p.inner_iters, p.tol, p.xtol, p.fp32_scalars, 0, true, false);
-        ProfScope ps2(ctx, PS_SB_VEC, 4.0 * n_ * 16.0);
-        sb_shrink_kernel<<<vgrid, vblock, 0, os>>>(x, d_[0].get(), d_[1].get(), d_[2].get(),
-                                                    b_[0].get(), b_[1].get(), b_[2].get(), dm,
-                                                    p.lambda / p.mu, st_.get());
-        LC_CHECK_LAUNCH();
-        if (p.fp32_scalars)
-            sb_diff_kernel<float><<<nblk_, kThreads, 0, os>>>(x, xold_.get(), n_, part_.get(),
-                                                              counter_.get(), st_.get(), p.xtol);
+        for (int it = 0; it < inner; ++it) {
+            AtA(pp, ap_.get());
+            ProfScope ps(ctx, PS_CG_VEC, 4.0 * n_ * (inner > 1 ? 13.0 : 10.0));
+            if (fp32) {
+                lap_dot_kernel<float><<<sblk, kThreads, 0, os>>>(pp, ap_.get(), dm, tl, mu, part_.get(),
+                                                                counter_.get(), st_.get());
+                LC_CHECK_LAUNCH();
+                if (inner > 1)
+                    cg_update_kernel<float, true, true><<<nblk_, kThreads, 0, os>>>(
+                        x, r_.get(), pp, ap_.get(), ax_.get(), n_, part_.get(), counter_.get(), st_.get(), p.tol,
+                        p.xtol);
+                else
+                    cg_update_kernel<float, true, false><<<nblk_, kThreads, 0, os>>>(
+                        x, r_.get(), pp, ap_.get(), ax_.get(), n_, part_.get(), counter_.get(), st_.get(), p.tol,
+                        p.xtol);
+            } else {
+                lap_dot_kernel<double><<<sblk, kThreads, 0, os>>>(pp, ap_.get(), dm, tl, mu, part_.get(),
+                                                                 counter_.get(), st_.get());
+                LC_CHECK_LAUNCH();
+                if (inner > 1)
+                    cg_update_kernel<double, true, true><<<nblk_, kThreads, 0, os>>>(
+                        x, r_.get(), pp, ap_.get(), ax_.get(), n_, part_.get(), counter_.get(), st_.get(), p.tol,
+                        p.xtol);
+                else
+                    cg_update_kernel<double, true, false><<<nblk_, kThreads, 0, os>>>(
+                        x, r_.get(), pp, ap_.get(), ax_.get(), n_, part_.get(), counter_.get(), st_.get(), p.tol,
+                        p.xtol);
+            }
+            LC_CHECK_LAUNCH();
+            if (it + 1 < inner) {
+                p_update_kernel<<<nblk_, kThreads, 0, os>>>(p_.get(), r_.get(), n_, st_.get());
+                LC_CHECK_LAUNCH();
+            }
+        }
+        ProfScope ps(ctx, PS_SB_VEC, 4.0 * n_ * 12.0);
+        if (fp32)
+            sb_shrink_diff_kernel<float><<<sblk, kThreads, 0, os>>>(
+                x, xold_.get(), d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
+                tl, p.lambda / p.mu, part_.get(), counter_.get(), st_.get(), p.xtol);
         else
-            sb_diff_kernel<double><<<nblk_, kThreads, 0, os>>>(x, xold_.get(), n_, part_.get(),
-                                                               counter_.get(), st_.get(), p.xtol);
+            sb_shrink_diff_kernel<double><<<sblk, kThreads, 0, os>>>(
+                x, xold_.get(), d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
+                tl, p.lambda / p.mu, part_.get(), counter_.get(), st_.get(), p.xtol);
         LC_CHECK_LAUNCH();
     };
+    // exact operator products every `every` outer iterations (and always in
+    // the first one, which also sets up ax)
+    const int every = std::max(1, p.residual_refresh);
+    auto exact_at = [&](int it) { return it % every == 0; };
     const bool graph = p.use_graph != 0 && !ctx.prof.on && p.max_iters > 1;
-    if (graph && p.max_iters > 0) {
+    if (graph) {
         // the first outer iteration runs eagerly (it also fills the plan and
-        // launch-tuner caches the recorded launches rely on); the rest replay it
-        outer();
-        capture(ctx, outer);
+        // launch-tuner caches the recorded launches rely on); the graph holds
+        // the iteration that the other iterations, but the exact ones, replay
+        outer(true);
+        capture(ctx, [&] { outer(every == 1); });
     }
     const int poll = p.xtol > 0 ? std::max(1, p.poll_every) : 0;
     for (int it = graph ? 1 : 0; it < p.max_iters; ++it) {
-        if (graph)
+        if (graph && (every == 1 || !exact_at(it)))
             graph_.launch(s);
         else
-            outer();
+            outer(exact_at(it));
         if (poll > 0 && (it + 1) % poll == 0 && it + 1 < p.max_iters) {
             LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
             LC_CUDA(cudaStreamSynchronize(s));
@@ -471,7 +679,7 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
     if (stats) {
         stats->iters = host_st_->sb_iters;
         // outer iterations after the stop flag run no CG work
-        stats->cg_iters_total = host_st_->sb_iters * p.inner_iters;
+        stats->cg_iters_total = host_st_->sb_iters * inner;
         stats->residual = host_st_->res;
         stats->dx = host_st_->sb_rel;
         stats->stop_reason = host_st_->sb_done ? 2 : 0;

@@ -24,6 +24,10 @@ struct SolverParams {
     int fp32_scalars = 0;  // 1: float accumulation of dots (the reference GPU path)
     int poll_every = 8;    // iterations between host checks of the stop flag (0: never)
     int use_graph = 0;     // 1: replay CG iterations (Split-Bregman: outer iterations) as CUDA graphs
+    // Split-Bregman: recompute the operator product A x of the warm-started
+    // residual every this many outer iterations (1: every one); in between it
+    // is carried by the CG updates
+    int residual_refresh = 1;
 };
 
 struct SolverStats {
@@ -62,7 +66,7 @@ class Solver {
 
   private:
     void cg_run(Context &ctx, const Operator &A, const float *y, float *x, int iters, float tol,
-                float xtol, int fp32, int poll_every, bool in_sb, bool graph);
+                float xtol, int fp32, int poll_every, bool graph);
     // one CG iteration: Ap = A p, the fused scalar/vector updates, p = r + beta p
     void cg_iter(Context &ctx, const Operator &A, float *x, float tol, float xtol, int fp32);
     // records body into graph_ on the context's private stream
@@ -71,7 +75,7 @@ class Solver {
     long n_;
     int nblk_;
     DevBuf<float> r_, p_, ap_, xold_;
-    DevBuf<float> d_[3], b_[3], rhs_;
+    DevBuf<float> d_[3], b_[3], ax_;
     DevBuf<double> part_;
     DevBuf<unsigned> counter_;
     DevBuf<CGState> st_;
