@@ -22,16 +22,38 @@ __device__ __forceinline__ double dirichlet(double u, int n) {
 }
 
 // Per-angle coefficients of the fast PSF generator: uX = a . k, uY = b . k
-// (k = (kx, ky, kz)), and the phasors exp(i pi a0), exp(i pi a0 / nx),
-// exp(i pi b0), exp(i pi b0 / ny) that advance sin(pi uX), sin(pi uX / nx), ...
-// by one step in kx.
+// (k = (kx, ky, kz)), and (cos, sin) of pi a0, pi a0 / nx, pi b0, pi b0 / ny,
+// the steps of sin(pi uX), sin(pi uX / nx), ... from one kx to the next.
 struct PsfAngle {
     double a[3], b[3];
     double2 stepA, stepB, stepC, stepD;
 };
 
-__device__ __forceinline__ double2 crot(double2 p, double2 s) {
-    return make_double2(p.x * s.x - p.y * s.y, p.x * s.y + p.y * s.x);
+// sin(pi (u0 + s h)), s = 0, 1, ..., by the three-term recurrence
+// sin(x + t) = 2 cos t sin x - sin(x - t) with t = pi h: one FMA per step.
+// Over the S-step segments of the PSF rows the rounding error grows like
+// S^2 eps (sin(n t) / sin t <= n bounds the propagation of each error).
+struct SinSeq {
+    double prev, cur, two_c;
+    // step = (cos pi h, sin pi h)
+    __device__ __forceinline__ void init(double u0, double2 step) {
+        double s0, c0;
+        sincospi(u0, &s0, &c0);
+        cur = s0;
+        prev = s0 * step.x - c0 * step.y;
+        two_c = 2.0 * step.x;
+    }
+    __device__ __forceinline__ void advance() {
+        const double n = fma(two_c, cur, -prev);
+        prev = cur;
+        cur = n;
+    }
+};
+
+// Dirichlet term sin(pi u) / sin(pi u / n) from the two sines, or from the
+// closed form near its poles
+__device__ __forceinline__ double dirichlet_term(double num, double den, double u, int n) {
+    return fabs(den) > 1e-6 ? num / den : dirichlet(u, n);
 }
 
 __device__ __forceinline__ int mirror_index(int j, int P) {
@@ -42,12 +64,12 @@ __device__ __forceinline__ int mirror_index(int j, int P) {
 
 // Rows of K (all kx of one (kz, ky)) in segments of S values of kx.  The sum over
 // angles uses the Dirichlet closed form, with sin(pi u) and sin(pi u / n)
-// advanced along kx by complex rotations (FP64; rounding grows by ~1e-16 per
-// step over S steps) and evaluated directly whenever the denominator is small.
+// advanced along kx by the three-term sine recurrence (FP64) and evaluated in
+// closed form whenever the denominator is small.
 // Only the half space kz <= 0 (2D: ky <= 0) is summed; K(-k) = K(k) fills the
 // rest.
 template <int DIM, int S>
-__global__ void __launch_bounds__(128) psf_rows_kernel(const PsfAngle *__restrict__ angles, int ntheta,
+__global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__restrict__ angles, int ntheta,
                                                       const int *__restrict__ groups, int ngroups,
                                                       int nx, int ny, int P1, int P2, int P3,
                                                       double *__restrict__ K) {
@@ -84,70 +106,140 @@ __global__ void __launch_bounds__(128) psf_rows_kernel(const PsfAngle *__restric
             // uX = a . k does not depend on theta (a is the first column of
             // transpose(Rx(theta) Ry(beta) Rz(gamma)), which Rx leaves alone), so
             // within a group of angles of equal (beta, gamma) the sum factors:
-            // K = sum_groups D_nx(uX) * sum_{theta in group} D_ny(uY)
+            // K = sum_groups D_nx(uX) * sum_{theta in group} D_ny(uY).  Four
+            // (then two, then one) angles share one division.
             for (int gi = 0; gi < ngroups; ++gi) {
                 const int i0 = gst[gi], i1 = gst[gi + 1];
                 double ay[S];
 #pragma unroll
                 for (int s = 0; s < S; ++s) ay[s] = 0.0;
-                for (int i = i0; i < i1; ++i) {
-                    const PsfAngle &A = ang[i];
-                    const double uY0 = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
-                    double2 pC, pD;
-                    sincospi(uY0, &pC.y, &pC.x);
-                    sincospi(uY0 * inv_ny, &pD.y, &pD.x);
+                int i = i0;
+                // four angles per division:
+                // a/b + c/d + e/f + g/h = ((a d + c b) f h + (e h + g f) b d) / (b d f h)
+                for (; i + 3 < i1; i += 4) {
+                    const PsfAngle &A = ang[i], &B = ang[i + 1], &C = ang[i + 2], &D = ang[i + 3];
+                    const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
+                    const double uB = B.b[0] * kx0 + B.b[1] * ky + B.b[2] * kz;
+                    const double uC = C.b[0] * kx0 + C.b[1] * ky + C.b[2] * kz;
+                    const double uD = D.b[0] * kx0 + D.b[1] * ky + D.b[2] * kz;
+                    SinSeq nA, dA, nB, dB, nC, dC, nD, dD;
+                    nA.init(uA, A.stepC);
+                    dA.init(uA * inv_ny, A.stepD);
+                    nB.init(uB, B.stepC);
+                    dB.init(uB * inv_ny, B.stepD);
+                    nC.init(uC, C.stepC);
+                    dC.init(uC * inv_ny, C.stepD);
+                    nD.init(uD, D.stepC);
+                    dD.init(uD * inv_ny, D.stepD);
 #pragma unroll
                     for (int s = 0; s < S; ++s) {
-                        ay[s] += fabs(pD.y) > 1e-6 ? pC.y / pD.y : dirichlet(uY0 + (double)s * A.b[0], ny);
-                        pC = crot(pC, A.stepC);
-                        pD = crot(pD, A.stepD);
+                        if (fabs(dA.cur) > 1e-6 && fabs(dB.cur) > 1e-6 && fabs(dC.cur) > 1e-6 &&
+                            fabs(dD.cur) > 1e-6) {
+                            const double pab = fma(nA.cur, dB.cur, nB.cur * dA.cur), qab = dA.cur * dB.cur;
+                            const double pcd = fma(nC.cur, dD.cur, nD.cur * dC.cur), qcd = dC.cur * dD.cur;
+                            ay[s] += fma(pab, qcd, pcd * qab) / (qab * qcd);
+                        } else {
+                            const double sd = (double)s;
+                            ay[s] += dirichlet_term(nA.cur, dA.cur, uA + sd * A.b[0], ny) +
+                                     dirichlet_term(nB.cur, dB.cur, uB + sd * B.b[0], ny) +
+                                     dirichlet_term(nC.cur, dC.cur, uC + sd * C.b[0], ny) +
+                                     dirichlet_term(nD.cur, dD.cur, uD + sd * D.b[0], ny);
+                        }
+                        nA.advance();
+                        dA.advance();
+                        nB.advance();
+                        dB.advance();
+                        nC.advance();
+                        dC.advance();
+                        nD.advance();
+                        dD.advance();
+                    }
+                }
+                for (; i + 1 < i1; i += 2) {
+                    const PsfAngle &A = ang[i], &B = ang[i + 1];
+                    const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
+                    const double uB = B.b[0] * kx0 + B.b[1] * ky + B.b[2] * kz;
+                    SinSeq nA, dA, nB, dB;
+                    nA.init(uA, A.stepC);
+                    dA.init(uA * inv_ny, A.stepD);
+                    nB.init(uB, B.stepC);
+                    dB.init(uB * inv_ny, B.stepD);
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        if (fabs(dA.cur) > 1e-6 && fabs(dB.cur) > 1e-6) {
+                            ay[s] += fma(nA.cur, dB.cur, nB.cur * dA.cur) / (dA.cur * dB.cur);
+                        } else {
+                            ay[s] += dirichlet_term(nA.cur, dA.cur, uA + (double)s * A.b[0], ny) +
+                                     dirichlet_term(nB.cur, dB.cur, uB + (double)s * B.b[0], ny);
+                        }
+                        nA.advance();
+                        dA.advance();
+                        nB.advance();
+                        dB.advance();
+                    }
+                }
+                if (i < i1) {
+                    const PsfAngle &A = ang[i];
+                    const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
+                    SinSeq nA, dA;
+                    nA.init(uA, A.stepC);
+                    dA.init(uA * inv_ny, A.stepD);
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        ay[s] += dirichlet_term(nA.cur, dA.cur, uA + (double)s * A.b[0], ny);
+                        nA.advance();
+                        dA.advance();
                     }
                 }
                 const PsfAngle &A = ang[i0];
                 const double uX0 = A.a[0] * kx0 + A.a[1] * ky + A.a[2] * kz;
-                double2 pA, pB;
-                sincospi(uX0, &pA.y, &pA.x);
-                sincospi(uX0 * inv_nx, &pB.y, &pB.x);
+                SinSeq nX, dX;
+                nX.init(uX0, A.stepA);
+                dX.init(uX0 * inv_nx, A.stepB);
 #pragma unroll
                 for (int s = 0; s < S; ++s) {
-                    const double dX =
-                        fabs(pB.y) > 1e-6 ? pA.y / pB.y : dirichlet(uX0 + (double)s * A.a[0], nx);
-                    acc[s] = fma(dX, ay[s], acc[s]);
-                    pA = crot(pA, A.stepA);
-                    pB = crot(pB, A.stepB);
+                    acc[s] = fma(dirichlet_term(nX.cur, dX.cur, uX0 + (double)s * A.a[0], nx), ay[s], acc[s]);
+                    nX.advance();
+                    dX.advance();
                 }
             }
-        }
-        for (int i = 0; DIM == 2 && i < ntheta; ++i) {
-            const PsfAngle &A = ang[i];
-            const double uX0 = A.a[0] * kx0 + A.a[1] * ky + A.a[2] * kz;
-            double2 pA, pB, pC = make_double2(1.0, 0.0), pD = make_double2(1.0, 0.0);
-            sincospi(uX0, &pA.y, &pA.x);
-            sincospi(uX0 * inv_nx, &pB.y, &pB.x);
-            double uY0 = 0.0;
-            if (DIM == 3) {
-                uY0 = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
-                sincospi(uY0, &pC.y, &pC.x);
-                sincospi(uY0 * inv_ny, &pD.y, &pD.x);
-            }
+        } else {
+            // 2D: K = sum_theta D_nx(uX), two angles per division
+            int i = 0;
+            for (; i + 1 < ntheta; i += 2) {
+                const PsfAngle &A = ang[i], &B = ang[i + 1];
+                const double uA = A.a[0] * kx0 + A.a[1] * ky;
+                const double uB = B.a[0] * kx0 + B.a[1] * ky;
+                SinSeq nA, dA, nB, dB;
+                nA.init(uA, A.stepA);
+                dA.init(uA * inv_nx, A.stepB);
+                nB.init(uB, B.stepA);
+                dB.init(uB * inv_nx, B.stepB);
 #pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const bool okX = fabs(pB.y) > 1e-6;
-                const bool okY = DIM != 3 || fabs(pD.y) > 1e-6;
-                if (okX && okY) {
-                    // one division: D_X D_Y = (sin(pi uX) sin(pi uY)) / (sin(pi uX/nx) sin(pi uY/ny))
-                    acc[s] += DIM == 3 ? (pA.y * pC.y) / (pB.y * pD.y) : pA.y / pB.y;
-                } else {
-                    double dX = okX ? pA.y / pB.y : dirichlet(uX0 + (double)s * A.a[0], nx);
-                    double dY = 1.0;
-                    if (DIM == 3) dY = okY ? pC.y / pD.y : dirichlet(uY0 + (double)s * A.b[0], ny);
-                    acc[s] += dX * dY;
+                for (int s = 0; s < S; ++s) {
+                    if (fabs(dA.cur) > 1e-6 && fabs(dB.cur) > 1e-6) {
+                        acc[s] += fma(nA.cur, dB.cur, nB.cur * dA.cur) / (dA.cur * dB.cur);
+                    } else {
+                        acc[s] += dirichlet_term(nA.cur, dA.cur, uA + (double)s * A.a[0], nx) +
+                                  dirichlet_term(nB.cur, dB.cur, uB + (double)s * B.a[0], nx);
+                    }
+                    nA.advance();
+                    dA.advance();
+                    nB.advance();
+                    dB.advance();
                 }
-                pA = crot(pA, A.stepA);
-                pB = crot(pB, A.stepB);
-                if (DIM == 3) {
-                    pC = crot(pC, A.stepC);
-                    pD = crot(pD, A.stepD);
+            }
+            if (i < ntheta) {
+                const PsfAngle &A = ang[i];
+                const double uA = A.a[0] * kx0 + A.a[1] * ky;
+                SinSeq nA, dA;
+                nA.init(uA, A.stepA);
+                dA.init(uA * inv_nx, A.stepB);
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    acc[s] += dirichlet_term(nA.cur, dA.cur, uA + (double)s * A.a[0], nx);
+                    nA.advance();
+                    dA.advance();
                 }
             }
         }
