@@ -303,6 +303,33 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def kernel_case(case: str, reps: int):
+    """Reduced cases for profiler captures of one kernel family at the
+    workload's padded volume [29, 721, 721] (P = [64, 1458, 1458]); prints
+    timings, not a benchmark line.
+      toeplitz       PSF from the workload's 360 angles, then `reps` A^T A applies
+      split_bregman  PSF from 12 of the angles (cheap to build), then
+                     Split-Bregman with `reps` outer iterations, one CG each"""
+    import torch
+    import laminocam_b200 as lc
+    n1, n = 29, 721
+    nth = NANGLES if case == "toeplitz" else 12
+    th = np.arange(nth) * 2 * np.pi / nth
+    pg = lc.PolarGrid(th, np.full(nth, -GAMMA_DEG * np.pi / 180.0), np.zeros(nth), DET[0], DET[1])
+    psf = lc.PointSpreadFunction(pg, (n1, n, n))
+    x = torch.rand((n1, n, n), device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+    torch.cuda.synchronize()
+    t0 = time.time()
+    if case == "toeplitz":
+        for _ in range(reps):
+            psf.convolve(x)
+    else:
+        lc.split_bregman(psf, x, torch.zeros_like(x), LAM, MU, reps, 1, 0.0, 0.0)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": case, "P": list(psf.P), "reps": reps,
+                      "ms_per_rep": (time.time() - t0) * 1e3 / reps}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -321,7 +348,12 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="reduced case for profiler captures: recon_dims [15,255,255], 180 angles, "
                          "255x255 detector, 5 outer iterations (not a benchmark line)")
+    ap.add_argument("--kernel-case", choices=["toeplitz", "split_bregman"],
+                    help="reduced case for a profiler capture of one kernel family (not a benchmark line)")
+    ap.add_argument("--reps", type=int, default=3, help="applies or outer iterations of --kernel-case")
     args = ap.parse_args()
+    if args.kernel_case:
+        return kernel_case(args.kernel_case, args.reps)
     if args.small:
         global RECON_DIMS, NANGLES, DET, OUTER, N_ELLIPSOIDS
         RECON_DIMS, NANGLES, DET, OUTER, N_ELLIPSOIDS = (15, 255, 255), 180, (255, 255), 5, 10

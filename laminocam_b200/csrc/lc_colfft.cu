@@ -48,8 +48,17 @@ constexpr size_t col_smem() {
     return ((size_t)col_nv<MODE>() * M * kCols + 2 * (size_t)M) * sizeof(float2);
 }
 
+// CTAs per SM the register budget is sized for: three for the small CTAs,
+// fewer for the long lines (whose threads hold up to 2 x 16 elements)
+template <int R0, int R1, int R2>
+constexpr int col_min_blocks() {
+    constexpr int t = RegPlan<R0, R1, R2>::NT * kCols;
+    return t <= 352 ? 3 : (t <= 448 ? 2 : 1);
+}
+
 template <int R0, int R1, int R2, int MODE>
-__global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kCols, 3) col_fft_kernel(ColArgs a) {
+__global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kCols, (col_min_blocks<R0, R1, R2>()))
+    col_fft_kernel(ColArgs a) {
     using P = RegPlan<R0, R1, R2>;
     constexpr int M = P::M, RM = P::RM, C = kCols;
     constexpr bool SPLIT = MODE >= CM_SPLIT_IN;

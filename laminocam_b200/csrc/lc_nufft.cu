@@ -255,17 +255,43 @@ __global__ void bin_scatter_kernel(PolarPts pts, GridCfg g, int W, int *cursor, 
 // flush forms (H 2^20 + L) / (F 2^20) in FP64.  The sums are exact, so the
 // tile's content does not depend on the order of the atomics; the resolution
 // 1 / (F 2^20) is below 2^-40 m.
+//
+// The accumulators take the raw bit patterns of the rounded floats, whose
+// integer values sit above the bits of 1.5 * 2^23 (B): a cell reached by K
+// points holds sum h + K B (mod 2^32).  K is the number of footprints that
+// cover the cell, a 7-wide box sum per axis of the histogram of footprint
+// corners (one atomic per point), so the flush subtracts K B exactly.
 constexpr int kSpreadThreads = 256;
 constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
-constexpr int kRoundMagicBits = 0x4B400000;
+constexpr unsigned kRoundMagicBits = 0x4B400000u;
 
-// hi += round(v), lo += round((v - round(v)) 2^20) for |v| < 2^22
-__device__ __forceinline__ void fixed_add(int *hi, int *lo, float v) {
-    const float y1 = v + kRoundMagic;
+// hi += round(a b) + B, lo += round((a b - round(a b)) 2^20) + B, |a b| < 2^22
+__device__ __forceinline__ void fixed_add(int *hi, int *lo, float a, float b) {
+    const float y1 = fmaf(a, b, kRoundMagic);
     const float h = y1 - kRoundMagic;
-    const float y2 = fmaf(v - h, 1048576.0f, kRoundMagic);
-    atomicAdd(hi, __float_as_int(y1) - kRoundMagicBits);
-    atomicAdd(lo, __float_as_int(y2) - kRoundMagicBits);
+    const float y2 = fmaf(fmaf(a, b, -h), 1048576.0f, kRoundMagic);
+    atomicAdd(hi, __float_as_int(y1));
+    atomicAdd(lo, __float_as_int(y2));
+}
+
+// cnt[q] <- sum of cnt[q - d], d in [0, w), along one axis of a tile of
+// tx x ty x tz cells (in place: a thread walks each of its lines downwards
+// with a sliding window, so the values it still reads are the original ones)
+__device__ __forceinline__ void box_sum_axis(int *cnt, int axis, int w, int tx, int ty, int tz) {
+    const int plane = tx * ty;
+    const int n = axis == 0 ? tx : (axis == 1 ? ty : tz);
+    const int stride = axis == 0 ? 1 : (axis == 1 ? tx : plane);
+    const int nlines = axis == 0 ? ty * tz : (axis == 1 ? tx * tz : plane);
+    for (int line = threadIdx.x; line < nlines; line += blockDim.x) {
+        const int base = axis == 0 ? line * tx : (axis == 1 ? (line % tx) + (line / tx) * plane : line);
+        int win = 0;
+        for (int q = max(0, n - w); q < n; ++q) win += cnt[base + q * stride];
+        for (int q = n - 1; q >= 0; --q) {
+            const int cq = cnt[base + q * stride];
+            cnt[base + q * stride] = win;
+            win += (q - w >= 0 ? cnt[base + (q - w) * stride] : 0) - cq;
+        }
+    }
 }
 
 template <int DIM, int W>
@@ -297,11 +323,12 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
     int *lre = hre + acc_n;                        // low words, real parts
     int *him = lre + acc_n;
     int *lim = him + acc_n;
-    int *order = lim + acc_n;
+    int *kcnt = lim + acc_n;  // footprint corners per cell, then footprints per cell
+    int *order = kcnt + tsize;
     constexpr int kKeys = 8;  // points per thread in the bucketing pass (maxpts <= 8 * threads)
     int key[kKeys];
     const int tid = threadIdx.x;
-    for (long idx = tid; idx < 4 * acc_n; idx += blockDim.x) hre[idx] = 0;
+    for (long idx = tid; idx < 4 * acc_n + tsize; idx += blockDim.x) hre[idx] = 0;
     if (tid < 32) cnt[tid] = 0;
     if (tid == 0) cmax_bits = 0;
     __syncthreads();
@@ -329,6 +356,7 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
             }
             const int b = corner & 31;
             k = (b << 16) | atomicAdd(&cnt[b], 1);
+            atomicAdd(&kcnt[corner], 1);
             // |Re(c m)|, |Im(c m)| <= |Re c| + |Im c| for the unit phase m of the shift mode
             for (int s = 0; s < nvol; ++s) {
                 const float2 v = c[(long)s * cstride + j];
@@ -415,8 +443,8 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
                     const int row = dy * tx;
 #pragma unroll
                     for (int dx = 0; dx < W; ++dx) {
-                        fixed_add(hr + row + dx, lr + row + dx, vr * wk[0][dx]);
-                        fixed_add(hi + row + dx, li + row + dx, vi * wk[0][dx]);
+                        fixed_add(hr + row + dx, lr + row + dx, vr, wk[0][dx]);
+                        fixed_add(hi + row + dx, li + row + dx, vi, wk[0][dx]);
                     }
                 }
             } else {
@@ -434,8 +462,8 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
                         const int row = zo + dy * tx;
 #pragma unroll
                         for (int dx = 0; dx < W; ++dx) {
-                            fixed_add(hr + row + dx, lr + row + dx, vr * wk[0][dx]);
-                            fixed_add(hi + row + dx, li + row + dx, vi * wk[0][dx]);
+                            fixed_add(hr + row + dx, lr + row + dx, vr, wk[0][dx]);
+                            fixed_add(hi + row + dx, li + row + dx, vi, wk[0][dx]);
                         }
                     }
                 }
@@ -443,15 +471,23 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
         }
     }
     __syncthreads();
+    // footprints per cell: box sums of the corner histogram along each axis
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        box_sum_axis(kcnt, d, W, tx, ty, tz);
+        __syncthreads();
+    }
     // flush the tile (halos overlap neighbouring bins, so accumulate atomically)
     const double unscale = 1.0 / ((double)fscale * 1048576.0);
     for (long idx = tid; idx < acc_n; idx += blockDim.x) {
-        const int h1 = hre[idx], l1 = lre[idx], h2 = him[idx], l2 = lim[idx];
-        if ((h1 | l1 | h2 | l2) == 0) continue;
-        const float a = (float)(((double)h1 * 1048576.0 + (double)l1) * unscale);
-        const float b = (float)(((double)h2 * 1048576.0 + (double)l2) * unscale);
         const int s = (int)(idx / tsize);
         const int rr = (int)(idx - (long)s * tsize);
+        const unsigned kb = (unsigned)kcnt[rr] * kRoundMagicBits;
+        if (kcnt[rr] == 0) continue;
+        const int h1 = (int)((unsigned)hre[idx] - kb), l1 = (int)((unsigned)lre[idx] - kb);
+        const int h2 = (int)((unsigned)him[idx] - kb), l2 = (int)((unsigned)lim[idx] - kb);
+        const float a = (float)(((double)h1 * 1048576.0 + (double)l1) * unscale);
+        const float b = (float)(((double)h2 * 1048576.0 + (double)l2) * unscale);
         const int ix = rr % tx;
         const int iy = (rr / tx) % ty;
         const int iz = rr / plane;
@@ -703,9 +739,10 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
     // values read once, fine grid written once (plus the permutation)
     ProfScope ps(ctx, PS_SPREAD, (double)nvol * (8.0 * pts_.M + 8.0 * gvol) + 4.0 * pts_.M);
     // four 32-bit fixed-point accumulators per cell (high and low words of the
-    // real and imaginary parts)
+    // real and imaginary parts) per volume, a footprint count per cell, and the
+    // bucketed point order
     const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * 4 * sizeof(int);
-    const size_t bucket_bytes = (size_t)maxsub_ * sizeof(int);
+    const size_t bucket_bytes = (size_t)maxsub_ * sizeof(int) + (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(int);
     LC_REQUIRE(maxsub_ <= 8 * kSpreadThreads, "NUFFT spread: subproblem larger than the bucketing pass");
     LC_REQUIRE(maxsub_ <= 2048, "NUFFT spread: subproblem too large for the fixed-point sums");
     const int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);

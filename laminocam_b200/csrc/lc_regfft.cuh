@@ -188,11 +188,38 @@ struct RegPlan {
     static constexpr int RM = cmax(R0, cmax(R1, R2));      // registers per line
 };
 
-// Line lengths M with a register plan: X(M, R0, R1, R2), radices in stage order
+// Line lengths M with a register plan: X(M, R0, R1, R2), radices in stage
+// order.  Every 2^p 3^q length from 64 to 1296 whose three radices are at most
+// 16 with M / min(R) <= 144 threads per line.  An odd first radix keeps the
+// first stage's strided shared-memory writes free of bank conflicts.
 #define LC_LINE_PLANS(X) \
-    X(96, 8, 4, 3)       \
+    X(64, 4, 4, 4)       \
+    X(72, 3, 4, 6)       \
+    X(81, 9, 3, 3)       \
+    X(96, 3, 8, 4)       \
+    X(108, 3, 6, 6)      \
+    X(128, 8, 4, 4)      \
+    X(144, 9, 4, 4)      \
+    X(162, 9, 6, 3)      \
+    X(192, 3, 8, 8)      \
+    X(216, 9, 6, 4)      \
     X(243, 9, 9, 3)      \
-    X(729, 9, 9, 9)
+    X(256, 8, 8, 4)      \
+    X(288, 9, 8, 4)      \
+    X(324, 9, 6, 6)      \
+    X(384, 6, 8, 8)      \
+    X(432, 9, 6, 8)      \
+    X(486, 9, 9, 6)      \
+    X(512, 8, 8, 8)      \
+    X(576, 9, 8, 8)      \
+    X(648, 9, 9, 8)      \
+    X(729, 9, 9, 9)      \
+    X(768, 12, 8, 8)     \
+    X(864, 9, 12, 8)     \
+    X(972, 9, 9, 12)     \
+    X(1024, 16, 8, 8)    \
+    X(1152, 9, 16, 8)    \
+    X(1296, 9, 12, 12)
 
 inline bool line_plan_exists(int M) {
     switch (M) {

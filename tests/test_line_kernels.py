@@ -56,14 +56,21 @@ def test_toeplitz3d_line_kernels(lc, n):
     assert err < TOL, (n, psf.P, err)
 
 
-@pytest.mark.parametrize("n", SIZES)
+# one slice size per register plan: the half length P/2 of n (P = next_smooth(2n - 1))
+# walks 64, 72, 81, 96, 108, 128, ..., 1152, 1296 (every plan of the kernels)
+SIZES_2D = [60, 70, 77, 90, 100, 125, 140, 150, 180, 200, 230, 250, 270, 300, 340, 375, 400, 450,
+            500, 550, 600, 700, 750, 800, 900, 1000, 1100, 1200, 45, 115]
+
+
+@pytest.mark.parametrize("n", SIZES_2D)
 def test_toeplitz2d_line_kernels(lc, n):
     rng = np.random.default_rng(200 + n)
     nth = 16
     th = np.arange(nth) * np.pi / nth
     pg = lc.PolarGrid2D(th, n)
-    x = rng.random((2, n, n)).astype(np.float32)
-    psf = lc.PointSpreadFunction2D(pg, n, 2)
+    ns = 2 if n < 400 else 1
+    x = rng.random((ns, n, n)).astype(np.float32)
+    psf = lc.PointSpreadFunction2D(pg, n, ns)
     got = to_np(psf.convolve(x))
     want = oracle_convolve(psf, x)
     err = O.rel_l2(got, want)
