@@ -211,11 +211,11 @@ def mix_jobs(lc, count=MIX_JOBS, seed=3000):
     return jobs
 
 
-def serving_mix(lc, workers=4):
+def serving_mix(lc, workers=16):
     """The same 64 uneven 2D CG jobs (50 iterations each) solved (a) one at a time
     the plain way -- float scalars, a host check of the solver state after every
     iteration, no graphs, a PSF built per job -- and (b) submitted together to
-    the server: concurrent jobs on 4 streams, CUDA-graph iterations, FP64
+    the server: concurrent jobs on 16 streams, CUDA-graph iterations, FP64
     scalars, geometry-keyed PSF cache.  Wall-clock times, host buffers in and
     out.  The error of both forms against the FP64 oracle is measured on one
     small job (n = 63, 60 angles) of the same kind."""

@@ -1,5 +1,7 @@
 // PSF generation (closed form, FP64) and the fused-FFT Toeplitz apply.
 #include <algorithm>
+#include <array>
+#include <cmath>
 #include <tuple>
 
 #include "lc_toeplitz.hpp"
@@ -22,38 +24,56 @@ __device__ __forceinline__ double dirichlet(double u, int n) {
 }
 
 // Per-angle coefficients of the fast PSF generator: uX = a . k, uY = b . k
-// (k = (kx, ky, kz)), and (cos, sin) of pi a0, pi a0 / nx, pi b0, pi b0 / ny,
-// the steps of sin(pi uX), sin(pi uX / nx), ... from one kx to the next.
+// (k = (kx, ky, kz)), and (4 sin^2(t/2), sin t) for the steps h = a0, a0 / nx,
+// b0, b0 / ny of sin(pi uX), sin(pi uX / nx), ... from one kx to the next,
+// reduced to t = pi (h - round(h)).
 struct PsfAngle {
     double a[3], b[3];
     double2 stepA, stepB, stepC, stepD;
 };
 
-// sin(pi (u0 + s h)), s = 0, 1, ..., by the three-term recurrence
-// sin(x + t) = 2 cos t sin x - sin(x - t) with t = pi h: one FMA per step.
-// Over the S-step segments of the PSF rows the rounding error grows like
-// S^2 eps (sin(n t) / sin t <= n bounds the propagation of each error).
+// sin(pi (u0 + s h)), s = 0, 1, ..., by Reinsch's modification of the
+// three-term recurrence.  The step is first reduced to |h'| <= 1/2,
+// h' = h - round(h), using sin(pi (u0 + s h)) = (-1)^(s round(h)) sin(pi (u0 + s h'))
+// (|h| <= 1 here, so round(h) is odd exactly when |h| > 1/2).  With t = pi h',
+// lambda = 4 sin^2(t/2) and d_s = e_s - e_(s-1) for e_s = sin(pi (u0 + s h')):
+//   d_(s+1) = d_s - lambda e_s,   e_(s+1) = e_s + d_(s+1).
+// lambda carries t to full relative precision, which the plain recurrence
+// (2 cos t) loses for small t (a phase drift of ~eps/t per step).  Over 16
+// steps the error stays below 5e-16 for |h| <= 0.004 and 5e-15 for |h| <= 1
+// (checked against exact values), one FMA and one add per step.
+template <bool FLIP>
 struct SinSeq {
-    double prev, cur, two_c;
-    // step = (cos pi h, sin pi h)
-    __device__ __forceinline__ void init(double u0, double2 step) {
+    double cur, d, lam, flipf;
+    // step = (4 sin^2(t/2), sin t) of the reduced step; h = the unreduced step
+    __device__ __forceinline__ void init(double u0, double2 step, double h) {
         double s0, c0;
         sincospi(u0, &s0, &c0);
         cur = s0;
-        prev = s0 * step.x - c0 * step.y;
-        two_c = 2.0 * step.x;
+        lam = step.x;
+        d = fma(0.5 * step.x, s0, c0 * step.y);  // e_0 - e_(-1) = s0 (1 - cos t) + c0 sin t
+        flipf = (FLIP && fabs(h) > 0.5) ? -1.0 : 1.0;
     }
+    // sin(pi (u0 + s h)) at the current step s
+    __device__ __forceinline__ double val(int s) const { return (FLIP && (s & 1)) ? cur * flipf : cur; }
     __device__ __forceinline__ void advance() {
-        const double n = fma(two_c, cur, -prev);
-        prev = cur;
-        cur = n;
+        d = fma(-lam, cur, d);
+        cur += d;
     }
 };
+
+// Below this |sin(pi u / n)| a Dirichlet term is evaluated in closed form.
+// Above it the recurrences' absolute error (~5e-16) gives a term a relative
+// error of at most ~5e-10, and the kernel stays within ~1e-11 of the exact sum
+// (the spectrum is then stored in FP32).  A larger threshold sends most warps
+// through the closed form (0.07 % of the terms at 1e-3 already put 9 % of the
+// warp steps there) and costs several times the whole sum.
+constexpr double kDenMin = 1e-6;
 
 // Dirichlet term sin(pi u) / sin(pi u / n) from the two sines, or from the
 // closed form near its poles
 __device__ __forceinline__ double dirichlet_term(double num, double den, double u, int n) {
-    return fabs(den) > 1e-6 ? num / den : dirichlet(u, n);
+    return fabs(den) > kDenMin ? num / den : dirichlet(u, n);
 }
 
 __device__ __forceinline__ int mirror_index(int j, int P) {
@@ -67,11 +87,16 @@ __device__ __forceinline__ int mirror_index(int j, int P) {
 // advanced along kx by the three-term sine recurrence (FP64) and evaluated in
 // closed form whenever the denominator is small.
 // Only the half space kz <= 0 (2D: ky <= 0) is summed; K(-k) = K(k) fills the
-// rest.
+// rest.  With `mirror` the angle set is also closed under a reflection that
+// makes K even in one more axis, and a quarter of the grid is summed:
+//   3D  K(kx, ky, -kz) = K(k): rows with ky <= 0 of each plane kz <= 0, and
+//       K(-kx, -ky, kz), K(-k), K(kx, ky, -kz) from them (a per-angle pair
+//       whose a and b differ only in the sign of their kz coefficient);
+//   2D  K(-kx, ky) = K(k): kx <= 0 of each row ky <= 0 (pairs theta, pi - theta).
 template <int DIM, int S>
 __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__restrict__ angles, int ntheta,
                                                       const int *__restrict__ groups, int ngroups,
-                                                      int nx, int ny, int P1, int P2, int P3,
+                                                      int nx, int ny, int P1, int P2, int P3, int mirror,
                                                       double *__restrict__ K) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PsfAngle *ang = reinterpret_cast<PsfAngle *>(smem_raw);
@@ -79,9 +104,13 @@ __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__rest
     for (int i = threadIdx.x; i < ntheta; i += blockDim.x) ang[i] = angles[i];
     for (int i = threadIdx.x; i <= ngroups; i += blockDim.x) gst[i] = groups[i];
     __syncthreads();
-    const int nseg = (P3 + S - 1) / S;
-    // rows of the half space: 3D (jz <= P1/2, all jy); 2D (jy <= P2/2)
-    const long nrows_half = DIM == 3 ? (long)(P1 / 2 + 1) * P2 : (long)(P2 / 2 + 1);
+    // x range summed: all of it, or (2D mirror) jx <= P3/2
+    const int xend = (DIM == 2 && mirror) ? P3 / 2 + 1 : P3;
+    const int nseg = (xend + S - 1) / S;
+    // rows of the half space: 3D (jz <= P1/2, all jy, or jy <= P2/2 with the
+    // mirror); 2D (jy <= P2/2)
+    const int rows_per_plane = (DIM == 3 && mirror) ? P2 / 2 + 1 : P2;
+    const long nrows_half = DIM == 3 ? (long)(P1 / 2 + 1) * rows_per_plane : (long)(P2 / 2 + 1);
     const long items = nrows_half * nseg;
     const double inv_nx = 1.0 / (double)nx, inv_ny = 1.0 / (double)ny;
     for (long it = (long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
@@ -90,8 +119,8 @@ __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__rest
         const int seg = (int)(it - row * nseg);
         int jz = 0, jy;
         if (DIM == 3) {
-            jz = (int)(row / P2);
-            jy = (int)(row - (long)jz * P2);
+            jz = (int)(row / rows_per_plane);
+            jy = (int)(row - (long)jz * rows_per_plane);
         } else {
             jy = (int)row;
         }
@@ -122,28 +151,29 @@ __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__rest
                     const double uB = B.b[0] * kx0 + B.b[1] * ky + B.b[2] * kz;
                     const double uC = C.b[0] * kx0 + C.b[1] * ky + C.b[2] * kz;
                     const double uD = D.b[0] * kx0 + D.b[1] * ky + D.b[2] * kz;
-                    SinSeq nA, dA, nB, dB, nC, dC, nD, dD;
-                    nA.init(uA, A.stepC);
-                    dA.init(uA * inv_ny, A.stepD);
-                    nB.init(uB, B.stepC);
-                    dB.init(uB * inv_ny, B.stepD);
-                    nC.init(uC, C.stepC);
-                    dC.init(uC * inv_ny, C.stepD);
-                    nD.init(uD, D.stepC);
-                    dD.init(uD * inv_ny, D.stepD);
+                    SinSeq<true> nA, nB, nC, nD;
+                    SinSeq<false> dA, dB, dC, dD;
+                    nA.init(uA, A.stepC, A.b[0]);
+                    dA.init(uA * inv_ny, A.stepD, A.b[0] * inv_ny);
+                    nB.init(uB, B.stepC, B.b[0]);
+                    dB.init(uB * inv_ny, B.stepD, B.b[0] * inv_ny);
+                    nC.init(uC, C.stepC, C.b[0]);
+                    dC.init(uC * inv_ny, C.stepD, C.b[0] * inv_ny);
+                    nD.init(uD, D.stepC, D.b[0]);
+                    dD.init(uD * inv_ny, D.stepD, D.b[0] * inv_ny);
 #pragma unroll
                     for (int s = 0; s < S; ++s) {
-                        if (fabs(dA.cur) > 1e-6 && fabs(dB.cur) > 1e-6 && fabs(dC.cur) > 1e-6 &&
-                            fabs(dD.cur) > 1e-6) {
-                            const double pab = fma(nA.cur, dB.cur, nB.cur * dA.cur), qab = dA.cur * dB.cur;
-                            const double pcd = fma(nC.cur, dD.cur, nD.cur * dC.cur), qcd = dC.cur * dD.cur;
+                        if (fabs(dA.cur) > kDenMin && fabs(dB.cur) > kDenMin && fabs(dC.cur) > kDenMin &&
+                            fabs(dD.cur) > kDenMin) {
+                            const double pab = fma(nA.val(s), dB.cur, nB.val(s) * dA.cur), qab = dA.cur * dB.cur;
+                            const double pcd = fma(nC.val(s), dD.cur, nD.val(s) * dC.cur), qcd = dC.cur * dD.cur;
                             ay[s] += fma(pab, qcd, pcd * qab) / (qab * qcd);
                         } else {
                             const double sd = (double)s;
-                            ay[s] += dirichlet_term(nA.cur, dA.cur, uA + sd * A.b[0], ny) +
-                                     dirichlet_term(nB.cur, dB.cur, uB + sd * B.b[0], ny) +
-                                     dirichlet_term(nC.cur, dC.cur, uC + sd * C.b[0], ny) +
-                                     dirichlet_term(nD.cur, dD.cur, uD + sd * D.b[0], ny);
+                            ay[s] += dirichlet_term(nA.val(s), dA.cur, uA + sd * A.b[0], ny) +
+                                     dirichlet_term(nB.val(s), dB.cur, uB + sd * B.b[0], ny) +
+                                     dirichlet_term(nC.val(s), dC.cur, uC + sd * C.b[0], ny) +
+                                     dirichlet_term(nD.val(s), dD.cur, uD + sd * D.b[0], ny);
                         }
                         nA.advance();
                         dA.advance();
@@ -159,18 +189,19 @@ __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__rest
                     const PsfAngle &A = ang[i], &B = ang[i + 1];
                     const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
                     const double uB = B.b[0] * kx0 + B.b[1] * ky + B.b[2] * kz;
-                    SinSeq nA, dA, nB, dB;
-                    nA.init(uA, A.stepC);
-                    dA.init(uA * inv_ny, A.stepD);
-                    nB.init(uB, B.stepC);
-                    dB.init(uB * inv_ny, B.stepD);
+                    SinSeq<true> nA, nB;
+                    SinSeq<false> dA, dB;
+                    nA.init(uA, A.stepC, A.b[0]);
+                    dA.init(uA * inv_ny, A.stepD, A.b[0] * inv_ny);
+                    nB.init(uB, B.stepC, B.b[0]);
+                    dB.init(uB * inv_ny, B.stepD, B.b[0] * inv_ny);
 #pragma unroll
                     for (int s = 0; s < S; ++s) {
-                        if (fabs(dA.cur) > 1e-6 && fabs(dB.cur) > 1e-6) {
-                            ay[s] += fma(nA.cur, dB.cur, nB.cur * dA.cur) / (dA.cur * dB.cur);
+                        if (fabs(dA.cur) > kDenMin && fabs(dB.cur) > kDenMin) {
+                            ay[s] += fma(nA.val(s), dB.cur, nB.val(s) * dA.cur) / (dA.cur * dB.cur);
                         } else {
-                            ay[s] += dirichlet_term(nA.cur, dA.cur, uA + (double)s * A.b[0], ny) +
-                                     dirichlet_term(nB.cur, dB.cur, uB + (double)s * B.b[0], ny);
+                            ay[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.b[0], ny) +
+                                     dirichlet_term(nB.val(s), dB.cur, uB + (double)s * B.b[0], ny);
                         }
                         nA.advance();
                         dA.advance();
@@ -181,24 +212,26 @@ __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__rest
                 if (i < i1) {
                     const PsfAngle &A = ang[i];
                     const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
-                    SinSeq nA, dA;
-                    nA.init(uA, A.stepC);
-                    dA.init(uA * inv_ny, A.stepD);
+                    SinSeq<true> nA;
+                    SinSeq<false> dA;
+                    nA.init(uA, A.stepC, A.b[0]);
+                    dA.init(uA * inv_ny, A.stepD, A.b[0] * inv_ny);
 #pragma unroll
                     for (int s = 0; s < S; ++s) {
-                        ay[s] += dirichlet_term(nA.cur, dA.cur, uA + (double)s * A.b[0], ny);
+                        ay[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.b[0], ny);
                         nA.advance();
                         dA.advance();
                     }
                 }
                 const PsfAngle &A = ang[i0];
                 const double uX0 = A.a[0] * kx0 + A.a[1] * ky + A.a[2] * kz;
-                SinSeq nX, dX;
-                nX.init(uX0, A.stepA);
-                dX.init(uX0 * inv_nx, A.stepB);
+                SinSeq<true> nX;
+                SinSeq<false> dX;
+                nX.init(uX0, A.stepA, A.a[0]);
+                dX.init(uX0 * inv_nx, A.stepB, A.a[0] * inv_nx);
 #pragma unroll
                 for (int s = 0; s < S; ++s) {
-                    acc[s] = fma(dirichlet_term(nX.cur, dX.cur, uX0 + (double)s * A.a[0], nx), ay[s], acc[s]);
+                    acc[s] = fma(dirichlet_term(nX.val(s), dX.cur, uX0 + (double)s * A.a[0], nx), ay[s], acc[s]);
                     nX.advance();
                     dX.advance();
                 }
@@ -210,18 +243,19 @@ __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__rest
                 const PsfAngle &A = ang[i], &B = ang[i + 1];
                 const double uA = A.a[0] * kx0 + A.a[1] * ky;
                 const double uB = B.a[0] * kx0 + B.a[1] * ky;
-                SinSeq nA, dA, nB, dB;
-                nA.init(uA, A.stepA);
-                dA.init(uA * inv_nx, A.stepB);
-                nB.init(uB, B.stepA);
-                dB.init(uB * inv_nx, B.stepB);
+                SinSeq<true> nA, nB;
+                    SinSeq<false> dA, dB;
+                nA.init(uA, A.stepA, A.a[0]);
+                dA.init(uA * inv_nx, A.stepB, A.a[0] * inv_nx);
+                nB.init(uB, B.stepA, B.a[0]);
+                dB.init(uB * inv_nx, B.stepB, B.a[0] * inv_nx);
 #pragma unroll
                 for (int s = 0; s < S; ++s) {
-                    if (fabs(dA.cur) > 1e-6 && fabs(dB.cur) > 1e-6) {
-                        acc[s] += fma(nA.cur, dB.cur, nB.cur * dA.cur) / (dA.cur * dB.cur);
+                    if (fabs(dA.cur) > kDenMin && fabs(dB.cur) > kDenMin) {
+                        acc[s] += fma(nA.val(s), dB.cur, nB.val(s) * dA.cur) / (dA.cur * dB.cur);
                     } else {
-                        acc[s] += dirichlet_term(nA.cur, dA.cur, uA + (double)s * A.a[0], nx) +
-                                  dirichlet_term(nB.cur, dB.cur, uB + (double)s * B.a[0], nx);
+                        acc[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.a[0], nx) +
+                                  dirichlet_term(nB.val(s), dB.cur, uB + (double)s * B.a[0], nx);
                     }
                     nA.advance();
                     dA.advance();
@@ -232,12 +266,13 @@ __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__rest
             if (i < ntheta) {
                 const PsfAngle &A = ang[i];
                 const double uA = A.a[0] * kx0 + A.a[1] * ky;
-                SinSeq nA, dA;
-                nA.init(uA, A.stepA);
-                dA.init(uA * inv_nx, A.stepB);
+                SinSeq<true> nA;
+                    SinSeq<false> dA;
+                nA.init(uA, A.stepA, A.a[0]);
+                dA.init(uA * inv_nx, A.stepB, A.a[0] * inv_nx);
 #pragma unroll
                 for (int s = 0; s < S; ++s) {
-                    acc[s] += dirichlet_term(nA.cur, dA.cur, uA + (double)s * A.a[0], nx);
+                    acc[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.a[0], nx);
                     nA.advance();
                     dA.advance();
                 }
@@ -246,16 +281,46 @@ __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__rest
         const long plane = (long)P2 * P3;
         const int mz = DIM == 3 ? mirror_index(jz, P1) : 0;
         const int my = mirror_index(jy, P2);
-        const bool self_plane = DIM == 3 ? (mz == jz) : (my == jy);
+        auto put = [&](int z, int y, int x, double v) { K[(long)z * plane + (long)y * P3 + x] = v; };
+        if (!mirror) {
+            const bool self_plane = DIM == 3 ? (mz == jz) : (my == jy);
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const int jx = jx0 + s;
-            if (jx >= P3) break;
-            K[(long)jz * plane + (long)jy * P3 + jx] = acc[s];
-            if (self_plane) continue;  // its mirror is summed by another row of the half space
-            const int mx = mirror_index(jx, P3);
-            if ((DIM == 3 && mz < 0) || my < 0 || mx < 0) continue;
-            K[(long)mz * plane + (long)my * P3 + mx] = acc[s];
+            for (int s = 0; s < S; ++s) {
+                const int jx = jx0 + s;
+                if (jx >= P3) break;
+                put(jz, jy, jx, acc[s]);
+                if (self_plane) continue;  // its mirror is summed by another row of the half space
+                const int mx = mirror_index(jx, P3);
+                if ((DIM == 3 && mz < 0) || my < 0 || mx < 0) continue;
+                put(mz, my, mx, acc[s]);
+            }
+        } else if constexpr (DIM == 3) {
+            // (jz, jy, jx) summed; (jz, my, mx), (mz, my, mx), (mz, jy, jx) copied.
+            // A copy that lands on a summed row or plane is left to the sum.
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const int jx = jx0 + s;
+                if (jx >= P3) break;
+                const int mx = mirror_index(jx, P3);
+                put(jz, jy, jx, acc[s]);
+                if (my != jy && my >= 0 && mx >= 0) put(jz, my, mx, acc[s]);
+                if (mz != jz && mz >= 0) put(mz, jy, jx, acc[s]);
+                if (mz != jz && my != jy && mz >= 0 && my >= 0 && mx >= 0) put(mz, my, mx, acc[s]);
+            }
+        } else {
+            // (jy, jx <= P3/2) summed; (jy, mx), (my, mx), (my, jx) copied
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const int jx = jx0 + s;
+                if (jx >= xend) break;
+                const int mx = mirror_index(jx, P3);
+                put(0, jy, jx, acc[s]);
+                if (mx != jx && mx >= 0) put(0, jy, mx, acc[s]);
+                if (my != jy && my >= 0) {
+                    put(0, my, jx, acc[s]);
+                    if (mx >= 0) put(0, my, mx, acc[s]);
+                }
+            }
         }
     }
 }
@@ -524,11 +589,53 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
         nx = g_->pts.nr;
         ny = 1;
     }
+    // (4 sin^2(t/2), sin t) for t = pi h', h' = h - round(h) (|h| <= 1)
+    auto step = [&](double h) {
+        const double hr = h > 0.5 ? h - 1.0 : (h < -0.5 ? h + 1.0 : h);
+        const double q = std::sin(0.5 * pi * hr);
+        return make_double2(4.0 * q * q, std::sin(pi * hr));
+    };
     for (auto &A : tab) {
-        A.stepA = make_double2(std::cos(pi * A.a[0]), std::sin(pi * A.a[0]));
-        A.stepB = make_double2(std::cos(pi * A.a[0] / nx), std::sin(pi * A.a[0] / nx));
-        A.stepC = make_double2(std::cos(pi * A.b[0]), std::sin(pi * A.b[0]));
-        A.stepD = make_double2(std::cos(pi * A.b[0] / ny), std::sin(pi * A.b[0] / ny));
+        A.stepA = step(A.a[0]);
+        A.stepB = step(A.a[0] / nx);
+        A.stepC = step(A.b[0]);
+        A.stepD = step(A.b[0] / ny);
+    }
+    // Is the angle set closed under the reflection that makes K even in one
+    // more axis?  3D: (a, b) -> (a, b) with the kz coefficients negated;
+    // 2D: a -> a with the kx coefficient negated.  The multisets of keys
+    // (rounded to 1e-10) are compared; a key on a rounding boundary only costs
+    // the saving, never the result.
+    bool mirror = nth > 0;
+    {
+        // Dirichlet kernels are even, so a and -a (b and -b) give the same term:
+        // each vector is compared with the sign of its first nonzero component
+        // made positive
+        using Key = std::array<long long, 6>;
+        auto key = [](const PsfAngle &A, bool refl, bool three) {
+            auto q = [](double v) { return (long long)std::llround(v * 1e10); };
+            auto canon = [&](double x, double y, double z, long long *out) {
+                long long v[3] = {q(x), q(y), q(z)};
+                const long long lead = v[0] != 0 ? v[0] : (v[1] != 0 ? v[1] : v[2]);
+                for (int i = 0; i < 3; ++i) out[i] = lead < 0 ? -v[i] : v[i];
+            };
+            Key k{};
+            if (three) {
+                canon(A.a[0], A.a[1], refl ? -A.a[2] : A.a[2], &k[0]);
+                canon(A.b[0], A.b[1], refl ? -A.b[2] : A.b[2], &k[3]);
+            } else {
+                canon(refl ? -A.a[0] : A.a[0], A.a[1], 0.0, &k[0]);
+            }
+            return k;
+        };
+        std::vector<Key> k0(nth), k1(nth);
+        for (int i = 0; i < nth; ++i) {
+            k0[i] = key(tab[i], false, three_d_);
+            k1[i] = key(tab[i], true, three_d_);
+        }
+        std::sort(k0.begin(), k0.end());
+        std::sort(k1.begin(), k1.end());
+        mirror = mirror && k0 == k1;
     }
     // group the angles by their theta-independent vector a (equal beta and gamma)
     std::vector<int> order(nth);
@@ -557,8 +664,8 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
     long total = (long)P1 * P2 * P3;
     K.alloc(total, st);
     constexpr int S = 16;
-    const long nseg = (P3 + S - 1) / S;
-    const long items = (three_d_ ? (long)(P1 / 2 + 1) * P2 : (long)(P2 / 2 + 1)) * nseg;
+    const long nseg = ((!three_d_ && mirror ? P3 / 2 + 1 : P3) + S - 1) / S;
+    const long items = (three_d_ ? (long)(P1 / 2 + 1) * (mirror ? P2 / 2 + 1 : P2) : (long)(P2 / 2 + 1)) * nseg;
     size_t smem = sizeof(PsfAngle) * nth + sizeof(int) * groups.size();
     LC_REQUIRE(smem <= 220 * 1024, "Toeplitz: too many angles for one PSF launch");
     unsigned blocks = (unsigned)std::max<long>(1, std::min<long>((items + 127) / 128, (long)ctx.num_sms() * 16));
@@ -566,11 +673,12 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
         auto kern = psf_rows_kernel<3, S>;
         LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), ngroups, nx, ny, P1, P2, P3,
-                                        K.get());
+                                        mirror ? 1 : 0, K.get());
     } else {
         auto kern = psf_rows_kernel<2, S>;
         LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), 0, nx, ny, P1, P2, P3, K.get());
+        kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), 0, nx, ny, P1, P2, P3,
+                                        mirror ? 1 : 0, K.get());
     }
     LC_CHECK_LAUNCH();
     // planes of mode -P/2 have no mirror inside the grid; they are not needed
