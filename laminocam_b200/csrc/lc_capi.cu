@@ -261,20 +261,29 @@ void run_solver(lc_psf psf, int method, const float *rhs, float *x, const lc_sol
     if (!psf->solver) psf->solver = std::make_unique<Solver>(ctx, psf->T->nvox());
     Toeplitz *T = psf->T.get();
     Operator A = [&ctx, T](const float *in, float *out) { T->apply(ctx, in, out); };
+    // CG iterations fuse the direction update and p.Ap into the x passes
+    FusedOperator F;
+    F.caps = T->cg_caps();
+    F.partials = T->cg_partials();
+    const unsigned caps = F.caps;
+    F.apply = [&ctx, T, caps](const float *in, float *out, const CGFusion &f) {
+        T->apply(ctx, in, out, &f, caps);
+    };
     cudaEvent_t e0, e1;
     LC_CUDA(cudaEventCreate(&e0));
     LC_CUDA(cudaEventCreate(&e1));
     LC_CUDA(cudaEventRecord(e0, ctx.stream()));
     SolverStats st;
     SolverParams sp = to_sp(p);
-    if (method == 0) psf->solver->cg(ctx, A, rhs, x, sp, &st);
+    if (method == 0) psf->solver->cg(ctx, A, rhs, x, sp, &st, &F);
     else psf->solver->split_bregman(ctx, A, T->dims(), rhs, x, sp, &st);
     LC_CUDA(cudaEventRecord(e1, ctx.stream()));
     LC_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
+    const cudaError_t te = cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    LC_CUDA(te);
     if (stats) {
         stats->iters = st.iters;
         stats->cg_iters_total = st.cg_iters_total;

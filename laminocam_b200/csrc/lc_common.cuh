@@ -23,11 +23,20 @@ struct Error : std::runtime_error {
     Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
 };
 
-#define LC_CUDA(call)                                                                   \
-    do {                                                                                \
-        cudaError_t e_ = (call);                                                        \
-        if (e_ != cudaSuccess)                                                          \
-            throw ::lc::Error(3, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+// file name without its directories, for error messages
+constexpr const char *lc_basename(const char *p) {
+    const char *b = p;
+    for (const char *q = p; *q; ++q)
+        if (*q == '/') b = q + 1;
+    return b;
+}
+
+#define LC_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            throw ::lc::Error(3, std::string(#call) + " (" + ::lc::lc_basename(__FILE__) + ":" + \
+                                     std::to_string(__LINE__) + "): " + cudaGetErrorString(e_)); \
     } while (0)
 
 // Kernel launches issued by this library (every launch site is followed by

@@ -515,6 +515,7 @@ void launch_axis_fft(Context &ctx, const AxisFFT &a) {
     else LC_REQUIRE(a.n_out <= a.L, "axis FFT: n_out > L");
     if (a.n_outer <= 0 || a.n_inner <= 0 || a.n_out == 0) return;
     if (line_kernels_enabled() && (launch_col_fft(ctx.stream(), a) || launch_row_fft(ctx.stream(), a))) return;
+    LC_REQUIRE(a.cg_parts == 0, "axis FFT: fused CG work needs a register-plan row kernel");
 
     const FFTPlan &pl = ctx.plans().get(a.L, a.fp64, ctx.stream());
     const size_t esz = a.fp64 ? sizeof(double2) : sizeof(float2);

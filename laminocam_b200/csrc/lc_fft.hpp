@@ -8,6 +8,7 @@
 //    transforms whose lengths are odd.
 #pragma once
 
+#include "lc_cgstate.hpp"
 #include "lc_runtime.hpp"
 
 namespace lc {
@@ -60,7 +61,15 @@ struct AxisFFT {
     int sign2 = +1;
     bool fp64 = false;  // compute precision
     int lines_per_cta = 0;  // 0 = choose automatically
+    // CG work fused into a real row pass (row kernels only; see CGFusion):
+    // kFusedUpdate on IN_REAL_PACKED rows, whose input is then the direction p;
+    // kFusedDot on OUT_REAL_UNPACK rows, whose output is then A p
+    const CGFusion *cg = nullptr;
+    unsigned cg_parts = 0;
 };
+
+// CTAs of a real row pass over n_lines lines (the partials a fused dot needs)
+long row_fft_ctas(long n_lines);
 
 void launch_axis_fft(Context &ctx, const AxisFFT &a);
 

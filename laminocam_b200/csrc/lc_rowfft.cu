@@ -16,6 +16,7 @@
 #include <atomic>
 
 #include "lc_fft.hpp"
+#include "lc_reduce.cuh"
 #include "lc_regfft.cuh"
 
 namespace lc {
@@ -31,6 +32,9 @@ struct RowArgs {
     long n_lines, in_stride, out_stride;
     int n_in, n_out;
     float scale;
+    // fused CG work (R2C: direction update of the input; C2R: p . output)
+    CGFusion cg;
+    int cg_upd, cg_dot;
 };
 
 template <int R0, int R1, int R2>
@@ -55,13 +59,27 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
     constexpr int NA = M / R0;
     float2 v[1][RM];
     if constexpr (MODE == RM_R2C) {
-        const float *in = static_cast<const float *>(a.in) + (valid ? line : 0) * a.in_stride;
+        const long lo = (valid ? line : 0) * a.in_stride;
+        const float *in = static_cast<const float *>(a.in) + lo;
+        // fused direction update p = r + beta p (the input is p)
+        const bool upd = a.cg_upd && !a.cg.st->done;
+        const float beta = upd ? (float)a.cg.st->beta : 0.f;
         if (t < NA) {
 #pragma unroll
             for (int r = 0; r < R0; ++r) {
                 const int e = t + r * NA;
-                const float re = (valid && 2 * e < a.n_in) ? in[2 * e] : 0.f;
-                const float im = (valid && 2 * e + 1 < a.n_in) ? in[2 * e + 1] : 0.f;
+                float re = (valid && 2 * e < a.n_in) ? in[2 * e] : 0.f;
+                float im = (valid && 2 * e + 1 < a.n_in) ? in[2 * e + 1] : 0.f;
+                if (upd && valid) {
+                    if (2 * e < a.n_in) {
+                        re = fmaf(beta, re, a.cg.r[lo + 2 * e]);
+                        a.cg.p[lo + 2 * e] = re;
+                    }
+                    if (2 * e + 1 < a.n_in) {
+                        im = fmaf(beta, im, a.cg.r[lo + 2 * e + 1]);
+                        a.cg.p[lo + 2 * e + 1] = im;
+                    }
+                }
                 v[0][r] = make_float2(re, im);
             }
         }
@@ -111,13 +129,57 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
         }
         xform3<M, R0, R1, R2>(v, at, t, tw, +1);
         constexpr int NC = M / R2;
+        const bool dot = a.cg_dot && !a.cg.st->done;  // uniform over the grid
+        float accf = 0.f;
+        double accd = 0.0;
         if (t < NC && valid) {
-            float *out = static_cast<float *>(a.out) + line * a.out_stride;
+            const long lo = line * a.out_stride;
+            float *out = static_cast<float *>(a.out) + lo;
 #pragma unroll
             for (int r = 0; r < R2; ++r) {
                 const int e = t + r * NC;
-                if (2 * e < a.n_out) out[2 * e] = a.scale * v[0][r].x;
-                if (2 * e + 1 < a.n_out) out[2 * e + 1] = a.scale * v[0][r].y;
+                const float y0 = a.scale * v[0][r].x, y1 = a.scale * v[0][r].y;
+                if (2 * e < a.n_out) {
+                    out[2 * e] = y0;
+                    if (dot) {
+                        const float pv = a.cg.p[lo + 2 * e];
+                        accf += pv * y0;
+                        accd += (double)pv * (double)y0;
+                    }
+                }
+                if (2 * e + 1 < a.n_out) {
+                    out[2 * e + 1] = y1;
+                    if (dot) {
+                        const float pv = a.cg.p[lo + 2 * e + 1];
+                        accf += pv * y1;
+                        accd += (double)pv * (double)y1;
+                    }
+                }
+            }
+        }
+        if (dot) {
+            // p.Ap over the grid, then alpha and the |p.Ap| stop (as the CG dot kernel)
+            double pap = 0.0;
+            bool last;
+            if (a.cg.fp32) {
+                float vv[1] = {accf};
+                last = red_block_partials<float, 1>(vv, a.cg.part, a.cg.counter);
+                if (last) pap = red_total<float>(a.cg.part, 0, gridDim.x);
+            } else {
+                double vv[1] = {accd};
+                last = red_block_partials<double, 1>(vv, a.cg.part, a.cg.counter);
+                if (last) pap = red_total<double>(a.cg.part, 0, gridDim.x);
+            }
+            if (last && threadIdx.x == 0) {
+                CGState *st = a.cg.st;
+                st->pAp = pap;
+                if (fabs(pap) < 1e-10) {
+                    st->done = 1;
+                    st->reason = 3;
+                } else {
+                    st->alpha = a.cg.fp32 ? (double)((float)st->rs_old / (float)pap) : st->rs_old / pap;
+                }
+                *a.cg.counter = 0;
             }
         }
     }
@@ -154,6 +216,8 @@ bool launch_row_plan(cudaStream_t st, int M, int mode, const RowArgs &a, long bl
 
 }  // namespace
 
+long row_fft_ctas(long n_lines) { return (n_lines + kRowLines - 1) / kRowLines; }
+
 bool launch_row_fft(cudaStream_t st, const AxisFFT &a) {
     if (a.fp64 || a.n_inner != 1 || a.lines_per_cta > 0) return false;
     if (a.pre || a.linefac || a.post) return false;
@@ -179,6 +243,13 @@ bool launch_row_fft(cudaStream_t st, const AxisFFT &a) {
     ra.n_in = a.n_in;
     ra.n_out = a.n_out;
     ra.scale = (float)a.scale;
+    ra.cg_upd = ra.cg_dot = 0;
+    if (a.cg_parts) {
+        LC_REQUIRE(a.cg != nullptr, "row FFT: fused CG work without its state");
+        ra.cg = *a.cg;
+        ra.cg_upd = (mode == RM_R2C && (a.cg_parts & kFusedUpdate)) ? 1 : 0;
+        ra.cg_dot = (mode == RM_C2R && (a.cg_parts & kFusedDot)) ? 1 : 0;
+    }
     const long blocks = (a.n_outer + kRowLines - 1) / kRowLines;
     LC_REQUIRE(blocks < (1L << 31), "row FFT: grid too large");
     return launch_row_plan(st, M, mode, ra, blocks);

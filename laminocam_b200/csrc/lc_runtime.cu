@@ -234,7 +234,9 @@ Context::Context(int device, cudaStream_t stream) : device_(device) {
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
         uint64_t thr = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        // optional: without it freed pool memory returns to the device sooner
+        if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr) != cudaSuccess)
+            cudaGetLastError();
     }
 }
 

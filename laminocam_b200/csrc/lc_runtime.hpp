@@ -53,7 +53,9 @@ class DevBuf {
         if (n > n_) alloc(n, s);
     }
     void release() {
-        if (p_) cudaFreeAsync(p_, s_);
+        // a failed free (a leak) must not surface as the error of a later,
+        // unrelated call on this thread
+        if (p_ && cudaFreeAsync(p_, s_) != cudaSuccess) cudaGetLastError();
         p_ = nullptr;
         n_ = 0;
     }

@@ -269,6 +269,8 @@ void lc_server_s::worker_loop(int w) {
             j->t_start = Clock::now();
         }
         std::string msg;
+        // an error left on this thread by an earlier job must not fail this one
+        cudaGetLastError();
         const int rc = run_guarded(msg, [&] { run_job(w, *j); });
         if (rc != LC_OK) {
             // leave the worker's stream idle and its context usable

@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(kThreads) cg_init_kernel(const float *__restri
         if (threadIdx.x == 0) {
             st->y2 = y2;
             st->rs_old = r2;
+            st->beta = 0.0;  // p = r + 0 p: a direction update ahead of the first iteration keeps p
             st->iters = 0;
             st->done = 0;
             st->reason = 0;
@@ -437,8 +438,43 @@ void Solver::capture(Context &ctx, const std::function<void()> &body) {
     ctx.set_stream(user);
 }
 
-void Solver::cg_iter(Context &ctx, const Operator &A, float *x, float tol, float xtol, int fp32) {
+void Solver::cg_iter(Context &ctx, const Operator &A, float *x, float tol, float xtol, int fp32,
+                     const FusedOperator *F) {
     cudaStream_t s = ctx.stream();
+    if (F) {
+        // p = r + beta p ahead of the operator (beta = 0 in the first
+        // iteration), inside its first pass when it can; p.Ap inside its last
+        CGFusion f;
+        f.p = p_.get();
+        f.r = r_.get();
+        f.st = st_.get();
+        f.part = part_.get();
+        f.counter = counter_.get();
+        f.fp32 = fp32;
+        if (!(F->caps & kFusedUpdate)) {
+            p_update_kernel<<<nblk_, kThreads, 0, s>>>(p_.get(), r_.get(), n_, st_.get());
+            LC_CHECK_LAUNCH();
+        }
+        F->apply(p_.get(), ap_.get(), f);
+        ProfScope ps(ctx, PS_CG_VEC, 4.0 * n_ * ((F->caps & kFusedDot) ? 5.0 : 7.0));
+        if (!(F->caps & kFusedDot)) {
+            if (fp32)
+                dot_pap_kernel<float><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
+                                                                 counter_.get(), st_.get());
+            else
+                dot_pap_kernel<double><<<nblk_, kThreads, 0, s>>>(p_.get(), ap_.get(), n_, part_.get(),
+                                                                  counter_.get(), st_.get());
+            LC_CHECK_LAUNCH();
+        }
+        if (fp32)
+            cg_update_kernel<float><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), nullptr, n_,
+                                                               part_.get(), counter_.get(), st_.get(), tol, xtol);
+        else
+            cg_update_kernel<double><<<nblk_, kThreads, 0, s>>>(x, r_.get(), p_.get(), ap_.get(), nullptr, n_,
+                                                                part_.get(), counter_.get(), st_.get(), tol, xtol);
+        LC_CHECK_LAUNCH();
+        return;
+    }
     A(p_.get(), ap_.get());
     ProfScope ps(ctx, PS_CG_VEC, 4.0 * n_ * 10.0);
     if (fp32) {
@@ -463,7 +499,7 @@ void Solver::cg_iter(Context &ctx, const Operator &A, float *x, float tol, float
 }
 
 void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, int iters,
-                    float tol, float xtol, int fp32, int poll_every, bool graph) {
+                    float tol, float xtol, int fp32, int poll_every, bool graph, const FusedOperator *F) {
     cudaStream_t s = ctx.stream();
     A(x, ap_.get());
     // r <- A x0 (moved), then r = y - r, p = r
@@ -483,7 +519,7 @@ void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, i
     if (graph && iters > 1) {
         chunk = poll ? std::min(poll_every, iters) : std::min(iters, 8);
         capture(ctx, [&] {
-            for (int k = 0; k < chunk; ++k) cg_iter(ctx, A, x, tol, xtol, fp32);
+            for (int k = 0; k < chunk; ++k) cg_iter(ctx, A, x, tol, xtol, fp32, F);
         });
     }
     int it = 0;
@@ -492,7 +528,7 @@ void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, i
             graph_.launch(s);
             it += chunk;
         } else {
-            cg_iter(ctx, A, x, tol, xtol, fp32);
+            cg_iter(ctx, A, x, tol, xtol, fp32, F);
             it += 1;
         }
         const bool boundary = chunk > 0 || it % std::max(poll_every, 1) == 0;
@@ -505,14 +541,15 @@ void Solver::cg_run(Context &ctx, const Operator &A, const float *y, float *x, i
 }
 
 void Solver::cg(Context &ctx, const Operator &A, const float *y, float *x, const SolverParams &p,
-                SolverStats *stats) {
+                SolverStats *stats, const FusedOperator *F) {
     cudaStream_t s = ctx.stream();
     host_st_ = static_cast<CGState *>(ctx.pinned_scratch(sizeof(CGState)));
+    if (F && (F->caps & kFusedDot)) part_.ensure((long)std::max<long>(nblk_, F->partials) * kParts, s);
     reset_state_kernel<<<1, 1, 0, s>>>(st_.get());
     LC_CHECK_LAUNCH();
     int poll = (p.tol > 0 || p.xtol > 0) ? p.poll_every : 0;
     const bool graph = p.use_graph != 0 && !ctx.prof.on;
-    cg_run(ctx, A, y, x, p.max_iters, p.tol, p.xtol, p.fp32_scalars, poll, graph);
+    cg_run(ctx, A, y, x, p.max_iters, p.tol, p.xtol, p.fp32_scalars, poll, graph, F);
     graph_.reset();
     LC_CUDA(cudaMemcpyAsync(host_st_, st_.get(), sizeof(CGState), cudaMemcpyDeviceToHost, s));
     LC_CUDA(cudaStreamSynchronize(s));

@@ -10,6 +10,7 @@
 
 #include <functional>
 
+#include "lc_cgstate.hpp"
 #include "lc_runtime.hpp"
 
 namespace lc {
@@ -38,18 +39,15 @@ struct SolverStats {
     int stop_reason = 0;    // 0 max iters, 1 residual, 2 step, 3 |pAp| tiny
 };
 
-// device-resident solver state
-struct CGState {
-    double rs_old, pAp, alpha, beta;
-    double y2;
-    double res, dx;
-    int iters, done, reason, pad;
-    // Split-Bregman
-    double sb_diff2, sb_old2, sb_rel;
-    int sb_iters, sb_done;
-};
-
 using Operator = std::function<void(const float *in, float *out)>;
+
+// An operator that can take over CG work around its own passes (see
+// CGFusion): caps says which parts apply() performs.
+struct FusedOperator {
+    unsigned caps = 0;   // kFusedUpdate | kFusedDot
+    long partials = 0;   // CTAs whose partials a fused dot writes
+    std::function<void(const float *in, float *out, const CGFusion &f)> apply;
+};
 
 class Solver {
   public:
@@ -58,17 +56,21 @@ class Solver {
     Solver(const Solver &) = delete;
     Solver &operator=(const Solver &) = delete;
     // x (in: x0, out: solution); y = right-hand side
+    // With F, each iteration applies F (fusing the direction update and the
+    // dot product when F can) instead of A.
     void cg(Context &ctx, const Operator &A, const float *y, float *x, const SolverParams &p,
-            SolverStats *stats);
+            SolverStats *stats, const FusedOperator *F = nullptr);
     // A is the normal operator A^T A alone; mu * (-laplacian) is added here.
     void split_bregman(Context &ctx, const Operator &AtA, const long dims[3], const float *yT,
                        float *x, const SolverParams &p, SolverStats *stats);
 
   private:
     void cg_run(Context &ctx, const Operator &A, const float *y, float *x, int iters, float tol,
-                float xtol, int fp32, int poll_every, bool graph);
+                float xtol, int fp32, int poll_every, bool graph, const FusedOperator *F);
     // one CG iteration: Ap = A p, the fused scalar/vector updates, p = r + beta p
-    void cg_iter(Context &ctx, const Operator &A, float *x, float tol, float xtol, int fp32);
+    // (with F: p = r + beta p first, then Ap = A p with what F fuses)
+    void cg_iter(Context &ctx, const Operator &A, float *x, float tol, float xtol, int fp32,
+                 const FusedOperator *F);
     // records body into graph_ on the context's private stream
     void capture(Context &ctx, const std::function<void()> &body);
     CapturedGraph graph_;

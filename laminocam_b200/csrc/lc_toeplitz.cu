@@ -4,6 +4,7 @@
 #include <cmath>
 #include <tuple>
 
+#include "lc_regfft.cuh"
 #include "lc_toeplitz.hpp"
 
 namespace lc {
@@ -702,7 +703,16 @@ double Toeplitz::algorithmic_bytes() const {
     return 8.0 * (double)nvox() + 4.0 * (double)spectrum_elems();
 }
 
-void Toeplitz::apply(Context &ctx, const float *x, float *y) {
+unsigned Toeplitz::cg_caps() const {
+    const int P3 = P_[2];
+    return (P3 % 2 == 0 && line_kernels_enabled() && line_plan_exists(P3 / 2)) ? (kFusedUpdate | kFusedDot)
+                                                                                   : 0u;
+}
+
+long Toeplitz::cg_partials() const { return row_fft_ctas(n_[0] * n_[1]); }
+
+void Toeplitz::apply(Context &ctx, const float *x, float *y, const CGFusion *f, unsigned parts) {
+    LC_REQUIRE((parts & ~cg_caps()) == 0, "Toeplitz: CG fusion not available for this size");
     const long n1 = n_[0], n2 = n_[1], n3 = n_[2];
     const int P1 = P_[0], P2 = P_[1], P3 = P_[2];
     const int P3h = Ph_[2];
@@ -732,6 +742,8 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
             a.in_map = IN_REAL_PACKED;
             a.out_map = OUT_R2C_UNPACK;
         }
+        a.cg = f;
+        a.cg_parts = parts & kFusedUpdate;
         launch_axis_fft(ctx, a);
     }
     if (!three_d_) {
@@ -840,6 +852,8 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y) {
             a.in_map = IN_C2R_PACK;
             a.out_map = OUT_REAL_UNPACK;
         }
+        a.cg = f;
+        a.cg_parts = parts & kFusedDot;
         launch_axis_fft(ctx, a);
     }
 }

@@ -30,7 +30,14 @@ class Toeplitz {
     // spectrum.  Without work buffers the copy only holds the spectrum (a
     // cache entry) and cannot be applied.
     Toeplitz(Context &ctx, const Toeplitz &src, bool work = true);
-    void apply(Context &ctx, const float *x, float *y);
+    // y = A^T A x.  With f, the parts of `parts` (a subset of cg_caps()) of the
+    // surrounding CG iteration are fused into the x passes: x is then the
+    // direction f->p, updated in place.
+    void apply(Context &ctx, const float *x, float *y, const CGFusion *f = nullptr, unsigned parts = 0);
+    // CG work the apply can fuse (its x passes run the register-plan row kernel)
+    unsigned cg_caps() const;
+    // CTAs whose partials a fused dot product writes
+    long cg_partials() const;
     // y = A^T A x + mu * (-laplacian(x))
     void apply_reg(Context &ctx, const float *x, float *y, float mu);
 
