@@ -147,18 +147,45 @@ __global__ void __launch_bounds__(kThreads)
     if (st->done) return;
     const float a = (float)st->alpha;
     A v[3] = {A(0), A(0), A(0)};
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        const float api = ap[i], pi = p[i], xo = x[i], ro = r[i];
-        const float axo = AX ? ax[i] : 0.f;
-        float step = a * pi;
-        float xi = xo + step;
-        float ri = fmaf(-a, api, ro);
-        x[i] = xi;
-        if constexpr (STORE_R) r[i] = ri;
-        if constexpr (AX) ax[i] = fmaf(a, api, axo);
+    auto one = [&](float api, float pi, float xo, float ro, float axo, float &xi, float &ri, float &axn) {
+        const float step = a * pi;
+        xi = xo + step;
+        ri = fmaf(-a, api, ro);
+        axn = fmaf(a, api, axo);
         v[0] += (A)ri * (A)ri;
         v[1] += (A)step * (A)step;
         v[2] += (A)xi * (A)xi;
+    };
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
+    // float4 accesses (four times the bytes in flight per load) when every
+    // vector is 16-byte aligned and n is a multiple of 4
+    const unsigned long al = (unsigned long)x | (unsigned long)r | (unsigned long)p | (unsigned long)ap |
+                             (AX ? (unsigned long)ax : 0ul);
+    if ((al & 15ul) == 0 && (n & 3) == 0) {
+        const long n4 = n >> 2;
+        for (long i = tid; i < n4; i += nth) {
+            const float4 apv = reinterpret_cast<const float4 *>(ap)[i];
+            const float4 pv = reinterpret_cast<const float4 *>(p)[i];
+            const float4 xv = reinterpret_cast<const float4 *>(x)[i];
+            const float4 rv = reinterpret_cast<const float4 *>(r)[i];
+            const float4 av = AX ? reinterpret_cast<const float4 *>(ax)[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 xn, rn, an;
+            one(apv.x, pv.x, xv.x, rv.x, av.x, xn.x, rn.x, an.x);
+            one(apv.y, pv.y, xv.y, rv.y, av.y, xn.y, rn.y, an.y);
+            one(apv.z, pv.z, xv.z, rv.z, av.z, xn.z, rn.z, an.z);
+            one(apv.w, pv.w, xv.w, rv.w, av.w, xn.w, rn.w, an.w);
+            reinterpret_cast<float4 *>(x)[i] = xn;
+            if constexpr (STORE_R) reinterpret_cast<float4 *>(r)[i] = rn;
+            if constexpr (AX) reinterpret_cast<float4 *>(ax)[i] = an;
+        }
+    } else {
+        for (long i = tid; i < n; i += nth) {
+            float xi, ri, axn;
+            one(ap[i], p[i], x[i], r[i], AX ? ax[i] : 0.f, xi, ri, axn);
+            x[i] = xi;
+            if constexpr (STORE_R) r[i] = ri;
+            if constexpr (AX) ax[i] = axn;
+        }
     }
     if (block_partials<A, 3>(v, part, counter)) {
         double rs_new = total<A>(part, 0, gridDim.x);
@@ -209,6 +236,11 @@ struct Tiles {
     int tk, tj;      // tiles along n3 and n2
     int count;       // tk * tj * n1
     int qi, qj, qk;  // grid size = qi (tk tj) + qj tk + qk
+};
+
+struct TileGrid {
+    Tiles tl;
+    int blocks;
 };
 
 // body(i, j, k) for every voxel of this thread's tiles
@@ -409,8 +441,16 @@ __global__ void reset_state_kernel(CGState *st) {
 
 Solver::Solver(Context &ctx, long n) : n_(n) {
     cudaStream_t s = ctx.stream();
-    nblk_ = (int)std::max<long>(1, std::min<long>((n + kThreads * 4 - 1) / (kThreads * 4),
-                                                  (long)ctx.num_sms() * 4));
+    // the 1D vector kernels: one full wave of the CTAs that fit at once
+    int per_sm = 8;
+    for (const void *k : {(const void *)cg_update_kernel<double>, (const void *)cg_update_kernel<double, true, false>,
+                          (const void *)cg_init_kernel<double>, (const void *)dot_pap_kernel<double>,
+                          (const void *)p_update_kernel}) {
+        int b = 0;
+        LC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kThreads, 0));
+        per_sm = std::min(per_sm, std::max(b, 1));
+    }
+    nblk_ = (int)std::max<long>(1, std::min<long>((n + kThreads - 1) / kThreads, (long)ctx.num_sms() * per_sm));
     r_.alloc(n, s);
     p_.alloc(n, s);
     ap_.alloc(n, s);
@@ -589,30 +629,26 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
     const long ntiles = (long)tl.tk * tl.tj * dims[0];
     LC_REQUIRE(ntiles < (1L << 31), "split_bregman: too many tiles");
     tl.count = (int)ntiles;
-    // one full wave: the persistent grid is as large as the fewest CTAs of the
-    // three stencil kernels that fit on the device at once (a partial second
-    // wave would repeat a whole CTA's share of tiles on a few SMs)
-    int per_sm = 8;
-    {
+    // Each stencil kernel gets one full wave: its persistent grid is as large
+    // as the number of its CTAs that fit on the device at once (a partial
+    // second wave would repeat a whole CTA's share of tiles on a few SMs).
+    auto grid_for_kernel = [&](const void *k) {
         int b = 0;
-        auto fit = [&](const void *k) {
-            LC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kThreads, 0));
-            per_sm = std::min(per_sm, std::max(b, 1));
-        };
-        if (p.fp32_scalars) {
-            fit((const void *)sb_begin_kernel<float>);
-            fit((const void *)lap_dot_kernel<float>);
-            fit((const void *)sb_shrink_diff_kernel<float>);
-        } else {
-            fit((const void *)sb_begin_kernel<double>);
-            fit((const void *)lap_dot_kernel<double>);
-            fit((const void *)sb_shrink_diff_kernel<double>);
-        }
-    }
-    const int sblk = (int)std::max<long>(1, std::min<long>(ntiles, (long)ctx.num_sms() * per_sm));
-    tl.qi = sblk / (tl.tk * tl.tj);
-    tl.qj = (sblk - tl.qi * tl.tk * tl.tj) / tl.tk;
-    tl.qk = sblk - tl.qi * tl.tk * tl.tj - tl.qj * tl.tk;
+        LC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kThreads, 0));
+        TileGrid g;
+        g.tl = tl;
+        g.blocks = (int)std::max<long>(1, std::min<long>(ntiles, (long)ctx.num_sms() * std::max(b, 1)));
+        g.tl.qi = g.blocks / (tl.tk * tl.tj);
+        g.tl.qj = (g.blocks - g.tl.qi * tl.tk * tl.tj) / tl.tk;
+        g.tl.qk = g.blocks - g.tl.qi * tl.tk * tl.tj - g.tl.qj * tl.tk;
+        return g;
+    };
+    const bool f32 = p.fp32_scalars != 0;
+    const TileGrid g_begin = grid_for_kernel(f32 ? (const void *)sb_begin_kernel<float> : (const void *)sb_begin_kernel<double>);
+    const TileGrid g_lap = grid_for_kernel(f32 ? (const void *)lap_dot_kernel<float> : (const void *)lap_dot_kernel<double>);
+    const TileGrid g_shrink =
+        grid_for_kernel(f32 ? (const void *)sb_shrink_diff_kernel<float> : (const void *)sb_shrink_diff_kernel<double>);
+    const int sblk = std::max(g_begin.blocks, std::max(g_lap.blocks, g_shrink.blocks));
     part_.ensure((long)std::max(sblk, nblk_) * kParts, s);
     // With one CG iteration per outer iteration its direction is the residual
     // itself, so p and r share a buffer and r is not stored after the update.
@@ -632,20 +668,20 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
             const float *tx = exact ? ap_.get() : nullptr;
             float *pinit = inner > 1 ? p_.get() : nullptr;
             if (fp32)
-                sb_begin_kernel<float><<<sblk, kThreads, 0, os>>>(
+                sb_begin_kernel<float><<<g_begin.blocks, kThreads, 0, os>>>(
                     yT, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), tx, x,
-                    ax_.get(), r_.get(), pinit, dm, tl, mu, part_.get(), counter_.get(), st_.get());
+                    ax_.get(), r_.get(), pinit, dm, g_begin.tl, mu, part_.get(), counter_.get(), st_.get());
             else
-                sb_begin_kernel<double><<<sblk, kThreads, 0, os>>>(
+                sb_begin_kernel<double><<<g_begin.blocks, kThreads, 0, os>>>(
                     yT, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), tx, x,
-                    ax_.get(), r_.get(), pinit, dm, tl, mu, part_.get(), counter_.get(), st_.get());
+                    ax_.get(), r_.get(), pinit, dm, g_begin.tl, mu, part_.get(), counter_.get(), st_.get());
             LC_CHECK_LAUNCH();
         }
         for (int it = 0; it < inner; ++it) {
             AtA(pp, ap_.get());
             ProfScope ps(ctx, PS_CG_VEC, 4.0 * n_ * (inner > 1 ? 13.0 : 10.0));
             if (fp32) {
-                lap_dot_kernel<float><<<sblk, kThreads, 0, os>>>(pp, ap_.get(), dm, tl, mu, part_.get(),
+                lap_dot_kernel<float><<<g_lap.blocks, kThreads, 0, os>>>(pp, ap_.get(), dm, g_lap.tl, mu, part_.get(),
                                                                 counter_.get(), st_.get());
                 LC_CHECK_LAUNCH();
                 if (inner > 1)
@@ -657,7 +693,7 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
                         x, r_.get(), pp, ap_.get(), ax_.get(), n_, part_.get(), counter_.get(), st_.get(), p.tol,
                         p.xtol);
             } else {
-                lap_dot_kernel<double><<<sblk, kThreads, 0, os>>>(pp, ap_.get(), dm, tl, mu, part_.get(),
+                lap_dot_kernel<double><<<g_lap.blocks, kThreads, 0, os>>>(pp, ap_.get(), dm, g_lap.tl, mu, part_.get(),
                                                                  counter_.get(), st_.get());
                 LC_CHECK_LAUNCH();
                 if (inner > 1)
@@ -677,13 +713,13 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
         }
         ProfScope ps(ctx, PS_SB_VEC, 4.0 * n_ * 12.0);
         if (fp32)
-            sb_shrink_diff_kernel<float><<<sblk, kThreads, 0, os>>>(
+            sb_shrink_diff_kernel<float><<<g_shrink.blocks, kThreads, 0, os>>>(
                 x, xold_.get(), d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
-                tl, p.lambda / p.mu, part_.get(), counter_.get(), st_.get(), p.xtol);
+                g_shrink.tl, p.lambda / p.mu, part_.get(), counter_.get(), st_.get(), p.xtol);
         else
-            sb_shrink_diff_kernel<double><<<sblk, kThreads, 0, os>>>(
+            sb_shrink_diff_kernel<double><<<g_shrink.blocks, kThreads, 0, os>>>(
                 x, xold_.get(), d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
-                tl, p.lambda / p.mu, part_.get(), counter_.get(), st_.get(), p.xtol);
+                g_shrink.tl, p.lambda / p.mu, part_.get(), counter_.get(), st_.get(), p.xtol);
         LC_CHECK_LAUNCH();
     };
     // exact operator products every `every` outer iterations (and always in
