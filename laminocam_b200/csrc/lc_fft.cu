@@ -871,6 +871,7 @@ void bluestein_launch(Context &ctx, const BArgs &b, const FFTPlan &pl, long bloc
 
 void launch_bluestein(Context &ctx, const AxisDFT &a) {
     const BluesteinEntry &e = bluestein_tables(ctx, a.n, a.sign);
+    if (line_kernels_enabled() && launch_bluestein_lines(ctx.stream(), a, e)) return;
     const FFTPlan &pl = ctx.plans().get(e.L, false, ctx.stream());
     AxisFFT shape;  // only to pick the line grouping
     shape.L = e.L;

@@ -119,4 +119,9 @@ struct AxisDFT {
 
 void launch_axis_dft(Context &ctx, const AxisDFT &a);
 
+// Bluestein transforms with complex output whose convolution length is even
+// with a register plan for half of it, on the line kernels; false otherwise
+// (the generic Bluestein kernel then runs).
+bool launch_bluestein_lines(cudaStream_t st, const AxisDFT &a, const BluesteinEntry &e);
+
 }  // namespace lc
