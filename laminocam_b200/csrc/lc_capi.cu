@@ -516,9 +516,18 @@ int lc_psf_kernel(lc_context c, lc_psf p, double *host_out) {
 int lc_psf_spectrum(lc_context c, lc_psf p, float *host_out) {
     return guarded(c, [&] {
         LC_REQUIRE(p && host_out, "NULL argument");
-        LC_CUDA(cudaMemcpyAsync(host_out, p->T->spectrum(), p->T->spectrum_elems() * sizeof(float),
+        const Toeplitz &T = *p->T;
+        LC_CUDA(cudaMemcpyAsync(host_out, T.spectrum(), T.stored_spectrum_elems() * sizeof(float),
                                 cudaMemcpyDeviceToHost, c->ctx->stream()));
         LC_CUDA(cudaStreamSynchronize(c->ctx->stream()));
+        if (T.spectrum_zfold()) {
+            // the device keeps planes f1 <= P1/2; plane f1 > P1/2 equals plane P1 - f1
+            const int P1 = T.P()[0];
+            const long plane = T.spectrum_elems() / P1;
+            for (int f = P1 / 2 + 1; f < P1; ++f)
+                std::copy(host_out + (long)(P1 - f) * plane, host_out + (long)(P1 - f + 1) * plane,
+                          host_out + (long)f * plane);
+        }
     });
 }
 

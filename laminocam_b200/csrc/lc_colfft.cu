@@ -215,7 +215,7 @@ bool launch_col_fft(cudaStream_t st, const AxisFFT &a) {
     if (a.fp64 || a.in_t != E_C64 || a.out_t != E_C64 || a.n_inner <= 1) return false;
     if (a.in_map != IN_DIRECT) return false;
     if (!(a.out_map == OUT_DIRECT || (a.out_map == OUT_WINDOW && a.out_off == 0))) return false;
-    if (a.pre || a.linefac || a.post || a.scale != 1.0 || a.lines_per_cta > 0) return false;
+    if (a.pre || a.linefac || a.post || a.scale != 1.0 || a.lines_per_cta > 0 || a.mid_fold) return false;
     const int L = a.L;
     if (a.n_in < 0 || a.n_in > L || a.n_out < 0 || a.n_out > L) return false;
     const bool mid = a.mid != nullptr;

@@ -48,6 +48,7 @@ struct KArgs {
     double scale;
     const float *mid;
     long mid_ra;
+    int mid_fold;
     int logC;
     long blocks_per_outer;
 };
@@ -215,7 +216,8 @@ __global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
             const int cl = idx & (C - 1);
             const int f = idx >> logC;
             if (cl >= nlines) continue;
-            buf[idx] = cscale(buf[idx], (T)__ldg(mrow + (long)f * a.mid_ra + cl));
+            const int fr = (a.mid_fold && f > L / 2) ? L - f : f;
+            buf[idx] = cscale(buf[idx], (T)__ldg(mrow + (long)fr * a.mid_ra + cl));
         }
         __syncthreads();
         buf = smem_fft<T>(buf, alt, logC, pl, a.sign2);
@@ -340,6 +342,7 @@ KArgs make_kargs(const AxisFFT &a, int logC, long &blocks) {
     ka.scale = a.scale;
     ka.mid = a.mid;
     ka.mid_ra = a.mid_ra;
+    ka.mid_fold = a.mid_fold ? 1 : 0;
     ka.logC = logC;
     if (a.n_inner == 1) {
         blocks = (a.n_outer + C - 1) / C;
@@ -580,6 +583,7 @@ void launch_axis_fft_f32_with_plan(cudaStream_t stream, size_t max_smem, const A
     ka.scale = a.scale;
     ka.mid = a.mid;
     ka.mid_ra = a.mid_ra;
+    ka.mid_fold = a.mid_fold ? 1 : 0;
     ka.logC = logC;
     long blocks;
     if (a.n_inner == 1) {

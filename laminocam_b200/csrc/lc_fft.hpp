@@ -58,6 +58,7 @@ struct AxisFFT {
     // the value at FFT index f of line (o, c) is multiplied by mid[f*mid_ra + c]
     const float *mid = nullptr;
     long mid_ra = 0;
+    bool mid_fold = false;  // mid holds only f <= L/2; index f > L/2 reads L - f
     int sign2 = +1;
     bool fp64 = false;  // compute precision
     int lines_per_cta = 0;  // 0 = choose automatically
@@ -75,11 +76,12 @@ void launch_axis_fft(Context &ctx, const AxisFFT &a);
 
 // The Toeplitz z stage in place on `data` (n_inner columns, rows of n_inner
 // complex values): zero-pad n_in rows to L, FFT, multiply row f by the real
-// spec[f * n_inner + column], inverse FFT, keep n_out rows.  Register-resident
+// spec[f * n_inner + column] (with fold: rows f <= L/2 only, row L - f for
+// f > L/2), inverse FFT, keep n_out rows.  Register-resident
 // kernels for L in {16, 24, 32, 36, 48, 64, 72, 96, 128}; returns false for
 // other lengths (the caller then uses launch_axis_fft).
 bool launch_zconv(cudaStream_t st, float2 *data, long n_inner, int L, int n_in, int n_out,
-                  const float *spec);
+                  const float *spec, bool fold = false);
 
 // Column transforms (n_inner > 1) without index maps, per-index factors or
 // scale, in FP32 complex, as register-resident kernels with compile-time

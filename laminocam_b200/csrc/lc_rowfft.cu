@@ -43,7 +43,8 @@ constexpr size_t row_smem() {
     return ((size_t)M * kRowLines + 2 * (size_t)M) * sizeof(float2);
 }
 
-template <int R0, int R1, int R2, int MODE>
+// HOOK: the fused CG work of RowArgs (compiled out when unused)
+template <int R0, int R1, int R2, int MODE, bool HOOK>
 __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_kernel(RowArgs a) {
     using P = RegPlan<R0, R1, R2>;
     constexpr int M = P::M, RM = P::RM, NT = P::NT;
@@ -62,7 +63,7 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
         const long lo = (valid ? line : 0) * a.in_stride;
         const float *in = static_cast<const float *>(a.in) + lo;
         // fused direction update p = r + beta p (the input is p)
-        const bool upd = a.cg_upd && !a.cg.st->done;
+        const bool upd = HOOK && a.cg_upd && !a.cg.st->done;
         const float beta = upd ? (float)a.cg.st->beta : 0.f;
         if (t < NA) {
 #pragma unroll
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
         }
         xform3<M, R0, R1, R2>(v, at, t, tw, +1);
         constexpr int NC = M / R2;
-        const bool dot = a.cg_dot && !a.cg.st->done;  // uniform over the grid
+        const bool dot = HOOK && a.cg_dot && !a.cg.st->done;  // uniform over the grid
         float accf = 0.f;
         double accd = 0.0;
         if (t < NC && valid) {
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
                 const float y0 = a.scale * v[0][r].x, y1 = a.scale * v[0][r].y;
                 if (2 * e < a.n_out) {
                     out[2 * e] = y0;
-                    if (dot) {
+                    if constexpr (HOOK) if (dot) {
                         const float pv = a.cg.p[lo + 2 * e];
                         accf += pv * y0;
                         accd += (double)pv * (double)y0;
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
                 }
                 if (2 * e + 1 < a.n_out) {
                     out[2 * e + 1] = y1;
-                    if (dot) {
+                    if constexpr (HOOK) if (dot) {
                         const float pv = a.cg.p[lo + 2 * e + 1];
                         accf += pv * y1;
                         accd += (double)pv * (double)y1;
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
                 }
             }
         }
-        if (dot) {
+        if constexpr (HOOK) if (dot) {
             // p.Ap over the grid, then alpha and the |p.Ap| stop (as the CG dot kernel)
             double pap = 0.0;
             bool last;
@@ -185,10 +186,10 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
     }
 }
 
-template <int R0, int R1, int R2, int MODE>
+template <int R0, int R1, int R2, int MODE, bool HOOK>
 void launch_row_mode(cudaStream_t st, const RowArgs &a, long blocks) {
     constexpr size_t smem = row_smem<R0, R1, R2>();
-    auto kern = row_fft_kernel<R0, R1, R2, MODE>;
+    auto kern = row_fft_kernel<R0, R1, R2, MODE, HOOK>;
     static std::atomic<unsigned long long> configured{0};
     int dev = 0;
     LC_CUDA(cudaGetDevice(&dev));
@@ -203,10 +204,15 @@ void launch_row_mode(cudaStream_t st, const RowArgs &a, long blocks) {
 
 bool launch_row_plan(cudaStream_t st, int M, int mode, const RowArgs &a, long blocks) {
     switch (M) {
-#define LC_ROW_CASE(m, r0, r1, r2)                                                    \
-    case m:                                                                           \
-        if (mode == RM_R2C) launch_row_mode<r0, r1, r2, RM_R2C>(st, a, blocks);       \
-        else launch_row_mode<r0, r1, r2, RM_C2R>(st, a, blocks);                      \
+#define LC_ROW_CASE(m, r0, r1, r2)                                                      \
+    case m:                                                                             \
+        if (mode == RM_R2C) {                                                           \
+            if (a.cg_upd) launch_row_mode<r0, r1, r2, RM_R2C, true>(st, a, blocks);     \
+            else launch_row_mode<r0, r1, r2, RM_R2C, false>(st, a, blocks);             \
+        } else {                                                                        \
+            if (a.cg_dot) launch_row_mode<r0, r1, r2, RM_C2R, true>(st, a, blocks);     \
+            else launch_row_mode<r0, r1, r2, RM_C2R, false>(st, a, blocks);             \
+        }                                                                               \
         return true;
         LC_LINE_PLANS(LC_ROW_CASE)
 #undef LC_ROW_CASE

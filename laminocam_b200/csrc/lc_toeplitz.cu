@@ -501,7 +501,10 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         z.sign = -1;
         launch_axis_fft(ctx, z);
     }
-    long nR = spectrum_elems();
+    // an FFT along z of a kernel even in kz is even in f1: keep the planes
+    // f1 <= P1/2 (a prefix of the plane-major array)
+    zfold_ = three_d && kernel_mirror_;
+    long nR = stored_spectrum_elems();
     R_ = std::make_shared<DevBuf<float>>(nR, st);
     d2f_kernel<<<grid_for(nR, 256, ctx.num_sms()), 256, 0, st>>>(Rd.get(), R_->get(), nR);
     LC_CHECK_LAUNCH();
@@ -543,7 +546,8 @@ size_t Toeplitz::build_peak_bytes(const long dims[3], bool three_d) {
 }
 
 Toeplitz::Toeplitz(Context &ctx, const Toeplitz &src, bool work)
-    : three_d_(src.three_d_), g_(nullptr), R_(src.R_), scale_(src.scale_) {
+    : three_d_(src.three_d_), kernel_mirror_(src.kernel_mirror_), zfold_(src.zfold_), g_(nullptr), R_(src.R_),
+      scale_(src.scale_) {
     for (int d = 0; d < 3; ++d) {
         n_[d] = src.n_[d];
         P_[d] = src.P_[d];
@@ -638,6 +642,7 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
         std::sort(k1.begin(), k1.end());
         mirror = mirror && k0 == k1;
     }
+    kernel_mirror_ = mirror;
     // group the angles by their theta-independent vector a (equal beta and gamma)
     std::vector<int> order(nth);
     for (int i = 0; i < nth; ++i) order[i] = i;
@@ -700,7 +705,7 @@ void Toeplitz::kernel_fp64(Context &ctx, double *host_out) {
 
 double Toeplitz::algorithmic_bytes() const {
     // read x, write y, read the real spectrum octant once
-    return 8.0 * (double)nvox() + 4.0 * (double)spectrum_elems();
+    return 8.0 * (double)nvox() + 4.0 * (double)stored_spectrum_elems();
 }
 
 unsigned Toeplitz::cg_caps() const {
@@ -719,7 +724,7 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y, const CGFusion *f, 
     const double N = (double)n1 * n2 * n3;
     const double T1 = (double)n1 * n2 * P3h * 8.0;      // half-spectrum rows, complex
     const double T2 = (double)n1 * P2 * P3h * 8.0;      // after the y transform
-    const double Rb = 4.0 * (double)spectrum_elems();
+    const double Rb = 4.0 * (double)stored_spectrum_elems();
     // x rows: real -> half spectrum
     {
         ProfScope ps(ctx, PS_TOEP_X_FWD, 4.0 * N + T1);
@@ -787,7 +792,8 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y, const CGFusion *f, 
         }
         if (ProfScope ps(ctx, PS_TOEP_Z_MID, 2.0 * T2 + Rb);
             !(line_kernels_enabled() &&
-              launch_zconv(ctx.stream(), t2_.get(), (long)P2 * P3h, P1, (int)n1, (int)n1, R_->get()))) {
+              launch_zconv(ctx.stream(), t2_.get(), (long)P2 * P3h, P1, (int)n1, (int)n1, R_->get(),
+                           zfold_))) {
             AxisFFT a;
             a.in = t2_.get();
             a.in_t = E_C64;
@@ -805,6 +811,7 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y, const CGFusion *f, 
             a.sign = -1;
             a.mid = R_->get();
             a.mid_ra = (long)P2 * P3h;
+            a.mid_fold = zfold_;
             a.sign2 = +1;
             launch_axis_fft(ctx, a);
         }

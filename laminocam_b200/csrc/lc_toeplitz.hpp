@@ -45,7 +45,12 @@ class Toeplitz {
     const int *P() const { return P_; }
     bool three_d() const { return three_d_; }
     long nvox() const { return n_[0] * n_[1] * n_[2]; }
+    // elements of the real spectrum {P1, P2, P3/2+1}
     long spectrum_elems() const { return (long)P_[0] * P_[1] * Ph_[2]; }
+    // the planes of it kept on the device: all P1, or only f1 <= P1/2 when
+    // the kernel is even in kz (then R(P1 - f1) = R(f1), spectrum_zfold())
+    long stored_spectrum_elems() const { return (long)(zfold_ ? P_[0] / 2 + 1 : P_[0]) * P_[1] * Ph_[2]; }
+    bool spectrum_zfold() const { return zfold_; }
     const float *spectrum() const { return R_->get(); }
     size_t device_bytes() const {
         return spectrum_bytes() + (t1_.size() + t2_.size()) * sizeof(float2);
@@ -63,6 +68,8 @@ class Toeplitz {
   private:
     void build_kernel(Context &ctx, DevBuf<double> &K);
     bool three_d_;
+    bool kernel_mirror_ = false;  // the last kernel built is even in its mirror axis (kz in 3D)
+    bool zfold_ = false;          // spectrum stored for f1 <= P1/2 only
     long n_[3];
     int P_[3];
     int Ph_[3];

@@ -23,7 +23,7 @@ namespace {
 
 template <int A, int B, int C>
 __global__ void __launch_bounds__(C *(A > B ? A : B))
-    zconv_kernel(float2 *data, long n_inner, int n_in, int n_out, const float *__restrict__ spec) {
+    zconv_kernel(float2 *data, long n_inner, int n_in, int n_out, const float *__restrict__ spec, int fold) {
     constexpr int L = A * B;
     constexpr int TPL = A > B ? A : B;
     __shared__ float2 sm[L * C];
@@ -61,7 +61,9 @@ __global__ void __launch_bounds__(C *(A > B ? A : B))
         dft_reg<B>(v, -1);
 #pragma unroll
         for (int k2 = 0; k2 < B; ++k2) {
-            const float r = valid ? __ldg(spec + (long)(j + A * k2) * n_inner + col) : 0.f;
+            int f = j + A * k2;
+            if (fold && f > L / 2) f = L - f;
+            const float r = valid ? __ldg(spec + (long)f * n_inner + col) : 0.f;
             v[k2] = make_float2(v[k2].x * r, v[k2].y * r);
         }
         dft_reg<B>(v, +1);
@@ -88,30 +90,30 @@ __global__ void __launch_bounds__(C *(A > B ? A : B))
 }
 
 template <int A, int B, int C>
-void launch_z(cudaStream_t st, float2 *data, long n_inner, int n_in, int n_out, const float *spec) {
+void launch_z(cudaStream_t st, float2 *data, long n_inner, int n_in, int n_out, const float *spec, int fold) {
     constexpr int TPL = A > B ? A : B;
     const long blocks = (n_inner + C - 1) / C;
     LC_REQUIRE(blocks < (1L << 31), "z convolution: grid too large");
-    zconv_kernel<A, B, C><<<(unsigned)blocks, C * TPL, 0, st>>>(data, n_inner, n_in, n_out, spec);
+    zconv_kernel<A, B, C><<<(unsigned)blocks, C * TPL, 0, st>>>(data, n_inner, n_in, n_out, spec, fold);
     LC_CHECK_LAUNCH();
 }
 
 }  // namespace
 
 bool launch_zconv(cudaStream_t st, float2 *data, long n_inner, int L, int n_in, int n_out,
-                  const float *spec) {
+                  const float *spec, bool fold) {
     LC_REQUIRE(n_in >= 0 && n_in <= L && n_out >= 0 && n_out <= L, "z convolution: bad lengths");
     if (n_inner <= 0 || n_out == 0) return true;
     switch (L) {
-        case 16: launch_z<4, 4, 32>(st, data, n_inner, n_in, n_out, spec); return true;
-        case 24: launch_z<8, 3, 32>(st, data, n_inner, n_in, n_out, spec); return true;
-        case 32: launch_z<8, 4, 32>(st, data, n_inner, n_in, n_out, spec); return true;
-        case 36: launch_z<6, 6, 32>(st, data, n_inner, n_in, n_out, spec); return true;
-        case 48: launch_z<8, 6, 32>(st, data, n_inner, n_in, n_out, spec); return true;
-        case 64: launch_z<8, 8, 32>(st, data, n_inner, n_in, n_out, spec); return true;
-        case 72: launch_z<8, 9, 16>(st, data, n_inner, n_in, n_out, spec); return true;
-        case 96: launch_z<8, 12, 16>(st, data, n_inner, n_in, n_out, spec); return true;
-        case 128: launch_z<8, 16, 16>(st, data, n_inner, n_in, n_out, spec); return true;
+        case 16: launch_z<4, 4, 32>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
+        case 24: launch_z<8, 3, 32>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
+        case 32: launch_z<8, 4, 32>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
+        case 36: launch_z<6, 6, 32>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
+        case 48: launch_z<8, 6, 32>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
+        case 64: launch_z<8, 8, 32>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
+        case 72: launch_z<8, 9, 16>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
+        case 96: launch_z<8, 12, 16>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
+        case 128: launch_z<8, 16, 16>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
         default: return false;
     }
 }

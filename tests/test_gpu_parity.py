@@ -257,11 +257,16 @@ def test_psf_kernel_reflection_paths(lc, symmetric):
     g = np.full(nth, -np.deg2rad(25.0))
     dims = (5, 9, 9)
     pg = lc.PolarGrid(th, g, np.zeros(nth), nr, nc)
-    K = lc.PointSpreadFunction(pg, dims).kernel()
+    psf = lc.PointSpreadFunction(pg, dims)
+    K = psf.kernel()
     grid = O.Grid3D(th, g, np.zeros(nth), nr, nc)
     err = O.rel_l2(K, zero_unpaired(O.psf3d(grid, dims).kernel))
     print("3D kernel rel. error", symmetric, err)
     assert err < 1e-10, err
+    # the spectrum (kept for f1 <= P1/2 on the device when the kernel is even
+    # in kz) comes back whole: the real FFT of the zero-centred kernel
+    R = np.fft.rfftn(np.fft.ifftshift(K)).real
+    assert O.rel_l2(psf.spectrum(), R) < 1e-6
     # 2D
     nth, n = 20, 31
     th = np.arange(nth) * np.pi / nth if symmetric else np.sort(rng.uniform(0, np.pi, nth))
