@@ -282,6 +282,219 @@ def serving_mix(lc, workers=16):
     }
 
 
+STREAM_RATES = (5.0, 20.0, 80.0)
+STREAM_REQUESTS = 64
+STREAM_ITERS = 50
+STREAM_2D_SIZES = (255, 383, 511, 767, 1023, 1535, 2047)
+STREAM_2D_ANGLES = (180, 360, 720, 1080, 1800)
+STREAM_3D_DIMS = ((15, 255, 255), (21, 383, 383), (31, 511, 511))
+STREAM_3D_TILTS = (20, 25, 30, 35, 40, 45)
+STREAM_3D_ANGLES = 360
+
+
+def stream_requests(count=STREAM_REQUESTS, seed=3000):
+    """The served request mix: 70 % 2D slices (n from a ladder of odd sizes whose
+    steps are about x1.4, so a uniform pick is log-uniform over 255..2047;
+    180..1800 angles over [0, pi)), 30 % laminography volumes (three sizes with a
+    detector of the volume's width, 360 angles over [0, 2 pi), tilt 20..45
+    degrees in 5-degree steps so that geometries repeat), CG or Split-Bregman
+    with equal odds.  Returns (arrival time at rate 1, key, method); at rate r
+    the arrival times are these divided by r, so every rate sees the same
+    requests in the same order (open-loop Poisson arrivals)."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for _ in range(count):
+        t += rng.exponential(1.0)
+        if rng.random() < 0.7:
+            key = ("2d", STREAM_2D_SIZES[rng.integers(len(STREAM_2D_SIZES))],
+                   STREAM_2D_ANGLES[rng.integers(len(STREAM_2D_ANGLES))])
+        else:
+            key = ("3d", STREAM_3D_DIMS[rng.integers(len(STREAM_3D_DIMS))],
+                   STREAM_3D_TILTS[rng.integers(len(STREAM_3D_TILTS))])
+        out.append((t, key, "cg" if rng.random() < 0.5 else "sb"))
+    return out
+
+
+class StreamInputs:
+    """Host inputs per geometry of the stream, built once: one seeded phantom per
+    size, forward-projected on the GPU for each angle set or tilt, plus 1 %
+    noise (2D sinograms normalised by their maximum, as the reference's
+    prepare_sinogram does; 3D projections raw, MBIR normalises them)."""
+
+    def __init__(self, lc):
+        self.lc = lc
+        self.phantoms = {}
+        self.inputs = {}
+
+    def get(self, key):
+        if key in self.inputs:
+            return self.inputs[key]
+        import torch
+        from laminocam_b200 import synthetic as S
+        lc = self.lc
+        if key[0] == "2d":
+            _, n, nth = key
+            if n not in self.phantoms:
+                self.phantoms[n] = S.ellipse_phantom(n, 10, 1000 + n)
+            th = np.arange(nth) * np.pi / nth
+            s = lc.forward2d(torch.as_tensor(self.phantoms[n][None], device="cuda"),
+                             lc.PolarGrid2D(th, n)).cpu().numpy()
+            s = S.add_noise(s, NOISE, 2000 + n + nth)
+            val = (np.ascontiguousarray(s / s.max(), dtype=np.float32), th)
+        else:
+            _, dims, tilt = key
+            if dims not in self.phantoms:
+                self.phantoms[dims] = S.ellipsoid_phantom(dims, N_ELLIPSOIDS, 1000 + dims[0])
+            th = np.arange(STREAM_3D_ANGLES) * 2 * np.pi / STREAM_3D_ANGLES
+            gam = -tilt * np.pi / 180.0
+            pg = lc.PolarGrid(th, np.full(len(th), gam), np.zeros(len(th)), dims[1], dims[2])
+            p = lc.forward(torch.as_tensor(self.phantoms[dims], device="cuda"), pg)
+            p = p + NOISE * p.max() * torch.randn(
+                p.shape, device="cuda", generator=torch.Generator("cuda").manual_seed(2000 + tilt))
+            val = (np.ascontiguousarray(p.cpu().numpy(), dtype=np.float32), th, gam)
+            del pg
+        self.inputs[key] = val
+        return val
+
+
+def stream_params(lc, key, method, plain, iters=STREAM_ITERS):
+    """Plain: FP32 scalars, a host check of the solver state after every
+    iteration (a tolerance of 1e-30 keeps the check without ever stopping), no
+    graphs, the reference's residual schedule.  Served: FP64 scalars, a fixed
+    count, CUDA-graph iterations, the operator product carried for 16 outer
+    iterations."""
+    dims = (1, key[1], key[1]) if key[0] == "2d" else key[1]
+    stop = 1e-30 if plain else 0.0
+    common = dict(recon_dims=dims, max_iters=iters, inner_iters=1, lam=LAM, mu=MU,
+                  fp32_scalars=plain, use_graph=not plain, poll_every=1 if plain else 8)
+    if method == "cg":
+        return lc.ReconParams(regularizer="unconstrained", tol=stop, xtol=0.0, **common)
+    return lc.ReconParams(regularizer="split_bregman", tol=0.0, xtol=stop,
+                          residual_refresh=1 if plain else 16, **common)
+
+
+def serving_stream(lc, workers=16, count=STREAM_REQUESTS, rates=STREAM_RATES):
+    """The served request stream against plain sequential GPU solves, both
+    open-loop at the same Poisson arrival times.  Plain: one request at a time
+    through MBIR2D / MBIR in arrival order (a request waits for the previous
+    one), each building its own PSF.  Served: each request submitted to one
+    long-lived server at its arrival time; the server's PSF cache is cleared
+    before each rate, so hits come only from geometries repeated within the
+    stream.  Wall clock, host buffers in and out; recons/s = requests / (end of
+    the last request - start), latency = end - arrival."""
+    import torch
+    from oracle import oracle as O
+    reqs = stream_requests(count)
+    data = StreamInputs(lc)
+    for _, key, _ in reqs:
+        data.get(key)
+    torch.cuda.synchronize()
+
+    def plain_solve(key, method, iters=STREAM_ITERS):
+        d = data.get(key)
+        prm = stream_params(lc, key, method, True, iters)
+        if key[0] == "2d":
+            return lc.MBIR2D(d[0], d[1], prm)
+        return lc.MBIR([lc.Dataset(d[0], d[1], d[2], 0.0)], prm)
+
+    def submit(sv, key, method, iters=STREAM_ITERS):
+        d = data.get(key)
+        prm = stream_params(lc, key, method, False, iters)
+        if key[0] == "2d":
+            return sv.submit2d(d[0], d[1], prm)
+        return sv.submit3d([lc.Dataset(d[0], d[1], d[2], 0.0)], prm)
+
+    # untimed: one iteration of every geometry and method in both forms fills
+    # the FFT launch-tuner cache (shared by the process) and grows every
+    # worker's buffers, so neither form pays first-use costs in the timed runs
+    shapes = sorted({(k, m) for _, k, m in reqs}, key=str)
+    for k, m in shapes:
+        plain_solve(k, m, 1)
+    out = {"workload": f"{count} requests, Poisson arrivals (seed 3000): 70 % 2D slices n in "
+                       f"{list(STREAM_2D_SIZES)}, angles in {list(STREAM_2D_ANGLES)}; 30 % laminography "
+                       f"volumes {[list(d) for d in STREAM_3D_DIMS]}, tilt {list(STREAM_3D_TILTS)} deg, "
+                       f"{STREAM_3D_ANGLES} angles; CG {STREAM_ITERS} iterations or Split-Bregman "
+                       f"{STREAM_ITERS} outer x 1 inner (lambda {LAM}, mu {MU}), 50/50; 1 % noise",
+           "distinct_geometries": len({k for _, k, _ in reqs}),
+           "timing": "wall clock, host buffers in and out, open loop", "rates": []}
+    with lc.Server(workers=workers) as sv:
+        for _ in range(2):
+            ids = [submit(sv, k, m, 1) for k, m in shapes]
+            for j in ids:
+                sv.wait(j, 600)
+        for rate in rates:
+            # plain, in arrival order
+            t0 = time.perf_counter()
+            lat, plain_out, service = [], [], {}
+            for u, key, method in reqs:
+                arr = t0 + u / rate
+                now = time.perf_counter()
+                if now < arr:
+                    time.sleep(arr - now)
+                a = time.perf_counter()
+                plain_out.append(plain_solve(key, method))
+                b = time.perf_counter()
+                lat.append((b - arr) * 1e3)
+                cat = f"{key[0]}_{key[1] if key[0] == '2d' else key[1][0]}_{method}"
+                c = service.setdefault(cat, [0, 0.0])
+                c[0] += 1
+                c[1] += (b - a) * 1e3
+            t_plain = time.perf_counter() - t0
+            # served
+            sv.clear_psf_cache()
+            sv.reset_stats()
+            t0 = time.perf_counter()
+            subs = []
+            for u, key, method in reqs:
+                arr = t0 + u / rate
+                now = time.perf_counter()
+                if now < arr:
+                    time.sleep(arr - now)
+                subs.append((submit(sv, key, method), time.perf_counter() - arr))
+            res = [sv.wait(j, 600) for j, _ in subs]
+            t_served = time.perf_counter() - t0
+            st = sv.stats()
+            slat = [lag * 1e3 + r.latency_ms for (_, lag), r in zip(subs, res)]
+            diffs = [O.rel_l2(r.recon, p) for r, p in zip(res, plain_out)]
+            out["rates"].append({
+                "rate_req_s": rate,
+                "plain": {"recons_per_s": count / t_plain, "seconds": t_plain,
+                          "latency_ms_p50": float(np.percentile(lat, 50)),
+                          "latency_ms_p99": float(np.percentile(lat, 99)),
+                          "service_ms_by_kind": {k: {"requests": v[0], "total_ms": round(v[1], 1)}
+                                                 for k, v in sorted(service.items())}},
+                "served": {"recons_per_s": count / t_served, "seconds": t_served,
+                           "latency_ms_p50": float(np.percentile(slat, 50)),
+                           "latency_ms_p99": float(np.percentile(slat, 99)),
+                           "peak_running": st["peak_running"],
+                           "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9,
+                           "psf_hits": st["psf_hits"], "psf_misses": st["psf_misses"],
+                           "psf_hit_rate": st["psf_hits"] / max(1, st["psf_hits"] + st["psf_misses"])},
+                "speedup": t_plain / t_served,
+                "max_rel_l2_served_vs_plain": {
+                    m: max([d for d, (_, _, mm) in zip(diffs, reqs) if mm == m] or [0.0])
+                    for m in ("cg", "sb")},
+            })
+        # the error of both forms against the FP64 oracle on small jobs of the
+        # stream's two solver kinds
+        from laminocam_b200 import synthetic as S
+        th1 = np.arange(60) * np.pi / 60
+        s1 = lc.forward2d(S.ellipse_phantom(63, 10, 4000)[None], lc.PolarGrid2D(th1, 63)).cpu().numpy()
+        s1 = np.ascontiguousarray(S.add_noise(s1, NOISE, 4001), dtype=np.float32)
+        s1 /= s1.max()
+        key1 = ("2d", 63, 60)
+        data.inputs[key1] = (s1, th1)
+        err = {}
+        for m in ("cg", "sb"):
+            xs = sv.wait(submit(sv, key1, m), 600).recon
+            xp = plain_solve(key1, m)
+            xo = O.mbir2d(s1.astype(np.float64), th1, (1, 63, 63), method=m, max_iters=STREAM_ITERS,
+                          tol=0, xtol=0, lam=LAM, mu=MU)
+            err[m] = {"served": O.rel_l2(xs, xo), "plain": O.rel_l2(xp, xo)}
+        out["rel_l2_vs_fp64_oracle_n63"] = err
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -345,6 +558,12 @@ def main():
                          "CG updates in between")
     ap.add_argument("--no-mix", action="store_true",
                     help="skip the served-vs-plain 64-job 2D mix")
+    ap.add_argument("--no-stream", action="store_true",
+                    help="skip the served-vs-plain Poisson request stream")
+    ap.add_argument("--stream-only", action="store_true",
+                    help="run only the served-vs-plain Poisson request stream and print its figures")
+    ap.add_argument("--stream-requests", type=int, default=STREAM_REQUESTS,
+                    help="requests per arrival rate of the request stream")
     ap.add_argument("--small", action="store_true",
                     help="reduced case for profiler captures: recon_dims [15,255,255], 180 angles, "
                          "255x255 detector, 5 outer iterations (not a benchmark line)")
@@ -362,6 +581,7 @@ def main():
                        "angles": NANGLES, "detector": list(DET), "outer_iters": OUTER})
         args.no_cpu_baseline = True
         args.no_mix = True
+        args.no_stream = True
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -369,6 +589,12 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.stream_only:
+        import laminocam_b200 as lc
+        if rank == 0:
+            print(json.dumps({"serving_stream": serving_stream(lc, count=args.stream_requests)}),
+                  flush=True)
+        return
 
     import ctypes as C
 
@@ -537,6 +763,13 @@ def main():
         except Exception as ex:  # reported, not fatal
             serving = {"error": repr(ex)}
 
+    stream = None
+    if rank == 0 and world == 1 and not args.no_stream:
+        try:
+            stream = serving_stream(lc, count=args.stream_requests)
+        except Exception as ex:  # reported, not fatal
+            stream = {"error": repr(ex)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -558,7 +791,8 @@ def main():
                 "h2d_bytes_per_step": int(host_proj.numel() * 4),
                 "d2h_bytes_per_step": int(host_recon.numel() * 4)},
         "roofline": roof, "rooflines": rooflines, "kernels": prof[:12], "clocks": clk.summary(),
-        "serving": serving, "gpu_launches": int(launches), "cpu_baseline": cpu,
+        "serving": serving, "serving_stream": stream, "gpu_launches": int(launches),
+        "cpu_baseline": cpu,
         "solver": {"outer_iters": stats.iters, "cg_iters": stats.cg_iters_total, "dx": stats.dx,
                    "residual_refresh": args.residual_refresh,
                    "rel_l2_vs_exact_residual_schedule": schedule_check},

@@ -280,6 +280,9 @@ int lc_server_wait(lc_server server, long long job_id, double timeout_ms, lc_sol
 int lc_server_get_stats(lc_server server, lc_server_stats *out);
 /* clears the latency record and the counters (the PSF cache stays) */
 int lc_server_reset_stats(lc_server server);
+/* drops the cached Toeplitz spectra and zeroes the hit / miss counts; running
+ * jobs keep the spectrum they hold */
+int lc_server_clear_psf_cache(lc_server server);
 /* message of the last failed submit / wait on the server */
 const char *lc_server_last_error(lc_server server);
 

@@ -467,11 +467,20 @@ def MBIR2D(sinogram, theta, params: ReconParams, ctx: Optional[Context] = None, 
     return (out, _info(st)) if return_info else out
 
 
+def _stack_projs(datasets: Sequence[Dataset]) -> np.ndarray:
+    """Projections of all datasets stacked along the angle axis, contiguous
+    float32 (one contiguous float32 dataset is passed through without a copy)."""
+    if len(datasets) == 1:
+        return np.ascontiguousarray(datasets[0].projs, dtype=np.float32)
+    return np.ascontiguousarray(np.concatenate(
+        [np.asarray(d.projs, dtype=np.float32) for d in datasets], axis=0))
+
+
 def MBIR(datasets: Sequence[Dataset], params: ReconParams, ctx: Optional[Context] = None,
          return_info=False):
     """gpu::MBIR (src/gpu/mbir.cu:41-167): stacks datasets, normalises, pads, solves, crops."""
     ctx = ctx or Context.default()
-    projs = np.concatenate([np.asarray(d.projs, dtype=np.float32) for d in datasets], axis=0)
+    projs = _stack_projs(datasets)
     theta = np.concatenate([np.asarray(d.angles, dtype=np.float64) for d in datasets])
     gamma = np.concatenate([np.full(len(d.angles), d.gamma, dtype=np.float64) for d in datasets])
     beta = np.concatenate([np.full(len(d.angles), d.beta, dtype=np.float64) for d in datasets])
@@ -557,8 +566,7 @@ class Server:
         return jid.value
 
     def submit3d(self, datasets: Sequence[Dataset], params: ReconParams) -> int:
-        projs = np.ascontiguousarray(np.concatenate(
-            [np.asarray(d.projs, dtype=np.float32) for d in datasets], axis=0))
+        projs = _stack_projs(datasets)
         theta = np.concatenate([np.asarray(d.angles, dtype=np.float64) for d in datasets])
         gamma = np.concatenate([np.full(len(d.angles), d.gamma, dtype=np.float64) for d in datasets])
         beta = np.concatenate([np.full(len(d.angles), d.beta, dtype=np.float64) for d in datasets])
@@ -606,6 +614,12 @@ class Server:
 
     def reset_stats(self):
         self.lib.lc_server_reset_stats(self.handle)
+
+    def clear_psf_cache(self):
+        """Drops the cached Toeplitz spectra and zeroes the hit / miss counts."""
+        rc = self.lib.lc_server_clear_psf_cache(self.handle)
+        if rc != 0:
+            self._fail(rc, "clear_psf_cache")
 
     def close(self):
         if getattr(self, "handle", None):

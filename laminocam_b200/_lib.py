@@ -104,6 +104,7 @@ SIGNATURES = {
     "lc_server_wait": (i32, [vp, C.c_longlong, f64, C.POINTER(SolverStats), C.POINTER(JobInfo)]),
     "lc_server_get_stats": (i32, [vp, C.POINTER(ServerStats)]),
     "lc_server_reset_stats": (i32, [vp]),
+    "lc_server_clear_psf_cache": (i32, [vp]),
     "lc_server_last_error": (C.c_char_p, [vp]),
 }
 

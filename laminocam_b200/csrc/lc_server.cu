@@ -113,11 +113,14 @@ class PsfCache {
         return T;
     }
 
-    void clear() {
+    // drops every entry (jobs holding a spectrum keep their copy) and, with
+    // `counters`, zeroes the hit and miss counts
+    void clear(bool counters = false) {
         std::lock_guard<std::mutex> lk(mu_);
         map_.clear();
         lru_.clear();
         used_ = 0;
+        if (counters) hits_ = misses_ = 0;
     }
     void counters(long &hits, long &misses, size_t &used, long &entries) {
         std::lock_guard<std::mutex> lk(mu_);
@@ -532,6 +535,12 @@ int lc_server_reset_stats(lc_server sv) {
     sv->have_first = false;
     sv->peak_in_use = sv->in_use;
     sv->peak_running = sv->running;
+    return LC_OK;
+}
+
+int lc_server_clear_psf_cache(lc_server sv) {
+    if (!sv) return LC_ERR_INVALID;
+    if (sv->cache) sv->cache->clear(true);
     return LC_OK;
 }
 

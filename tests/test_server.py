@@ -142,6 +142,24 @@ def test_server_result_matches_oracle(lc):
     assert O.rel_l2(r.recon, xo) < RECON_TOL
 
 
+def test_server_psf_cache_clear(lc):
+    """Clearing the cache drops the spectra and zeroes the counts: the next job
+    of a cached geometry builds its PSF again, with the same result."""
+    s, th = sino2d(lc, 63, 60, 31)
+    prm = params2d(lc, 63, "split_bregman", 3)
+    with lc.Server(workers=1) as sv:
+        a = sv.wait(sv.submit2d(s, th, prm), WAIT_S)
+        b = sv.wait(sv.submit2d(s, th, prm), WAIT_S)
+        assert not a.psf_hit and b.psf_hit
+        sv.clear_psf_cache()
+        st = sv.stats()
+        assert st["psf_hits"] == st["psf_misses"] == st["psf_cache_entries"] == 0
+        c = sv.wait(sv.submit2d(s, th, prm), WAIT_S)
+        assert not c.psf_hit
+        assert sv.stats()["psf_misses"] == 1
+    assert O.rel_l2(c.recon, a.recon) < RECON_TOL
+
+
 def test_server_isolates_failing_job(lc):
     s, th = sino2d(lc, 63, 60, 31)
     good = params2d(lc, 63, "unconstrained", 4)
