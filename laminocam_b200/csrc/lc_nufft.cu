@@ -14,6 +14,7 @@ namespace lc {
 // ---------------------------------------------------------------------------
 void geometry_init_2d(Context &ctx, PolarGeometry &g, const double *theta, int ntheta, int nr) {
     LC_REQUIRE(ntheta > 0 && nr > 0, "geometry: ntheta and nradial must be positive");
+    LC_REQUIRE((long)ntheta * nr < (1L << 31), "geometry: too many points");
     g.theta.assign(theta, theta + ntheta);
     std::vector<double2> cs(ntheta);
     for (int i = 0; i < ntheta; ++i) cs[i] = make_double2(std::cos(theta[i]), std::sin(theta[i]));
@@ -25,6 +26,7 @@ void geometry_init_2d(Context &ctx, PolarGeometry &g, const double *theta, int n
     g.pts.nr = nr;
     g.pts.M = (long)ntheta * nr;
     g.pts.cs = g.cs.get();
+    g.pts.div_angle = make_fastdiv((unsigned)nr);
 }
 
 void geometry_init_3d(Context &ctx, PolarGeometry &g, const double *theta, const double *gamma,
@@ -60,6 +62,8 @@ void geometry_init_3d(Context &ctx, PolarGeometry &g, const double *theta, const
     g.pts.ncols = ncols;
     g.pts.M = (long)ntheta * nrows * ncols;
     g.pts.rot = g.rot.get();
+    g.pts.div_angle = make_fastdiv((unsigned)nrows * (unsigned)ncols);
+    g.pts.div_col = make_fastdiv((unsigned)ncols);
 }
 
 // ---------------------------------------------------------------------------
@@ -128,8 +132,12 @@ struct GridCfg {
     int nb[3];
     int hw[3];
     int td[3];   // tile extent per dim
+    double inv_nf[3];
+    FastDiv div_tx, div_ty;  // by the tile extents along x and y
     float beta;
 };
+
+__device__ __forceinline__ unsigned fast_div(unsigned n, FastDiv f) { return (__umulhi(n, f.m) + n) >> f.s; }
 
 struct PointInfo {
     double c[3];  // x, y, z
@@ -138,9 +146,10 @@ struct PointInfo {
 };
 
 __device__ __forceinline__ void point_at(const PolarPts &p, long j, PointInfo &pi) {
+    const unsigned jj = (unsigned)j;  // M < 2^31
     if (p.dim == 2) {
-        int i = (int)(j / p.nr);
-        int m = (int)(j - (long)i * p.nr);
+        const int i = (int)fast_div(jj, p.div_angle);
+        const int m = (int)(jj - (unsigned)i * (unsigned)p.nr);
         double r = ((double)m + 0.5) * (2.0 * kPi / p.nr) - kPi;
         double2 cs = p.cs[i];
         pi.c[0] = cs.x * r;
@@ -150,11 +159,10 @@ __device__ __forceinline__ void point_at(const PolarPts &p, long j, PointInfo &p
         pi.qX = r;
         pi.qY = 0.0;
     } else {
-        long per = (long)p.nrows * p.ncols;
-        int i = (int)(j / per);
-        long rem = j - (long)i * per;
-        int a = (int)(rem / p.ncols);
-        int b = (int)(rem - (long)a * p.ncols);
+        const unsigned i = fast_div(jj, p.div_angle);
+        const unsigned rem = jj - i * ((unsigned)p.nrows * (unsigned)p.ncols);
+        const unsigned ua = fast_div(rem, p.div_col);
+        const int a = (int)ua, b = (int)(rem - ua * (unsigned)p.ncols);
         double qX = ((double)b + 0.5) * (2.0 * kPi / p.ncols) - kPi;
         double qY = ((double)a + 0.5) * (2.0 * kPi / p.nrows) - kPi;
         const double *R = p.rot + 6 * (long)i;
@@ -163,7 +171,7 @@ __device__ __forceinline__ void point_at(const PolarPts &p, long j, PointInfo &p
         pi.c[2] = R[4] * qX + R[5] * qY;
         pi.qX = qX;
         pi.qY = qY;
-        pi.angle = i;
+        pi.angle = (int)i;
     }
 }
 
@@ -172,10 +180,13 @@ __device__ __forceinline__ bool in_band(const PointInfo &pi) {
 }
 
 // wrapped fine-grid coordinate u in [0, nf), its cell, first covered cell l0
-// and the float offset u - l0
-__device__ __forceinline__ void place(double x, int nf, int W, int &cell, int &l0, float &off) {
+// and the float offset u - l0 (inv_nf = 1 / nf; a quotient one off is
+// corrected, so the result equals the wrap by exact division)
+__device__ __forceinline__ void place(double x, int nf, double inv_nf, int W, int &cell, int &l0,
+                                      float &off) {
     double u = x * (double)nf * kInv2Pi;
-    u -= (double)nf * floor(u / (double)nf);
+    u -= (double)nf * floor(u * inv_nf);
+    if (u < 0.0) u += (double)nf;
     if (u >= (double)nf) u -= (double)nf;
     if (u < 0.0) u = 0.0;
     cell = (int)floor(u);
@@ -185,6 +196,26 @@ __device__ __forceinline__ void place(double x, int nf, int W, int &cell, int &l
     off = (float)(u - lo);
 }
 
+// v wrapped into [0, n) for v in [-n, 3n)
+__device__ __forceinline__ int wrap_near(int v, int n) {
+    if (v >= n) v -= n;
+    if (v >= n) v -= n;
+    if (v < 0) v += n;
+    return v;
+}
+
+// fine-grid offset of tile cell rr (x fastest) of the tile starting at S
+template <int DIM>
+__device__ __forceinline__ long tile_cell_to_grid(int rr, const GridCfg &g, const int (&S)[3]) {
+    const unsigned q = fast_div((unsigned)rr, g.div_tx);  // row of the tile: iy + ty iz
+    const int ix = rr - (int)q * g.td[0];
+    const unsigned iz = DIM == 3 ? fast_div(q, g.div_ty) : 0u;
+    const int iy = (int)q - (int)iz * g.td[1];
+    long gi = (long)wrap_near(S[0] + ix, g.nf[0]) + (long)wrap_near(S[1] + iy, g.nf[1]) * g.nf[0];
+    if (DIM == 3) gi += (long)wrap_near(S[2] + (int)iz, g.nf[2]) * ((long)g.nf[0] * g.nf[1]);
+    return gi;
+}
+
 template <int DIM>
 __device__ __forceinline__ int bin_of(const PointInfo &pi, const GridCfg &g, int W) {
     int b = 0, mul = 1;
@@ -192,7 +223,7 @@ __device__ __forceinline__ int bin_of(const PointInfo &pi, const GridCfg &g, int
     for (int d = 0; d < DIM; ++d) {
         int cell, l0;
         float off;
-        place(pi.c[d], g.nf[d], W, cell, l0, off);
+        place(pi.c[d], g.nf[d], g.inv_nf[d], W, cell, l0, off);
         b += (cell / g.bs[d]) * mul;
         mul *= g.nb[d];
     }
@@ -236,11 +267,24 @@ __global__ void bin_scatter_kernel(PolarPts pts, GridCfg g, int W, int *cursor, 
 // ---- spreading ----------------------------------------------------------
 // One thread spreads one point over its W^DIM footprint with shared-memory
 // atomics into a planar tile.  All lanes of a warp issue each atomic
-// instruction at the same footprint offset, so their addresses differ by the
-// differences of their footprint corners.  The points of a subproblem are
-// therefore first bucketed by the shared-memory bank of their corner (corner
-// index mod 32), and in round r lane i spreads the r-th point of bank i: the
-// 32 addresses of every atomic instruction fall in 32 distinct banks.
+// instruction at the same footprint step, so two lanes conflict exactly when
+// their footprint corners fall in the same shared-memory bank (corner index
+// mod 32).  The points of a subproblem are bucketed by corner bank and spread
+// in passes in which the unrotated points hold distinct banks:
+//   * full rounds (every bank still holds a point): lane b takes the next
+//     point of bank b;
+//   * tail rounds (some banks have run out; round r holds the banks with more
+//     than r points, so the sets shrink with r), 3D: the lowest round left
+//     takes the highest round left along on its free lanes when some rotation
+//     fits.  A rotated point visits its footprint planes in an order shifted
+//     by rho modulo W, so at every step it sits at bank b + d1 or b + d2 of
+//     the unrotated frame, d1 = rho P and d2 = (rho - W) P mod 32 with P the
+//     plane stride; the rotation fits when both banks of every point of the
+//     high round are clear of the low round's banks.  The pairing depends on
+//     the bank counts alone, so every warp walks it and spreads the passes
+//     that fall to it.  (2D tiles run the tail rounds one by one.)
+// The accumulation is exact and order-free (below): the schedule decides the
+// speed, never the result.
 //
 // The tile accumulates in exact fixed point with 32-bit integer atomics,
 // which run about four times faster than float atomics in shared memory.
@@ -265,13 +309,33 @@ constexpr int kSpreadThreads = 256;
 constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
 constexpr unsigned kRoundMagicBits = 0x4B400000u;
 
-// hi += round(a b) + B, lo += round((a b - round(a b)) 2^20) + B, |a b| < 2^22
-__device__ __forceinline__ void fixed_add(int *hi, int *lo, float a, float b) {
+// shared-memory atomic add without return at a 32-bit shared address plus a
+// compile-time byte offset, so one address register serves a footprint row
+template <int OFF>
+__device__ __forceinline__ void red_shared(unsigned addr, int v) {
+    asm volatile("red.shared.add.u32 [%0+%2], %1;" ::"r"(addr), "r"(v), "n"(OFF) : "memory");
+}
+
+// hi += round(a b) + B, lo += round((a b - round(a b)) 2^20) + B, |a b| < 2^22,
+// at cell DX of the rows starting at the shared addresses hi and lo
+template <int DX>
+__device__ __forceinline__ void fixed_add(unsigned hi, unsigned lo, float a, float b) {
     const float y1 = fmaf(a, b, kRoundMagic);
     const float h = y1 - kRoundMagic;
     const float y2 = fmaf(fmaf(a, b, -h), 1048576.0f, kRoundMagic);
-    atomicAdd(hi, __float_as_int(y1));
-    atomicAdd(lo, __float_as_int(y2));
+    red_shared<4 * DX>(hi, __float_as_int(y1));
+    red_shared<4 * DX>(lo, __float_as_int(y2));
+}
+
+// one footprint row of W cells, real and imaginary parts
+template <int W, int DX = 0>
+__device__ __forceinline__ void spread_row(unsigned hr, unsigned lr, unsigned hi, unsigned li, float vr,
+                                           float vi, const float (&wx)[W]) {
+    if constexpr (DX < W) {
+        fixed_add<DX>(hr, lr, vr, wx[DX]);
+        fixed_add<DX>(hi, li, vi, wx[DX]);
+        spread_row<W, DX + 1>(hr, lr, hi, li, vr, vi, wx);
+    }
 }
 
 // cnt[q] <- sum of cnt[q - d], d in [0, w), along one axis of a tile of
@@ -290,6 +354,103 @@ __device__ __forceinline__ void box_sum_axis(int *cnt, int axis, int w, int tx, 
             const int cq = cnt[base + q * stride];
             cnt[base + q * stride] = win;
             win += (q - w >= 0 ? cnt[base + (q - w) * stride] : 0) - cq;
+        }
+    }
+}
+
+// position of the k-th (from 0) set bit of m, k < popc(m)
+__device__ __forceinline__ int kth_bit(unsigned m, int k) {
+    int pos = 0;
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1) {
+        const int c = __popc(m & ((1u << w) - 1u));
+        if (k >= c) {
+            k -= c;
+            m >>= w;
+            pos += w;
+        }
+    }
+    return pos;
+}
+
+// Bank offsets (mod 32) that a point of a 3D tile whose footprint planes are
+// visited rotated by rot (1 <= rot < W) occupies relative to the unrotated lanes
+template <int W>
+__device__ __forceinline__ void rot_banks(int rot, int plane, int &d1, int &d2) {
+    d1 = (plane * rot) & 31;
+    d2 = (plane * (rot - W)) & 31;
+}
+
+// Spreads point j; in 3D its footprint planes are visited in the order rotated
+// by rot (0: in order).
+template <int DIM, int W>
+__device__ __forceinline__ void spread_point(const PolarPts &pts, const GridCfg &g,
+                                             const float2 *__restrict__ c, long cstride, int nvol, int j,
+                                             int mode, const float2 *__restrict__ shifts, const int (&S)[3],
+                                             int tx, int plane, int tsize, unsigned sm_hre,
+                                             unsigned plane_bytes, float fscale, int rot) {
+    const float inv_hw = 2.0f / (float)W;
+    PointInfo pi;
+    point_at(pts, j, pi);
+    float2 mult = make_float2(fscale, 0.f);
+    if (mode == PT_SHIFT) {
+        const float2 sh = shifts[pi.angle];
+        const double ph = pi.qX * (double)sh.x + pi.qY * (double)sh.y;
+        double sn, cs;
+        sincos(ph, &sn, &cs);
+        mult = make_float2((float)cs * fscale, (float)-sn * fscale);
+    }
+    // wk[d][m]: weight of the cell at offset m along axis d (3D z: (m + rot) mod W)
+    float wk[DIM][W];
+    int corner = 0;
+    {
+        const int stride[3] = {1, tx, plane};
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            int cell, l0;
+            float off;
+            place(pi.c[d], g.nf[d], g.inv_nf[d], W, cell, l0, off);
+            corner += (l0 - S[d]) * stride[d];
+            const int r = d == 2 ? rot : 0;
+#pragma unroll
+            for (int m = 0; m < W; ++m) {
+                int mm = m + r;
+                if (mm >= W) mm -= W;
+                wk[d][m] = es_evalf(((float)mm - off) * inv_hw, g.beta);
+            }
+        }
+    }
+    for (int s = 0; s < nvol; ++s) {
+        float2 v = c[(long)s * cstride + j];
+        v = mode == PT_SHIFT ? cmul(v, mult) : make_float2(v.x * fscale, v.y * fscale);
+        // 32-bit shared addresses of the footprint corner in the four planes
+        const unsigned hr = sm_hre + 4u * (unsigned)(s * tsize + corner);
+        const unsigned lr = hr + plane_bytes, hi = lr + plane_bytes, li = hi + plane_bytes;
+        if constexpr (DIM == 2) {
+#pragma unroll
+            for (int dy = 0; dy < W; ++dy) {
+                const float vr = v.x * wk[1][dy], vi = v.y * wk[1][dy];
+                const unsigned row = 4u * (unsigned)(dy * tx);
+                spread_row<W>(hr + row, lr + row, hi + row, li + row, vr, vi, wk[0]);
+            }
+        } else {
+#pragma unroll 1
+            for (int dz = 0; dz < W; ++dz) {
+                float wz = wk[2][0];
+#pragma unroll
+                for (int m = 1; m < W; ++m)
+                    if (dz == m) wz = wk[2][m];
+                int zz = dz + rot;
+                if (zz >= W) zz -= W;
+                const float zr = v.x * wz, zi = v.y * wz;
+                const unsigned zo = 4u * (unsigned)(zz * plane);
+#pragma unroll
+                for (int dy = 0; dy < W; ++dy) {
+                    const float vr = zr * wk[1][dy], vi = zi * wk[1][dy];
+                    const unsigned row = zo + 4u * (unsigned)(dy * tx);
+                    spread_row<W>(hr + row, lr + row, hi + row, li + row, vr, vi, wk[0]);
+                }
+            }
         }
     }
 }
@@ -324,7 +485,7 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
     int *him = lre + acc_n;
     int *lim = him + acc_n;
     int *kcnt = lim + acc_n;  // footprint corners per cell, then footprints per cell
-    int *order = kcnt + tsize;
+    unsigned short *order = reinterpret_cast<unsigned short *>(kcnt + tsize);  // points by bank
     constexpr int kKeys = 8;  // points per thread in the bucketing pass (maxpts <= 8 * threads)
     int key[kKeys];
     const int tid = threadIdx.x;
@@ -351,7 +512,7 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
             for (int d = 0; d < DIM; ++d) {
                 int cell, l0;
                 float off;
-                place(pi.c[d], g.nf[d], W, cell, l0, off);
+                place(pi.c[d], g.nf[d], g.inv_nf[d], W, cell, l0, off);
                 corner += (l0 - S[d]) * stride[d];
             }
             const int b = corner & 31;
@@ -371,21 +532,21 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
     __syncthreads();
     if (tid < 32) {
         const int v = cnt[tid];
-        int incl = v, m = v;
+        int incl = v, mx = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int t = __shfl_up_sync(0xffffffffu, incl, o);
             if (tid >= o) incl += t;
-            m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+            mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         }
         start[tid] = incl - v;
-        if (tid == 0) maxcnt = m;
+        if (tid == 0) maxcnt = mx;
     }
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < kKeys; ++q) {
         const int k = key[q];
-        if (k >= 0) order[start[k >> 16] + (k & 0xffff)] = tid + q * (int)blockDim.x;
+        if (k >= 0) order[start[k >> 16] + (k & 0xffff)] = (unsigned short)(tid + q * (int)blockDim.x);
     }
     // fixed-point scale F = 2^k: F m <= 2^21 and F n m < 2^30
     float fscale = 1.f;
@@ -400,75 +561,48 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
     }
     __syncthreads();
 
-    // ---- spread: in round r, lane i takes the r-th point of bank i ----
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    const float inv_hw = 2.0f / (float)W;
-    const int mycnt = cnt[lane], mystart = start[lane];
-    for (int r = warp; r < maxcnt; r += nwarps) {
-        if (r >= mycnt) continue;
-        const int j = perm[sp.y + order[mystart + r]];
-        PointInfo pi;
-        point_at(pts, j, pi);
-        float2 mult = make_float2(fscale, 0.f);
-        if (mode == PT_SHIFT) {
-            const float2 sh = shifts[pi.angle];
-            const double ph = pi.qX * (double)sh.x + pi.qY * (double)sh.y;
-            double sn, cs;
-            sincos(ph, &sn, &cs);
-            mult = make_float2((float)cs * fscale, (float)-sn * fscale);
+    const unsigned sm_hre = (unsigned)__cvta_generic_to_shared(hre);
+    const unsigned plane_bytes = 4u * (unsigned)acc_n;  // bytes between the hre, lre, him, lim planes
+    const int mycnt = cnt[lane], mystart = start[lane], nrounds = maxcnt;
+    // ---- rounds 0 .. nrounds-1 in passes; round r holds the banks with more
+    // than r points, so the sets shrink with r.  In 3D the lowest round left
+    // (banks A_lo) takes the highest round left (A_hi) along when some plane
+    // rotation keeps both banks of every A_hi point clear of A_lo; the points
+    // of A_hi then fill the free lanes in bank order.  Every warp walks the
+    // same pairing and spreads the passes that fall to it (one call site keeps
+    // the unrolled footprint code in the instruction cache once).
+    int od1 = 0, od2 = 0;  // lane o tests the plane rotation o + 1
+    if (DIM == 3 && lane < W - 1) rot_banks<W>(lane + 1, plane, od1, od2);
+    for (int i = 0, j = nrounds - 1, pass = 0; i <= j; ++pass) {
+        const unsigned alo = __ballot_sync(0xffffffffu, mycnt > i);
+        unsigned ahi = 0;
+        int rot = 0;
+        if (DIM == 3 && i < j && alo != 0xffffffffu) {
+            ahi = __ballot_sync(0xffffffffu, mycnt > j);
+            const bool ok = lane < W - 1 && __popc(alo) + __popc(ahi) <= 32 &&
+                            !(__funnelshift_l(ahi, ahi, od1) & alo) && !(__funnelshift_l(ahi, ahi, od2) & alo);
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (m) rot = __ffs(m);
+            else ahi = 0;
         }
-        float wk[DIM][W];
-        int corner = 0;
-        {
-            const int stride[3] = {1, tx, plane};
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                int cell, l0;
-                float off;
-                place(pi.c[d], g.nf[d], W, cell, l0, off);
-                corner += (l0 - S[d]) * stride[d];
-#pragma unroll
-                for (int m = 0; m < W; ++m) wk[d][m] = es_evalf(((float)m - off) * inv_hw, g.beta);
-            }
-        }
-        for (int s = 0; s < nvol; ++s) {
-            float2 v = c[(long)s * cstride + j];
-            v = mode == PT_SHIFT ? cmul(v, mult) : make_float2(v.x * fscale, v.y * fscale);
-            int *hr = hre + (long)s * tsize + corner, *lr = lre + (long)s * tsize + corner;
-            int *hi = him + (long)s * tsize + corner, *li = lim + (long)s * tsize + corner;
-            if constexpr (DIM == 2) {
-#pragma unroll
-                for (int dy = 0; dy < W; ++dy) {
-                    const float vr = v.x * wk[1][dy], vi = v.y * wk[1][dy];
-                    const int row = dy * tx;
-#pragma unroll
-                    for (int dx = 0; dx < W; ++dx) {
-                        fixed_add(hr + row + dx, lr + row + dx, vr, wk[0][dx]);
-                        fixed_add(hi + row + dx, li + row + dx, vi, wk[0][dx]);
-                    }
-                }
-            } else {
-#pragma unroll 1
-                for (int dz = 0; dz < W; ++dz) {
-                    float wz = wk[2][0];
-#pragma unroll
-                    for (int m = 1; m < W; ++m)
-                        if (dz == m) wz = wk[2][m];
-                    const float zr = v.x * wz, zi = v.y * wz;
-                    const int zo = dz * plane;
-#pragma unroll
-                    for (int dy = 0; dy < W; ++dy) {
-                        const float vr = zr * wk[1][dy], vi = zi * wk[1][dy];
-                        const int row = zo + dy * tx;
-#pragma unroll
-                        for (int dx = 0; dx < W; ++dx) {
-                            fixed_add(hr + row + dx, lr + row + dx, vr, wk[0][dx]);
-                            fixed_add(hi + row + dx, li + row + dx, vi, wk[0][dx]);
-                        }
-                    }
+        if (pass % nwarps == warp) {
+            int p = -1, prot = 0;
+            if ((alo >> lane) & 1u) {
+                p = order[mystart + i];
+            } else if (ahi) {
+                const int k = __popc(~alo & ((1u << lane) - 1u));  // rank among the free lanes
+                if (k < __popc(ahi)) {
+                    p = order[start[kth_bit(ahi, k)] + j];
+                    prot = rot;
                 }
             }
+            if (p >= 0)
+                spread_point<DIM, W>(pts, g, c, cstride, nvol, perm[sp.y + p], mode, shifts, S, tx, plane,
+                                     tsize, sm_hre, plane_bytes, fscale, prot);
         }
+        ++i;
+        if (ahi) --j;
     }
     __syncthreads();
     // footprints per cell: box sums of the corner histogram along each axis
@@ -479,21 +613,18 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
     }
     // flush the tile (halos overlap neighbouring bins, so accumulate atomically)
     const double unscale = 1.0 / ((double)fscale * 1048576.0);
-    for (long idx = tid; idx < acc_n; idx += blockDim.x) {
-        const int s = (int)(idx / tsize);
-        const int rr = (int)(idx - (long)s * tsize);
-        const unsigned kb = (unsigned)kcnt[rr] * kRoundMagicBits;
-        if (kcnt[rr] == 0) continue;
-        const int h1 = (int)((unsigned)hre[idx] - kb), l1 = (int)((unsigned)lre[idx] - kb);
-        const int h2 = (int)((unsigned)him[idx] - kb), l2 = (int)((unsigned)lim[idx] - kb);
-        const float a = (float)(((double)h1 * 1048576.0 + (double)l1) * unscale);
-        const float b = (float)(((double)h2 * 1048576.0 + (double)l2) * unscale);
-        const int ix = rr % tx;
-        const int iy = (rr / tx) % ty;
-        const int iz = rr / plane;
-        long gi = (long)wrap(S[0] + ix, g.nf[0]) + (long)wrap(S[1] + iy, g.nf[1]) * g.nf[0];
-        if (DIM == 3) gi += (long)wrap(S[2] + iz, g.nf[2]) * g.nf[0] * g.nf[1];
-        atomicAdd(grid + (long)s * gstride + gi, make_float2(a, b));
+    for (int s = 0; s < nvol; ++s) {
+        for (int rr = tid; rr < tsize; rr += blockDim.x) {
+            const int k = kcnt[rr];
+            if (k == 0) continue;
+            const unsigned kb = (unsigned)k * kRoundMagicBits;
+            const int idx = s * tsize + rr;
+            const int h1 = (int)((unsigned)hre[idx] - kb), l1 = (int)((unsigned)lre[idx] - kb);
+            const int h2 = (int)((unsigned)him[idx] - kb), l2 = (int)((unsigned)lim[idx] - kb);
+            const float a = (float)(((double)h1 * 1048576.0 + (double)l1) * unscale);
+            const float b = (float)(((double)h2 * 1048576.0 + (double)l2) * unscale);
+            atomicAdd(grid + (long)s * gstride + tile_cell_to_grid<DIM>(rr, g, S), make_float2(a, b));
+        }
     }
 }
 
@@ -522,16 +653,9 @@ __global__ void __launch_bounds__(256) interp_kernel(PolarPts pts, GridCfg g,
     for (int d = 0; d < DIM; ++d) S[d] = bcoord[d] * g.bs[d] - g.hw[d];
     const int tx = g.td[0], ty = g.td[1], tz = DIM == 3 ? g.td[2] : 1;
     const int tsize = tx * ty * tz;
-    for (int idx = threadIdx.x; idx < nvol * tsize; idx += blockDim.x) {
-        int s = idx / tsize;
-        int r = idx - s * tsize;
-        int ix = r % tx;
-        int iy = (r / tx) % ty;
-        int iz = r / (tx * ty);
-        long gi = (long)wrap(S[0] + ix, g.nf[0]) + (long)wrap(S[1] + iy, g.nf[1]) * g.nf[0];
-        if (DIM == 3) gi += (long)wrap(S[2] + iz, g.nf[2]) * g.nf[0] * g.nf[1];
-        tile[idx] = __ldg(grid + (long)s * gstride + gi);
-    }
+    for (int s = 0; s < nvol; ++s)
+        for (int r = threadIdx.x; r < tsize; r += blockDim.x)
+            tile[s * tsize + r] = __ldg(grid + (long)s * gstride + tile_cell_to_grid<DIM>(r, g, S));
     __syncthreads();
     const float inv_hw = 2.0f / (float)W;
     for (int p = threadIdx.x; p < sp.z; p += blockDim.x) {
@@ -549,7 +673,7 @@ __global__ void __launch_bounds__(256) interp_kernel(PolarPts pts, GridCfg g,
         for (int d = 0; d < DIM; ++d) {
             int cell, l0;
             float off;
-            place(pi.c[d], g.nf[d], W, cell, l0, off);
+            place(pi.c[d], g.nf[d], g.inv_nf[d], W, cell, l0, off);
             lo[d] = l0 - S[d];
             if (d < 2) {
 #pragma unroll
@@ -649,7 +773,10 @@ GridCfg make_cfg(int dim, const int nf[3], const int bs[3], const int nb[3], int
         g.nb[d] = nb[d];
         g.hw[d] = d < dim ? lo : 0;
         g.td[d] = d < dim ? bs[d] + w : 1;
+        g.inv_nf[d] = 1.0 / (double)nf[d];
     }
+    g.div_tx = make_fastdiv((unsigned)g.td[0]);
+    g.div_ty = make_fastdiv((unsigned)g.td[1]);
     g.beta = (float)beta;
     return g;
 }
@@ -739,10 +866,11 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
     // values read once, fine grid written once (plus the permutation)
     ProfScope ps(ctx, PS_SPREAD, (double)nvol * (8.0 * pts_.M + 8.0 * gvol) + 4.0 * pts_.M);
     // four 32-bit fixed-point accumulators per cell (high and low words of the
-    // real and imaginary parts) per volume, a footprint count per cell, and the
-    // bucketed point order
+    // real and imaginary parts) per volume, a footprint count per cell and the
+    // bucketed point order (16 bits per point)
     const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * 4 * sizeof(int);
-    const size_t bucket_bytes = (size_t)maxsub_ * sizeof(int) + (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(int);
+    const size_t bucket_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(int) +
+                                (size_t)maxsub_ * sizeof(unsigned short);
     LC_REQUIRE(maxsub_ <= 8 * kSpreadThreads, "NUFFT spread: subproblem larger than the bucketing pass");
     LC_REQUIRE(maxsub_ <= 2048, "NUFFT spread: subproblem too large for the fixed-point sums");
     const int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);

@@ -16,13 +16,28 @@
 
 namespace lc {
 
+// n / d for 0 <= n < 2^31 by a multiply and a shift (Granlund and Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994): with
+// 2^(s-1) < d <= 2^s and m = floor(2^32 (2^s - d) / d) + 1,
+// n / d = (umulhi(n, m) + n) >> s  (the sum stays below 2^32 for n < 2^31).
+struct FastDiv {
+    unsigned m = 1, s = 0;
+};
+
+inline FastDiv make_fastdiv(unsigned d) {
+    FastDiv f;
+    while ((1ull << f.s) < d) ++f.s;
+    f.m = (unsigned)(((1ull << 32) * ((1ull << f.s) - d)) / d + 1);
+    return f;
+}
+
 // Polar grid description.  2D: x = r cos(theta), y = r sin(theta),
 // r_m = (m+1/2) 2pi/nr - pi (include/polar_grid2d.h:50-65).  3D: rows of the
 // detector lattice rotated by transpose(Rx(theta) Ry(beta) Rz(gamma))
 // (include/polar_grid.h:52-94, include/rotation.h:28-56).
 struct PolarPts {
     int dim = 2;
-    long M = 0;
+    long M = 0;  // below 2^31 (the bin sort stores point indices as int)
     int ntheta = 0;
     // 2D
     int nr = 0;
@@ -30,6 +45,8 @@ struct PolarPts {
     // 3D
     int nrows = 0, ncols = 0;
     const double *rot = nullptr;  // R00 R01 R10 R11 R20 R21 per angle
+    // point index -> angle (by nr in 2D, nrows * ncols in 3D) and, in 3D, row (by ncols)
+    FastDiv div_angle, div_col;
 };
 
 struct PolarGeometry {
