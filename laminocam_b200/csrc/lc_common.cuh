@@ -345,6 +345,16 @@ __device__ __forceinline__ float es_evalf(float z, float beta) {
     return s > 0.0f ? expf(beta * (sqrtf(s) - 1.0f)) : 0.0f;
 }
 
+// The same kernel as 2^x with x = beta_l2e (sqrt(1 - z^2) - 1), beta_l2e =
+// beta log2(e) rounded to float: exp2f and a correctly rounded square root.
+// Rounding beta_l2e and the product moves x by at most 2^-23 |x|, so a weight
+// 2^x changes by at most 2^-23 ln(2) |x| 2^x <= 4.4e-8 of the peak weight 1,
+// besides exp2f's own error of 2 ulp.
+__device__ __forceinline__ float es_eval2f(float z, float beta_l2e) {
+    const float s = fmaf(-z, z, 1.0f);
+    return s > 0.0f ? exp2f(beta_l2e * (__fsqrt_rn(s) - 1.0f)) : 0.0f;
+}
+
 // Fine-grid placement of a coordinate x (radians, any real value, taken
 // 2*pi-periodic) on a grid of nf cells of width 2*pi/nf.  Computes the first
 // covered cell l0 (not yet wrapped) and the offset of x from l0 in cells, in

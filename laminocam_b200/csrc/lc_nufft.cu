@@ -134,7 +134,7 @@ struct GridCfg {
     int td[3];   // tile extent per dim
     double inv_nf[3];
     FastDiv div_tx, div_ty;  // by the tile extents along x and y
-    float beta;
+    float beta_l2e;          // ES beta times log2(e)
 };
 
 __device__ __forceinline__ unsigned fast_div(unsigned n, FastDiv f) { return (__umulhi(n, f.m) + n) >> f.s; }
@@ -416,7 +416,7 @@ __device__ __forceinline__ void spread_point(const PolarPts &pts, const GridCfg 
             for (int m = 0; m < W; ++m) {
                 int mm = m + r;
                 if (mm >= W) mm -= W;
-                wk[d][m] = es_evalf(((float)mm - off) * inv_hw, g.beta);
+                wk[d][m] = es_eval2f(((float)mm - off) * inv_hw, g.beta_l2e);
             }
         }
     }
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
                   float2 *__restrict__ grid, long gstride, int mode,
                   const float2 *__restrict__ shifts, int maxpts) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int cnt[32], start[32], maxcnt, cmax_bits;
+    __shared__ int cnt[32], start[32], mincnt, maxcnt, cmax_bits;
     const int4 sp = subs[blockIdx.x];
     int bcoord[3] = {0, 0, 0};
     {
@@ -532,15 +532,19 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
     __syncthreads();
     if (tid < 32) {
         const int v = cnt[tid];
-        int incl = v, mx = v;
+        int incl = v, mn = v, mx = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int t = __shfl_up_sync(0xffffffffu, incl, o);
             if (tid >= o) incl += t;
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
             mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         }
         start[tid] = incl - v;
-        if (tid == 0) maxcnt = mx;
+        if (tid == 0) {
+            mincnt = mn;
+            maxcnt = mx;
+        }
     }
     __syncthreads();
 #pragma unroll
@@ -564,45 +568,62 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     const unsigned sm_hre = (unsigned)__cvta_generic_to_shared(hre);
     const unsigned plane_bytes = 4u * (unsigned)acc_n;  // bytes between the hre, lre, him, lim planes
-    const int mycnt = cnt[lane], mystart = start[lane], nrounds = maxcnt;
+    const int mycnt = cnt[lane], mystart = start[lane], nrounds = maxcnt, nfull = mincnt;
     // ---- rounds 0 .. nrounds-1 in passes; round r holds the banks with more
-    // than r points, so the sets shrink with r.  In 3D the lowest round left
-    // (banks A_lo) takes the highest round left (A_hi) along when some plane
-    // rotation keeps both banks of every A_hi point clear of A_lo; the points
-    // of A_hi then fill the free lanes in bank order.  Every warp walks the
-    // same pairing and spreads the passes that fall to it (one call site keeps
-    // the unrolled footprint code in the instruction cache once).
+    // than r points, so the sets shrink with r.  Rounds below nfull hold every
+    // bank.  In 3D the lowest tail round left (banks A_lo) takes the highest
+    // round left (A_hi) along when some plane rotation keeps both banks of
+    // every A_hi point clear of A_lo; the points of A_hi then fill the free
+    // lanes in bank order.  Every warp walks the same pairing of the tail and
+    // spreads the passes that fall to it (one call site keeps the unrolled
+    // footprint code in the instruction cache once).
     int od1 = 0, od2 = 0;  // lane o tests the plane rotation o + 1
     if (DIM == 3 && lane < W - 1) rot_banks<W>(lane + 1, plane, od1, od2);
-    for (int i = 0, j = nrounds - 1, pass = 0; i <= j; ++pass) {
-        const unsigned alo = __ballot_sync(0xffffffffu, mycnt > i);
-        unsigned ahi = 0;
-        int rot = 0;
-        if (DIM == 3 && i < j && alo != 0xffffffffu) {
-            ahi = __ballot_sync(0xffffffffu, mycnt > j);
-            const bool ok = lane < W - 1 && __popc(alo) + __popc(ahi) <= 32 &&
-                            !(__funnelshift_l(ahi, ahi, od1) & alo) && !(__funnelshift_l(ahi, ahi, od2) & alo);
-            const unsigned m = __ballot_sync(0xffffffffu, ok);
-            if (m) rot = __ffs(m);
-            else ahi = 0;
-        }
-        if (pass % nwarps == warp) {
-            int p = -1, prot = 0;
-            if ((alo >> lane) & 1u) {
-                p = order[mystart + i];
-            } else if (ahi) {
-                const int k = __popc(~alo & ((1u << lane) - 1u));  // rank among the free lanes
-                if (k < __popc(ahi)) {
-                    p = order[start[kth_bit(ahi, k)] + j];
-                    prot = rot;
+    int wi = nfull, wj = nrounds - 1, wpass = nfull;  // tail walk: next pass and its rounds
+    for (int pass = warp;; pass += nwarps) {
+        int i = pass, j = 0, rot = 0;
+        unsigned alo = 0xffffffffu, ahi = 0;
+        if (pass >= nfull) {
+            bool found = false;
+            while (wi <= wj) {
+                const unsigned lo = __ballot_sync(0xffffffffu, mycnt > wi);
+                unsigned hi = 0;
+                int r = 0;
+                if (DIM == 3 && wi < wj) {
+                    hi = __ballot_sync(0xffffffffu, mycnt > wj);
+                    const bool ok = lane < W - 1 && __popc(lo) + __popc(hi) <= 32 &&
+                                    !(__funnelshift_l(hi, hi, od1) & lo) && !(__funnelshift_l(hi, hi, od2) & lo);
+                    const unsigned m = __ballot_sync(0xffffffffu, ok);
+                    if (m) r = __ffs(m);
+                    else hi = 0;
                 }
+                if (wpass++ == pass) {
+                    i = wi;
+                    j = wj;
+                    alo = lo;
+                    ahi = hi;
+                    rot = r;
+                    found = true;
+                }
+                ++wi;
+                if (hi) --wj;
+                if (found) break;
             }
-            if (p >= 0)
-                spread_point<DIM, W>(pts, g, c, cstride, nvol, perm[sp.y + p], mode, shifts, S, tx, plane,
-                                     tsize, sm_hre, plane_bytes, fscale, prot);
+            if (!found) break;
         }
-        ++i;
-        if (ahi) --j;
+        int p = -1, prot = 0;
+        if ((alo >> lane) & 1u) {
+            p = order[mystart + i];
+        } else if (ahi) {
+            const int k = __popc(~alo & ((1u << lane) - 1u));  // rank among the free lanes
+            if (k < __popc(ahi)) {
+                p = order[start[kth_bit(ahi, k)] + j];
+                prot = rot;
+            }
+        }
+        if (p >= 0)
+            spread_point<DIM, W>(pts, g, c, cstride, nvol, perm[sp.y + p], mode, shifts, S, tx, plane, tsize,
+                                 sm_hre, plane_bytes, fscale, prot);
     }
     __syncthreads();
     // footprints per cell: box sums of the corner histogram along each axis
@@ -677,7 +698,7 @@ __global__ void __launch_bounds__(256) interp_kernel(PolarPts pts, GridCfg g,
             lo[d] = l0 - S[d];
             if (d < 2) {
 #pragma unroll
-                for (int m = 0; m < W; ++m) wk[d][m] = es_evalf(((float)m - off) * inv_hw, g.beta);
+                for (int m = 0; m < W; ++m) wk[d][m] = es_eval2f(((float)m - off) * inv_hw, g.beta_l2e);
             } else {
                 offz = off;
             }
@@ -715,7 +736,7 @@ __global__ void __launch_bounds__(256) interp_kernel(PolarPts pts, GridCfg g,
                         zr = fmaf(rr, wk[1][dy], zr);
                         zi = fmaf(ri, wk[1][dy], zi);
                     }
-                    const float wz = es_evalf(((float)dz - offz) * inv_hw, g.beta);
+                    const float wz = es_eval2f(((float)dz - offz) * inv_hw, g.beta_l2e);
                     ar = fmaf(zr, wz, ar);
                     ai = fmaf(zi, wz, ai);
                 }
@@ -777,7 +798,7 @@ GridCfg make_cfg(int dim, const int nf[3], const int bs[3], const int nb[3], int
     }
     g.div_tx = make_fastdiv((unsigned)g.td[0]);
     g.div_ty = make_fastdiv((unsigned)g.td[1]);
-    g.beta = (float)beta;
+    g.beta_l2e = (float)(beta * 1.4426950408889634074);
     return g;
 }
 
