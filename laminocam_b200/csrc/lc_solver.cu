@@ -297,16 +297,16 @@ __device__ __forceinline__ float lap_at(const float *__restrict__ x, int idx, in
 }
 
 // Start of a Split-Bregman outer iteration (src/bregman.cpp:36-94):
-//   rhs = yT - mu div(d - b)   (div = sum over axes of the zero-padded
-//                               central difference; rhs is not stored)
+//   rhs = yT - mu div(q),  q = d - b as stored by sb_shrink_diff
+//                          (div = sum over axes of the zero-padded central
+//                          difference; rhs is not stored)
 //   ax  = tx - mu lap(x)       when tx (= A^T A x) is given, else the carried ax
 //   r = rhs - ax,  p = r (when p is given);  partials rhs.rhs, r.r
 // i.e. the warm-started CG initialisation of src/conjgrad.cpp:33-76.
 template <typename A>
 __global__ void __launch_bounds__(kThreads)
-    sb_begin_kernel(const float *__restrict__ yT, const float *__restrict__ d0, const float *__restrict__ d1,
-                    const float *__restrict__ d2, const float *__restrict__ b0, const float *__restrict__ b1,
-                    const float *__restrict__ b2, const float *__restrict__ tx, const float *__restrict__ x,
+    sb_begin_kernel(const float *__restrict__ yT, const float *__restrict__ q0, const float *__restrict__ q1,
+                    const float *__restrict__ q2, const float *__restrict__ tx, const float *__restrict__ x,
                     float *__restrict__ ax, float *__restrict__ r, float *__restrict__ p, Dims dm, Tiles tl,
                     float mu, double *part, unsigned *counter, CGState *st) {
     if (st->sb_done) {
@@ -317,10 +317,9 @@ __global__ void __launch_bounds__(kThreads)
     const int sj = dm.n3, si = dm.n2 * dm.n3;
     for_voxels(tl, dm, [&](int i, int j, int k) {
         const int idx = i * si + j * sj + k;
-        auto dv = [&](const float *d, const float *b, int o) { return d[idx + o] - b[idx + o]; };
-        const float dk = (k + 1 < dm.n3 ? dv(d0, b0, 1) : 0.f) - (k >= 1 ? dv(d0, b0, -1) : 0.f);
-        const float dj = (j + 1 < dm.n2 ? dv(d1, b1, sj) : 0.f) - (j >= 1 ? dv(d1, b1, -sj) : 0.f);
-        const float di = (i + 1 < dm.n1 ? dv(d2, b2, si) : 0.f) - (i >= 1 ? dv(d2, b2, -si) : 0.f);
+        const float dk = (k + 1 < dm.n3 ? q0[idx + 1] : 0.f) - (k >= 1 ? q0[idx - 1] : 0.f);
+        const float dj = (j + 1 < dm.n2 ? q1[idx + sj] : 0.f) - (j >= 1 ? q1[idx - sj] : 0.f);
+        const float di = (i + 1 < dm.n1 ? q2[idx + si] : 0.f) - (i >= 1 ? q2[idx - si] : 0.f);
         const float rhs = fmaf(-mu, 0.5f * dk + 0.5f * dj + 0.5f * di, yT[idx]);
         float a;
         if (tx) {
@@ -385,11 +384,13 @@ __global__ void __launch_bounds__(kThreads) lap_dot_kernel(const float *__restri
 
 // End of an outer iteration: g = grad x; t = g + b; s = |t|;
 // d = max(0, s - lam/mu) t / (s + 1e-8); b += g - d; then the relative change
-// |x - xold| / |xold| (partials) and xold = x
+// |x - xold| / |xold| (partials) and xold = x.  d is read only as d - b (the
+// next sb_begin), so q = d - b is stored in its place: the same float as the
+// difference of the stored d and b.
 template <typename A>
 __global__ void __launch_bounds__(kThreads)
-    sb_shrink_diff_kernel(const float *__restrict__ x, float *__restrict__ xold, float *__restrict__ d0,
-                          float *__restrict__ d1, float *__restrict__ d2, float *__restrict__ b0,
+    sb_shrink_diff_kernel(const float *__restrict__ x, float *__restrict__ xold, float *__restrict__ q0,
+                          float *__restrict__ q1, float *__restrict__ q2, float *__restrict__ b0,
                           float *__restrict__ b1, float *__restrict__ b2, Dims dm, Tiles tl, float thresh,
                           double *part, unsigned *counter, CGState *st, float xtol) {
     if (st->sb_done) return;
@@ -408,12 +409,13 @@ __global__ void __launch_bounds__(kThreads)
         const float m = fmaxf(0.f, s - thresh);
         const float inv = 1.0f / (s + 1e-8f);
         const float e0 = m * (t0 * inv), e1 = m * (t1 * inv), e2 = m * (t2 * inv);
-        d0[idx] = e0;
-        d1[idx] = e1;
-        d2[idx] = e2;
-        b0[idx] = c0 + (g0 - e0);
-        b1[idx] = c1 + (g1 - e1);
-        b2[idx] = c2 + (g2 - e2);
+        const float n0 = c0 + (g0 - e0), n1 = c1 + (g1 - e1), n2 = c2 + (g2 - e2);
+        q0[idx] = e0 - n0;
+        q1[idx] = e1 - n1;
+        q2[idx] = e2 - n2;
+        b0[idx] = n0;
+        b1[idx] = n1;
+        b2[idx] = n2;
         const float df = xi - xo;
         v[0] += (A)df * (A)df;
         v[1] += (A)xo * (A)xo;
@@ -611,9 +613,9 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
     host_st_ = static_cast<CGState *>(ctx.pinned_scratch(sizeof(CGState)));
     const int inner = std::max(0, p.inner_iters);
     for (int a = 0; a < 3; ++a) {
-        d_[a].ensure(n_, s);
+        q_[a].ensure(n_, s);
         b_[a].ensure(n_, s);
-        d_[a].zero(s);
+        q_[a].zero(s);
         b_[a].zero(s);
     }
     ax_.ensure(n_, s);
@@ -664,16 +666,17 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
         const cudaStream_t os = ctx.stream();
         if (exact) AtA(x, ap_.get());
         {
-            ProfScope ps(ctx, PS_SB_VEC, 4.0 * n_ * (exact ? 11.0 : 9.0) + (inner > 1 ? 4.0 * n_ : 0.0));
+            // yT, q[3] and A x (carried: read; exact: A^T A x and x read, A x written), r written
+            ProfScope ps(ctx, PS_SB_VEC, 4.0 * n_ * (exact ? 8.0 : 6.0) + (inner > 1 ? 4.0 * n_ : 0.0));
             const float *tx = exact ? ap_.get() : nullptr;
             float *pinit = inner > 1 ? p_.get() : nullptr;
             if (fp32)
                 sb_begin_kernel<float><<<g_begin.blocks, kThreads, 0, os>>>(
-                    yT, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), tx, x,
+                    yT, q_[0].get(), q_[1].get(), q_[2].get(), tx, x,
                     ax_.get(), r_.get(), pinit, dm, g_begin.tl, mu, part_.get(), counter_.get(), st_.get());
             else
                 sb_begin_kernel<double><<<g_begin.blocks, kThreads, 0, os>>>(
-                    yT, d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), tx, x,
+                    yT, q_[0].get(), q_[1].get(), q_[2].get(), tx, x,
                     ax_.get(), r_.get(), pinit, dm, g_begin.tl, mu, part_.get(), counter_.get(), st_.get());
             LC_CHECK_LAUNCH();
         }
@@ -714,11 +717,11 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
         ProfScope ps(ctx, PS_SB_VEC, 4.0 * n_ * 12.0);
         if (fp32)
             sb_shrink_diff_kernel<float><<<g_shrink.blocks, kThreads, 0, os>>>(
-                x, xold_.get(), d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
+                x, xold_.get(), q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
                 g_shrink.tl, p.lambda / p.mu, part_.get(), counter_.get(), st_.get(), p.xtol);
         else
             sb_shrink_diff_kernel<double><<<g_shrink.blocks, kThreads, 0, os>>>(
-                x, xold_.get(), d_[0].get(), d_[1].get(), d_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
+                x, xold_.get(), q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
                 g_shrink.tl, p.lambda / p.mu, part_.get(), counter_.get(), st_.get(), p.xtol);
         LC_CHECK_LAUNCH();
     };

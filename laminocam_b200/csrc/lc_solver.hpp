@@ -77,7 +77,7 @@ class Solver {
     long n_;
     int nblk_;
     DevBuf<float> r_, p_, ap_, xold_;
-    DevBuf<float> d_[3], b_[3], ax_;
+    DevBuf<float> q_[3], b_[3], ax_;  // q = d - b (Split-Bregman), b, carried A x
     DevBuf<double> part_;
     DevBuf<unsigned> counter_;
     DevBuf<CGState> st_;
