@@ -94,8 +94,8 @@ __device__ __forceinline__ int mirror_index(int j, int P) {
 //       K(-kx, -ky, kz), K(-k), K(kx, ky, -kz) from them (a per-angle pair
 //       whose a and b differ only in the sign of their kz coefficient);
 //   2D  K(-kx, ky) = K(k): kx <= 0 of each row ky <= 0 (pairs theta, pi - theta).
-template <int DIM, int S>
-__global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__restrict__ angles, int ntheta,
+template <int DIM, int S, bool ONE_GROUP>
+__global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const PsfAngle *__restrict__ angles, int ntheta,
                                                       const int *__restrict__ groups, int ngroups,
                                                       int nx, int ny, int P1, int P2, int P3, int mirror,
                                                       double *__restrict__ K) {
@@ -129,16 +129,20 @@ __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__rest
         const double kx0 = (double)(jx0 - P3 / 2);
         const double ky = (double)(jy - P2 / 2);
         const double kz = DIM == 3 ? (double)(jz - P1 / 2) : 0.0;
+        // one group (every angle of equal beta and gamma): acc is formed from ay
+        // after the angle sum, so the two arrays are never live together
         double acc[S];
+        if constexpr (!ONE_GROUP) {
 #pragma unroll
-        for (int s = 0; s < S; ++s) acc[s] = 0.0;
+            for (int s = 0; s < S; ++s) acc[s] = 0.0;
+        }
         if constexpr (DIM == 3) {
             // uX = a . k does not depend on theta (a is the first column of
             // transpose(Rx(theta) Ry(beta) Rz(gamma)), which Rx leaves alone), so
             // within a group of angles of equal (beta, gamma) the sum factors:
             // K = sum_groups D_nx(uX) * sum_{theta in group} D_ny(uY).  Four
             // (then two, then one) angles share one division.
-            for (int gi = 0; gi < ngroups; ++gi) {
+            for (int gi = 0; gi < (ONE_GROUP ? 1 : ngroups); ++gi) {
                 const int i0 = gst[gi], i1 = gst[gi + 1];
                 double ay[S];
 #pragma unroll
@@ -232,7 +236,8 @@ __global__ void __launch_bounds__(128, 1) psf_rows_kernel(const PsfAngle *__rest
                 dX.init(uX0 * inv_nx, A.stepB, A.a[0] * inv_nx);
 #pragma unroll
                 for (int s = 0; s < S; ++s) {
-                    acc[s] = fma(dirichlet_term(nX.val(s), dX.cur, uX0 + (double)s * A.a[0], nx), ay[s], acc[s]);
+                    const double tX = dirichlet_term(nX.val(s), dX.cur, uX0 + (double)s * A.a[0], nx);
+                    acc[s] = ONE_GROUP ? tX * ay[s] : fma(tX, ay[s], acc[s]);
                     nX.advance();
                     dX.advance();
                 }
@@ -676,12 +681,12 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
     LC_REQUIRE(smem <= 220 * 1024, "Toeplitz: too many angles for one PSF launch");
     unsigned blocks = (unsigned)std::max<long>(1, std::min<long>((items + 127) / 128, (long)ctx.num_sms() * 16));
     if (three_d_) {
-        auto kern = psf_rows_kernel<3, S>;
+        auto kern = ngroups == 1 ? psf_rows_kernel<3, S, true> : psf_rows_kernel<3, S, false>;
         LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), ngroups, nx, ny, P1, P2, P3,
                                         mirror ? 1 : 0, K.get());
     } else {
-        auto kern = psf_rows_kernel<2, S>;
+        auto kern = psf_rows_kernel<2, S, false>;
         LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), 0, nx, ny, P1, P2, P3,
                                         mirror ? 1 : 0, K.get());
