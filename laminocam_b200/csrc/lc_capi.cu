@@ -61,7 +61,6 @@ __global__ void norm_pad_kernel(const float *__restrict__ in, long nt, long n2, 
     unsigned b = *max_bits;
     b = (b & 0x80000000u) ? (b & 0x7fffffffu) : ~b;
     float mx = __uint_as_float(b);
-    float inv = mx > 0.f ? 1.0f / mx : 1.0f;
     bool scale = mx > 0.f;
     long total = nt * N2 * N3;
     for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
@@ -75,7 +74,6 @@ __global__ void norm_pad_kernel(const float *__restrict__ in, long nt, long n2, 
             if (scale) v = v / mx;
         }
         out[idx] = v;
-        (void)inv;
     }
 }
 

@@ -11,8 +11,6 @@ namespace lc {
 
 namespace {
 
-constexpr double kPiD = 3.14159265358979323846;
-
 // sum_{m=0}^{n-1} exp(i u (2 pi/n)(m - (n-1)/2)) = sin(pi u) / sin(pi u / n)
 __device__ __forceinline__ double dirichlet(double u, int n) {
     double v = u / (double)n;
