@@ -10,7 +10,8 @@ struct CGState {
     double y2;
     double res, dx;
     int iters, done, reason, pad;
-    // Split-Bregman
+    // Split-Bregman: |x - x_old|^2 and |x_old|^2 of the outer iteration (when
+    // the CG update forms them), the relative change
     double sb_diff2, sb_old2, sb_rel;
     int sb_iters, sb_done;
 };

@@ -138,8 +138,12 @@ __global__ void __launch_bounds__(kThreads) dot_pap_kernel(const float *__restri
 // to date this way between exact recomputations).  STORE_R: false when no
 // later kernel reads r (one CG iteration per outer iteration, where p and r
 // may then share a buffer: both are only read then, which the restrict
-// qualifiers allow).
-template <typename A, bool AX = false, bool STORE_R = true>
+// qualifiers allow).  SB_CHANGE (one CG iteration per Split-Bregman outer
+// iteration, which is then the whole change of x): the second and third sums
+// are |x_new - x_old|^2 and |x_old|^2 of the stored floats, kept in
+// st->sb_diff2 and st->sb_old2 for the outer change test, in place of the
+// CG step test.
+template <typename A, bool AX = false, bool STORE_R = true, bool SB_CHANGE = false>
 __global__ void __launch_bounds__(kThreads)
     cg_update_kernel(float *__restrict__ x, float *__restrict__ r, const float *__restrict__ p,
                      const float *__restrict__ ap, float *__restrict__ ax, long n, double *part,
@@ -153,8 +157,14 @@ __global__ void __launch_bounds__(kThreads)
         ri = fmaf(-a, api, ro);
         axn = fmaf(a, api, axo);
         v[0] += (A)ri * (A)ri;
-        v[1] += (A)step * (A)step;
-        v[2] += (A)xi * (A)xi;
+        if constexpr (SB_CHANGE) {
+            const float df = xi - xo;
+            v[1] += (A)df * (A)df;
+            v[2] += (A)xo * (A)xo;
+        } else {
+            v[1] += (A)step * (A)step;
+            v[2] += (A)xi * (A)xi;
+        }
     };
     const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
     // float4 accesses (four times the bytes in flight per load) when every
@@ -195,16 +205,22 @@ __global__ void __launch_bounds__(kThreads)
             st->beta = (double)((A)rs_new / (A)st->rs_old);
             st->rs_old = rs_new;
             double res = sqrt(rs_new) / (sqrt(st->y2) + 1e-8);
-            double dx = sqrt(s2) / (sqrt(x2) + 1e-8);
             st->res = res;
-            st->dx = dx;
             st->iters += 1;
-            if (res < (double)tol) {
-                st->done = 1;
-                st->reason = 1;
-            } else if (dx < (double)xtol) {
-                st->done = 1;
-                st->reason = 2;
+            if constexpr (SB_CHANGE) {
+                // the CG ends after this iteration; the outer test uses the change
+                st->sb_diff2 = s2;
+                st->sb_old2 = x2;
+            } else {
+                double dx = sqrt(s2) / (sqrt(x2) + 1e-8);
+                st->dx = dx;
+                if (res < (double)tol) {
+                    st->done = 1;
+                    st->reason = 1;
+                } else if (dx < (double)xtol) {
+                    st->done = 1;
+                    st->reason = 2;
+                }
             }
             *counter = 0;
         }
@@ -345,6 +361,8 @@ __global__ void __launch_bounds__(kThreads)
             st->reason = 0;
             st->res = 0;
             st->dx = 0;
+            st->sb_diff2 = 0;  // an update skipped by the |p.Ap| stop leaves x unchanged
+            st->sb_old2 = 0;
             *counter = 0;
         }
     }
@@ -387,7 +405,9 @@ __global__ void __launch_bounds__(kThreads) lap_dot_kernel(const float *__restri
 // |x - xold| / |xold| (partials) and xold = x.  d is read only as d - b (the
 // next sb_begin), so q = d - b is stored in its place: the same float as the
 // difference of the stored d and b.
-template <typename A>
+// Without XOLD the change sums come from the CG update (st->sb_diff2,
+// st->sb_old2) and xold is not touched.
+template <typename A, bool XOLD>
 __global__ void __launch_bounds__(kThreads)
     sb_shrink_diff_kernel(const float *__restrict__ x, float *__restrict__ xold, float *__restrict__ q0,
                           float *__restrict__ q1, float *__restrict__ q2, float *__restrict__ b0,
@@ -399,7 +419,7 @@ __global__ void __launch_bounds__(kThreads)
     for_voxels(tl, dm, [&](int i, int j, int k) {
         const int idx = i * si + j * sj + k;
         // every load first (the buffers are distinct), then the stores
-        const float xi = x[idx], xo = xold[idx];
+        const float xi = x[idx], xo = XOLD ? xold[idx] : 0.f;
         const float c0 = b0[idx], c1 = b1[idx], c2 = b2[idx];
         const float g0 = 0.5f * ((k + 1 < dm.n3 ? x[idx + 1] : 0.f) - (k >= 1 ? x[idx - 1] : 0.f));
         const float g1 = 0.5f * ((j + 1 < dm.n2 ? x[idx + sj] : 0.f) - (j >= 1 ? x[idx - sj] : 0.f));
@@ -416,14 +436,16 @@ __global__ void __launch_bounds__(kThreads)
         b0[idx] = n0;
         b1[idx] = n1;
         b2[idx] = n2;
-        const float df = xi - xo;
-        v[0] += (A)df * (A)df;
-        v[1] += (A)xo * (A)xo;
-        xold[idx] = xi;
+        if constexpr (XOLD) {
+            const float df = xi - xo;
+            v[0] += (A)df * (A)df;
+            v[1] += (A)xo * (A)xo;
+            xold[idx] = xi;
+        }
     });
     if (block_partials<A, 2>(v, part, counter)) {
-        double d2s = total<A>(part, 0, gridDim.x);
-        double o2 = total<A>(part, 1, gridDim.x);
+        double d2s = XOLD ? total<A>(part, 0, gridDim.x) : st->sb_diff2;
+        double o2 = XOLD ? total<A>(part, 1, gridDim.x) : st->sb_old2;
         if (threadIdx.x == 0) {
             double rel = sqrt(d2s) / (sqrt(o2) + 1e-8);
             st->sb_rel = rel;
@@ -445,7 +467,7 @@ Solver::Solver(Context &ctx, long n) : n_(n) {
     cudaStream_t s = ctx.stream();
     // the 1D vector kernels: one full wave of the CTAs that fit at once
     int per_sm = 8;
-    for (const void *k : {(const void *)cg_update_kernel<double>, (const void *)cg_update_kernel<double, true, false>,
+    for (const void *k : {(const void *)cg_update_kernel<double>, (const void *)cg_update_kernel<double, true, false, true>,
                           (const void *)cg_init_kernel<double>, (const void *)dot_pap_kernel<double>,
                           (const void *)p_update_kernel}) {
         int b = 0;
@@ -619,8 +641,13 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
         b_[a].zero(s);
     }
     ax_.ensure(n_, s);
-    xold_.ensure(n_, s);
-    LC_CUDA(cudaMemcpyAsync(xold_.get(), x, n_ * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    // with one CG iteration per outer iteration the CG update forms the change
+    // sums; more need the iterate of the previous outer iteration
+    const bool keep_xold = inner > 1;
+    if (keep_xold) {
+        xold_.ensure(n_, s);
+        LC_CUDA(cudaMemcpyAsync(xold_.get(), x, n_ * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    }
     reset_state_kernel<<<1, 1, 0, s>>>(st_.get());
     LC_CHECK_LAUNCH();
     const float mu = p.mu;
@@ -648,8 +675,10 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
     const bool f32 = p.fp32_scalars != 0;
     const TileGrid g_begin = grid_for_kernel(f32 ? (const void *)sb_begin_kernel<float> : (const void *)sb_begin_kernel<double>);
     const TileGrid g_lap = grid_for_kernel(f32 ? (const void *)lap_dot_kernel<float> : (const void *)lap_dot_kernel<double>);
-    const TileGrid g_shrink =
-        grid_for_kernel(f32 ? (const void *)sb_shrink_diff_kernel<float> : (const void *)sb_shrink_diff_kernel<double>);
+    const TileGrid g_shrink = grid_for_kernel(
+        f32 ? (keep_xold ? (const void *)sb_shrink_diff_kernel<float, true> : (const void *)sb_shrink_diff_kernel<float, false>)
+            : (keep_xold ? (const void *)sb_shrink_diff_kernel<double, true>
+                         : (const void *)sb_shrink_diff_kernel<double, false>));
     const int sblk = std::max(g_begin.blocks, std::max(g_lap.blocks, g_shrink.blocks));
     part_.ensure((long)std::max(sblk, nblk_) * kParts, s);
     // With one CG iteration per outer iteration its direction is the residual
@@ -692,7 +721,7 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
                         x, r_.get(), pp, ap_.get(), ax_.get(), n_, part_.get(), counter_.get(), st_.get(), p.tol,
                         p.xtol);
                 else
-                    cg_update_kernel<float, true, false><<<nblk_, kThreads, 0, os>>>(
+                    cg_update_kernel<float, true, false, true><<<nblk_, kThreads, 0, os>>>(
                         x, r_.get(), pp, ap_.get(), ax_.get(), n_, part_.get(), counter_.get(), st_.get(), p.tol,
                         p.xtol);
             } else {
@@ -704,7 +733,7 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
                         x, r_.get(), pp, ap_.get(), ax_.get(), n_, part_.get(), counter_.get(), st_.get(), p.tol,
                         p.xtol);
                 else
-                    cg_update_kernel<double, true, false><<<nblk_, kThreads, 0, os>>>(
+                    cg_update_kernel<double, true, false, true><<<nblk_, kThreads, 0, os>>>(
                         x, r_.get(), pp, ap_.get(), ax_.get(), n_, part_.get(), counter_.get(), st_.get(), p.tol,
                         p.xtol);
             }
@@ -714,15 +743,29 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
                 LC_CHECK_LAUNCH();
             }
         }
-        ProfScope ps(ctx, PS_SB_VEC, 4.0 * n_ * 12.0);
-        if (fp32)
-            sb_shrink_diff_kernel<float><<<g_shrink.blocks, kThreads, 0, os>>>(
-                x, xold_.get(), q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
-                g_shrink.tl, p.lambda / p.mu, part_.get(), counter_.get(), st_.get(), p.xtol);
-        else
-            sb_shrink_diff_kernel<double><<<g_shrink.blocks, kThreads, 0, os>>>(
-                x, xold_.get(), q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
-                g_shrink.tl, p.lambda / p.mu, part_.get(), counter_.get(), st_.get(), p.xtol);
+        // x and b[3] read, q[3] and b[3] written (and xold read and written)
+        ProfScope ps(ctx, PS_SB_VEC, 4.0 * n_ * (keep_xold ? 12.0 : 10.0));
+        float *xo = keep_xold ? xold_.get() : nullptr;
+        const float th = p.lambda / p.mu;
+        if (fp32) {
+            if (keep_xold)
+                sb_shrink_diff_kernel<float, true><<<g_shrink.blocks, kThreads, 0, os>>>(
+                    x, xo, q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
+                    g_shrink.tl, th, part_.get(), counter_.get(), st_.get(), p.xtol);
+            else
+                sb_shrink_diff_kernel<float, false><<<g_shrink.blocks, kThreads, 0, os>>>(
+                    x, xo, q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
+                    g_shrink.tl, th, part_.get(), counter_.get(), st_.get(), p.xtol);
+        } else {
+            if (keep_xold)
+                sb_shrink_diff_kernel<double, true><<<g_shrink.blocks, kThreads, 0, os>>>(
+                    x, xo, q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
+                    g_shrink.tl, th, part_.get(), counter_.get(), st_.get(), p.xtol);
+            else
+                sb_shrink_diff_kernel<double, false><<<g_shrink.blocks, kThreads, 0, os>>>(
+                    x, xo, q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
+                    g_shrink.tl, th, part_.get(), counter_.get(), st_.get(), p.xtol);
+        }
         LC_CHECK_LAUNCH();
     };
     // exact operator products every `every` outer iterations (and always in
