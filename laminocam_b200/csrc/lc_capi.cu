@@ -490,6 +490,8 @@ int lc_psf_create(lc_context c, lc_geometry g, int n1, int n2, int n3, lc_psf *o
         p->owner = c;
         p->geom = g;
         p->T = std::make_unique<Toeplitz>(*c->ctx, g->g, dims, three);
+        // complete on return: the caller may use it on another stream
+        LC_CUDA(cudaStreamSynchronize(c->ctx->stream()));
         *out = p.release();
     });
 }
@@ -624,7 +626,8 @@ namespace lc {
 void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nrows, int ncols,
                  const double *theta, const double *gamma, const double *beta, const float *shifts,
                  const int *recon_dims, const lc_recon_params *p, float *dout,
-                 lc_solver_stats *stats, const PsfProvider *psfp, bool *psf_hit) {
+                 lc_solver_stats *stats, const PsfProvider *psfp, bool *psf_hit,
+                 const std::function<void()> &load_input) {
     LC_REQUIRE(theta && gamma && beta && recon_dims && p, "NULL argument");
     LC_REQUIRE(ntheta > 0 && nrows > 0 && ncols > 0, "sizes must be positive");
     LC_REQUIRE(recon_dims[0] > 0 && recon_dims[1] > 0 && recon_dims[2] > 0,
@@ -648,6 +651,17 @@ void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nrows, in
         PC = ncols;
     }
     const long np = (long)ntheta * nrows * ncols;
+    lc_geometry g = nullptr;
+    int rc = lc_geometry3d_create(c, theta, gamma, beta, shifts, ntheta, (int)PR, (int)PC, &g);
+    if (rc) throw Error(rc == LC_ERR_INVALID ? 1 : 3, c->err);
+    std::unique_ptr<lc_geometry_s> gown(g);
+    // the PSF depends on the angles only: it is built while the projections
+    // may still be arriving
+    lc_psf_s psf;
+    psf.owner = c;
+    psf.geom = g;
+    psf.T = make_psf(ctx, g->g, N, true, psfp, psf_hit);
+    if (load_input) load_input();
     DevBuf<unsigned> mx(1, s);
     mx.zero(s);
     max_kernel<<<grid_for(np, 256, ctx.num_sms()), 256, 0, s>>>(dprojs_in, np, mx.get());
@@ -657,10 +671,6 @@ void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nrows, in
         dprojs_in, ntheta, nrows, ncols, dproj.get(), PR, PC, (PR - nrows) / 2, (PC - ncols) / 2,
         mx.get());
     LC_CHECK_LAUNCH();
-    lc_geometry g = nullptr;
-    int rc = lc_geometry3d_create(c, theta, gamma, beta, shifts, ntheta, (int)PR, (int)PC, &g);
-    if (rc) throw Error(rc == LC_ERR_INVALID ? 1 : 3, c->err);
-    std::unique_ptr<lc_geometry_s> gown(g);
     const long nvp = N[0] * N[1] * N[2];
     DevBuf<float> yT(nvp, s), x(nvp, s);
     do_backproj3d(g, dproj.get(), (int)N[0], (int)N[1], (int)N[2], shifts != nullptr, yT.get(),
@@ -668,10 +678,6 @@ void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nrows, in
     dproj.release();
     g->work.release();
     g->plans.clear();
-    lc_psf_s psf;
-    psf.owner = c;
-    psf.geom = g;
-    psf.T = make_psf(ctx, g->g, N, true, psfp, psf_hit);
     x.zero(s);
     run_solver(&psf, p->method, yT.get(), x.get(), &p->solver, stats);
     const long nv = (long)recon_dims[0] * recon_dims[1] * recon_dims[2];
@@ -695,15 +701,46 @@ int lc_mbir3d(lc_context c, const float *projs, int ntheta, int nrows, int ncols
         Context &ctx = *c->ctx;
         cudaStream_t s = ctx.stream();
         const long np = (long)ntheta * nrows * ncols;
-        DevBuf<float> draw;
-        draw.upload(projs, np, s);
         const long nv = (long)recon_dims[0] * recon_dims[1] * recon_dims[2];
         LC_REQUIRE(nv > 0, "recon_dims must be positive");
+        // the projections travel on the copy stream while the geometry and
+        // the PSF are built; the buffer is allocated (and later freed) in the
+        // order of the context stream
+        DevBuf<float> draw(np, s);
         DevBuf<float> out(nv, s);
-        mbir3d_core(c, draw.get(), ntheta, nrows, ncols, theta, gamma, beta, shifts, recon_dims, p,
-                    out.get(), stats, nullptr, nullptr);
-        LC_CUDA(cudaMemcpyAsync(recon, out.get(), nv * sizeof(float), cudaMemcpyDeviceToHost, s));
-        LC_CUDA(cudaStreamSynchronize(s));
+        cudaStream_t cs = ctx.copy_stream();
+        cudaEvent_t allocated = nullptr, arrived = nullptr;
+        LC_CUDA(cudaEventCreateWithFlags(&allocated, cudaEventDisableTiming));
+        const cudaError_t e2 = cudaEventCreateWithFlags(&arrived, cudaEventDisableTiming);
+        if (e2 != cudaSuccess) {
+            cudaEventDestroy(allocated);
+            LC_CUDA(e2);
+        }
+        auto done = [&] {
+            cudaEventDestroy(allocated);
+            cudaEventDestroy(arrived);
+        };
+        try {
+            // recorded before the PSF work is queued, so the copy waits only
+            // for the allocation
+            LC_CUDA(cudaEventRecord(allocated, s));
+            auto load = [&] {
+                LC_CUDA(cudaStreamWaitEvent(cs, allocated, 0));
+                LC_CUDA(cudaMemcpyAsync(draw.get(), projs, np * sizeof(float), cudaMemcpyHostToDevice, cs));
+                LC_CUDA(cudaEventRecord(arrived, cs));
+                LC_CUDA(cudaStreamWaitEvent(s, arrived, 0));
+            };
+            mbir3d_core(c, draw.get(), ntheta, nrows, ncols, theta, gamma, beta, shifts, recon_dims, p,
+                        out.get(), stats, nullptr, nullptr, load);
+            LC_CUDA(cudaMemcpyAsync(recon, out.get(), nv * sizeof(float), cudaMemcpyDeviceToHost, s));
+            LC_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            // the copy may still be running into the buffer: finish it first
+            cudaStreamSynchronize(cs);
+            done();
+            throw;
+        }
+        done();
     });
 }
 

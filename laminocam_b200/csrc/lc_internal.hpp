@@ -51,11 +51,15 @@ void mbir2d_core(lc_context c, const float *dsino, int ns, int ntheta, int nradi
                  const double *theta, const int *recon_dims, const lc_recon_params *p,
                  float *drecon, lc_solver_stats *stats, const PsfProvider *psf, bool *psf_hit);
 
-// gpu::MBIR on device projections {ntheta, nrows, ncols}; drecon = recon_dims
+// gpu::MBIR on device projections {ntheta, nrows, ncols}; drecon = recon_dims.
+// load_input (optional) runs once the geometry and the PSF, which need only
+// the angles, are queued: it starts filling dprojs and makes the context
+// stream wait for it, so the upload overlaps the PSF construction.
 void mbir3d_core(lc_context c, const float *dprojs, int ntheta, int nrows, int ncols,
                  const double *theta, const double *gamma, const double *beta, const float *shifts,
                  const int *recon_dims, const lc_recon_params *p, float *drecon,
-                 lc_solver_stats *stats, const PsfProvider *psf, bool *psf_hit);
+                 lc_solver_stats *stats, const PsfProvider *psf, bool *psf_hit,
+                 const std::function<void()> &load_input = {});
 
 // padded size of the reference: int(n * factor) in float, forced odd
 long odd_pad(long n, float factor);

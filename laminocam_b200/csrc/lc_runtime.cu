@@ -240,6 +240,14 @@ Context::Context(int device, cudaStream_t stream) : device_(device) {
     }
 }
 
+cudaStream_t Context::copy_stream() {
+    if (!copy_stream_) {
+        DeviceGuard g(device_);
+        LC_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+    }
+    return copy_stream_;
+}
+
 void *Context::pinned_scratch(size_t bytes) {
     if (bytes > pinned_bytes_) {
         // pinned allocation and release synchronise the whole device, so the
@@ -257,6 +265,10 @@ Context::~Context() {
     cudaSetDevice(device_);
     plans_.clear();
     if (pinned_) cudaFreeHost(pinned_);
+    if (copy_stream_) {
+        cudaStreamSynchronize(copy_stream_);
+        cudaStreamDestroy(copy_stream_);
+    }
     if (own_stream_) {
         cudaStreamSynchronize(own_stream_);
         cudaStreamDestroy(own_stream_);

@@ -190,6 +190,9 @@ class Context {
     // the context's private stream: graphs are captured there (the caller's
     // stream may be the legacy default stream, which cannot capture)
     cudaStream_t capture_stream() const { return own_stream_; }
+    // a second private stream for host-to-device copies that overlap work on
+    // stream() (created on first use)
+    cudaStream_t copy_stream();
     // A pinned host buffer of at least `bytes`, owned by the context and
     // reused by its solvers for device-to-host copies of small state.  The
     // pointer stays valid until a larger request or the context's end.
@@ -205,6 +208,7 @@ class Context {
     int device_;
     cudaStream_t stream_;
     cudaStream_t own_stream_ = nullptr;
+    cudaStream_t copy_stream_ = nullptr;
     PlanCache plans_;
     void *pinned_ = nullptr;
     size_t pinned_bytes_ = 0;

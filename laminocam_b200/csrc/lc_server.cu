@@ -92,6 +92,8 @@ class PsfCache {
         std::shared_ptr<Toeplitz> T;
         try {
             T = std::make_shared<Toeplitz>(ctx, g, dims, three_d);
+            // other workers read the spectrum on their own streams
+            LC_CUDA(cudaStreamSynchronize(ctx.stream()));
         } catch (...) {
             lk.lock();
             building_.erase(key);

@@ -511,7 +511,8 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
     R_ = std::make_shared<DevBuf<float>>(nR, st);
     d2f_kernel<<<grid_for(nR, 256, ctx.num_sms()), 256, 0, st>>>(Rd.get(), R_->get(), nR);
     LC_CHECK_LAUNCH();
-    LC_CUDA(cudaStreamSynchronize(st));
+    // the spectrum is complete in the order of st; callers that hand it to
+    // other streams synchronise first (buffers here are freed in stream order)
     // work buffers
     if (three_d) {
         t1_.alloc(n_[0] * n_[1] * Ph_[2], st);
@@ -693,7 +694,8 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
     // planes of mode -P/2 have no mirror inside the grid; they are not needed
     zero_unpaired_kernel<<<grid_for(total, 256, ctx.num_sms()), 256, 0, st>>>(K.get(), P1, P2, P3);
     LC_CHECK_LAUNCH();
-    LC_CUDA(cudaStreamSynchronize(st));  // the angle table is released on return
+    // the angle table is freed in the order of st; the host tables were
+    // staged by their uploads
 }
 
 void Toeplitz::kernel_fp64(Context &ctx, double *host_out) {

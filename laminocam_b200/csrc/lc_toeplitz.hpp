@@ -23,7 +23,9 @@ namespace lc {
 class Toeplitz {
   public:
     // dims = {n1, n2, n3}: volume (3D) or stack of n1 independent n2 x n3
-    // slices (2D, n2 == n3 required by the reference API).
+    // slices (2D, n2 == n3 required by the reference API).  The spectrum is
+    // built in the order of ctx.stream() and may still be in flight on
+    // return.
     Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], bool three_d);
     // shares src's spectrum (read-only) and, with `work`, owns fresh work
     // buffers on ctx's stream: concurrent jobs on one geometry use one
