@@ -15,13 +15,21 @@
 //   Y_b[k1]        = sum_a x[b + B a] w^(B a k1)            (DFT_A in thread b)
 //   X[k1 + A k2]   = sum_b (Y_b[k1] w^(b k1)) w^(A b k2)    (DFT_B in thread k1)
 // and the inverse runs the same steps backwards with conjugate roots.
+//
+// HALF (n_in, n_out <= L/2, always so for a Toeplitz line, L >= 2 n - 1 with
+// L even): the inputs x[b + B a] with a >= A/2 vanish and the outputs with
+// a >= A/2 are not kept, so the outer radix-A steps run as two DFTs of A/2
+// (the even/odd split of the column kernels): forward
+// Y[2m] = DFT_{A/2}(x)[m], Y[2m+1] = DFT_{A/2}(x h)[m] with
+// h(a) = exp(-2 pi i a / A) = w^(B a); inverse
+// x[a] = DFT+_{A/2}(Y_even)[a] + conj h(a) DFT+_{A/2}(Y_odd)[a].
 #include "lc_fft.hpp"
 #include "lc_regfft.cuh"
 
 namespace lc {
 namespace {
 
-template <int A, int B, int C>
+template <int A, int B, int C, bool HALF>
 __global__ void __launch_bounds__(C *(A > B ? A : B))
     zconv_kernel(float2 *data, long n_inner, int n_in, int n_out, const float *__restrict__ spec, int fold) {
     constexpr int L = A * B;
@@ -38,16 +46,33 @@ __global__ void __launch_bounds__(C *(A > B ? A : B))
     const bool valid = col < n_inner;
     float2 v[TPL];
     // forward, radix A in thread b = j: x[b + B a] -> Y_b[k1] w^(b k1)
+    constexpr int AH = HALF ? A / 2 : A;  // radix-A inputs (outputs) that can be nonzero (kept)
     if (j < B) {
 #pragma unroll
-        for (int a = 0; a < A; ++a) {
+        for (int a = 0; a < AH; ++a) {
             const int n = j + B * a;
             v[a] = (valid && n < n_in) ? data[(long)n * n_inner + col] : make_float2(0.f, 0.f);
         }
     }
     __syncthreads();  // twiddle table ready
     if (j < B) {
-        dft_reg<A>(v, -1);
+        if constexpr (HALF) {
+            float2 e[AH], o[AH];
+#pragma unroll
+            for (int a = 0; a < AH; ++a) {
+                e[a] = v[a];
+                o[a] = a ? cmul(v[a], tw[a * B]) : v[a];
+            }
+            dft_reg<AH>(e, -1);
+            dft_reg<AH>(o, -1);
+#pragma unroll
+            for (int m = 0; m < AH; ++m) {
+                v[2 * m] = e[m];
+                v[2 * m + 1] = o[m];
+            }
+        } else {
+            dft_reg<A>(v, -1);
+        }
 #pragma unroll
         for (int k1 = 1; k1 < A; ++k1) v[k1] = cmul(v[k1], tw[(j * k1) % L]);
 #pragma unroll
@@ -80,9 +105,25 @@ __global__ void __launch_bounds__(C *(A > B ? A : B))
     if (j < B) {
 #pragma unroll
         for (int k1 = 0; k1 < A; ++k1) v[k1] = sm[(k1 * B + j) * C + cl];
-        dft_reg<A>(v, +1);
+        if constexpr (HALF) {
+            float2 e[AH], o[AH];
 #pragma unroll
-        for (int a = 0; a < A; ++a) {
+            for (int m = 0; m < AH; ++m) {
+                e[m] = v[2 * m];
+                o[m] = v[2 * m + 1];
+            }
+            dft_reg<AH>(e, +1);
+            dft_reg<AH>(o, +1);
+#pragma unroll
+            for (int a = 0; a < AH; ++a) {
+                const float2 h = tw[a * B];
+                v[a] = a ? cadd(e[a], cmul(make_float2(h.x, -h.y), o[a])) : cadd(e[a], o[a]);
+            }
+        } else {
+            dft_reg<A>(v, +1);
+        }
+#pragma unroll
+        for (int a = 0; a < AH; ++a) {
             const int n = j + B * a;
             if (valid && n < n_out) data[(long)n * n_inner + col] = v[a];
         }
@@ -94,7 +135,12 @@ void launch_z(cudaStream_t st, float2 *data, long n_inner, int n_in, int n_out, 
     constexpr int TPL = A > B ? A : B;
     const long blocks = (n_inner + C - 1) / C;
     LC_REQUIRE(blocks < (1L << 31), "z convolution: grid too large");
-    zconv_kernel<A, B, C><<<(unsigned)blocks, C * TPL, 0, st>>>(data, n_inner, n_in, n_out, spec, fold);
+    if (A % 2 == 0 && 2 * n_in <= A * B && 2 * n_out <= A * B)
+        zconv_kernel<A, B, C, (A % 2 == 0)><<<(unsigned)blocks, C * TPL, 0, st>>>(data, n_inner, n_in, n_out,
+                                                                                  spec, fold);
+    else
+        zconv_kernel<A, B, C, false><<<(unsigned)blocks, C * TPL, 0, st>>>(data, n_inner, n_in, n_out, spec,
+                                                                          fold);
     LC_CHECK_LAUNCH();
 }
 
