@@ -623,6 +623,43 @@ int lc_mbir2d(lc_context c, const float *sino, int ns, int ntheta, int nradial,
 
 namespace lc {
 
+void with_overlapped_upload(Context &ctx, float *dst, const float *src, long n,
+                            const std::function<void(const std::function<void()> &)> &body) {
+    cudaStream_t s = ctx.stream(), cs = ctx.copy_stream();
+    cudaEvent_t allocated = nullptr, arrived = nullptr;
+    LC_CUDA(cudaEventCreateWithFlags(&allocated, cudaEventDisableTiming));
+    const cudaError_t e2 = cudaEventCreateWithFlags(&arrived, cudaEventDisableTiming);
+    if (e2 != cudaSuccess) {
+        cudaEventDestroy(allocated);
+        LC_CUDA(e2);
+    }
+    auto done = [&] {
+        cudaEventDestroy(allocated);
+        cudaEventDestroy(arrived);
+    };
+    try {
+        // recorded before the body queues its work, so the copy waits only for
+        // the allocation of dst (stream-ordered on s)
+        LC_CUDA(cudaEventRecord(allocated, s));
+        bool started = false;
+        auto load = [&] {
+            LC_REQUIRE(!started, "upload started twice");
+            started = true;
+            LC_CUDA(cudaStreamWaitEvent(cs, allocated, 0));
+            LC_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyHostToDevice, cs));
+            LC_CUDA(cudaEventRecord(arrived, cs));
+            LC_CUDA(cudaStreamWaitEvent(s, arrived, 0));
+        };
+        body(load);
+    } catch (...) {
+        // the copy may still be running into dst: let it finish first
+        cudaStreamSynchronize(cs);
+        done();
+        throw;
+    }
+    done();
+}
+
 void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nrows, int ncols,
                  const double *theta, const double *gamma, const double *beta, const float *shifts,
                  const int *recon_dims, const lc_recon_params *p, float *dout,
@@ -704,43 +741,15 @@ int lc_mbir3d(lc_context c, const float *projs, int ntheta, int nrows, int ncols
         const long nv = (long)recon_dims[0] * recon_dims[1] * recon_dims[2];
         LC_REQUIRE(nv > 0, "recon_dims must be positive");
         // the projections travel on the copy stream while the geometry and
-        // the PSF are built; the buffer is allocated (and later freed) in the
-        // order of the context stream
+        // the PSF are built
         DevBuf<float> draw(np, s);
         DevBuf<float> out(nv, s);
-        cudaStream_t cs = ctx.copy_stream();
-        cudaEvent_t allocated = nullptr, arrived = nullptr;
-        LC_CUDA(cudaEventCreateWithFlags(&allocated, cudaEventDisableTiming));
-        const cudaError_t e2 = cudaEventCreateWithFlags(&arrived, cudaEventDisableTiming);
-        if (e2 != cudaSuccess) {
-            cudaEventDestroy(allocated);
-            LC_CUDA(e2);
-        }
-        auto done = [&] {
-            cudaEventDestroy(allocated);
-            cudaEventDestroy(arrived);
-        };
-        try {
-            // recorded before the PSF work is queued, so the copy waits only
-            // for the allocation
-            LC_CUDA(cudaEventRecord(allocated, s));
-            auto load = [&] {
-                LC_CUDA(cudaStreamWaitEvent(cs, allocated, 0));
-                LC_CUDA(cudaMemcpyAsync(draw.get(), projs, np * sizeof(float), cudaMemcpyHostToDevice, cs));
-                LC_CUDA(cudaEventRecord(arrived, cs));
-                LC_CUDA(cudaStreamWaitEvent(s, arrived, 0));
-            };
+        with_overlapped_upload(ctx, draw.get(), projs, np, [&](const std::function<void()> &load) {
             mbir3d_core(c, draw.get(), ntheta, nrows, ncols, theta, gamma, beta, shifts, recon_dims, p,
                         out.get(), stats, nullptr, nullptr, load);
             LC_CUDA(cudaMemcpyAsync(recon, out.get(), nv * sizeof(float), cudaMemcpyDeviceToHost, s));
             LC_CUDA(cudaStreamSynchronize(s));
-        } catch (...) {
-            // the copy may still be running into the buffer: finish it first
-            cudaStreamSynchronize(cs);
-            done();
-            throw;
-        }
-        done();
+        });
     });
 }
 

@@ -61,6 +61,13 @@ void mbir3d_core(lc_context c, const float *dprojs, int ntheta, int nrows, int n
                  lc_solver_stats *stats, const PsfProvider *psf, bool *psf_hit,
                  const std::function<void()> &load_input = {});
 
+// body(load): load() copies n floats from host src into dst (allocated in the
+// order of ctx.stream()) on the context's copy stream and makes ctx.stream()
+// wait for them, so work the body queued before calling it overlaps the copy.
+// On an exception the copy is finished before dst can be released.
+void with_overlapped_upload(Context &ctx, float *dst, const float *src, long n,
+                            const std::function<void(const std::function<void()> &)> &body);
+
 // padded size of the reference: int(n * factor) in float, forced odd
 long odd_pad(long n, float factor);
 

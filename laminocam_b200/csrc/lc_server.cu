@@ -239,14 +239,18 @@ void lc_server_s::run_job(int w, Job &j) {
     const long nin = (long)j.d0 * j.d1 * j.d2;
     const long nv = (long)j.recon_dims[0] * j.recon_dims[1] * j.recon_dims[2];
     DevBuf<float> din, dout(nv, s);
-    din.upload(j.in, nin, s);
     if (!j.three_d) {
+        din.upload(j.in, nin, s);
         mbir2d_core(c, din.get(), j.d0, j.d1, j.d2, j.theta.data(), j.recon_dims, &j.p, dout.get(),
                     &j.stats, pp, &j.psf_hit);
     } else {
-        mbir3d_core(c, din.get(), j.d0, j.d1, j.d2, j.theta.data(), j.gamma.data(), j.beta.data(),
-                    j.shifts.empty() ? nullptr : j.shifts.data(), j.recon_dims, &j.p, dout.get(),
-                    &j.stats, pp, &j.psf_hit);
+        // the projections arrive while the geometry and (on a cache miss) the PSF are built
+        din.alloc(nin, s);
+        with_overlapped_upload(*c->ctx, din.get(), j.in, nin, [&](const std::function<void()> &load) {
+            mbir3d_core(c, din.get(), j.d0, j.d1, j.d2, j.theta.data(), j.gamma.data(), j.beta.data(),
+                        j.shifts.empty() ? nullptr : j.shifts.data(), j.recon_dims, &j.p, dout.get(),
+                        &j.stats, pp, &j.psf_hit, load);
+        });
     }
     LC_CUDA(cudaMemcpyAsync(j.out, dout.get(), nv * sizeof(float), cudaMemcpyDeviceToHost, s));
     LC_CUDA(cudaStreamSynchronize(s));
