@@ -747,23 +747,23 @@ __global__ void __launch_bounds__(256) interp_kernel(PolarPts pts, GridCfg g,
 }
 
 template <int DIM, int W>
-void launch_spread_w(dim3 grid, size_t smem, cudaStream_t st, const PolarPts &pts,
+void launch_spread_w(const Context &ctx, dim3 grid, size_t smem, cudaStream_t st, const PolarPts &pts,
                      const GridCfg &g, const float2 *c, long cstride, int nvol, const int *perm,
                      const int4 *subs, float2 *out, long gstride, int mode, const float2 *shifts,
                      int maxpts) {
     auto kern = spread_kernel<DIM, W>;
-    LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_max_dynamic_smem(ctx, kern);
     kern<<<grid, kSpreadThreads, smem, st>>>(pts, g, c, cstride, nvol, perm, subs, out, gstride,
                                              mode, shifts, maxpts);
     LC_CHECK_LAUNCH();
 }
 
 template <int DIM, int W>
-void launch_interp_w(dim3 grid, int threads, size_t smem, cudaStream_t st, const PolarPts &pts,
-                     const GridCfg &g, const float2 *gr, long gstride, int nvol, const int *perm,
-                     const int4 *subs, float2 *c, long cstride, int mode) {
+void launch_interp_w(const Context &ctx, dim3 grid, int threads, size_t smem, cudaStream_t st,
+                     const PolarPts &pts, const GridCfg &g, const float2 *gr, long gstride, int nvol,
+                     const int *perm, const int4 *subs, float2 *c, long cstride, int mode) {
     auto kern = interp_kernel<DIM, W>;
-    LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_max_dynamic_smem(ctx, kern);
     kern<<<grid, threads, smem, st>>>(pts, g, gr, gstride, nvol, perm, subs, c, cstride, mode);
     LC_CHECK_LAUNCH();
 }
@@ -903,11 +903,11 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
         float2 *gv = grid + (long)v0 * gvol;
         dim3 gd(nsub_);
         if (dim_ == 2) {
-            LC_W_SWITCH(w_, (launch_spread_w<2, WW>(gd, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
+            LC_W_SWITCH(w_, (launch_spread_w<2, WW>(ctx, gd, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
                                                    perm_.get(), subs_.get(), gv, gvol, mode, shifts_,
                                                    maxsub_)));
         } else {
-            LC_W_SWITCH(w_, (launch_spread_w<3, WW>(gd, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
+            LC_W_SWITCH(w_, (launch_spread_w<3, WW>(ctx, gd, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
                                                    perm_.get(), subs_.get(), gv, gvol, mode, shifts_,
                                                    maxsub_)));
         }
@@ -927,10 +927,10 @@ void NufftPlan::interp(Context &ctx, const float2 *grid, int nvol, float2 *c, Pt
         float2 *cv = c + (long)v0 * pts_.M;
         dim3 gd(nsub_);
         if (dim_ == 2) {
-            LC_W_SWITCH(w_, (launch_interp_w<2, WW>(gd, 256, smem, ctx.stream(), pts_, g, gv, gvol, nv,
+            LC_W_SWITCH(w_, (launch_interp_w<2, WW>(ctx, gd, 256, smem, ctx.stream(), pts_, g, gv, gvol, nv,
                                                    perm_.get(), subs_.get(), cv, pts_.M, mode)));
         } else {
-            LC_W_SWITCH(w_, (launch_interp_w<3, WW>(gd, 256, smem, ctx.stream(), pts_, g, gv, gvol, nv,
+            LC_W_SWITCH(w_, (launch_interp_w<3, WW>(ctx, gd, 256, smem, ctx.stream(), pts_, g, gv, gvol, nv,
                                                    perm_.get(), subs_.get(), cv, pts_.M, mode)));
         }
     }

@@ -237,6 +237,19 @@ class CapturedGraph {
     long kernels_ = 0;
 };
 
+// Raises a kernel's dynamic shared-memory limit to all the device allows
+// beside the kernel's static shared memory.  The limit is a property of the
+// function shared by every thread of the process: setting it to each launch's
+// own size would let a concurrent launch (a server worker) lower it between
+// another thread's set and launch.  This value is the same from every thread.
+template <typename K>
+void allow_max_dynamic_smem(const Context &ctx, K kern) {
+    cudaFuncAttributes fa;
+    LC_CUDA(cudaFuncGetAttributes(&fa, kern));
+    LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(ctx.max_smem() - fa.sharedSizeBytes)));
+}
+
 // Makes `dev` current for the lifetime of the guard.
 class DeviceGuard {
   public:

@@ -681,12 +681,12 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
     unsigned blocks = (unsigned)std::max<long>(1, std::min<long>((items + 127) / 128, (long)ctx.num_sms() * 16));
     if (three_d_) {
         auto kern = ngroups == 1 ? psf_rows_kernel<3, S, true> : psf_rows_kernel<3, S, false>;
-        LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        allow_max_dynamic_smem(ctx, kern);
         kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), ngroups, nx, ny, P1, P2, P3,
                                         mirror ? 1 : 0, K.get());
     } else {
         auto kern = psf_rows_kernel<2, S, false>;
-        LC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        allow_max_dynamic_smem(ctx, kern);
         kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), 0, nx, ny, P1, P2, P3,
                                         mirror ? 1 : 0, K.get());
     }

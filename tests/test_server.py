@@ -160,6 +160,27 @@ def test_server_psf_cache_clear(lc):
     assert O.rel_l2(c.recon, a.recon) < RECON_TOL
 
 
+def test_server_many_workers_uneven_jobs(lc):
+    """48 workers on 48 slices of different sizes and angle counts.  The PSF
+    and spreading kernels take job-dependent shared memory and launch from
+    many threads at once; every job must succeed and equal its one-job run."""
+    rng = np.random.default_rng(77)
+    jobs = []
+    for k in range(48):
+        n = int(rng.choice([63, 95, 127]))
+        nth = int(rng.integers(90, 721))
+        s, th = sino2d(lc, n, nth, 500 + k)
+        jobs.append((s, th, n))
+    with lc.Server(workers=48) as sv:
+        ids = [sv.submit2d(s, th, params2d(lc, n, "split_bregman", 3)) for s, th, n in jobs]
+        res = [sv.wait(j, WAIT_S) for j in ids]
+        st = sv.stats()
+    assert st["completed"] == len(jobs) and st["failed"] == 0
+    for (s, th, n), r in list(zip(jobs, res))[:6]:
+        ref = lc.MBIR2D(s, th, params2d(lc, n, "split_bregman", 3))
+        assert O.rel_l2(r.recon, ref) < RECON_TOL
+
+
 def test_server_isolates_failing_job(lc):
     s, th = sino2d(lc, 63, 60, 31)
     good = params2d(lc, 63, "unconstrained", 4)
