@@ -211,11 +211,11 @@ def mix_jobs(lc, count=MIX_JOBS, seed=3000):
     return jobs
 
 
-def serving_mix(lc, workers=16):
+def serving_mix(lc, workers=32):
     """The same 64 uneven 2D CG jobs (50 iterations each) solved (a) one at a time
     the plain way -- float scalars, a host check of the solver state after every
     iteration, no graphs, a PSF built per job -- and (b) submitted together to
-    the server: concurrent jobs on 16 streams, CUDA-graph iterations, FP64
+    the server: concurrent jobs on 32 streams, CUDA-graph iterations, FP64
     scalars, geometry-keyed PSF cache.  Wall-clock times, host buffers in and
     out.  The error of both forms against the FP64 oracle is measured on one
     small job (n = 63, 60 angles) of the same kind."""
@@ -373,7 +373,7 @@ def stream_params(lc, key, method, plain, iters=STREAM_ITERS):
                           residual_refresh=1 if plain else 16, **common)
 
 
-def serving_stream(lc, workers=16, count=STREAM_REQUESTS, rates=STREAM_RATES):
+def serving_stream(lc, workers=32, count=STREAM_REQUESTS, rates=STREAM_RATES):
     """The served request stream against plain sequential GPU solves, both
     open-loop at the same Poisson arrival times.  Plain: one request at a time
     through MBIR2D / MBIR in arrival order (a request waits for the previous
