@@ -441,45 +441,15 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
     DevBuf<double2> a, b;
     DevBuf<double> Rd(spectrum_elems(), st);
     const int P1 = P_[0], P2 = P_[1], P3 = P_[2], P3h = Ph_[2];
-    // A kernel even in kz (the mirror mode of build_kernel) has a real z
-    // transform, even in f1, on every (ky, kx) column, and each transformed
-    // plane stays point-symmetric.  The z pass then goes first, on the real
-    // kernel, and keeps the planes f1 <= P1/2; the x and y passes run on those
-    // planes only, and y writes the real part.
-    const bool zfirst = three_d && kernel_mirror_;
-    const int Pz = zfirst ? P1 / 2 + 1 : P1;  // planes through the x and y passes
-    DevBuf<double> Kz;
-    const double *xin = K.get();
-    if (zfirst) {
-        Kz.alloc((long)Pz * P2 * P3, st);
-        AxisFFT z;
-        z.in = K.get();
-        z.in_t = E_F64;
-        z.out = Kz.get();
-        z.out_t = E_F64;
-        z.fp64 = true;
-        z.n_outer = 1;
-        z.n_inner = (long)P2 * P3;
-        z.in_ostride = 0;
-        z.out_ostride = 0;
-        z.n_in = P1;
-        z.in_map = IN_MODES;
-        z.L = P1;
-        z.n_out = Pz;
-        z.sign = -1;
-        launch_axis_fft(ctx, z);
-        K.release();
-        xin = Kz.get();
-    }
-    a.alloc((long)Pz * P2 * P3h, st);
+    a.alloc((long)P1 * P2 * P3h, st);
     {
         AxisFFT x;
-        x.in = xin;
+        x.in = K.get();
         x.in_t = E_F64;
         x.out = a.get();
         x.out_t = E_C128;
         x.fp64 = true;
-        x.n_outer = (long)Pz * P2;
+        x.n_outer = (long)P1 * P2;
         x.n_inner = 1;
         x.in_ostride = P3;
         x.out_ostride = P3h;
@@ -491,13 +461,12 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         launch_axis_fft(ctx, x);
     }
     K.release();
-    Kz.release();
     {
         AxisFFT y;
         y.in = a.get();
         y.in_t = E_C128;
         y.fp64 = true;
-        y.n_outer = Pz;
+        y.n_outer = P1;
         y.n_inner = P3h;
         y.in_ostride = (long)P2 * P3h;
         y.out_ostride = (long)P2 * P3h;
@@ -506,7 +475,7 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         y.L = P2;
         y.n_out = P2;
         y.sign = -1;
-        if (three_d && !zfirst) {
+        if (three_d) {
             b.alloc((long)P1 * P2 * P3h, st);
             y.out = b.get();
             y.out_t = E_C128;
@@ -517,7 +486,7 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         launch_axis_fft(ctx, y);
     }
     a.release();
-    if (three_d && !zfirst) {
+    if (three_d) {
         AxisFFT z;
         z.in = b.get();
         z.in_t = E_C128;
