@@ -200,19 +200,24 @@ long lc_kernel_launches(void);
  * forbids cudaMalloc/cudaFree after start-up because they can synchronise the
  * device): y = A^T A x for nslices slices of n x n, like lc_sysmat_toeplitz on
  * a 2D PSF, without any allocation.  The intermediate spectrum lives in a
- * 16 MiB array compiled into the library (held by every GPU that loads it
- * until the process exits).
+ * 16 MiB array and the transform's twiddles in a 32 KiB array, both compiled
+ * into the library (held by every GPU that loads it until the process exits).
  *   stream:   cudaStream_t the work is issued on (NULL = legacy default stream)
  *   spectrum: device, the PSF's real half spectrum {P, P/2+1}, as returned by
  *             lc_psf_spectrum for a 2D PSF of image size n
  *   P:        the PSF grid, next 2^p 3^q >= 2n-1 (lc_psf_info)
  *   x, y:     device {nslices, n, n}
  * Limits: P <= 4096 and nslices * n * (P/2+1) <= 2^21; larger sizes return
- * LC_ERR_TOO_LARGE.  The first call on a device looks up the array's device
- * address; make that first call before any stream capture.  All calls share
- * the array and its contents are left over from the previous call: calls that
- * overlap on the GPU (other streams, other threads) race and must be
- * serialised by the caller. */
+ * LC_ERR_TOO_LARGE.  CUDA loads the library's device code on its first use on
+ * a device, and that load places the two arrays in device memory: make one
+ * call on each device before reserving its memory and before any stream
+ * capture.  The set-up call lc_sysmat2d_toeplitz_noalloc(NULL, NULL, 0, NULL,
+ * NULL, 0, 0) does only that (the current device) and returns LC_OK.  Every
+ * call looks up the arrays' device addresses again, so a cudaDeviceReset in
+ * between is harmless.  All calls share both arrays, which keep the previous
+ * call's contents, and each call rewrites the twiddles for its own P: calls
+ * that overlap on the GPU (other streams, other threads) race, even on
+ * disjoint outputs, and must be serialised by the caller. */
 int lc_sysmat2d_toeplitz_noalloc(void *stream, const float *spectrum, int P, const float *x,
                                  float *y, int nslices, int n);
 

@@ -12,11 +12,17 @@
 // The scratch array (16 MiB) and the twiddle table (32 KiB) below are
 // file-scope __device__ arrays: every GPU that loads the library holds them
 // until the process exits.  In host code their names are host-side stand-ins,
-// not device addresses, so the set-up below looks up their device addresses
-// with cudaGetSymbolAddress once per device (with that device current) and
-// passes those to the kernels.
-#include <mutex>
-
+// not device addresses, so every call looks up their device addresses with
+// cudaGetSymbolAddress for the current device and passes those to the
+// kernels.  Looking them up per call (a table lookup once the module is
+// loaded) keeps the addresses right after a cudaDeviceReset, which unloads
+// the module; a per-device cache would keep stale ones.
+//
+// CUDA loads a library's device code lazily, on its first use on a device,
+// and that load is what places the two arrays in device memory.  A caller
+// that reserves the whole device must therefore make one call first: the
+// set-up call (all pointers NULL, all sizes 0) only loads the module and
+// resolves the addresses, and later calls allocate nothing.
 #include "../../include/laminocam.h"
 #include "lc_fft.hpp"
 
@@ -25,23 +31,9 @@ namespace {
 
 constexpr long kScratchElems = 2L * 1024 * 1024;  // float2 elements: 16 MiB
 constexpr int kMaxP = 4096;                        // longest transform (twiddle table size)
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) float2 g_noalloc_scratch[kScratchElems];
 static __device__ __align__(256) float2 g_noalloc_twiddles[kMaxP];
-
-struct DeviceSlots {
-    std::mutex mu;
-    bool ready[kMaxDevices] = {};
-    float2 *scratch[kMaxDevices] = {};
-    float2 *twiddles[kMaxDevices] = {};
-    size_t max_smem[kMaxDevices] = {};
-};
-
-DeviceSlots &slots() {
-    static DeviceSlots s;
-    return s;
-}
 
 // tw[m] = exp(-2 pi i m / L), evaluated with sincospi in double precision
 __global__ void noalloc_twiddle_kernel(float2 *tw, int L) {
@@ -54,27 +46,19 @@ __global__ void noalloc_twiddle_kernel(float2 *tw, int L) {
 
 bool plan_radices(int L, FFTPlan &pl) { return fft_factorise(L, pl); }
 
-// Device addresses of the static arrays for the current device, looked up
-// once per device.
-bool setup_current_device(int &dev, float2 *&scratch, float2 *&tw, size_t &max_smem) {
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
-    DeviceSlots &s = slots();
-    std::lock_guard<std::mutex> lk(s.mu);
-    if (!s.ready[dev]) {
-        void *p = nullptr, *q = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return false;
-        if (cudaGetSymbolAddress(&q, g_noalloc_twiddles) != cudaSuccess) return false;
-        int smem = 0;
-        if (cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
-            return false;
-        s.scratch[dev] = static_cast<float2 *>(p);
-        s.twiddles[dev] = static_cast<float2 *>(q);
-        s.max_smem[dev] = (size_t)smem;
-        s.ready[dev] = true;
-    }
-    scratch = s.scratch[dev];
-    tw = s.twiddles[dev];
-    max_smem = s.max_smem[dev];
+// Device addresses of the static arrays on the current device and its
+// shared-memory limit, looked up on every call.
+bool resolve_current_device(float2 *&scratch, float2 *&tw, size_t &max_smem) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    void *p = nullptr, *q = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return false;
+    if (cudaGetSymbolAddress(&q, g_noalloc_twiddles) != cudaSuccess) return false;
+    int smem = 0;
+    if (cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+    scratch = static_cast<float2 *>(p);
+    tw = static_cast<float2 *>(q);
+    max_smem = (size_t)smem;
     return true;
 }
 
@@ -85,16 +69,17 @@ using namespace lc;
 
 extern "C" int lc_sysmat2d_toeplitz_noalloc(void *stream, const float *spectrum, int P, const float *x,
                                             float *y, int nslices, int n) {
+    float2 *scratch = nullptr, *tw = nullptr;
+    size_t max_smem = 0;
+    if (!spectrum && !x && !y && nslices == 0 && n == 0 && P == 0)  // set-up call
+        return resolve_current_device(scratch, tw, max_smem) ? LC_OK : LC_ERR_CUDA;
     if (!spectrum || !x || !y || nslices <= 0 || n <= 0 || P <= 0) return LC_ERR_INVALID;
     if (P != (int)next_smooth23(2L * n - 1)) return LC_ERR_INVALID;
     const long P3h = P / 2 + 1;
     if (P > kMaxP || (long)nslices * n * P3h > kScratchElems) return LC_ERR_TOO_LARGE;
     FFTPlan pl{};
     if (!plan_radices(P, pl)) return LC_ERR_INVALID;
-    int dev = 0;
-    float2 *scratch = nullptr, *tw = nullptr;
-    size_t max_smem = 0;
-    if (!setup_current_device(dev, scratch, tw, max_smem)) return LC_ERR_CUDA;
+    if (!resolve_current_device(scratch, tw, max_smem)) return LC_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
     try {
         noalloc_twiddle_kernel<<<(P + 255) / 256, 256, 0, s>>>(tw, P);

@@ -288,26 +288,65 @@ __global__ void bin_scatter_kernel(PolarPts pts, GridCfg g, int W, int *cursor, 
 //
 // The tile accumulates in exact fixed point with 32-bit integer atomics,
 // which run about four times faster than float atomics in shared memory.
-// Each real contribution v (a float) is scaled by a power of two F chosen per
-// subproblem and split as  v F = h + l / 2^20  with integers h and l: h is v F
-// rounded to an integer and l the remainder times 2^20, rounded.  Both come
-// from adding 1.5 * 2^23, which places the integer in the low mantissa bits
-// (|v F| < 2^22), so no conversion instruction is needed.  With m the largest
-// |Re c| + |Im c| of the subproblem's n points (weights are at most 1),
-// F = 2^k <= 2^21 / m bounds |v F| and F <= 2^30 / (n m) keeps the sums of h
-// below 2^31; |l| <= 2^19 and n <= 2^11 keep the sums of l below 2^31.  The
-// flush forms (H 2^20 + L) / (F 2^20) in FP64.  The sums are exact, so the
-// tile's content does not depend on the order of the atomics; the resolution
-// 1 / (F 2^20) is below 2^-40 m.
-//
-// The accumulators take the raw bit patterns of the rounded floats, whose
-// integer values sit above the bits of 1.5 * 2^23 (B): a cell reached by K
-// points holds sum h + K B (mod 2^32).  K is the number of footprints that
-// cover the cell, a 7-wide box sum per axis of the histogram of footprint
-// corners (one atomic per point), so the flush subtracts K B exactly.
+// Each real contribution v (a float) is scaled by one power of two F for the
+// whole launch and split as  v F = h + l / 2^20  with integers h and l: h is
+// v F rounded to an integer and l the remainder times 2^20, rounded.  Both
+// come from adding 1.5 * 2^23, which places the integer in the low mantissa
+// bits (|v F| < 2^22), so no conversion instruction is needed.  F comes from
+// m, the largest |Re c| + |Im c| of all values of the launch (weights are at
+// most 1, and a unit phase keeps each part below |c|), see fix_exponent.  The
+// flush adds the exact tile sum  T = H 2^20 + L  of each cell to a 64-bit
+// integer per real and imaginary part of the fine grid, and a conversion pass
+// forms T / (F 2^20).  Every sum is an exact integer at one scale, so the fine
+// grid depends neither on the order of the atomics nor on how the points of
+// a bin are cut into subproblems: a backprojection is bit-for-bit repeatable.
+// The resolution 1 / (F 2^20) is below 2^-38 m.
 constexpr int kSpreadThreads = 256;
 constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
 constexpr unsigned kRoundMagicBits = 0x4B400000u;
+
+// Exponent e of the launch's fixed-point scale F = 2^e, from m (the largest
+// |Re c| + |Im c|), nmax (most points of one subproblem) and kmax (an upper
+// bound on the footprints that cover one fine-grid cell):
+//   F m <= 2^21            so |v F| < 2^22 for the rounding by 1.5 2^23;
+//   F nmax m < 2^30        so a tile's sums of h stay below 2^31 (the sums of
+//                          l stay below 2^19 nmax <= 2^30 for nmax <= 2^11);
+//   F kmax m 2^20 < 2^61   so a cell's 64-bit sum (plus the rounding terms,
+//                          below kmax 2^20) stays below 2^62.
+__host__ __device__ __forceinline__ int fix_exponent(float m, int nmax, long kmax) {
+    if (!(m > 0.f)) return 0;
+    int e1, e2, e3;
+    frexp((double)m, &e1);                 // m < 2^e1
+    frexp((double)nmax * (double)m, &e2);  // nmax m < 2^e2
+    frexp((double)kmax * (double)m, &e3);  // kmax m < 2^e3
+    const int a = 21 - e1, b = 30 - e2, c = 41 - e3;
+    return a < b ? (a < c ? a : c) : (b < c ? b : c);
+}
+
+// m = max |Re c| + |Im c| over n values, as the bits of a non-negative float
+// (integer order equals float order); *bits must start at 0
+__global__ void value_bound_kernel(const float2 *__restrict__ c, long n, int *bits) {
+    float m = 0.f;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const float2 v = c[i];
+        m = fmaxf(m, fabsf(v.x) + fabsf(v.y));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(bits, __float_as_int(m));
+}
+
+// fine grid <- T / (F 2^20) from the two 64-bit fixed-point sums per cell
+__global__ void fix_to_float_kernel(const long long *__restrict__ fix, float2 *__restrict__ grid, long n,
+                                    const int *__restrict__ mbits, int nmax, long kmax) {
+    const int e = fix_exponent(__int_as_float(*mbits), nmax, kmax);
+    const double unscale = ldexp(1.0, -(e + 20));
+    const longlong2 *f2 = reinterpret_cast<const longlong2 *>(fix);
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const longlong2 t = f2[i];
+        grid[i] = make_float2((float)((double)t.x * unscale), (float)((double)t.y * unscale));
+    }
+}
 
 // shared-memory atomic add without return at a 32-bit shared address plus a
 // compile-time byte offset, so one address register serves a footprint row
@@ -459,10 +498,11 @@ template <int DIM, int W>
 __global__ void __launch_bounds__(kSpreadThreads, 2)
     spread_kernel(PolarPts pts, GridCfg g, const float2 *__restrict__ c, long cstride, int nvol,
                   const int *__restrict__ perm, const int4 *__restrict__ subs,
-                  float2 *__restrict__ grid, long gstride, int mode,
-                  const float2 *__restrict__ shifts, int maxpts) {
+                  unsigned long long *__restrict__ fix, long gstride, int mode,
+                  const float2 *__restrict__ shifts, int maxpts, const int *__restrict__ mbits,
+                  long kmax) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int cnt[32], start[32], mincnt, maxcnt, cmax_bits;
+    __shared__ int cnt[32], start[32], mincnt, maxcnt;
     const int4 sp = subs[blockIdx.x];
     int bcoord[3] = {0, 0, 0};
     {
@@ -491,11 +531,9 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
     const int tid = threadIdx.x;
     for (long idx = tid; idx < 4 * acc_n + tsize; idx += blockDim.x) hre[idx] = 0;
     if (tid < 32) cnt[tid] = 0;
-    if (tid == 0) cmax_bits = 0;
     __syncthreads();
 
-    // ---- bucket the points by the bank of their footprint corner; bound |c| ----
-    float cmax = 0.f;
+    // ---- bucket the points by the bank of their footprint corner ----
 #pragma unroll
     for (int q = 0; q < kKeys; ++q) {
         const int p = tid + q * (int)blockDim.x;
@@ -518,17 +556,9 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
             const int b = corner & 31;
             k = (b << 16) | atomicAdd(&cnt[b], 1);
             atomicAdd(&kcnt[corner], 1);
-            // |Re(c m)|, |Im(c m)| <= |Re c| + |Im c| for the unit phase m of the shift mode
-            for (int s = 0; s < nvol; ++s) {
-                const float2 v = c[(long)s * cstride + j];
-                cmax = fmaxf(cmax, fabsf(v.x) + fabsf(v.y));
-            }
         }
         key[q] = k;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cmax = fmaxf(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
-    if ((tid & 31) == 0 && cmax > 0.f) atomicMax(&cmax_bits, __float_as_int(cmax));  // >= 0: int order
     __syncthreads();
     if (tid < 32) {
         const int v = cnt[tid];
@@ -552,17 +582,8 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
         const int k = key[q];
         if (k >= 0) order[start[k >> 16] + (k & 0xffff)] = (unsigned short)(tid + q * (int)blockDim.x);
     }
-    // fixed-point scale F = 2^k: F m <= 2^21 and F n m < 2^30
-    float fscale = 1.f;
-    {
-        const float m = __int_as_float(cmax_bits);
-        if (m > 0.f) {
-            int e1, e2;
-            frexpf(m, &e1);                         // m in [2^(e1-1), 2^e1)
-            frexpf((float)max(sp.z, 1) * m, &e2);   // n m in [2^(e2-1), 2^e2)
-            fscale = ldexpf(1.f, min(21 - e1, 30 - e2));
-        }
-    }
+    // the launch's fixed-point scale F = 2^e (fix_exponent)
+    const float fscale = ldexpf(1.f, fix_exponent(__int_as_float(*mbits), maxpts, kmax));
     __syncthreads();
 
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
@@ -632,8 +653,8 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
         box_sum_axis(kcnt, d, W, tx, ty, tz);
         __syncthreads();
     }
-    // flush the tile (halos overlap neighbouring bins, so accumulate atomically)
-    const double unscale = 1.0 / ((double)fscale * 1048576.0);
+    // flush the tile's exact sums (halos overlap neighbouring bins, so add
+    // atomically; integer sums make the order irrelevant)
     for (int s = 0; s < nvol; ++s) {
         for (int rr = tid; rr < tsize; rr += blockDim.x) {
             const int k = kcnt[rr];
@@ -642,9 +663,10 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
             const int idx = s * tsize + rr;
             const int h1 = (int)((unsigned)hre[idx] - kb), l1 = (int)((unsigned)lre[idx] - kb);
             const int h2 = (int)((unsigned)him[idx] - kb), l2 = (int)((unsigned)lim[idx] - kb);
-            const float a = (float)(((double)h1 * 1048576.0 + (double)l1) * unscale);
-            const float b = (float)(((double)h2 * 1048576.0 + (double)l2) * unscale);
-            atomicAdd(grid + (long)s * gstride + tile_cell_to_grid<DIM>(rr, g, S), make_float2(a, b));
+            const long long a = (long long)h1 * 1048576 + l1, b = (long long)h2 * 1048576 + l2;
+            unsigned long long *cell = fix + 2 * ((long)s * gstride + tile_cell_to_grid<DIM>(rr, g, S));
+            atomicAdd(cell, (unsigned long long)a);
+            atomicAdd(cell + 1, (unsigned long long)b);
         }
     }
 }
@@ -749,12 +771,12 @@ __global__ void __launch_bounds__(256) interp_kernel(PolarPts pts, GridCfg g,
 template <int DIM, int W>
 void launch_spread_w(const Context &ctx, dim3 grid, size_t smem, cudaStream_t st, const PolarPts &pts,
                      const GridCfg &g, const float2 *c, long cstride, int nvol, const int *perm,
-                     const int4 *subs, float2 *out, long gstride, int mode, const float2 *shifts,
-                     int maxpts) {
+                     const int4 *subs, unsigned long long *out, long gstride, int mode,
+                     const float2 *shifts, int maxpts, const int *mbits, long kmax) {
     auto kern = spread_kernel<DIM, W>;
     allow_max_dynamic_smem(ctx, kern);
     kern<<<grid, kSpreadThreads, smem, st>>>(pts, g, c, cstride, nvol, perm, subs, out, gstride,
-                                             mode, shifts, maxpts);
+                                             mode, shifts, maxpts, mbits, kmax);
     LC_CHECK_LAUNCH();
 }
 
@@ -869,6 +891,26 @@ void NufftPlan::sort_points(Context &ctx) {
         acc += hc[b];
     }
     LC_REQUIRE(acc == pts_.M, "NUFFT: bin sort lost points");
+    // footprints over one cell: a footprint reaches at most w/2 + 1 <= bs
+    // cells beyond its point's cell, so only points of the bin and of its
+    // neighbours (wrapped, each counted once) can cover a cell of the bin;
+    // the neighbourhood sums are separable box sums of the bin counts
+    {
+        std::vector<long> a(hc.begin(), hc.end()), t(nbins);
+        const long stride[3] = {1, nb_[0], (long)nb_[0] * nb_[1]};
+        for (int k = 0; k < 3; ++k) {
+            const int n = nb_[k];
+            const int lo = n >= 3 ? -1 : 0, hi = n >= 2 ? 1 : 0;  // distinct wrapped offsets
+            for (long b = 0; b < nbins; ++b) {
+                const int c = (int)((b / stride[k]) % n);
+                long sum = 0;
+                for (int d = lo; d <= hi; ++d) sum += a[b + (long)(((c + d + n) % n) - c) * stride[k]];
+                t[b] = sum;
+            }
+            a.swap(t);
+        }
+        kmax_ = std::max<long>(1, *std::max_element(a.begin(), a.end()));
+    }
     nsub_ = (int)subs.size();
     LC_REQUIRE(nsub_ > 0, "NUFFT: no points");
     subs_.upload(subs.data(), subs.size(), st);
@@ -884,6 +926,7 @@ void NufftPlan::sort_points(Context &ctx) {
 void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, PtMode mode) {
     GridCfg g = make_cfg(dim_, nf_, bs_, nb_, w_, beta_);
     const long gvol = (long)nf_[0] * nf_[1] * nf_[2];
+    cudaStream_t st = ctx.stream();
     // values read once, fine grid written once (plus the permutation)
     ProfScope ps(ctx, PS_SPREAD, (double)nvol * (8.0 * pts_.M + 8.0 * gvol) + 4.0 * pts_.M);
     // four 32-bit fixed-point accumulators per cell (high and low words of the
@@ -894,23 +937,42 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
                                 (size_t)maxsub_ * sizeof(unsigned short);
     LC_REQUIRE(maxsub_ <= 8 * kSpreadThreads, "NUFFT spread: subproblem larger than the bucketing pass");
     LC_REQUIRE(maxsub_ <= 2048, "NUFFT spread: subproblem too large for the fixed-point sums");
+    // one fixed-point scale for all values of the launch: bound them first
+    mbits_.ensure(1, st);
+    fix_.ensure(2 * gvol * nvol, st);
+    LC_CUDA(cudaMemsetAsync(mbits_.get(), 0, sizeof(int), st));
+    LC_CUDA(cudaMemsetAsync(fix_.get(), 0, 2 * gvol * nvol * sizeof(long long), st));
+    {
+        const long n = (long)nvol * pts_.M;
+        const long blocks = std::max<long>(1, std::min<long>((n + 255) / 256, (long)ctx.num_sms() * 8));
+        value_bound_kernel<<<(unsigned)blocks, 256, 0, st>>>(c, n, mbits_.get());
+        LC_CHECK_LAUNCH();
+    }
+    unsigned long long *fix = reinterpret_cast<unsigned long long *>(fix_.get());
     const int vchunk = (int)std::max<size_t>(1, (96 * 1024) / tile_bytes);
     for (int v0 = 0; v0 < nvol; v0 += vchunk) {
         const int nv = std::min(vchunk, nvol - v0);
         const size_t smem = tile_bytes * nv + bucket_bytes;
         LC_REQUIRE(smem <= ctx.max_smem(), "NUFFT spread: tile does not fit shared memory");
         const float2 *cv = c + (long)v0 * pts_.M;
-        float2 *gv = grid + (long)v0 * gvol;
+        unsigned long long *fv = fix + 2 * (long)v0 * gvol;
         dim3 gd(nsub_);
         if (dim_ == 2) {
-            LC_W_SWITCH(w_, (launch_spread_w<2, WW>(ctx, gd, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
-                                                   perm_.get(), subs_.get(), gv, gvol, mode, shifts_,
-                                                   maxsub_)));
+            LC_W_SWITCH(w_, (launch_spread_w<2, WW>(ctx, gd, smem, st, pts_, g, cv, pts_.M, nv,
+                                                   perm_.get(), subs_.get(), fv, gvol, mode, shifts_,
+                                                   maxsub_, mbits_.get(), kmax_)));
         } else {
-            LC_W_SWITCH(w_, (launch_spread_w<3, WW>(ctx, gd, smem, ctx.stream(), pts_, g, cv, pts_.M, nv,
-                                                   perm_.get(), subs_.get(), gv, gvol, mode, shifts_,
-                                                   maxsub_)));
+            LC_W_SWITCH(w_, (launch_spread_w<3, WW>(ctx, gd, smem, st, pts_, g, cv, pts_.M, nv,
+                                                   perm_.get(), subs_.get(), fv, gvol, mode, shifts_,
+                                                   maxsub_, mbits_.get(), kmax_)));
         }
+    }
+    {
+        const long n = gvol * nvol;
+        const long blocks = std::max<long>(1, std::min<long>((n + 255) / 256, (long)ctx.num_sms() * 8));
+        fix_to_float_kernel<<<(unsigned)blocks, 256, 0, st>>>(fix_.get(), grid, n, mbits_.get(), maxsub_,
+                                                               kmax_);
+        LC_CHECK_LAUNCH();
     }
 }
 
@@ -941,7 +1003,6 @@ void NufftPlan::type1_real(Context &ctx, const float2 *c, int nvol, float *out, 
     cudaStream_t st = ctx.stream();
     const long gvol = (long)nf_[0] * nf_[1] * nf_[2];
     grid_.ensure(gvol * nvol, st);
-    LC_CUDA(cudaMemsetAsync(grid_.get(), 0, gvol * nvol * sizeof(float2), st));
     spread(ctx, c, nvol, grid_.get(), mode);
     const int n3 = modes_[0], n2 = modes_[1], n1 = modes_[2];
     const int fx = nf_[0], fy = nf_[1], fz = nf_[2];

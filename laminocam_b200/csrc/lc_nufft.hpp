@@ -110,7 +110,10 @@ class NufftPlan {
     DevBuf<int4> subs_;
     int nsub_ = 0;
     int maxsub_ = 1024;  // most points of one spreading subproblem
+    long kmax_ = 1;      // bound on the footprints that cover one fine-grid cell
     DevBuf<float2> grid_, h1_, h2_;
+    DevBuf<long long> fix_;  // 64-bit fixed-point fine grid of the spreading (re, im)
+    DevBuf<int> mbits_;      // bound on the spread values (float bits)
 };
 
 }  // namespace lc

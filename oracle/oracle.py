@@ -27,11 +27,12 @@ This is a numpy restatement, in double precision, of the reference's CPU path
 * orchestration          src/gpu/mbir2d.cu:36-85, src/gpu/mbir.cu:41-167,
                          include/mbir2d_prep.h:44-65
 
-Pinning: the reference ships no golden vectors.  This oracle is pinned (a) against
-a direct long-double NUDFT / DFT restated independently in ``oracle/nudft_ref.c``,
-and (b) against the reference's own C++ sources compiled unmodified against
-self-written FFTW/FINUFFT shim headers (``oracle/ref_build/``), when
-``/root/reference`` is available.  See ``tests/test_oracle.py``.
+Pinning: the reference ships no golden vectors.  This oracle is pinned against
+the reference's own C++ sources compiled unmodified against self-written
+FFTW/FINUFFT shim headers (``oracle/ref_build/``), whose direct long-double
+DFT and NUDFT sums are restated independently of this module, whenever the
+reference sources are available to build them (``LAMINOCAM_REF``).  See
+``tests/test_oracle.py``.
 """
 from __future__ import annotations
 
@@ -207,6 +208,38 @@ def nudft2_3d(F, x, y, z, iflag=-1):
         for a in range(n1):
             acc += Ez[:, a] * np.sum((Ey @ F[a]) * Ex, axis=1)
         out[sl] = acc
+    return out
+
+
+def lattice_type1_modes(C, theta, gamma, beta, nrows, ncols, modes, iflag=+1, mask=False):
+    """Selected modes of the 3D type-1 sum over the rotated detector lattices
+    of polar_grid3d: f_k = sum_j c_j exp(iflag i k.x_j) for each row (kz, ky,
+    kx) of ``modes``, exactly, with c = C (ntheta, nrows, ncols), times the
+    |q| <= pi mask when ``mask``.  Per angle the exponent is qX (k.R[:, 0]) +
+    qY (k.R[:, 1]), so the lattice sum factors into a matrix product of
+    nrows x ncols values with two exponential vectors: O(M K) work for K
+    modes, the direct sum at full-size grids."""
+    modes = np.asarray(modes, dtype=np.float64).reshape(-1, 3)
+    kz, ky, kx = modes[:, 0], modes[:, 1], modes[:, 2]
+    qX = (np.arange(ncols) + 0.5) * (2.0 * PI / ncols) - PI
+    qY = (np.arange(nrows) + 0.5) * (2.0 * PI / nrows) - PI
+    out = np.zeros(modes.shape[0], dtype=np.complex128)
+    for i in range(len(theta)):
+        R = rotation_transpose(theta[i], gamma[i], beta[i])
+        u = kx * R[0, 0] + ky * R[1, 0] + kz * R[2, 0]
+        v = kx * R[0, 1] + ky * R[1, 1] + kz * R[2, 1]
+        Eb = np.exp(iflag * 1j * np.outer(qX, u))   # (ncols, K)
+        Ea = np.exp(iflag * 1j * np.outer(qY, v))   # (nrows, K)
+        if C is None and not mask:  # unit weights: the sum factors completely
+            out += Ea.sum(axis=0) * Eb.sum(axis=0)
+            continue
+        Ci = np.ones((nrows, ncols), dtype=np.complex128) if C is None else np.asarray(C[i], dtype=np.complex128)
+        if mask:
+            x = R[0, 0] * qX[None, :] + R[0, 1] * qY[:, None]
+            y = R[1, 0] * qX[None, :] + R[1, 1] * qY[:, None]
+            z = R[2, 0] * qX[None, :] + R[2, 1] * qY[:, None]
+            Ci = Ci * ((np.abs(x) <= PI) & (np.abs(y) <= PI) & (np.abs(z) <= PI))
+        out += np.sum(Ea * (Ci @ Eb), axis=0)
     return out
 
 
@@ -529,6 +562,30 @@ def cgsolver(A, y, x0, max_iter, tol, xtol, pap_floor=1e-10, history=None):
     else:
         it = max_iter
     return CGResult(x, it, res, dxv)
+
+
+def cgsolver_fp32(A, y, max_iter):
+    """The CG of cgsolver (x0 = 0, fixed iteration count) as an FP32 device
+    code computes it: vectors and operator outputs rounded to float32, the
+    scalars alpha and beta and the dot products in FP64.  A check of how far
+    any FP32 CG drifts from FP64 CG on the same operator."""
+    f32 = np.float32
+    r = np.asarray(y, dtype=f32)
+    x = np.zeros_like(r)
+    p = r.copy()
+    rs_old = float(np.vdot(r.astype(np.float64), r.astype(np.float64)))
+    for _ in range(max_iter):
+        Ap = np.asarray(A(p.astype(np.float64)), dtype=f32)
+        pAp = float(np.vdot(p.astype(np.float64), Ap.astype(np.float64)))
+        if pAp == 0.0:
+            break
+        alpha = rs_old / pAp
+        x = (x + f32(alpha) * p).astype(f32)
+        r = (r - f32(alpha) * Ap).astype(f32)
+        rs_new = float(np.vdot(r.astype(np.float64), r.astype(np.float64)))
+        p = (r + f32(rs_new / rs_old) * p).astype(f32)
+        rs_old = rs_new
+    return x.astype(np.float64)
 
 
 EPSILON = 1e-8

@@ -93,9 +93,10 @@ def test_solvers_2d_golden(lc, f):
 def test_cg_long_run_objective(lc):
     """Config-1 geometry (n=255, 180 angles), CG(10/25/50): the quadratic objective
     phi(x) = x.A^T A x / 2 - x.A^T y that CG minimises, evaluated in FP64, agrees
-    with the FP64 oracle's to 1e-3 (iterates themselves drift by ~1e-2 after
-    ~10 iterations in any FP32 CG, including an FP32 numpy emulation; the FP32
-    operators' ~1e-6 error puts the objective gap near 2e-4)."""
+    with the FP64 oracle's to 5e-4 (measured about 2e-4).  The iterates
+    themselves drift by ~1e-2 after ~10 iterations in any FP32 CG; the FP32
+    emulation in tests/test_oracle.py shows the same drift on the CPU, and
+    test_cg50_drift_is_the_fp32_drift below ties the two together."""
     from laminocam_b200 import synthetic as S
     n, nth = 255, 180
     th = np.arange(nth) * np.pi / nth
@@ -115,7 +116,7 @@ def test_cg_long_run_objective(lc):
                             return_info=True)
         assert info.iters == iters
         x = x.astype(np.float64)
-        assert abs(phi(x) - phi(ref)) / abs(phi(ref)) < 1e-3, iters
+        assert abs(phi(x) - phi(ref)) / abs(phi(ref)) < 5e-4, iters
     # the residual stopping rule fires (reason 1) well before max_iters
     _, info = lc.MBIR2D(sino, th, lc.ReconParams(recon_dims=(1, n, n), max_iters=200, tol=0.05, xtol=0),
                         return_info=True)
@@ -166,7 +167,7 @@ def test_mbir3d_golden(lc):
     rd = tuple(int(v) for v in g["recon_dims"])
     ds = [lc.Dataset(g["projs"], g["theta"], float(g["gamma"]), 0.0)]
     x = lc.MBIR(ds, lc.ReconParams(regularizer="unconstrained", recon_dims=rd, max_iters=6, tol=0, xtol=0))
-    assert O.rel_l2(x, g["cg6"]) < 1e-3
+    assert O.rel_l2(x, g["cg6"]) < RECON_TOL
     x = lc.MBIR(ds, lc.ReconParams(regularizer="split_bregman", recon_dims=rd, max_iters=3, tol=0, xtol=0))
     assert O.rel_l2(x, g["sb3"]) < RECON_TOL
 
@@ -274,3 +275,72 @@ def test_psf_kernel_reflection_paths(lc, symmetric):
     err = O.rel_l2(K, zero_unpaired(O.psf2d(th, n, n).kernel))
     print("2D kernel rel. error", symmetric, err)
     assert err < 1e-10, err
+
+
+def test_cg50_drift_is_the_fp32_drift(lc):
+    """Unregularised CG(50) on a noisy ellipse sinogram (n = 63, 60 angles):
+    the GPU's distance to the FP64 oracle is no larger than that of an FP32
+    CG emulated in numpy on the oracle's own operator (FP32 vectors and
+    operator outputs, FP64 scalars), so the drift is the precision of any
+    FP32 CG on these normal equations, not an error of the CUDA path.  CG(5)
+    stays within the 1e-4 reconstruction bound."""
+    from laminocam_b200 import synthetic as S
+    n, nth = 63, 60
+    th = np.arange(nth) * np.pi / nth
+    ph = S.ellipse_phantom(n, 10, 1001)
+    sino = to_np(lc.forward2d(ph[None], lc.PolarGrid2D(th, n))).astype(np.float32)
+    sino = S.add_noise(sino, 0.01, 2001)
+    sino = (sino / sino.max()).astype(np.float32)
+    s64 = sino.astype(np.float64)
+    rhs = O.backproj2d(s64, th, (1, n, n))
+    psf = O.psf2d(th, n, n)
+    A = lambda v: O.convolve2d(v, psf)
+    for iters in (5, 50):
+        ref = O.cgsolver(A, rhs, np.zeros_like(rhs), iters, 0, 0).x
+        emu = O.cgsolver_fp32(A, rhs, iters)
+        x = lc.MBIR2D(sino, th, lc.ReconParams(recon_dims=(1, n, n), max_iters=iters, tol=0, xtol=0))
+        e_gpu, e_emu = O.rel_l2(x, ref), O.rel_l2(emu, ref)
+        print(f"CG({iters}) rel L2 vs FP64: GPU {e_gpu:.3e}, FP32 emulation {e_emu:.3e}")
+        if iters == 5:
+            assert e_gpu < RECON_TOL
+        else:
+            assert e_gpu < 3.0 * e_emu
+
+
+def test_backprojection_is_repeatable(lc):
+    """The spreading sums every contribution in exact 64-bit fixed point at one
+    scale per launch, so two backprojections of the same data are bit-identical
+    (2D, and 3D tilted with shifts, whose points go through the mask and the
+    phase)."""
+    import torch
+    rng = np.random.default_rng(41)
+    n, nth = 127, 150
+    th = np.arange(nth) * np.pi / nth
+    y = rng.standard_normal((2, nth, n)).astype(np.float32)
+    pg = lc.PolarGrid2D(th, n)
+    a = lc.backproj2d(y, pg, (2, n, n))
+    b = lc.backproj2d(y, pg, (2, n, n))
+    assert torch.equal(a, b)
+    nth3 = 40
+    th3 = np.arange(nth3) * 2 * np.pi / nth3
+    pg3 = lc.PolarGrid(th3, np.full(nth3, -0.5), np.full(nth3, 0.03), 47, 47,
+                       shifts=rng.normal(scale=1.5, size=(nth3, 2)).astype(np.float32))
+    p = rng.standard_normal((nth3, 47, 47)).astype(np.float32)
+    a = lc.backproj(p, pg3, (9, 47, 47), shifts=True)
+    b = lc.backproj(p, pg3, (9, 47, 47), shifts=True)
+    assert torch.equal(a, b)
+
+
+def test_reconstruction_is_repeatable(lc):
+    """Fifty CG iterations from the same sinogram give the same bits twice:
+    backprojection, PSF, Toeplitz passes and the solver's reductions are all
+    order-independent."""
+    from laminocam_b200 import synthetic as S
+    n, nth = 127, 120
+    th = np.arange(nth) * np.pi / nth
+    sino = to_np(lc.forward2d(S.ellipse_phantom(n, 8, 7)[None], lc.PolarGrid2D(th, n))).astype(np.float32)
+    sino = (sino / sino.max()).astype(np.float32)
+    p = lc.ReconParams(recon_dims=(1, n, n), max_iters=50, tol=0, xtol=0)
+    a = lc.MBIR2D(sino, th, p)
+    b = lc.MBIR2D(sino, th, p)
+    assert np.array_equal(a, b)

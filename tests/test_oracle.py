@@ -212,3 +212,32 @@ def test_pin_split_bregman_against_reference():
     a = R.mbir2d(sino, th, 11, "sb", 3, 0.0, 0.0, lam=0.1, mu=5.0, inner=2)
     b = O.mbir2d(sino, th, (1, 11, 11), "sb", 3, 0.0, 0.0, lam=0.1, mu=5.0, inner=2)
     assert O.rel_l2(b, a) < 1e-10
+
+
+def test_fp32_cg_drifts_from_fp64_cg():
+    """Unregularised CG on a noisy ellipse sinogram (n = 63, 60 angles), run by
+    the oracle in FP64 and by an FP32 emulation of the same CG on the same
+    FP64 operator (only the vectors and the operator outputs are rounded to
+    float32).  After 5 iterations the two agree within the 1e-4
+    reconstruction bound; after 50 they are more than 1e-2 apart.  The
+    normal equations of tomography without density compensation are so
+    ill-conditioned that CG amplifies rounding at the 1e-7 level into a
+    percent-level difference of the iterate, whatever the code that
+    computes it: a long FP32 CG cannot be held to 1e-4 of FP64 CG."""
+    from laminocam_b200 import synthetic as S
+    n, nth = 63, 60
+    th = np.arange(nth) * np.pi / nth
+    ph = S.ellipse_phantom(n, 10, 1001)
+    sino = O.forward2d(ph[None].astype(np.float64), th, n)
+    sino = S.add_noise(sino.astype(np.float32), 0.01, 2001).astype(np.float64)
+    sino /= sino.max()
+    rhs = O.backproj2d(sino, th, (1, n, n))
+    psf = O.psf2d(th, n, n)
+    A = lambda v: O.convolve2d(v, psf)
+    drift = {}
+    for iters in (5, 50):
+        ref = O.cgsolver(A, rhs, np.zeros_like(rhs), iters, 0, 0).x
+        drift[iters] = O.rel_l2(O.cgsolver_fp32(A, rhs, iters), ref)
+    print("FP32 CG drift from FP64 CG:", drift)
+    assert drift[5] < 1e-4
+    assert drift[50] > 1e-2

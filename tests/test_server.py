@@ -1,16 +1,14 @@
 """The reconstruction server (lc_server_*) and CUDA-graph replay of the solvers.
 
-Every result the server computes, alone or among concurrent jobs, must equal
-what the one-job drivers (lc_mbir2d / lc_mbir3d) return for the same
-arguments within 1e-4 relative L2, the reconstruction tolerance: the
-backprojection accumulates with float atomics, whose order varies from run to
-run, and unregularised FP32 CG amplifies those last-bit differences of the
-right-hand side (about 1e-7) by 1e3 to 1e4 within 8 iterations on these
-ill-conditioned normal operators, so the CG cases stop at 4 iterations.
-Graph replay of the solvers must equal eager launches bit for bit on the same
-inputs; a failing job must leave the other jobs and the server intact.  Every
-wait has a time limit, so a stuck job fails the test instead of stalling the
-run.
+Every result the server computes, alone or among concurrent jobs, equals what
+the one-job drivers (lc_mbir2d / lc_mbir3d) return for the same arguments bit
+for bit: the backprojection sums in exact fixed point, the PSF and the
+Toeplitz passes are fixed arithmetic per element, and the solver's reductions
+are fixed-order, so neither the other jobs on the device nor a cached PSF
+change a result.  The CG cases run 50 iterations, the configuration's count.
+Graph replay of the solvers equals eager launches bit for bit; a failing job
+must leave the other jobs and the server intact.  Every wait has a time limit,
+so a stuck job fails the test instead of stalling the run.
 """
 import numpy as np
 import pytest
@@ -77,15 +75,13 @@ def test_graph_replay_matches_eager(lc):
 
 
 def test_graph_replay_through_the_driver(lc):
-    """MBIR2D with graphs against MBIR2D without: the backprojection's float
-    atomics make the right-hand sides differ in the last bits, so the bound is
-    the reconstruction tolerance."""
+    """MBIR2D with graphs against MBIR2D without: the same bits."""
     s, th = sino2d(lc, 95, 90, 11)
-    for method, iters in (("unconstrained", 4), ("split_bregman", 5)):
+    for method, iters in (("unconstrained", 50), ("split_bregman", 5)):
         a = lc.MBIR2D(s, th, params2d(lc, 95, method, iters, graph=False))
         b, info = lc.MBIR2D(s, th, params2d(lc, 95, method, iters, graph=True), return_info=True)
         assert info.iters == iters
-        assert O.rel_l2(b, a) < RECON_TOL
+        assert np.array_equal(b, a)
 
 
 def test_graph_replay_with_tolerance_stop(lc):
@@ -109,8 +105,8 @@ def test_graph_replay_with_tolerance_stop(lc):
 
 
 def test_server_results_match_single_jobs(lc):
-    jobs2d = [(63, 60, 1, "unconstrained", 4), (95, 120, 2, "split_bregman", 4),
-              (127, 90, 3, "unconstrained", 4), (63, 60, 4, "split_bregman", 3)]
+    jobs2d = [(63, 60, 1, "unconstrained", 50), (95, 120, 2, "split_bregman", 4),
+              (127, 90, 3, "unconstrained", 50), (63, 60, 4, "split_bregman", 3)]
     data = [sino2d(lc, n, nth, seed) for n, nth, seed, _, _ in jobs2d]
     ref = [lc.MBIR2D(s, th, params2d(lc, n, m, it))
            for (n, _, _, m, it), (s, th) in zip(jobs2d, data)]
@@ -128,7 +124,7 @@ def test_server_results_match_single_jobs(lc):
         res = [sv.wait(j, WAIT_S) for j in ids]
         st = sv.stats()
     for r, e in zip(res, (ref + [ref3]) * 2):
-        assert O.rel_l2(r.recon, e) < RECON_TOL
+        assert np.array_equal(r.recon, e)
     assert st["completed"] == len(ids) and st["failed"] == 0
     assert st["psf_hits"] >= 5 and all(r.psf_hit for r in res[5:])
     assert st["p99_ms"] >= st["p50_ms"] > 0
@@ -157,7 +153,7 @@ def test_server_psf_cache_clear(lc):
         c = sv.wait(sv.submit2d(s, th, prm), WAIT_S)
         assert not c.psf_hit
         assert sv.stats()["psf_misses"] == 1
-    assert O.rel_l2(c.recon, a.recon) < RECON_TOL
+    assert np.array_equal(c.recon, a.recon)
 
 
 def test_server_many_workers_uneven_jobs(lc):
@@ -178,12 +174,12 @@ def test_server_many_workers_uneven_jobs(lc):
     assert st["completed"] == len(jobs) and st["failed"] == 0
     for (s, th, n), r in list(zip(jobs, res))[:6]:
         ref = lc.MBIR2D(s, th, params2d(lc, n, "split_bregman", 3))
-        assert O.rel_l2(r.recon, ref) < RECON_TOL
+        assert np.array_equal(r.recon, ref)
 
 
 def test_server_isolates_failing_job(lc):
     s, th = sino2d(lc, 63, 60, 31)
-    good = params2d(lc, 63, "unconstrained", 4)
+    good = params2d(lc, 63, "unconstrained", 50)
     bad = lc.ReconParams(regularizer="unconstrained", recon_dims=(2, 63, 63), max_iters=4)
     ref = lc.MBIR2D(s, th, good)
     with lc.Server(workers=2) as sv:
@@ -197,7 +193,7 @@ def test_server_isolates_failing_job(lc):
         st = sv.stats()
         rd = sv.wait(sv.submit2d(s, th, good), WAIT_S)  # still serving after the failure
     for r in (ra, rc, rd):
-        assert O.rel_l2(r.recon, ref) < RECON_TOL
+        assert np.array_equal(r.recon, ref)
     assert st["failed"] == 1 and st["completed"] == 2
 
 
@@ -221,4 +217,4 @@ def test_server_admission_respects_budget(lc):
     assert st["peak_admitted_bytes"] <= 2.5 * one
     assert 1 <= st["peak_running"] <= 2
     for r in res[1:]:
-        assert O.rel_l2(r.recon, res[0].recon) < RECON_TOL
+        assert np.array_equal(r.recon, res[0].recon)
