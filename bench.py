@@ -163,33 +163,64 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(sample_outer: int = 1):
-    """The FP64 oracle's Split-Bregman outer iteration at the padded size on host
-    cores (scipy.fft workers), extrapolated to 100 outer iterations."""
-    from oracle import oracle as O
+REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+
+
+def reference_cpu_run(warmup: int, steps: int, full: bool = False):
+    """The reference's own CPU path on this workload, timed on the host cores:
+    its sources (src/projection.cpp, gradient.cpp, conjgrad.cpp, bregman.cpp,
+    finitediff.cpp, mbir.cpp, include/toeplitz.h) compiled unmodified in float
+    against self-written multithreaded FFTW / FINUFFT stand-ins
+    (oracle/ref_build, target ref_bench; FINUFFT at the reference's float
+    tolerance 5e-4, include/finufft_plan.h:71).  The projections are the
+    reference's own forward() of the same seeded phantom plus 1% noise.
+    Returns the setup time (the calls of tomocam::MBIR before its solver:
+    normalisation, padding, polar grid, backprojection, PSF), the times of
+    `steps` single Split-Bregman outer iterations after `warmup` untimed ones,
+    and, with `full`, one complete tomocam::MBIR of 100 outer iterations."""
+    import tempfile
+    from laminocam_b200 import synthetic as S
+    if not os.path.exists(REF_BENCH):
+        raise RuntimeError("oracle/_ref/ref_bench is not built (needs the reference sources at build time)")
     cores = os.cpu_count() or 1
-    O.set_fft_workers(cores)
-    n = (29, 721, 721)
-    P = tuple(O.next_fast_dim(2 * v - 1) for v in n)
-    rng = np.random.default_rng(0)
-    # a real, point-symmetric spectrum of the right shape stands in for the PSF
-    khat = np.abs(rng.standard_normal((P[0], P[1], P[2] // 2 + 1))).astype(np.float64)
-    psf = O.PSF3D(P, None, khat)
-    yT = rng.random(n)
-    A = lambda v: O.convolve3d(v, psf)
-    t0 = time.perf_counter()
-    O.split_bregman(A, yT, np.zeros(n), LAM, MU, sample_outer, 1, 1e-5, 0.0)
-    dt = (time.perf_counter() - t0) / sample_outer
-    return {"value": 1.0 / (OUTER * dt), "unit": "recons/s", "cores": cores, "kind": "port",
-            "sample": f"{sample_outer} Split-Bregman outer iteration(s) of the FP64 oracle at the "
-                      f"padded size 29x721x721 ({dt:.2f} s each, scipy.fft with {cores} workers), "
-                      f"extrapolated to 100 outer iterations; backprojection and PSF setup excluded"}
+    with tempfile.TemporaryDirectory() as td:
+        ph = os.path.join(td, "phantom.f32")
+        S.ellipsoid_phantom(RECON_DIMS, N_ELLIPSOIDS, 1000).astype(np.float32).tofile(ph)
+        cmd = [REF_BENCH, "lamino", ph, *map(str, RECON_DIMS), str(NANGLES), str(GAMMA_DEG), str(warmup),
+               str(steps)] + (["full"] if full else [])
+        out = subprocess.run(cmd, capture_output=True, text=True, check=True,
+                             env=dict(os.environ, OMP_NUM_THREADS=str(cores))).stdout
+    rec = [json.loads(line) for line in out.splitlines() if line.startswith("{")]
+    setup = next(r for r in rec if r["phase"] == "setup")
+    outer = [r["seconds"] for r in rec if r["phase"] == "outer"]
+    fullr = next((r["seconds"] for r in rec if r["phase"] == "full"), None)
+    recon_s = setup["seconds"] + OUTER * float(np.mean(outer))
+    return {"cores": cores, "setup_s": setup["seconds"], "backproj_s": setup["backproj_s"],
+            "psf_s": setup["psf_s"], "outer_s": outer, "recon_s": recon_s, "full_s": fullr}
+
+
+def cpu_baseline():
+    """Bounded sample of the reference's CPU path (setup and two outer
+    iterations, about a minute of host time), scaled to one reconstruction."""
+    r = reference_cpu_run(0, 2)
+    return {"value": 1.0 / r["recon_s"], "unit": "recons/s", "cores": r["cores"], "kind": "reference",
+            "sample": f"the reference's own sources (float, FINUFFT tol 5e-4) on self-written "
+                      f"multithreaded FFTW/FINUFFT stand-ins, {r['cores']} OpenMP threads: setup "
+                      f"(backprojection + PSF) {r['setup_s']:.1f} s measured once, 2 Split-Bregman outer "
+                      f"iterations at {np.mean(r['outer_s']):.2f} s each; one reconstruction = setup + "
+                      f"100 outer iterations = {r['recon_s']:.1f} s",
+            "setup_s": r["setup_s"], "outer_s": float(np.mean(r["outer_s"]))}
 
 
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one Toeplitz apply at the
 # padded workload volume [29, 721, 721]: x rows 60 + 64 MB, y forward 122 + 193,
 # z 387 + 203, y inverse 247 + 98, x inverse 122 + 31
 TOEPLITZ_APPLY_DRAM_BYTES = 1527e6
+
+# padded detector of the workload (511 -> int(511 * 1.4142) forced odd)
+PADDED_DET = (721, 721)
+# conflict-free 32-bit shared-memory reductions per clock per SM (B200, probe)
+SHARED_RED_PER_CLK_SM = 30.9
 
 MIX_JOBS = 64
 MIX_ITERS = 50
@@ -501,22 +532,36 @@ def serving_stream(lc, workers=32, count=STREAM_REQUESTS, rates=STREAM_RATES):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's own CPU path (reference_cpu_run) on
+    this workload.  A step is one Split-Bregman outer iteration of the
+    reference's code at the workload size; the setup (backprojection and PSF)
+    runs once before the warm-up and is timed too.  value = 1 / (setup + the
+    workload's 100 outer iterations x the mean timed outer iteration): one
+    reconstruction's worth of the reference's measured work, in recons/s.
+    Under torchrun only rank 0 runs."""
     if rank != 0:
         return
-    steps = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        info = cpu_baseline(1)
-        if i >= args.warmup:
-            steps.append(1.0 / info["value"])
-    sec = float(np.mean(steps))
-    v = 1.0 / sec
+    try:
+        r = reference_cpu_run(args.warmup, args.steps, full=args.reference_full)
+    except Exception as ex:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed to run: {ex}"}),
+              flush=True)
+        return
+    v = 1.0 / r["recon_s"]
+    sec = float(np.mean(r["outer_s"]))
     line = {"metric": METRIC, "value": v, "unit": "recons/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": CONFIG, "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": "recons/s", "cores": info["cores"], "kind": "port",
-                             "sample": info["sample"]},
+            "value_basis": f"1 / (setup + {OUTER} x mean outer iteration); a step is one outer iteration",
+            "reference_times_s": {"setup": r["setup_s"], "backproj": r["backproj_s"], "psf": r["psf_s"],
+                                  "outer_mean": sec, "outer_steps": [round(t, 3) for t in r["outer_s"]],
+                                  "full_reconstruction": r["full_s"]},
+            "cpu_baseline": {"value": v, "unit": "recons/s", "cores": r["cores"], "kind": "reference",
+                             "sample": f"the reference's own sources in float on self-written multithreaded "
+                                       f"FFTW/FINUFFT stand-ins (FINUFFT tol 5e-4), {r['cores']} threads: "
+                                       f"setup once, {args.warmup} untimed and {args.steps} timed outer "
+                                       f"iterations"},
             "e2e": {"value": v, "unit": "recons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -575,6 +620,10 @@ def main():
     ap.add_argument("--kernel-case", choices=["toeplitz", "split_bregman"],
                     help="reduced case for a profiler capture of one kernel family (not a benchmark line)")
     ap.add_argument("--reps", type=int, default=3, help="applies or outer iterations of --kernel-case")
+    ap.add_argument("--reference-full", action="store_true",
+                    help="with --impl reference: also run one complete reconstruction of the reference's "
+                         "code (tomocam::MBIR, 100 outer iterations) and report its time beside the "
+                         "sampled value")
     args = ap.parse_args()
     if args.kernel_case:
         return kernel_case(args.kernel_case, args.reps)
@@ -705,9 +754,8 @@ def main():
 
     # end to end through the host-buffer API
     step_e2e()
-    e2e_ms, _ = timed(step_e2e, max(1, min(args.steps, 3)))
-    e2e_steps = max(1, min(args.steps, 3))
-    e2e_value = e2e_steps * world / (e2e_ms / 1e3)
+    e2e_ms, _ = timed(step_e2e, args.steps)
+    e2e_value = args.steps * world / (e2e_ms / 1e3)
 
     # roofline of the dominant kernel section
     prof = []
@@ -729,11 +777,10 @@ def main():
         units.append({"name": "toeplitz_apply (" + "+".join(p["name"][9:] for p in toep) + ")",
                       "launches": applies, "total_ms": tot_ms, "avg_ms": tot_ms / applies,
                       "gbs": tot_b / tot_ms / 1e6, "bytes_per_launch": tot_b / applies})
-    # The roofline object is the dominant section of the iterations (launched
-    # every outer iteration); the one-off setup sections (spreading, bound by
-    # shared-memory atomics, and the FP64 PSF) are listed in "rooflines" only.
-    iterative = [u for u in units if u["launches"] >= 2]
-    dom = max(iterative or units, key=lambda d: d["total_ms"]) if units else None
+    # The roofline object is the section with the most time in the step,
+    # one-off sections (the spreading) included; every section is listed in
+    # "rooflines".
+    dom = max(units, key=lambda d: d["total_ms"]) if units else None
     rooflines = [{"section": u["name"], "launches": u["launches"], "avg_ms": u["avg_ms"],
                   "achieved_gbs": u["gbs"], "frac": u["gbs"] / peak} for u in
                  sorted(units, key=lambda d: -d["total_ms"])]
@@ -750,22 +797,48 @@ def main():
                 "bytes_per_launch": dom["bytes_per_launch"], "avg_launch_ms": dom["avg_ms"],
                 "traffic": traffic}
 
+    # The spreading against its own bound: every cell update of a footprint
+    # is four 32-bit shared-memory reductions (fixed-point high and low words
+    # of the real and imaginary parts), and an SM retires about 31 of them per
+    # clock (a conflict-free probe measured 30.9).
+    spread_roof = None
+    sp = next((u for u in units if u["name"] == "nufft_spread"), None)
+    if sp and not args.small:
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = clk.summary().get("sm_mhz") or 1965.0
+        w = 7  # ES kernel width at NUFFT tolerance 1e-6
+        cells = float(NANGLES) * PADDED_DET[0] * PADDED_DET[1] * w ** 3
+        bound_ms = cells * 4.0 / (SHARED_RED_PER_CLK_SM * sms * mhz * 1e6) * 1e3
+        spread_roof = {"bound": "shared-memory reductions", "cell_updates": cells,
+                       "reductions_per_cell": 4, "peak_reductions_per_clk_per_sm": SHARED_RED_PER_CLK_SM,
+                       "bound_ms": bound_ms, "avg_launch_ms": sp["avg_ms"], "frac": bound_ms / sp["avg_ms"],
+                       "hbm_gbs": sp["gbs"], "hbm_frac": sp["gbs"] / peak}
+
     # the same reconstruction with the operator product recomputed in every
-    # outer iteration (the reference's schedule): relative L2 difference
+    # outer iteration (the reference's schedule): its rate and its relative L2
+    # difference from the carried schedule's result
     schedule_check = None
+    exact_value = None
     if args.residual_refresh != 1:
         carried = drecon.clone()
         exact_params = lc.ReconParams(regularizer="split_bregman", recon_dims=RECON_DIMS, max_iters=OUTER,
                                       inner_iters=1, lam=LAM, mu=MU, tol=1e-5, xtol=0.0, use_graph=True,
                                       residual_refresh=1).to_c()
-        ctx.sync_stream()
-        rc = lib.lc_mbir3d_device(ctx.handle, C.c_void_p(dproj.data_ptr()), nth, nr, nc, tp, gp, bp,
-                                  None, rd, C.byref(exact_params), C.c_void_p(drecon.data_ptr()), None)
-        if rc:
-            raise RuntimeError(lib.lc_last_error(ctx.handle).decode())
+
+        def step_exact():
+            ctx.sync_stream()
+            rc = lib.lc_mbir3d_device(ctx.handle, C.c_void_p(dproj.data_ptr()), nth, nr, nc, tp, gp, bp,
+                                      None, rd, C.byref(exact_params), C.c_void_p(drecon.data_ptr()), None)
+            if rc:
+                raise RuntimeError(lib.lc_last_error(ctx.handle).decode())
+
+        step_exact()
         torch.cuda.synchronize()
         schedule_check = float(torch.linalg.vector_norm((carried - drecon).double())
                                / torch.linalg.vector_norm(drecon.double()))
+        k_exact = max(1, min(args.steps, 5))
+        exact_ms, _ = timed(step_exact, k_exact)
+        exact_value = k_exact * world / (exact_ms / 1e3)
 
     serving = None
     if rank == 0 and world == 1 and not args.no_mix:
@@ -784,9 +857,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline(1)
+            cpu = cpu_baseline()
         except Exception as ex:  # reported, not fatal
-            cpu = {"value": None, "unit": "recons/s", "cores": os.cpu_count(), "kind": "port",
+            cpu = {"value": None, "unit": "recons/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {ex}"}
 
     lats_sorted = sorted(lats)
@@ -804,6 +877,8 @@ def main():
         "roofline": roof, "rooflines": rooflines, "kernels": prof[:12], "clocks": clk.summary(),
         "serving": serving, "serving_stream": stream, "gpu_launches": int(launches),
         "cpu_baseline": cpu,
+        "spread_roofline": spread_roof,
+        "value_reference_schedule": exact_value,
         "solver": {"outer_iters": stats.iters, "cg_iters": stats.cg_iters_total, "dx": stats.dx,
                    "residual_refresh": args.residual_refresh,
                    "rel_l2_vs_exact_residual_schedule": schedule_check},

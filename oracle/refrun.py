@@ -95,3 +95,51 @@ def mbir3d(projs, theta, gamma, beta, recon_dims, method, iters, tol, xtol, lam=
     out = run("mbir3d", [[nth, nrows, ncols, *recon_dims, m, iters, tol, xtol, lam, mu, inner,
                           gamma, beta], theta, projs])
     return out.reshape(recon_dims)
+
+
+def bench_path() -> str:
+    return os.path.join(REF_DIR, "ref_bench")
+
+
+def bench_available() -> bool:
+    return os.path.exists(bench_path())
+
+
+def _run_bench(op: str, values) -> np.ndarray:
+    flat = np.concatenate([np.ravel(np.asarray(v, dtype=np.float64)) for v in values])
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.f64")
+        fout = os.path.join(td, "out.f64")
+        flat.tofile(fin)
+        subprocess.run([bench_path(), op, fin, fout], check=True,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1)))
+        return np.fromfile(fout, dtype=np.float64)
+
+
+def fast_fft(kind: str, a, sign: int = -1, double: bool = True, shape=None):
+    """The timing build's FFTW stand-in: kind 'c2c' (a complex, any rank),
+    'r2c' (a real), 'c2r' (a half spectrum; shape = the real output shape)."""
+    a = np.asarray(a)
+    k = {"c2c": 0, "r2c": 1, "c2r": 2}[kind]
+    dims = list(a.shape) if kind != "c2r" else list(shape)
+    data = np.stack([a.real, a.imag], axis=-1).ravel() if np.iscomplexobj(a) or kind != "r2c" else a.ravel()
+    out = _run_bench("check_fft", [[k, 1 if double else 0, len(dims)], dims, [sign], data])
+    if kind == "c2r":
+        return out.reshape(dims)
+    if kind == "r2c":
+        dims = dims[:-1] + [dims[-1] // 2 + 1]
+    return out.view(np.complex128).reshape(dims)
+
+
+def fast_nufft(nu_type: int, dim: int, modes, iflag: int, tol: float, x, y, z, data, double: bool = True):
+    """The timing build's FINUFFT stand-in: type 1 (data = c[M] -> f[modes])
+    or type 2 (data = f -> c[M]); modes = (n1, n2, n3), dimension 1 fastest."""
+    M = len(x)
+    nm = list(modes) + [1] * (3 - len(modes))
+    zz = np.zeros(M) if z is None else z
+    yy = np.zeros(M) if y is None else y
+    d = np.asarray(data, dtype=np.complex128).ravel()
+    out = _run_bench("check_nufft", [[nu_type, dim], nm, [iflag, tol, 1 if double else 0, M], x, yy, zz,
+                                     np.stack([d.real, d.imag], axis=-1).ravel()])
+    out = out.view(np.complex128)
+    return out.reshape(nm[2], nm[1], nm[0])[:, :, :] if nu_type == 1 else out

@@ -1,7 +1,7 @@
 """CPU checks of bench.py: the served request stream's workload (seeded,
 70 % slices / 30 % volumes, CG or Split-Bregman with equal odds, the size and
-angle ladders) and the reference arm's JSON line, which runs the FP64 oracle
-on the host and needs no GPU."""
+angle ladders) and the reference arm's JSON line, which runs the reference's
+own CPU path (oracle/_ref/ref_bench) on the host and needs no GPU."""
 import json
 import os
 import subprocess
@@ -55,8 +55,13 @@ def test_stream_params_forms():
 
 
 def test_reference_arm_prints_its_line():
-    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    """The reduced profiling case (--small) keeps the reference's CPU run short."""
+    from oracle import refrun
+    if not refrun.bench_available():
+        import pytest
+        pytest.skip("oracle/_ref/ref_bench is not built")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
+                        "--warmup", "1", "--small"], capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference"
@@ -64,4 +69,11 @@ def test_reference_arm_prints_its_line():
               "config", "cpu_baseline", "e2e"):
         assert k in line, k
     assert line["value"] > 0 and line["unit"] == "recons/s"
-    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "reference"
+    t = line["reference_times_s"]
+    assert len(t["outer_steps"]) == 2 and t["setup"] > 0
+    # value is one reconstruction's worth of the measured work: setup + the
+    # workload's outer iterations (100; 5 in the reduced case)
+    outer = line["config"]["outer_iters"]
+    assert abs(1.0 / line["value"] - (t["setup"] + outer * t["outer_mean"])) < 1e-6 * (1.0 / line["value"])
+    assert abs(line["ms_per_step"] - 1e3 * t["outer_mean"]) < 1e-6 * line["ms_per_step"]

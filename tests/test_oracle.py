@@ -241,3 +241,46 @@ def test_fp32_cg_drifts_from_fp64_cg():
     print("FP32 CG drift from FP64 CG:", drift)
     assert drift[5] < 1e-4
     assert drift[50] > 1e-2
+
+
+@pytest.mark.skipif(not R.bench_available(), reason="oracle/_ref/ref_bench is not built")
+def test_timing_build_fft_matches_numpy():
+    """The FFTW stand-in of the timing build (multithreaded Stockham / Bluestein)
+    against numpy: complex transforms of both signs including non-2^p 3^q
+    lengths, and real transforms with even and odd last dimensions."""
+    rng = np.random.default_rng(0)
+    for shp in [(8,), (9,), (7,), (721,), (3, 5, 4), (16, 24, 18), (5, 7, 11)]:
+        a = rng.standard_normal(shp) + 1j * rng.standard_normal(shp)
+        for sign in (-1, 1):
+            want = np.fft.fftn(a) if sign < 0 else np.fft.ifftn(a) * a.size
+            assert O.rel_l2(R.fast_fft("c2c", a, sign), want) < 1e-13, (shp, sign)
+    for shp in [(10,), (6, 12), (4, 6, 18), (3, 5, 7), (2, 3, 1458), (2, 729)]:
+        a = rng.standard_normal(shp)
+        h = np.fft.rfftn(a)
+        assert O.rel_l2(R.fast_fft("r2c", a), h) < 1e-13, shp
+        want = np.fft.irfftn(h, s=shp, axes=tuple(range(len(shp)))) * a.size
+        assert O.rel_l2(R.fast_fft("c2r", h, shape=shp), want) < 1e-13, shp
+
+
+@pytest.mark.skipif(not R.bench_available(), reason="oracle/_ref/ref_bench is not built")
+@pytest.mark.parametrize("tol", [1e-6, 5e-4])
+def test_timing_build_nufft_matches_exact_sums(tol):
+    """The FINUFFT stand-in of the timing build (ES kernel, colour-scheduled
+    spreading) against the exact non-uniform DFTs, type 1 and 2 in 2D and 3D,
+    within twice its requested tolerance (FINUFFT's tolerance is an estimate
+    of the relative error, not a bound; the reference's float path asks
+    5e-4); the 3D type 1 case cuts the fine grid into many y and z blocks."""
+    rng = np.random.default_rng(1)
+    M = 3000
+    x, y, z = (rng.uniform(-np.pi, np.pi, M) for _ in range(3))
+    c = rng.standard_normal(M) + 1j * rng.standard_normal(M)
+    n2, n3 = 12, 17
+    assert O.rel_l2(R.fast_nufft(1, 2, (n3, n2), +1, tol, x, y, None, c)[0],
+                    O.nudft1_2d(c[None], x, y, n2, n3, +1)[0]) < 2 * tol
+    F = rng.standard_normal((n2, n3)) + 1j * rng.standard_normal((n2, n3))
+    assert O.rel_l2(R.fast_nufft(2, 2, (n3, n2), -1, tol, x, y, None, F), O.nudft2_2d(F[None], x, y, -1)[0]) < 2 * tol
+    n1, n2, n3 = 40, 70, 30
+    assert O.rel_l2(R.fast_nufft(1, 3, (n3, n2, n1), +1, tol, x, y, z, c),
+                    O.nudft1_3d(c, x, y, z, n1, n2, n3, +1)) < 2 * tol
+    F = rng.standard_normal((6, 10, 9)) + 1j * rng.standard_normal((6, 10, 9))
+    assert O.rel_l2(R.fast_nufft(2, 3, (9, 10, 6), -1, tol, x, y, z, F), O.nudft2_3d(F, x, y, z, -1)) < 2 * tol
