@@ -177,6 +177,29 @@ int lc_mbir3d_device(lc_context ctx, const float *projs, int ntheta, int nrows, 
                      const float *shifts, const int *recon_dims, const lc_recon_params *p,
                      float *recon, lc_solver_stats *stats);
 
+/* ---- cross-job batching (replaces the reference's one-slice-at-a-time loops,
+ * include/gpu/nufft.h:92-95 and include/gpu/toeplitz2d.h:68-76, for many
+ * independent slices) -------------------------------------------------------
+ * One 2D reconstruction job: a prepared sinogram {1, ntheta, nradial} in host
+ * memory, its angles (radians), the image size n and a host output {n, n}. */
+typedef struct {
+    const float *sinogram;
+    int ntheta, nradial;
+    const double *theta;
+    int n;
+    float *recon;
+} lc_job2d;
+/* gpu::MBIR2D with CG (method 0) for njobs independent slices of any sizes:
+ * each job's setup (upload, backprojection, FP64 PSF) runs on one of
+ * setup_workers worker streams (<= 0: 8), then all jobs iterate in lockstep,
+ * every CG stage one launch over the whole batch (p->solver.use_graph replays
+ * eight iterations as a CUDA graph).  Each job stops on its own tests.  A
+ * job's result does not depend on the other jobs of the batch.  stats (NULL,
+ * or njobs entries) receives each job's iteration count and stop reason.
+ * Returns when every recon is in host memory. */
+int lc_mbir2d_batch(lc_context ctx, const lc_job2d *jobs, int njobs, const lc_recon_params *p,
+                    int setup_workers, lc_solver_stats *stats);
+
 /* ---- profiling (no counterpart in the reference, which has only a wall-clock
  * Timer, include/timer.h:30-64) ---------------------------------------- */
 typedef struct {

@@ -19,7 +19,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import LaminocamError, ReconParamsC, SolverParams, SolverStats
+from ._lib import Job2D, LaminocamError, ReconParamsC, SolverParams, SolverStats
 
 __all__ = [
     "Context", "PolarGrid2D", "PolarGrid", "PointSpreadFunction2D", "PointSpreadFunction",
@@ -465,6 +465,36 @@ def MBIR2D(sinogram, theta, params: ReconParams, ctx: Optional[Context] = None, 
     _check(ctx.lib.lc_mbir2d(ctx.handle, sp, ns, nth, nr, tp, rd, C.byref(rp),
                              out.ctypes.data_as(C.POINTER(C.c_float)), C.byref(st)), ctx)
     return (out, _info(st)) if return_info else out
+
+
+def MBIR2D_batch(jobs, params: ReconParams, ctx: Optional[Context] = None, setup_workers: int = 8,
+                 return_info=False):
+    """Many independent 2D CG reconstructions batched across jobs
+    (lc_mbir2d_batch): jobs is a sequence of (sinogram {ntheta, nr} or
+    {1, ntheta, nr}, theta, n).  Every CG stage is one launch over all jobs;
+    the result of a job does not depend on the other jobs.  Returns the list
+    of {1, n, n} reconstructions (and the per-job SolveInfo)."""
+    ctx = ctx or Context.default()
+    if params.regularizer != "unconstrained":
+        raise LaminocamError("MBIR2D_batch: batched jobs use CG (regularizer 'unconstrained')")
+    keep, arr = [], (Job2D * len(jobs))()
+    outs = []
+    for k, (sino, theta, n) in enumerate(jobs):
+        s = np.ascontiguousarray(sino, dtype=np.float32)
+        s = s.reshape(s.shape[-2], s.shape[-1])
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        o = np.empty((1, int(n), int(n)), dtype=np.float32)
+        keep += [s, th]
+        outs.append(o)
+        arr[k].sinogram = s.ctypes.data_as(C.POINTER(C.c_float))
+        arr[k].ntheta, arr[k].nradial = s.shape
+        arr[k].theta = th.ctypes.data_as(C.POINTER(C.c_double))
+        arr[k].n = int(n)
+        arr[k].recon = o.ctypes.data_as(C.POINTER(C.c_float))
+    st = (SolverStats * len(jobs))()
+    rp = params.to_c()
+    _check(ctx.lib.lc_mbir2d_batch(ctx.handle, arr, len(jobs), C.byref(rp), int(setup_workers), st), ctx)
+    return (outs, [_info(x) for x in st]) if return_info else outs
 
 
 def _stack_projs(datasets: Sequence[Dataset]) -> np.ndarray:

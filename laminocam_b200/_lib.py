@@ -51,6 +51,11 @@ class ServerStats(C.Structure):
                 ("psf_cache_bytes", C.c_double)]
 
 
+class Job2D(C.Structure):
+    _fields_ = [("sinogram", C.POINTER(C.c_float)), ("ntheta", C.c_int), ("nradial", C.c_int),
+                ("theta", C.POINTER(C.c_double)), ("n", C.c_int), ("recon", C.POINTER(C.c_float))]
+
+
 vp = C.c_void_p
 i32 = C.c_int
 f64 = C.c_double
@@ -90,6 +95,8 @@ SIGNATURES = {
                         C.POINTER(ReconParamsC), fptr, C.POINTER(SolverStats)]),
     "lc_mbir3d_device": (i32, [vp, vp, i32, i32, i32, dptr, dptr, dptr, fptr, C.POINTER(C.c_int),
                                C.POINTER(ReconParamsC), vp, C.POINTER(SolverStats)]),
+    "lc_mbir2d_batch": (i32, [vp, C.POINTER(Job2D), i32, C.POINTER(ReconParamsC), i32,
+                              C.POINTER(SolverStats)]),
     "lc_profile_enable": (i32, [vp, i32]),
     "lc_kernel_launches": (C.c_long, []),
     "lc_sysmat2d_toeplitz_noalloc": (i32, [vp, vp, i32, vp, vp, i32, i32]),

@@ -53,12 +53,19 @@ struct KArgs {
     long blocks_per_outer;
 };
 
+struct FFTBatchItem {
+    KArgs a;
+    FFTPlan pl;
+    long first_block;
+    const int *skip;
+};
+
 // One CTA transforms C = 1 << logC lines.  Rows (n_inner == 1) are C
 // consecutive lines, each contiguous in memory, walked line by line so that
 // consecutive threads touch consecutive addresses; otherwise the CTA takes C
 // adjacent inner indices c of one outer index o and consecutive threads walk c.
 template <typename T, typename TI, typename TO>
-__global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
+__device__ __forceinline__ void axis_fft_body(const KArgs &a, const FFTPlan &pl, long bid) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using V = cx<T>;
     const int logC = a.logC;
@@ -75,11 +82,11 @@ __global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
     const bool rows = (a.n_inner == 1);
     long o_base, c_base;
     if (rows) {
-        o_base = (long)blockIdx.x << logC;
+        o_base = bid << logC;
         c_base = 0;
     } else {
-        o_base = (long)blockIdx.x / a.blocks_per_outer;
-        c_base = ((long)blockIdx.x % a.blocks_per_outer) << logC;
+        o_base = bid / a.blocks_per_outer;
+        c_base = (bid % a.blocks_per_outer) << logC;
     }
     // lines of this CTA that exist
     const int nlines = rows ? (int)min((long)C, a.n_outer - o_base) : (int)min((long)C, a.n_inner - c_base);
@@ -288,6 +295,28 @@ __global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
 }
 
 template <typename T, typename TI, typename TO>
+__global__ void axis_fft_kernel(KArgs a, FFTPlan pl) {
+    axis_fft_body<T, TI, TO>(a, pl, (long)blockIdx.x);
+}
+
+// One launch over many FP32 transforms: CTA b runs block b - first_block of
+// the item whose range holds b (items sorted by first_block); an item whose
+// skip flag is set (a finished job) does nothing.
+template <typename TI, typename TO>
+__global__ void axis_fft_batch_kernel(const FFTBatchItem *__restrict__ items, int nitems) {
+    const long b = (long)blockIdx.x;
+    int lo = 0, hi = nitems - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].first_block <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const FFTBatchItem &it = items[lo];
+    if (it.skip && *it.skip) return;
+    axis_fft_body<float, TI, TO>(it.a, it.pl, b - it.first_block);
+}
+
+template <typename T, typename TI, typename TO>
 void launch_t(Context &ctx, const KArgs &ka, const FFTPlan &pl, int threads, size_t smem,
               long blocks) {
     auto kern = axis_fft_kernel<T, TI, TO>;
@@ -491,6 +520,89 @@ TuneVal autotune(Context &ctx, const AxisFFT &a0, const FFTPlan &pl) {
 }
 
 }  // namespace
+
+// ---- batched launches ------------------------------------------------------
+// A CTA of a batched launch holds at most this many elements per buffer
+// (lines x length), except that column transforms keep at least two lines.
+constexpr int kBatchElems = 4096;
+constexpr int kBatchThreads = 256;
+
+struct AxisFFTBatch::Impl {
+    std::vector<FFTBatchItem> items;
+    DevBuf<FFTBatchItem> dev;
+    size_t smem = 0;
+    long blocks = 0;
+    int in_real = -1, out_real = -1;
+};
+
+AxisFFTBatch::AxisFFTBatch() : impl_(new Impl) {}
+AxisFFTBatch::~AxisFFTBatch() = default;
+bool AxisFFTBatch::empty() const { return impl_->items.empty(); }
+long AxisFFTBatch::blocks() const { return impl_->blocks; }
+
+void AxisFFTBatch::add(Context &ctx, const AxisFFT &a, const int *skip) {
+    LC_REQUIRE(!a.fp64 && !a.cg && a.lines_per_cta == 0, "batched axis FFT: FP32 transforms without CG fusion");
+    LC_REQUIRE((a.in_t == E_F32 || a.in_t == E_C64) && (a.out_t == E_F32 || a.out_t == E_C64),
+               "batched axis FFT: float or float2 elements only");
+    const int ir = a.in_t == E_F32, orl = a.out_t == E_F32;
+    LC_REQUIRE(impl_->in_real < 0 || (impl_->in_real == ir && impl_->out_real == orl),
+               "batched axis FFT: all transforms of a batch share their element types");
+    LC_REQUIRE(is_smooth23(a.L), "batched axis FFT: lengths must be 2^p 3^q");
+    if (a.in_map == IN_HERM) LC_REQUIRE(a.n_in == a.L / 2 + 1, "IN_HERM needs n_in = L/2+1");
+    else if (a.in_map != IN_C2R_PACK) LC_REQUIRE(a.n_in <= (a.in_map == IN_REAL_PACKED ? 2 * a.L : a.L), "axis FFT: n_in > L");
+    LC_REQUIRE(!a.mid || a.n_inner > 1, "axis FFT: a spectral multiply needs column lines");
+    if (a.n_outer <= 0 || a.n_inner <= 0 || a.n_out == 0) return;
+    impl_->in_real = ir;
+    impl_->out_real = orl;
+    int logC = 0;
+    if (a.n_inner == 1) {
+        while ((a.L << (logC + 1)) <= kBatchElems && (1L << (logC + 1)) <= a.n_outer) ++logC;
+    } else {
+        while (logC < 4 && (1L << (logC + 1)) <= 2 * a.n_inner &&
+               ((a.L << (logC + 1)) <= kBatchElems || logC == 0))
+            ++logC;
+    }
+    const size_t need = 2 * ((size_t)a.L << logC) * sizeof(float2);
+    LC_REQUIRE(need <= ctx.max_smem(), "batched axis FFT: line does not fit shared memory");
+    FFTBatchItem it{};
+    long nb = 0;
+    it.a = make_kargs(a, logC, nb);
+    it.pl = ctx.plans().get(a.L, false, ctx.stream());
+    it.first_block = impl_->blocks;
+    it.skip = skip;
+    impl_->items.push_back(it);
+    impl_->blocks += nb;
+    impl_->smem = std::max(impl_->smem, need);
+    LC_REQUIRE(impl_->blocks < (1L << 31), "batched axis FFT: grid too large");
+}
+
+template <typename TI, typename TO>
+static void batch_launch_t(const Context &ctx, const FFTBatchItem *items, int n, long blocks, size_t smem) {
+    axis_fft_batch_kernel<TI, TO><<<(unsigned)blocks, kBatchThreads, smem, ctx.stream()>>>(items, n);
+    LC_CHECK_LAUNCH();
+}
+
+void AxisFFTBatch::finalize(Context &ctx) {
+    if (impl_->items.empty()) return;
+    impl_->dev.upload(impl_->items.data(), impl_->items.size(), ctx.stream());
+    // the shared-memory limit is set here, outside any stream capture
+    if (impl_->in_real && impl_->out_real) allow_max_dynamic_smem(ctx, axis_fft_batch_kernel<float, float>);
+    else if (impl_->in_real) allow_max_dynamic_smem(ctx, axis_fft_batch_kernel<float, float2>);
+    else if (impl_->out_real) allow_max_dynamic_smem(ctx, axis_fft_batch_kernel<float2, float>);
+    else allow_max_dynamic_smem(ctx, axis_fft_batch_kernel<float2, float2>);
+}
+
+void AxisFFTBatch::launch(Context &ctx) const {
+    if (impl_->items.empty()) return;
+    LC_REQUIRE(impl_->dev.size() == impl_->items.size(), "batched axis FFT: finalize() before launch()");
+    const FFTBatchItem *d = impl_->dev.get();
+    const int n = (int)impl_->items.size();
+    if (impl_->in_real && impl_->out_real) batch_launch_t<float, float>(ctx, d, n, impl_->blocks, impl_->smem);
+    else if (impl_->in_real) batch_launch_t<float, float2>(ctx, d, n, impl_->blocks, impl_->smem);
+    else if (impl_->out_real) batch_launch_t<float2, float>(ctx, d, n, impl_->blocks, impl_->smem);
+    else batch_launch_t<float2, float2>(ctx, d, n, impl_->blocks, impl_->smem);
+}
+
 
 // LC_LINE_KERNELS=0 routes every transform through the generic kernel (for
 // A/B timing of the register-plan line kernels).
@@ -744,6 +856,7 @@ struct BArgs {
 template <typename TI, typename TO>
 __global__ void bluestein_kernel(BArgs a, FFTPlan pl) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    const long bid = (long)blockIdx.x;
     const int logC = a.logC, C = 1 << logC, L = a.L, n = a.n;
     float2 *buf = reinterpret_cast<float2 *>(smem_raw);
     float2 *alt = buf + ((long)L << logC);
@@ -753,11 +866,11 @@ __global__ void bluestein_kernel(BArgs a, FFTPlan pl) {
     const bool rows = (a.n_inner == 1);
     long o_base, c_base;
     if (rows) {
-        o_base = (long)blockIdx.x << logC;
+        o_base = bid << logC;
         c_base = 0;
     } else {
-        o_base = (long)blockIdx.x / a.blocks_per_outer;
-        c_base = ((long)blockIdx.x % a.blocks_per_outer) << logC;
+        o_base = bid / a.blocks_per_outer;
+        c_base = (bid % a.blocks_per_outer) << logC;
     }
     const int nlines = rows ? (int)min((long)C, a.n_outer - o_base) : (int)min((long)C, a.n_inner - c_base);
     for (int idx = tid; idx < ((L - n) << logC); idx += nt)

@@ -8,6 +8,8 @@
 //    transforms whose lengths are odd.
 #pragma once
 
+#include <memory>
+
 #include "lc_cgstate.hpp"
 #include "lc_runtime.hpp"
 
@@ -67,6 +69,31 @@ struct AxisFFT {
     // kFusedDot on OUT_REAL_UNPACK rows, whose output is then A p
     const CGFusion *cg = nullptr;
     unsigned cg_parts = 0;
+};
+
+// Many FP32 transforms with one element-type pairing (float or float2 in and
+// out) as one launch of the generic kernel: each keeps its own length
+// (2^p 3^q), plan, index maps, strides, spectral multiply and lines per CTA;
+// all share the CTA size and the dynamic shared memory of the largest.  An
+// optional per-transform flag (device int, nonzero = skip) lets finished jobs
+// drop out without rebuilding the batch.  add() the transforms, finalize()
+// once (uploads the table on the context stream), then launch() as often as
+// needed: launch() only launches, so it can be captured into a graph.
+class AxisFFTBatch {
+  public:
+    AxisFFTBatch();
+    ~AxisFFTBatch();
+    AxisFFTBatch(const AxisFFTBatch &) = delete;
+    AxisFFTBatch &operator=(const AxisFFTBatch &) = delete;
+    void add(Context &ctx, const AxisFFT &a, const int *skip = nullptr);
+    void finalize(Context &ctx);
+    void launch(Context &ctx) const;
+    bool empty() const;
+    long blocks() const;
+
+  private:
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
 };
 
 // CTAs of a real row pass over n_lines lines (the partials a fused dot needs)

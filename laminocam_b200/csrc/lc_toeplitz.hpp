@@ -54,6 +54,8 @@ class Toeplitz {
     long stored_spectrum_elems() const { return (long)(zfold_ ? P_[0] / 2 + 1 : P_[0]) * P_[1] * Ph_[2]; }
     bool spectrum_zfold() const { return zfold_; }
     const float *spectrum() const { return R_->get(); }
+    // factor of the last pass: 1 / (P1 P2 P3 n2 n3) (3D) or 1 / (P^2 n) (2D)
+    double scale() const { return scale_; }
     size_t device_bytes() const {
         return spectrum_bytes() + (t1_.size() + t2_.size()) * sizeof(float2);
     }

@@ -8,6 +8,13 @@
 //   ref_bench check_fft   <in.f64> <out.f64>   FFTW-shim transform (tests)
 //   ref_bench check_nufft <in.f64> <out.f64>   FINUFFT-shim transform (tests)
 //   ref_bench lamino <phantom.f32> <n1> <n2> <n3> <nangles> <gamma_deg> <warmup> <steps> [full]
+//   ref_prec  forward2d  <in.f64> <out.f64>     forward2d in double (tol 1e-12)
+//   ref_prec  precision2d <in.f64> <out.f64>    backproj2d, sysmat2d(x, PSF), CG and
+//                                               Split-Bregman in double, for the
+//                                               precision study
+// (ref_prec is this file built with -DLC_GPU_STENCIL: the zero-padded finite
+// differences of the reference's GPU build, gpu_stencil.h, in place of
+// src/finitediff.cpp, whose interior-only stencil vanishes on single slices.)
 //
 // lamino: the laminography Split-Bregman workload in float, the reference's
 // CPU precision.  Projections are the reference's own forward() of the given
@@ -42,6 +49,10 @@
 #include "recon_params.h"
 #include "toeplitz.h"
 #include "tomocam.h"
+#include "toeplitz2d.h"
+#ifdef LC_GPU_STENCIL
+#include "gpu_stencil.h"
+#endif
 
 using namespace tomocam;
 
@@ -225,9 +236,11 @@ int main(int argc, char **argv) {
     }
     try {
         const std::string op = argv[1];
-        if (op == "lamino") {
+        if (op == "lamino" || op == "forward2d" || op == "precision2d") {
             // the reference prints per-iteration progress; keep stdout for the JSON lines
             std::cout.setstate(std::ios::failbit);
+        }
+        if (op == "lamino") {
             return lamino(argc, argv);
         }
         if (argc != 4) throw std::runtime_error("expected <in> <out>");
@@ -241,6 +254,37 @@ int main(int argc, char **argv) {
             int sign = (int)v[pos++];
             out = prec ? check_fft_t<double>(v, pos, kind, rank, n.data(), sign)
                        : check_fft_t<float>(v, pos, kind, rank, n.data(), sign);
+        } else if (op == "forward2d") {  // n nth nr theta[nth] vol[n n] -> sino[nth nr]
+            const size_t n = (size_t)v[pos++], nth = (size_t)v[pos++], nr = (size_t)v[pos++];
+            std::vector<double> th(v.begin() + pos, v.begin() + pos + nth);
+            pos += nth;
+            Array<double> vol(dims_t{1, n, n});
+            for (size_t i = 0; i < n * n; ++i) vol[i] = v[pos + i];
+            cpu::PolarGrid2D<double> pg(th, nr);
+            Array<double> s = forward2d(vol, pg);
+            out.assign(s.begin(), s.end());
+        } else if (op == "precision2d") {
+            // n nth nr cg_iters sb_outer sb_inner lam mu theta[nth] sino[nth nr] xprobe[n n]
+            //   -> rhs, A^T A xprobe (Toeplitz), CG recon, Split-Bregman recon (each n n)
+            const size_t n = (size_t)v[pos++], nth = (size_t)v[pos++], nr = (size_t)v[pos++];
+            const size_t cg_iters = (size_t)v[pos++], sb_outer = (size_t)v[pos++], sb_inner = (size_t)v[pos++];
+            const double lam = v[pos++], mu = v[pos++];
+            std::vector<double> th(v.begin() + pos, v.begin() + pos + nth);
+            pos += nth;
+            Array<double> sino(dims_t{1, nth, nr}), xp(dims_t{1, n, n});
+            for (size_t i = 0; i < nth * nr; ++i) sino[i] = v[pos + i];
+            pos += nth * nr;
+            for (size_t i = 0; i < n * n; ++i) xp[i] = v[pos + i];
+            cpu::PolarGrid2D<double> pg(th, nr);
+            const dims_t rd{1, n, n};
+            Array<double> rhs = backproj2d(sino, pg, rd);
+            cpu::PointSpreadFunction2D<double> psf(pg, n);
+            opt::Function<double> A = [&psf](const Array<double> &x) { return sysmat2d(x, psf); };
+            Array<double> ax = A(xp);
+            auto x0 = Array<double>::zeros(rd);
+            Array<double> cg = opt::cgsolver<double>(A, rhs, x0, cg_iters, 0.0, 0.0);
+            Array<double> sb = opt::split_bregman<double>(A, rhs, x0, lam, mu, sb_outer, sb_inner, 0.0, 0.0);
+            for (const Array<double> *a : {&rhs, &ax, &cg, &sb}) out.insert(out.end(), a->begin(), a->end());
         } else if (op == "check_nufft") {
             int type = (int)v[pos++], dim = (int)v[pos++];
             int64_t nm[3] = {(int64_t)v[pos], (int64_t)v[pos + 1], (int64_t)v[pos + 2]};
