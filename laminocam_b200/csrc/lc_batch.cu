@@ -1,24 +1,31 @@
 // Cross-job batching of unregularised 2D CG reconstructions: the jobs of a
 // batch (one slice each, any image size n and angle count) iterate in
-// lockstep, and every stage of an iteration is ONE launch over all of them.
+// lockstep, and every stage of an iteration is launched once for the whole
+// batch, or once per Toeplitz grid size P for the FFT passes.
 //
 // The reference solves slices one at a time: include/gpu/nufft.h:92-95 runs
 // one cuFINUFFT execute per slice, include/gpu/toeplitz2d.h:68-76 one Thrust
 // multiply per slice, src/gpu/conjgrad.cu:45-108 a handful of launches and
-// host syncs per iteration per job.  Here an iteration is six launches for
-// the whole batch:
-//   p = r + beta p                     work list of (job, chunk) items
-//   Toeplitz x rows (R2C)              AxisFFTBatch: (job, row group) CTAs
-//   Toeplitz y columns x spectrum      AxisFFTBatch: (job, column group) CTAs
-//   Toeplitz x rows (C2R, scaled)      AxisFFTBatch
-//   p.Ap and alpha                     (job, chunk) items
-//   x += alpha p, r -= alpha Ap, beta  (job, chunk) items
+// host syncs per iteration per job.  Here an iteration is:
+//   p = r + beta p                      one launch, (job, chunk) work items
+//   per grid size P, in parallel graph branches, over the jobs of that P:
+//     Toeplitz x rows (R2C)             one launch, (job, row group) CTAs
+//     Toeplitz y columns x spectrum     one launch, (job, column group) CTAs
+//     Toeplitz x rows (C2R, scaled)     one launch
+//   p.Ap and alpha                      one launch, (job, chunk) items
+//   x += alpha p, r -= alpha Ap, beta   one launch, (job, chunk) items
+// The FFT passes use the register-plan row and column kernels (batched over
+// an item table) where a plan covers P, else the generic shared-memory kernel
+// (AxisFFTBatch); a launch per P keeps the compile-time plan of those
+// kernels, and the branches run concurrently.
+//
 // Every job keeps its own FP64 scalars (CGState) and stopping tests in device
 // memory; a job whose test fired, or whose iteration budget is spent, turns
 // the later launches into no-ops for its CTAs.  Each job's reductions are
 // per-chunk FP64 partials summed by the job's last CTA (a per-job ticket) in
-// chunk order, and the chunking depends on the job's size alone, so a job's
-// result is bit-for-bit the same whatever else is in the batch.
+// chunk order, and the chunking and FFT kernels depend on the job's size
+// alone, so a job's result is bit-for-bit the same whatever else is in the
+// batch.
 //
 // The setup of every job (sinogram upload, bin sort, backprojection, FP64
 // PSF) runs on a pool of worker contexts, each with its own stream; the
@@ -28,6 +35,7 @@
 #include <atomic>
 #include <cmath>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -35,6 +43,27 @@
 #include "lc_internal.hpp"
 #include "lc_solver.hpp"
 #include "lc_toeplitz.hpp"
+
+// Host time of the setup phases (geometry, backprojection queued, PSF
+// queued, stream drained), summed over jobs, printed to stderr when the
+// library is built with -DLC_BATCH_TRACE (a profiling build).
+#ifdef LC_BATCH_TRACE
+#include <chrono>
+#include <cstdio>
+static double g_batch_t[4];
+static std::mutex g_batch_mu;
+#define LC_BATCH_T0() auto lc_bt_prev = std::chrono::steady_clock::now()
+#define LC_BATCH_T(k)                                                                          \
+    do {                                                                                       \
+        auto lc_bt_now = std::chrono::steady_clock::now();                                     \
+        std::lock_guard<std::mutex> lc_bt_lk(g_batch_mu);                                      \
+        g_batch_t[k] += std::chrono::duration<double, std::milli>(lc_bt_now - lc_bt_prev).count(); \
+        lc_bt_prev = lc_bt_now;                                                                \
+    } while (0)
+#else
+#define LC_BATCH_T0() ((void)0)
+#define LC_BATCH_T(k) ((void)0)
+#endif
 
 namespace lc {
 
@@ -247,7 +276,6 @@ class BatchCG2D {
         for (int j = 0; j < J; ++j) {
             const Toeplitz &T = *jobs_[j].T;
             LC_REQUIRE(!T.three_d() && T.dims()[0] == 1, "batch: 2D operators of one slice only");
-            LC_REQUIRE(T.P()[2] % 2 == 0, "batch: the Toeplitz grid must be even");
             const long n = T.nvox();
             voff[j] = vtot;
             vtot += (n + 3) & ~3L;  // 16-byte aligned vectors
@@ -282,15 +310,34 @@ class BatchCG2D {
             v.xtol = jobs_[j].xtol;
             for (int c = 0; c < v.nchunks; ++c) items.push_back(make_int2(j, c));
             part0 += v.nchunks;
-            add_toeplitz(ctx, T, v.p, v.ap, h_.get() + hoff[j], &st_.get()[j].done);
+            Group &g = group_for(T.P()[2]);
+            add_toeplitz(ctx, g, T, v.p, v.ap, h_.get() + hoff[j], &st_.get()[j].done);
         }
         vjobs_.upload(vj.data(), J, s);
         items_.upload(items.data(), items.size(), s);
         nitems_ = (int)items.size();
-        rows_fwd_.finalize(ctx);
-        cols_.finalize(ctx);
-        rows_inv_.finalize(ctx);
-        host_vj_ = std::move(vj);
+        for (auto &g : groups_)
+            for (Stage *st : {&g->fwd, &g->col, &g->inv}) st->finalize(ctx);
+        // side streams of the per-grid branches (created here, outside any capture)
+        const int nside = (int)std::min<size_t>(groups_.size(), 8);
+        side_.resize(nside, nullptr);
+        join_.resize(nside, nullptr);
+        for (int i = 0; i < nside; ++i) {
+            LC_CUDA(cudaStreamCreateWithFlags(&side_[i], cudaStreamNonBlocking));
+            LC_CUDA(cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming));
+        }
+        LC_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    }
+
+    ~BatchCG2D() {
+        for (cudaStream_t x : side_)
+            if (x) {
+                cudaStreamSynchronize(x);
+                cudaStreamDestroy(x);
+            }
+        for (cudaEvent_t e : join_)
+            if (e) cudaEventDestroy(e);
+        if (fork_) cudaEventDestroy(fork_);
     }
 
     // Runs every job to its stopping test or iteration budget.
@@ -311,15 +358,14 @@ class BatchCG2D {
             const int k = std::min(chunk, maxit - done);
             if (use_graph && k == chunk) {
                 if (!graph.ready()) {
-                    ctx.set_stream(ctx.capture_stream());
-                    graph.capture(ctx.capture_stream(), [&] {
-                        for (int i = 0; i < chunk; ++i) iteration(ctx);
+                    const cudaStream_t cs = ctx.capture_stream();
+                    graph.capture(cs, [&] {
+                        for (int i = 0; i < chunk; ++i) iteration(cs);
                     });
-                    ctx.set_stream(s);
                 }
                 graph.launch(s);
             } else {
-                for (int i = 0; i < k; ++i) iteration(ctx);
+                for (int i = 0; i < k; ++i) iteration(s);
             }
             if (poll && done + k < maxit) {
                 std::vector<CGState> hs(jobs_.size());
@@ -337,16 +383,57 @@ class BatchCG2D {
         LC_CUDA(cudaStreamSynchronize(s));
     }
 
-    long launches_per_iteration() const { return 6; }
-
   private:
-    void iteration(Context &ctx) {
-        cudaStream_t s = ctx.stream();
+    // one FFT pass of the jobs of one grid size: the register-plan kernels
+    // when a plan covers it, else the generic kernel
+    struct Stage {
+        RegLineBatch reg;
+        AxisFFTBatch gen;
+        bool generic = false;
+        void add(Context &ctx, const AxisFFT &a, const int *skip) {
+            if (!generic && reg.add(a, skip)) return;
+            LC_REQUIRE(reg.empty(), "batch: the jobs of one grid size take different kernels");
+            generic = true;
+            gen.add(ctx, a, skip);
+        }
+        void finalize(Context &ctx) {
+            if (generic) gen.finalize(ctx);
+            else reg.finalize(ctx);
+        }
+        void launch(cudaStream_t st) const {
+            if (generic) gen.launch(st);
+            else reg.launch(st);
+        }
+    };
+    struct Group {
+        int P = 0;
+        Stage fwd, col, inv;
+    };
+
+    Group &group_for(int P) {
+        for (auto &g : groups_)
+            if (g->P == P) return *g;
+        groups_.emplace_back(new Group);
+        groups_.back()->P = P;
+        return *groups_.back();
+    }
+
+    void iteration(cudaStream_t s) {
         batch_p_update_kernel<<<nitems_, kVecThreads, 0, s>>>(vjobs_.get(), items_.get(), st_.get());
         LC_CHECK_LAUNCH();
-        rows_fwd_.launch(ctx);
-        cols_.launch(ctx);
-        rows_inv_.launch(ctx);
+        // the grid sizes' Toeplitz passes as parallel branches
+        LC_CUDA(cudaEventRecord(fork_, s));
+        for (size_t i = 0; i < side_.size(); ++i) LC_CUDA(cudaStreamWaitEvent(side_[i], fork_, 0));
+        for (size_t g = 0; g < groups_.size(); ++g) {
+            const cudaStream_t b = side_[g % side_.size()];
+            groups_[g]->fwd.launch(b);
+            groups_[g]->col.launch(b);
+            groups_[g]->inv.launch(b);
+        }
+        for (size_t i = 0; i < side_.size(); ++i) {
+            LC_CUDA(cudaEventRecord(join_[i], side_[i]));
+            LC_CUDA(cudaStreamWaitEvent(s, join_[i], 0));
+        }
         batch_dot_kernel<<<nitems_, kVecThreads, 0, s>>>(vjobs_.get(), items_.get(), st_.get(), part_.get(),
                                                          counters_.get());
         LC_CHECK_LAUNCH();
@@ -355,11 +442,15 @@ class BatchCG2D {
         LC_CHECK_LAUNCH();
     }
 
-    // the three passes of the 2D Toeplitz apply (lc_toeplitz.cu) as items of
-    // the three batched launches
-    void add_toeplitz(Context &ctx, const Toeplitz &T, const float *p, float *ap, float2 *h, const int *skip) {
+    // The three passes of the 2D Toeplitz apply (lc_toeplitz.cu) as items of
+    // the group's three launches.  Real rows of an even grid run as complex
+    // rows of half the length (even/odd packing), of an odd grid (3^q) as
+    // complex rows of the full length.
+    void add_toeplitz(Context &ctx, Group &g, const Toeplitz &T, const float *p, float *ap, float2 *h,
+                      const int *skip) {
         const long n = T.dims()[1];
         const int P = T.P()[2], Ph = P / 2 + 1;
+        const bool even = P % 2 == 0;
         AxisFFT a;
         a.in = p;
         a.in_t = E_F32;
@@ -370,12 +461,12 @@ class BatchCG2D {
         a.in_ostride = n;
         a.out_ostride = Ph;
         a.n_in = (int)n;
-        a.L = P / 2;
+        a.L = even ? P / 2 : P;
         a.n_out = Ph;
-        a.in_map = IN_REAL_PACKED;
-        a.out_map = OUT_R2C_UNPACK;
+        a.in_map = even ? IN_REAL_PACKED : IN_DIRECT;
+        a.out_map = even ? OUT_R2C_UNPACK : OUT_DIRECT;
         a.sign = -1;
-        rows_fwd_.add(ctx, a, skip);
+        g.fwd.add(ctx, a, skip);
         AxisFFT b;
         b.in = h;
         b.in_t = E_C64;
@@ -394,7 +485,7 @@ class BatchCG2D {
         b.mid = T.spectrum();
         b.mid_ra = Ph;
         b.sign2 = +1;
-        cols_.add(ctx, b, skip);
+        g.col.add(ctx, b, skip);
         AxisFFT c;
         c.in = h;
         c.in_t = E_C64;
@@ -405,18 +496,17 @@ class BatchCG2D {
         c.in_ostride = Ph;
         c.out_ostride = n;
         c.n_in = Ph;
-        c.L = P / 2;
+        c.L = even ? P / 2 : P;
         c.n_out = (int)n;
-        c.in_map = IN_C2R_PACK;
-        c.out_map = OUT_REAL_UNPACK;
+        c.in_map = even ? IN_C2R_PACK : IN_HERM;
+        c.out_map = even ? OUT_REAL_UNPACK : OUT_WINDOW;
         c.out_off = 0;
         c.sign = +1;
         c.scale = T.scale();
-        rows_inv_.add(ctx, c, skip);
+        g.inv.add(ctx, c, skip);
     }
 
     std::vector<Job> jobs_;
-    std::vector<VecJob> host_vj_;
     DevBuf<float> vec_;
     DevBuf<float2> h_;
     DevBuf<CGState> st_;
@@ -425,7 +515,10 @@ class BatchCG2D {
     DevBuf<VecJob> vjobs_;
     DevBuf<int2> items_;
     int nitems_ = 0;
-    AxisFFTBatch rows_fwd_, cols_, rows_inv_;
+    std::vector<std::unique_ptr<Group>> groups_;
+    std::vector<cudaStream_t> side_;
+    std::vector<cudaEvent_t> join_;
+    cudaEvent_t fork_ = nullptr;
 };
 
 }  // namespace lc
@@ -448,10 +541,11 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
         cudaStream_t s = ctx.stream();
         const int nw = std::max(1, std::min(setup_workers > 0 ? setup_workers : 8, njobs));
         // per job: right-hand side and Toeplitz operator, built on the workers
-        std::vector<std::unique_ptr<lc_context_s>> wctx(nw);
-        for (int w = 0; w < nw; ++w) {
-            wctx[w].reset(new lc_context_s);
-            wctx[w]->ctx = std::make_shared<Context>(ctx.device(), nullptr);
+        // (contexts kept in the caller's context for later calls)
+        auto &wctx = c->batch_workers;
+        while ((int)wctx.size() < nw) {
+            wctx.emplace_back(new lc_context_s);
+            wctx.back()->ctx = std::make_shared<Context>(ctx.device(), nullptr);
         }
         std::vector<DevBuf<float>> rhs(njobs), xs(njobs);
         std::vector<std::shared_ptr<Toeplitz>> ops(njobs);
@@ -464,6 +558,7 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
             for (int j = next++; j < njobs; j = next++) {
                 const lc_job2d &q = jobs[j];
                 const int rc = run_guarded(errs[j], [&] {
+                    LC_BATCH_T0();
                     cudaStream_t ws = wx.stream();
                     DevBuf<float> dsino;
                     dsino.upload(q.sinogram, (size_t)q.ntheta * q.nradial, ws);
@@ -471,23 +566,36 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
                     const int grc = lc_geometry2d_create(wc, q.theta, q.ntheta, q.nradial, &g);
                     if (grc) throw Error(grc == LC_ERR_INVALID ? 1 : 3, wc->err);
                     std::unique_ptr<lc_geometry_s> gown(g);
+                    LC_BATCH_T(0);
                     const long nv = (long)q.n * q.n;
                     rhs[j].alloc(nv, ws);
                     xs[j].alloc(nv, ws);
                     LC_CUDA(cudaMemsetAsync(xs[j].get(), 0, nv * sizeof(float), ws));
                     const int brc = lc_backproj2d(wc, g, dsino.get(), 1, q.n, q.n, rhs[j].get(), p->nufft_tol);
                     if (brc) throw Error(brc == LC_ERR_INVALID ? 1 : 3, wc->err);
+                    LC_BATCH_T(1);
                     const long dims[3] = {1, q.n, q.n};
                     ops[j] = std::make_shared<Toeplitz>(wx, g->g, dims, false);
+                    LC_BATCH_T(2);
                     LC_CUDA(cudaStreamSynchronize(ws));
+                    LC_BATCH_T(3);
                 });
                 if (rc && errs[j].empty()) errs[j] = "setup failed";
             }
         };
+#ifdef LC_BATCH_TRACE
+        for (double &v : g_batch_t) v = 0;
+        const auto lc_t0 = std::chrono::steady_clock::now();
+#endif
         std::vector<std::thread> th;
         for (int w = 1; w < nw; ++w) th.emplace_back(work, w);
         work(0);
         for (auto &t : th) t.join();
+#ifdef LC_BATCH_TRACE
+        std::fprintf(stderr, "batch setup wall %.2f ms; summed over jobs: geometry %.2f backproj %.2f psf %.2f drain %.2f\n",
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - lc_t0).count(),
+                     g_batch_t[0], g_batch_t[1], g_batch_t[2], g_batch_t[3]);
+#endif
         for (int j = 0; j < njobs; ++j)
             if (!errs[j].empty()) throw Error(1, "job " + std::to_string(j) + ": " + errs[j]);
         std::vector<BatchCG2D::Job> bj(njobs);
@@ -515,6 +623,6 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
         for (auto &o : ops) o.reset();
         for (auto &b : rhs) b.release();
         for (auto &b : xs) b.release();
-        for (auto &w : wctx) LC_CUDA(cudaStreamSynchronize(w->ctx->stream()));
+        for (int w = 0; w < nw; ++w) LC_CUDA(cudaStreamSynchronize(wctx[w]->ctx->stream()));
     });
 }

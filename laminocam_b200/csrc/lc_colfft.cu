@@ -19,6 +19,8 @@
 // n <= P/2 values and the cropped result keeps n.  Both halves go through the
 // same thread as two independent instruction streams.
 #include <atomic>
+#include <cstring>
+#include <vector>
 
 #include "lc_fft.hpp"
 #include "lc_regfft.cuh"
@@ -57,8 +59,7 @@ constexpr int col_min_blocks() {
 }
 
 template <int R0, int R1, int R2, int MODE>
-__global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kCols, (col_min_blocks<R0, R1, R2>()))
-    col_fft_kernel(ColArgs a) {
+__device__ __forceinline__ void col_fft_body(const ColArgs &a, long bid) {
     using P = RegPlan<R0, R1, R2>;
     constexpr int M = P::M, RM = P::RM, C = kCols;
     constexpr bool SPLIT = MODE >= CM_SPLIT_IN;
@@ -68,8 +69,8 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kCols, (col_min_block
     float2 *th = tw + M;               // exp(-pi i m / M)
     load_line_twiddles<M>(tw);
     const int c = threadIdx.x % C, t = threadIdx.x / C;
-    const long o = (long)blockIdx.x / a.bpo;
-    const long col = ((long)blockIdx.x - o * a.bpo) * C + c;
+    const long o = bid / a.bpo;
+    const long col = (bid - o * a.bpo) * C + c;
     const bool valid = col < a.n_inner;
     const long ni = a.n_inner;
     const float2 *in = a.in + o * a.in_ostride + col;
@@ -173,6 +174,59 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kCols, (col_min_block
 }
 
 template <int R0, int R1, int R2, int MODE>
+__global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kCols, (col_min_blocks<R0, R1, R2>()))
+    col_fft_kernel(ColArgs a) {
+    col_fft_body<R0, R1, R2, MODE>(a, (long)blockIdx.x);
+}
+
+// one launch over several column transforms of one plan and mode: CTA b runs
+// block b - first_block of the item whose range holds b
+struct ColBatchItem {
+    ColArgs a;
+    long first_block;
+    const int *skip;
+};
+
+template <int R0, int R1, int R2, int MODE>
+__global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kCols, (col_min_blocks<R0, R1, R2>()))
+    col_fft_batch_kernel(const ColBatchItem *__restrict__ items, int nitems) {
+    const long b = (long)blockIdx.x;
+    int lo = 0, hi = nitems - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].first_block <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    if (items[lo].skip && *items[lo].skip) return;
+    col_fft_body<R0, R1, R2, MODE>(items[lo].a, b - items[lo].first_block);
+}
+
+template <int R0, int R1, int R2, int MODE>
+void col_batch_configure() {
+    LC_CUDA(cudaFuncSetAttribute(col_fft_batch_kernel<R0, R1, R2, MODE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem<R0, R1, R2, MODE>()));
+}
+
+template <int R0, int R1, int R2, int MODE>
+void col_batch_launch(cudaStream_t st, const void *items, int n, long blocks) {
+    col_fft_batch_kernel<R0, R1, R2, MODE><<<(unsigned)blocks, RegPlan<R0, R1, R2>::NT * kCols,
+                                             col_smem<R0, R1, R2, MODE>(), st>>>(
+        static_cast<const ColBatchItem *>(items), n);
+    LC_CHECK_LAUNCH();
+}
+
+template <int R0, int R1, int R2>
+void col_batch_fns(int mode, RegBatchKey &k) {
+    switch (mode) {
+        case CM_PLAIN: k.launch = col_batch_launch<R0, R1, R2, CM_PLAIN>; k.configure = col_batch_configure<R0, R1, R2, CM_PLAIN>; break;
+        case CM_PLAIN_MID: k.launch = col_batch_launch<R0, R1, R2, CM_PLAIN_MID>; k.configure = col_batch_configure<R0, R1, R2, CM_PLAIN_MID>; break;
+        case CM_SPLIT_IN: k.launch = col_batch_launch<R0, R1, R2, CM_SPLIT_IN>; k.configure = col_batch_configure<R0, R1, R2, CM_SPLIT_IN>; break;
+        case CM_SPLIT_OUT: k.launch = col_batch_launch<R0, R1, R2, CM_SPLIT_OUT>; k.configure = col_batch_configure<R0, R1, R2, CM_SPLIT_OUT>; break;
+        default: k.launch = col_batch_launch<R0, R1, R2, CM_SPLIT_MID>; k.configure = col_batch_configure<R0, R1, R2, CM_SPLIT_MID>; break;
+    }
+}
+
+template <int R0, int R1, int R2, int MODE>
 void launch_mode(cudaStream_t st, const ColArgs &a, long blocks) {
     constexpr size_t smem = col_smem<R0, R1, R2, MODE>();
     auto kern = col_fft_kernel<R0, R1, R2, MODE>;
@@ -211,7 +265,9 @@ bool launch_plan_for(cudaStream_t st, int M, int mode, const ColArgs &a, long bl
 
 }  // namespace
 
-bool launch_col_fft(cudaStream_t st, const AxisFFT &a) {
+// The column plan of a transform: M and the mode, and its arguments; false
+// when no register plan covers it.
+static bool col_plan_args(const AxisFFT &a, int &M, int &mode, ColArgs &ca) {
     if (a.fp64 || a.in_t != E_C64 || a.out_t != E_C64 || a.n_inner <= 1) return false;
     if (a.in_map != IN_DIRECT) return false;
     if (!(a.out_map == OUT_DIRECT || (a.out_map == OUT_WINDOW && a.out_off == 0))) return false;
@@ -219,7 +275,8 @@ bool launch_col_fft(cudaStream_t st, const AxisFFT &a) {
     const int L = a.L;
     if (a.n_in < 0 || a.n_in > L || a.n_out < 0 || a.n_out > L) return false;
     const bool mid = a.mid != nullptr;
-    int M = L, mode = mid ? CM_PLAIN_MID : CM_PLAIN;
+    M = L;
+    mode = mid ? CM_PLAIN_MID : CM_PLAIN;
     if (L % 2 == 0 && line_plan_exists(L / 2)) {
         const int h = L / 2;
         if (mid && a.n_in <= h && a.n_out <= h) {
@@ -234,8 +291,6 @@ bool launch_col_fft(cudaStream_t st, const AxisFFT &a) {
         }
     }
     if (!line_plan_exists(M)) return false;
-    if (a.n_outer <= 0 || a.n_out == 0) return true;
-    ColArgs ca;
     ca.in = static_cast<const float2 *>(a.in);
     ca.out = static_cast<float2 *>(a.out);
     ca.n_inner = a.n_inner;
@@ -248,9 +303,40 @@ bool launch_col_fft(cudaStream_t st, const AxisFFT &a) {
     ca.sign2 = a.sign2;
     ca.spec = a.mid;
     ca.spec_ra = a.mid_ra;
+    return true;
+}
+
+bool launch_col_fft(cudaStream_t st, const AxisFFT &a) {
+    int M = 0, mode = 0;
+    ColArgs ca;
+    if (!col_plan_args(a, M, mode, ca)) return false;
+    if (a.n_outer <= 0 || a.n_out == 0) return true;
     const long blocks = a.n_outer * ca.bpo;
     LC_REQUIRE(blocks < (1L << 31), "column FFT: grid too large");
     return launch_plan_for(st, M, mode, ca, blocks);
+}
+
+bool col_batch_item(const AxisFFT &a, const int *skip, long first_block, RegBatchKey &key,
+                    std::vector<unsigned char> &item, long &blocks) {
+    int M = 0, mode = 0;
+    ColArgs ca;
+    if (!col_plan_args(a, M, mode, ca)) return false;
+    key.kind = 1;
+    key.M = M;
+    key.mode = mode;
+    key.item_size = sizeof(ColBatchItem);
+    switch (M) {
+#define LC_COL_BATCH_CASE(m, r0, r1, r2) \
+    case m: col_batch_fns<r0, r1, r2>(mode, key); break;
+        LC_LINE_PLANS(LC_COL_BATCH_CASE)
+#undef LC_COL_BATCH_CASE
+        default: return false;
+    }
+    blocks = a.n_outer * ca.bpo;
+    ColBatchItem it{ca, first_block, skip};
+    item.resize(sizeof it);
+    std::memcpy(item.data(), &it, sizeof it);
+    return true;
 }
 
 }  // namespace lc

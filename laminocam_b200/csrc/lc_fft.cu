@@ -524,21 +524,35 @@ TuneVal autotune(Context &ctx, const AxisFFT &a0, const FFTPlan &pl) {
 // ---- batched launches ------------------------------------------------------
 // A CTA of a batched launch holds at most this many elements per buffer
 // (lines x length), except that column transforms keep at least two lines.
-constexpr int kBatchElems = 4096;
-constexpr int kBatchThreads = 256;
+#ifndef LC_BATCH_ELEMS
+#define LC_BATCH_ELEMS 4096
+#endif
+#ifndef LC_BATCH_THREADS
+#define LC_BATCH_THREADS 256
+#endif
+constexpr int kBatchElems = LC_BATCH_ELEMS;
+constexpr int kBatchThreads = LC_BATCH_THREADS;
+// Items are launched in shared-memory classes (<= 32 KB, <= 64 KB, more per
+// CTA), so that small transforms keep several CTAs per SM beside large ones.
+constexpr size_t kBatchClassSmem[2] = {32 * 1024, 64 * 1024};
 
 struct AxisFFTBatch::Impl {
-    std::vector<FFTBatchItem> items;
-    DevBuf<FFTBatchItem> dev;
-    size_t smem = 0;
-    long blocks = 0;
+    struct Group {
+        std::vector<FFTBatchItem> items;
+        DevBuf<FFTBatchItem> dev;
+        size_t smem = 0;
+        long blocks = 0;
+    };
+    Group g[3];
     int in_real = -1, out_real = -1;
 };
 
 AxisFFTBatch::AxisFFTBatch() : impl_(new Impl) {}
 AxisFFTBatch::~AxisFFTBatch() = default;
-bool AxisFFTBatch::empty() const { return impl_->items.empty(); }
-long AxisFFTBatch::blocks() const { return impl_->blocks; }
+bool AxisFFTBatch::empty() const {
+    return impl_->g[0].items.empty() && impl_->g[1].items.empty() && impl_->g[2].items.empty();
+}
+long AxisFFTBatch::blocks() const { return impl_->g[0].blocks + impl_->g[1].blocks + impl_->g[2].blocks; }
 
 void AxisFFTBatch::add(Context &ctx, const AxisFFT &a, const int *skip) {
     LC_REQUIRE(!a.fp64 && !a.cg && a.lines_per_cta == 0, "batched axis FFT: FP32 transforms without CG fusion");
@@ -549,42 +563,51 @@ void AxisFFTBatch::add(Context &ctx, const AxisFFT &a, const int *skip) {
                "batched axis FFT: all transforms of a batch share their element types");
     LC_REQUIRE(is_smooth23(a.L), "batched axis FFT: lengths must be 2^p 3^q");
     if (a.in_map == IN_HERM) LC_REQUIRE(a.n_in == a.L / 2 + 1, "IN_HERM needs n_in = L/2+1");
-    else if (a.in_map != IN_C2R_PACK) LC_REQUIRE(a.n_in <= (a.in_map == IN_REAL_PACKED ? 2 * a.L : a.L), "axis FFT: n_in > L");
+    else if (a.in_map == IN_C2R_PACK) LC_REQUIRE(a.n_in == a.L + 1, "IN_C2R_PACK needs n_in = L+1");
+    else LC_REQUIRE(a.n_in <= (a.in_map == IN_REAL_PACKED ? 2 * a.L : a.L), "axis FFT: n_in > L");
+    if (a.out_map == OUT_WINDOW) LC_REQUIRE(a.out_off >= 0 && a.out_off + a.n_out <= a.L, "window");
+    else if (a.out_map == OUT_R2C_UNPACK) LC_REQUIRE(a.n_out <= a.L + 1, "axis FFT: n_out > L+1");
+    else if (a.out_map == OUT_REAL_UNPACK) LC_REQUIRE(a.n_out <= 2 * a.L, "axis FFT: n_out > 2L");
+    else LC_REQUIRE(a.n_out <= a.L, "axis FFT: n_out > L");
     LC_REQUIRE(!a.mid || a.n_inner > 1, "axis FFT: a spectral multiply needs column lines");
     if (a.n_outer <= 0 || a.n_inner <= 0 || a.n_out == 0) return;
     impl_->in_real = ir;
     impl_->out_real = orl;
     int logC = 0;
+    const size_t cap = std::min<size_t>(ctx.max_smem(), 160 * 1024);
+    auto fits = [&](int lc) { return 2 * ((size_t)a.L << lc) * sizeof(float2) <= cap; };
     if (a.n_inner == 1) {
         while ((a.L << (logC + 1)) <= kBatchElems && (1L << (logC + 1)) <= a.n_outer) ++logC;
     } else {
         while (logC < 4 && (1L << (logC + 1)) <= 2 * a.n_inner &&
-               ((a.L << (logC + 1)) <= kBatchElems || logC == 0))
+               ((a.L << (logC + 1)) <= kBatchElems || (logC == 0 && fits(1))))
             ++logC;
     }
     const size_t need = 2 * ((size_t)a.L << logC) * sizeof(float2);
     LC_REQUIRE(need <= ctx.max_smem(), "batched axis FFT: line does not fit shared memory");
+    Impl::Group &grp = impl_->g[need <= kBatchClassSmem[0] ? 0 : (need <= kBatchClassSmem[1] ? 1 : 2)];
     FFTBatchItem it{};
     long nb = 0;
     it.a = make_kargs(a, logC, nb);
     it.pl = ctx.plans().get(a.L, false, ctx.stream());
-    it.first_block = impl_->blocks;
+    it.first_block = grp.blocks;
     it.skip = skip;
-    impl_->items.push_back(it);
-    impl_->blocks += nb;
-    impl_->smem = std::max(impl_->smem, need);
-    LC_REQUIRE(impl_->blocks < (1L << 31), "batched axis FFT: grid too large");
+    grp.items.push_back(it);
+    grp.blocks += nb;
+    grp.smem = std::max(grp.smem, need);
+    LC_REQUIRE(grp.blocks < (1L << 31), "batched axis FFT: grid too large");
 }
 
 template <typename TI, typename TO>
-static void batch_launch_t(const Context &ctx, const FFTBatchItem *items, int n, long blocks, size_t smem) {
-    axis_fft_batch_kernel<TI, TO><<<(unsigned)blocks, kBatchThreads, smem, ctx.stream()>>>(items, n);
+static void batch_launch_t(cudaStream_t st, const FFTBatchItem *items, int n, long blocks, size_t smem) {
+    axis_fft_batch_kernel<TI, TO><<<(unsigned)blocks, kBatchThreads, smem, st>>>(items, n);
     LC_CHECK_LAUNCH();
 }
 
 void AxisFFTBatch::finalize(Context &ctx) {
-    if (impl_->items.empty()) return;
-    impl_->dev.upload(impl_->items.data(), impl_->items.size(), ctx.stream());
+    for (Impl::Group &grp : impl_->g)
+        if (!grp.items.empty()) grp.dev.upload(grp.items.data(), grp.items.size(), ctx.stream());
+    if (empty()) return;
     // the shared-memory limit is set here, outside any stream capture
     if (impl_->in_real && impl_->out_real) allow_max_dynamic_smem(ctx, axis_fft_batch_kernel<float, float>);
     else if (impl_->in_real) allow_max_dynamic_smem(ctx, axis_fft_batch_kernel<float, float2>);
@@ -592,15 +615,60 @@ void AxisFFTBatch::finalize(Context &ctx) {
     else allow_max_dynamic_smem(ctx, axis_fft_batch_kernel<float2, float2>);
 }
 
-void AxisFFTBatch::launch(Context &ctx) const {
-    if (impl_->items.empty()) return;
-    LC_REQUIRE(impl_->dev.size() == impl_->items.size(), "batched axis FFT: finalize() before launch()");
-    const FFTBatchItem *d = impl_->dev.get();
-    const int n = (int)impl_->items.size();
-    if (impl_->in_real && impl_->out_real) batch_launch_t<float, float>(ctx, d, n, impl_->blocks, impl_->smem);
-    else if (impl_->in_real) batch_launch_t<float, float2>(ctx, d, n, impl_->blocks, impl_->smem);
-    else if (impl_->out_real) batch_launch_t<float2, float>(ctx, d, n, impl_->blocks, impl_->smem);
-    else batch_launch_t<float2, float2>(ctx, d, n, impl_->blocks, impl_->smem);
+struct RegLineBatch::Impl {
+    RegBatchKey key;
+    std::vector<unsigned char> items;
+    DevBuf<unsigned char> dev;
+    int n = 0;
+    long blocks = 0;
+};
+
+RegLineBatch::RegLineBatch() : impl_(new Impl) {}
+RegLineBatch::~RegLineBatch() = default;
+bool RegLineBatch::empty() const { return impl_->n == 0; }
+
+bool RegLineBatch::add(const AxisFFT &a, const int *skip) {
+    if (!line_kernels_enabled()) return false;
+    if (a.n_outer <= 0 || a.n_inner <= 0 || a.n_out == 0) return false;
+    RegBatchKey k;
+    std::vector<unsigned char> item;
+    long nb = 0;
+    const bool ok = a.n_inner == 1 ? row_batch_item(a, skip, impl_->blocks, k, item, nb)
+                                   : col_batch_item(a, skip, impl_->blocks, k, item, nb);
+    if (!ok) return false;
+    if (impl_->n > 0 && (k.kind != impl_->key.kind || k.M != impl_->key.M || k.mode != impl_->key.mode))
+        return false;
+    impl_->key = k;
+    impl_->items.insert(impl_->items.end(), item.begin(), item.end());
+    impl_->blocks += nb;
+    impl_->n += 1;
+    LC_REQUIRE(impl_->blocks < (1L << 31), "batched line FFT: grid too large");
+    return true;
+}
+
+void RegLineBatch::finalize(Context &ctx) {
+    if (impl_->n == 0) return;
+    impl_->dev.upload(impl_->items.data(), impl_->items.size(), ctx.stream());
+    impl_->key.configure();  // outside any stream capture
+}
+
+void RegLineBatch::launch(cudaStream_t st) const {
+    if (impl_->n == 0) return;
+    LC_REQUIRE(impl_->dev.size() == impl_->items.size(), "batched line FFT: finalize() before launch()");
+    impl_->key.launch(st, impl_->dev.get(), impl_->n, impl_->blocks);
+}
+
+void AxisFFTBatch::launch(cudaStream_t st) const {
+    for (const Impl::Group &grp : impl_->g) {
+        if (grp.items.empty()) continue;
+        LC_REQUIRE(grp.dev.size() == grp.items.size(), "batched axis FFT: finalize() before launch()");
+        const FFTBatchItem *d = grp.dev.get();
+        const int n = (int)grp.items.size();
+        if (impl_->in_real && impl_->out_real) batch_launch_t<float, float>(st, d, n, grp.blocks, grp.smem);
+        else if (impl_->in_real) batch_launch_t<float, float2>(st, d, n, grp.blocks, grp.smem);
+        else if (impl_->out_real) batch_launch_t<float2, float>(st, d, n, grp.blocks, grp.smem);
+        else batch_launch_t<float2, float2>(st, d, n, grp.blocks, grp.smem);
+    }
 }
 
 

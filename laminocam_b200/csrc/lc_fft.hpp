@@ -9,6 +9,7 @@
 #pragma once
 
 #include <memory>
+#include <vector>
 
 #include "lc_cgstate.hpp"
 #include "lc_runtime.hpp"
@@ -72,9 +73,10 @@ struct AxisFFT {
 };
 
 // Many FP32 transforms with one element-type pairing (float or float2 in and
-// out) as one launch of the generic kernel: each keeps its own length
+// out) as one launch of the generic kernel per shared-memory class (at most
+// three: up to 32 KB, 64 KB and more per CTA): each keeps its own length
 // (2^p 3^q), plan, index maps, strides, spectral multiply and lines per CTA;
-// all share the CTA size and the dynamic shared memory of the largest.  An
+// those of a class share the CTA size and the largest's shared memory.  An
 // optional per-transform flag (device int, nonzero = skip) lets finished jobs
 // drop out without rebuilding the batch.  add() the transforms, finalize()
 // once (uploads the table on the context stream), then launch() as often as
@@ -87,9 +89,46 @@ class AxisFFTBatch {
     AxisFFTBatch &operator=(const AxisFFTBatch &) = delete;
     void add(Context &ctx, const AxisFFT &a, const int *skip = nullptr);
     void finalize(Context &ctx);
-    void launch(Context &ctx) const;
+    void launch(cudaStream_t st) const;
     bool empty() const;
     long blocks() const;
+
+  private:
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+};
+
+// Which batched register-plan launch a transform takes: kernel kind (1
+// column, 2 row), plan length M and mode, and the functions that configure
+// and launch that kernel on a device table of items.
+struct RegBatchKey {
+    int kind = 0, M = 0, mode = 0;
+    size_t item_size = 0;
+    void (*configure)() = nullptr;
+    void (*launch)(cudaStream_t, const void *, int, long) = nullptr;
+};
+// The batch item of a transform for the register column (row) kernels; false
+// when no register plan covers it.  blocks = the CTAs it needs.
+bool col_batch_item(const AxisFFT &a, const int *skip, long first_block, RegBatchKey &key,
+                    std::vector<unsigned char> &item, long &blocks);
+bool row_batch_item(const AxisFFT &a, const int *skip, long first_block, RegBatchKey &key,
+                    std::vector<unsigned char> &item, long &blocks);
+
+// Register-plan line transforms (the row and column kernels) of several
+// transforms as one launch.  Every transform added must take the same kernel,
+// plan and mode: add() returns false, and adds nothing, when no register plan
+// covers the transform or it differs from those already added.  No fused CG
+// work.  finalize() once, then launch() as often as needed (capturable).
+class RegLineBatch {
+  public:
+    RegLineBatch();
+    ~RegLineBatch();
+    RegLineBatch(const RegLineBatch &) = delete;
+    RegLineBatch &operator=(const RegLineBatch &) = delete;
+    bool add(const AxisFFT &a, const int *skip = nullptr);
+    void finalize(Context &ctx);
+    void launch(cudaStream_t st) const;
+    bool empty() const;
 
   private:
     struct Impl;

@@ -6,6 +6,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <vector>
 #include <string>
 #include <tuple>
 
@@ -20,6 +21,9 @@
 struct lc_context_s {
     std::shared_ptr<lc::Context> ctx;
     std::string err;
+    // worker contexts of lc_mbir2d_batch's setup, created on first use and
+    // kept (with their streams) until this context is destroyed
+    std::vector<std::unique_ptr<lc_context_s>> batch_workers;
 };
 
 struct lc_geometry_s {

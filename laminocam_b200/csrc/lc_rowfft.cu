@@ -14,6 +14,8 @@
 // stores are contiguous.  The line crosses shared memory twice in the
 // transform, and once more in the forward unpack (which pairs k with M - k).
 #include <atomic>
+#include <cstring>
+#include <vector>
 
 #include "lc_fft.hpp"
 #include "lc_reduce.cuh"
@@ -45,7 +47,7 @@ constexpr size_t row_smem() {
 
 // HOOK: the fused CG work of RowArgs (compiled out when unused)
 template <int R0, int R1, int R2, int MODE, bool HOOK>
-__global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_kernel(RowArgs a) {
+__device__ __forceinline__ void row_fft_body(const RowArgs &a, long bid) {
     using P = RegPlan<R0, R1, R2>;
     constexpr int M = P::M, RM = P::RM, NT = P::NT;
     extern __shared__ __align__(16) float2 row_sm[];
@@ -53,7 +55,7 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
     float2 *th = tw + M;                  // h(m) = exp(-pi i m / M)
     load_line_twiddles<M>(tw);
     const int t = threadIdx.x % NT, c = threadIdx.x / NT;
-    const long line = (long)blockIdx.x * kRowLines + c;
+    const long line = bid * kRowLines + c;
     const bool valid = line < a.n_lines;
     float2 *buf = row_sm + c * M;
     const auto at = [&](int, int i) -> float2 & { return buf[i]; };
@@ -186,6 +188,48 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_ke
     }
 }
 
+// (HOOK's fused dot reduces over the whole grid: the plain launch only)
+template <int R0, int R1, int R2, int MODE, bool HOOK>
+__global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_kernel(RowArgs a) {
+    row_fft_body<R0, R1, R2, MODE, HOOK>(a, (long)blockIdx.x);
+}
+
+// one launch over several row transforms of one plan and mode (no fused CG
+// work): CTA b runs block b - first_block of the item whose range holds b
+struct RowBatchItem {
+    RowArgs a;
+    long first_block;
+    const int *skip;
+};
+
+template <int R0, int R1, int R2, int MODE>
+__global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines)
+    row_fft_batch_kernel(const RowBatchItem *__restrict__ items, int nitems) {
+    const long b = (long)blockIdx.x;
+    int lo = 0, hi = nitems - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].first_block <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    if (items[lo].skip && *items[lo].skip) return;
+    row_fft_body<R0, R1, R2, MODE, false>(items[lo].a, b - items[lo].first_block);
+}
+
+template <int R0, int R1, int R2, int MODE>
+void row_batch_configure() {
+    LC_CUDA(cudaFuncSetAttribute(row_fft_batch_kernel<R0, R1, R2, MODE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem<R0, R1, R2>()));
+}
+
+template <int R0, int R1, int R2, int MODE>
+void row_batch_launch(cudaStream_t st, const void *items, int n, long blocks) {
+    row_fft_batch_kernel<R0, R1, R2, MODE><<<(unsigned)blocks, RegPlan<R0, R1, R2>::NT * kRowLines,
+                                             row_smem<R0, R1, R2>(), st>>>(
+        static_cast<const RowBatchItem *>(items), n);
+    LC_CHECK_LAUNCH();
+}
+
 template <int R0, int R1, int R2, int MODE, bool HOOK>
 void launch_row_mode(cudaStream_t st, const RowArgs &a, long blocks) {
     constexpr size_t smem = row_smem<R0, R1, R2>();
@@ -224,11 +268,12 @@ bool launch_row_plan(cudaStream_t st, int M, int mode, const RowArgs &a, long bl
 
 long row_fft_ctas(long n_lines) { return (n_lines + kRowLines - 1) / kRowLines; }
 
-bool launch_row_fft(cudaStream_t st, const AxisFFT &a) {
+// The row plan of a transform (M, mode) and its arguments; false when no
+// register plan covers it.
+static bool row_plan_args(const AxisFFT &a, int &M, int &mode, RowArgs &ra) {
     if (a.fp64 || a.n_inner != 1 || a.lines_per_cta > 0) return false;
     if (a.pre || a.linefac || a.post) return false;
-    const int M = a.L;
-    int mode;
+    M = a.L;
     if (a.in_map == IN_REAL_PACKED && a.out_map == OUT_R2C_UNPACK && a.in_t == E_F32 && a.out_t == E_C64 &&
         a.sign < 0 && a.n_in <= 2 * M && a.n_out <= M + 1) {
         mode = RM_R2C;
@@ -239,8 +284,6 @@ bool launch_row_fft(cudaStream_t st, const AxisFFT &a) {
         return false;
     }
     if (!line_plan_exists(M)) return false;
-    if (a.n_outer <= 0 || a.n_out == 0) return true;
-    RowArgs ra;
     ra.in = a.in;
     ra.out = a.out;
     ra.n_lines = a.n_outer;
@@ -250,6 +293,14 @@ bool launch_row_fft(cudaStream_t st, const AxisFFT &a) {
     ra.n_out = a.n_out;
     ra.scale = (float)a.scale;
     ra.cg_upd = ra.cg_dot = 0;
+    return true;
+}
+
+bool launch_row_fft(cudaStream_t st, const AxisFFT &a) {
+    int M = 0, mode = 0;
+    RowArgs ra;
+    if (!row_plan_args(a, M, mode, ra)) return false;
+    if (a.n_outer <= 0 || a.n_out == 0) return true;
     if (a.cg_parts) {
         LC_REQUIRE(a.cg != nullptr, "row FFT: fused CG work without its state");
         ra.cg = *a.cg;
@@ -259,6 +310,38 @@ bool launch_row_fft(cudaStream_t st, const AxisFFT &a) {
     const long blocks = (a.n_outer + kRowLines - 1) / kRowLines;
     LC_REQUIRE(blocks < (1L << 31), "row FFT: grid too large");
     return launch_row_plan(st, M, mode, ra, blocks);
+}
+
+bool row_batch_item(const AxisFFT &a, const int *skip, long first_block, RegBatchKey &key,
+                    std::vector<unsigned char> &item, long &blocks) {
+    if (a.cg_parts) return false;
+    int M = 0, mode = 0;
+    RowArgs ra;
+    if (!row_plan_args(a, M, mode, ra)) return false;
+    key.kind = 2;
+    key.M = M;
+    key.mode = mode;
+    key.item_size = sizeof(RowBatchItem);
+    switch (M) {
+#define LC_ROW_BATCH_CASE(m, r0, r1, r2)                                   \
+    case m:                                                                \
+        if (mode == RM_R2C) {                                              \
+            key.launch = row_batch_launch<r0, r1, r2, RM_R2C>;             \
+            key.configure = row_batch_configure<r0, r1, r2, RM_R2C>;       \
+        } else {                                                           \
+            key.launch = row_batch_launch<r0, r1, r2, RM_C2R>;             \
+            key.configure = row_batch_configure<r0, r1, r2, RM_C2R>;       \
+        }                                                                  \
+        break;
+        LC_LINE_PLANS(LC_ROW_BATCH_CASE)
+#undef LC_ROW_BATCH_CASE
+        default: return false;
+    }
+    blocks = (a.n_outer + kRowLines - 1) / kRowLines;
+    RowBatchItem it{ra, first_block, skip};
+    item.resize(sizeof it);
+    std::memcpy(item.data(), &it, sizeof it);
+    return true;
 }
 
 }  // namespace lc

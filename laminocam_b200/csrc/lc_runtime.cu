@@ -226,10 +226,13 @@ Context::Context(int device, cudaStream_t stream) : device_(device) {
     DeviceGuard g(device);
     LC_CUDA(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
     stream_ = stream ? stream : own_stream_;
-    cudaDeviceProp prop;
-    LC_CUDA(cudaGetDeviceProperties(&prop, device));
-    num_sms_ = prop.multiProcessorCount;
-    max_smem_ = prop.sharedMemPerBlockOptin;
+    // two attributes (cudaGetDeviceProperties fills the whole table, which
+    // takes milliseconds)
+    int sms = 0, smem = 0;
+    LC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    LC_CUDA(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    num_sms_ = sms;
+    max_smem_ = (size_t)smem;
     // keep freed pool memory cached in the process instead of returning it
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
