@@ -333,6 +333,67 @@ def serving_mix(lc, workers=32):
     }
 
 
+# config-4 precision study: one large slice, three precisions of the same path
+PREC_N, PREC_ANGLES, PREC_ELLIPSES, PREC_NOISE = 2047, 1800, 60, 0.005
+PREC_CG, PREC_SB_OUTER, PREC_SB_INNER, PREC_LAM, PREC_MU = 200, 30, 2, 0.05, 10.0
+
+
+def precision_study(lc, n=PREC_N, nth=PREC_ANGLES, cg_iters=PREC_CG, sb_outer=PREC_SB_OUTER,
+                    sb_inner=PREC_SB_INNER):
+    """One n x n ellipse slice (60 ellipses), nth angles over [0, 180), 0.5 %
+    noise, CG(200) and Split-Bregman (lambda 0.05, mu 10, 30 outer x 2 inner),
+    computed three ways and compared with the FP64 oracle (the reference's own
+    double path: its sources on the timing build's stand-ins at FINUFFT tol
+    1e-12, oracle/_ref/ref_prec):
+      default   this build: FP32 spreading, FFTs and vectors, FP64 PSF kernel
+                and FP64 CG scalars and reductions
+      all_fp32  this build with the PSF kernel from a FP32 NUFFT of ones (the
+                reference GPU's construction) and FP32 CG scalars and dots
+                (the reference GPU's float accumulation, src/gpu/array_ops.cu:210-213)
+      reference_float  the reference's own float CPU path (FINUFFT tol 5e-4,
+                include/finufft_plan.h:71), for context
+    Relative L2 errors of the projection (noise free), the backprojection of
+    the noisy sinogram, A^T A of the phantom, and the two reconstructions."""
+    import torch
+    from laminocam_b200 import synthetic as S
+    from oracle import oracle as O
+    from oracle import refrun as R
+    th = np.arange(nth) * np.pi / nth
+    ph = S.ellipse_phantom(n, PREC_ELLIPSES, 1000)[None].astype(np.float64)
+    xprobe = ph / ph.max()
+    p64 = R.ref_forward2d(ph, th, n)
+    sino = S.add_noise(p64.astype(np.float32), PREC_NOISE, 2000)
+    sino = np.ascontiguousarray(sino / sino.max(), dtype=np.float32)
+    s64 = sino.astype(np.float64)
+    ref = R.ref_precision2d(s64, th, n, xprobe, cg_iters, sb_outer, sb_inner, PREC_LAM, PREC_MU)
+    ref32 = R.ref_precision2d(s64, th, n, xprobe, cg_iters, sb_outer, sb_inner, PREC_LAM, PREC_MU, double=False)
+    p32ref = R.ref_forward2d(ph, th, n, double=False)
+    names = ("backprojection", "AtA", "recon_cg", "recon_sb")
+    out = {"workload": f"{n}x{n} slice, {PREC_ELLIPSES} ellipses, {nth} angles over [0,180), "
+                       f"{PREC_NOISE * 100:.1f}% noise; CG {cg_iters} iterations; Split-Bregman "
+                       f"lambda {PREC_LAM}, mu {PREC_MU}, {sb_outer} outer x {sb_inner} inner",
+           "oracle": "the reference's double path (FINUFFT tol 1e-12) on the timing build's stand-ins"}
+    out["reference_float"] = {"projection": O.rel_l2(p32ref, p64),
+                              **{k: O.rel_l2(a, b) for k, a, b in zip(names, ref32, ref)}}
+    pg = lc.PolarGrid2D(th, n)
+    proj = lc.forward2d(ph.astype(np.float32), pg).cpu().numpy().astype(np.float64)
+    bp = lc.backproj2d(sino, pg, (1, n, n)).cpu().numpy().astype(np.float64)
+    for variant, f32 in (("default", False), ("all_fp32", True)):
+        psf = lc.PointSpreadFunction2D(pg, n, 1, psf_fp32=f32)
+        ax = psf.convolve(xprobe.astype(np.float32)).cpu().numpy().astype(np.float64)
+        del psf
+        cg = lc.MBIR2D(sino, th, lc.ReconParams(recon_dims=(1, n, n), max_iters=cg_iters, tol=0, xtol=0,
+                                               fp32_scalars=f32, psf_fp32=f32, use_graph=True))
+        sb = lc.MBIR2D(sino, th, lc.ReconParams(regularizer="split_bregman", recon_dims=(1, n, n),
+                                               max_iters=sb_outer, inner_iters=sb_inner, lam=PREC_LAM, mu=PREC_MU,
+                                               tol=0, xtol=0, fp32_scalars=f32, psf_fp32=f32, use_graph=True))
+        out[variant] = {"projection": O.rel_l2(proj, p64), "backprojection": O.rel_l2(bp, ref[0]),
+                        "AtA": O.rel_l2(ax, ref[1]), "recon_cg": O.rel_l2(cg, ref[2]),
+                        "recon_sb": O.rel_l2(sb, ref[3])}
+    torch.cuda.synchronize()
+    return out
+
+
 STREAM_RATES = (5.0, 20.0, 80.0)
 STREAM_REQUESTS = 64
 STREAM_ITERS = 50
@@ -635,6 +696,10 @@ def main():
     ap.add_argument("--kernel-case", choices=["toeplitz", "split_bregman"],
                     help="reduced case for a profiler capture of one kernel family (not a benchmark line)")
     ap.add_argument("--reps", type=int, default=3, help="applies or outer iterations of --kernel-case")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="run the precision study (2047x2047 slice, 1800 angles; default FP32 path with FP64 "
+                         "PSF and scalars, all-FP32, the reference's float path) against the FP64 oracle and "
+                         "print its JSON line (a few minutes of host time for the oracle)")
     ap.add_argument("--reference-full", action="store_true",
                     help="with --impl reference: also run one complete reconstruction of the reference's "
                          "code (tomocam::MBIR, 100 outer iterations) and report its time beside the "
@@ -658,6 +723,11 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.precision_study:
+        import laminocam_b200 as lc
+        if rank == 0:
+            print(json.dumps({"precision_study": precision_study(lc)}), flush=True)
+        return
     if args.stream_only:
         import laminocam_b200 as lc
         if rank == 0:

@@ -92,6 +92,11 @@ int lc_sysmat3d_nufft(lc_context ctx, lc_geometry g, const float *x, int n1, int
  * cpu/gpu::PointSpreadFunction (include/toeplitz.h:35-130) for a 3D geometry
  * (volume {n1, n2, n3}).  The kernel is generated in FP64 on the device. */
 int lc_psf_create(lc_context ctx, lc_geometry g, int n1, int n2, int n3, lc_psf *out);
+/* lc_psf_create with flags: LC_PSF_FP32_NUFFT builds the kernel as the
+ * reference GPU does (include/gpu/toeplitz2d.h:84-115), a FP32 type-1 NUFFT of
+ * ones at tol 1e-6, instead of the exact FP64 closed form. */
+#define LC_PSF_FP32_NUFFT 1
+int lc_psf_create_ex(lc_context ctx, lc_geometry g, int n1, int n2, int n3, int flags, lc_psf *out);
 int lc_psf_destroy(lc_psf psf);
 /* P[3]: PSF grid (P[0] = 1 for 2D); spectrum_elems: stored real spectrum size */
 int lc_psf_info(lc_psf psf, int *P, long *spectrum_elems);
@@ -150,6 +155,10 @@ typedef struct {
     lc_solver_params solver;
     double nufft_tol;     /* <= 0: 1e-6 */
     float pad_factor;     /* 3D only, ReconParams::PAD_FACTOR (1.4142) */
+    int psf_fp32;         /* 0: the PSF kernel exactly in FP64 (default); 1: as the
+                             reference GPU builds it, a FP32 type-1 NUFFT of ones at
+                             tol 1e-6 (include/gpu/toeplitz2d.h:84-115); the PSF
+                             cache is bypassed */
 } lc_recon_params;
 
 void lc_recon_params_default(lc_recon_params *p);

@@ -230,12 +230,13 @@ def backproj2d(sino, pg: PolarGrid2D, recon_dims, tol: float = DEFAULT_TOL):
 
 
 class _PSFBase:
-    def __init__(self, ctx, geom, dims):
+    def __init__(self, ctx, geom, dims, psf_fp32=False):
         self.ctx = ctx
         self.geom = geom
         self.dims_ = tuple(int(d) for d in dims)
         h = C.c_void_p()
-        _check(ctx.lib.lc_psf_create(ctx.handle, geom.handle, *self.dims_, C.byref(h)), ctx)
+        _check(ctx.lib.lc_psf_create_ex(ctx.handle, geom.handle, *self.dims_, 1 if psf_fp32 else 0, C.byref(h)),
+               ctx)
         self.handle = h
         P = (C.c_int * 3)()
         ne = C.c_long()
@@ -283,8 +284,10 @@ class _PSFBase:
 class PointSpreadFunction2D(_PSFBase):
     """PointSpreadFunction2D (include/toeplitz2d.h:40-126) for nslices slices of image_size^2."""
 
-    def __init__(self, pg: PolarGrid2D, image_size: int, nslices: int = 1):
-        super().__init__(pg.ctx, pg, (nslices, image_size, image_size))
+    def __init__(self, pg: PolarGrid2D, image_size: int, nslices: int = 1, psf_fp32: bool = False):
+        """psf_fp32: the kernel from a FP32 NUFFT of ones (the reference GPU's
+        construction) instead of the exact FP64 closed form."""
+        super().__init__(pg.ctx, pg, (nslices, image_size, image_size), psf_fp32)
 
     def psf_size(self):
         return self.P[1]
@@ -293,8 +296,8 @@ class PointSpreadFunction2D(_PSFBase):
 class PointSpreadFunction(_PSFBase):
     """PointSpreadFunction (include/toeplitz.h:35-130) for a volume of recon_dims."""
 
-    def __init__(self, pg: PolarGrid, recon_dims):
-        super().__init__(pg.ctx, pg, recon_dims)
+    def __init__(self, pg: PolarGrid, recon_dims, psf_fp32: bool = False):
+        super().__init__(pg.ctx, pg, recon_dims, psf_fp32)
 
 
 def sysmat2d(x, op, tol: float = DEFAULT_TOL):
@@ -421,6 +424,7 @@ class ReconParams:
     poll_every: int = 8
     use_graph: bool = False
     residual_refresh: int = 1
+    psf_fp32: bool = False  # PSF kernel from a FP32 NUFFT of ones (the reference GPU's way)
 
     def to_c(self) -> ReconParamsC:
         r = ReconParamsC()
@@ -431,6 +435,7 @@ class ReconParams:
                                   self.residual_refresh)
         r.nufft_tol = float(self.nufft_tol)
         r.pad_factor = float(self.pad_factor)
+        r.psf_fp32 = 1 if self.psf_fp32 else 0
         return r
 
 

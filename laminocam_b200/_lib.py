@@ -22,7 +22,7 @@ class SolverStats(C.Structure):
 
 class ReconParamsC(C.Structure):
     _fields_ = [("method", C.c_int), ("solver", SolverParams), ("nufft_tol", C.c_double),
-                ("pad_factor", C.c_float)]
+                ("pad_factor", C.c_float), ("psf_fp32", C.c_int)]
 
 
 class ProfileEntry(C.Structure):
@@ -80,6 +80,7 @@ SIGNATURES = {
     "lc_backproj3d": (i32, [vp, vp, vp, i32, i32, i32, i32, vp, f64]),
     "lc_sysmat3d_nufft": (i32, [vp, vp, vp, i32, i32, i32, vp, f64]),
     "lc_psf_create": (i32, [vp, vp, i32, i32, i32, C.POINTER(vp)]),
+    "lc_psf_create_ex": (i32, [vp, vp, i32, i32, i32, i32, C.POINTER(vp)]),
     "lc_psf_destroy": (i32, [vp]),
     "lc_psf_info": (i32, [vp, C.POINTER(C.c_int), C.POINTER(C.c_long)]),
     "lc_psf_kernel": (i32, [vp, vp, dptr]),

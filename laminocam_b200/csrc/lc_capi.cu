@@ -337,6 +337,7 @@ void lc_recon_params_default(lc_recon_params *p) {
     lc_solver_params_default(&p->solver);
     p->nufft_tol = 1e-6;
     p->pad_factor = 1.4142f;
+    p->psf_fp32 = 0;
 }
 
 int lc_context_create(int device, void *stream, lc_context *out) {
@@ -477,11 +478,16 @@ int lc_sysmat3d_nufft(lc_context c, lc_geometry g, const float *x, int n1, int n
 }
 
 int lc_psf_create(lc_context c, lc_geometry g, int n1, int n2, int n3, lc_psf *out) {
+    return lc_psf_create_ex(c, g, n1, n2, n3, 0, out);
+}
+
+int lc_psf_create_ex(lc_context c, lc_geometry g, int n1, int n2, int n3, int flags, lc_psf *out) {
     if (!out) return fail(c, LC_ERR_INVALID, "out is NULL");
     *out = nullptr;
     return guarded(c, [&] {
         LC_REQUIRE(g != nullptr, "geometry is NULL");
         LC_REQUIRE(n1 > 0 && n2 > 0 && n3 > 0, "sizes must be positive");
+        LC_REQUIRE((flags & ~LC_PSF_FP32_NUFFT) == 0, "unknown PSF flags");
         bool three = g->g.pts.dim == 3;
         if (!three) LC_REQUIRE(n2 == n3, "2D PSF needs square slices (n2 == n3)");
         long dims[3] = {n1, n2, n3};
@@ -489,7 +495,7 @@ int lc_psf_create(lc_context c, lc_geometry g, int n1, int n2, int n3, lc_psf *o
         p->keep = c->ctx;
         p->owner = c;
         p->geom = g;
-        p->T = std::make_unique<Toeplitz>(*c->ctx, g->g, dims, three);
+        p->T = std::make_unique<Toeplitz>(*c->ctx, g->g, dims, three, (flags & LC_PSF_FP32_NUFFT) != 0);
         // complete on return: the caller may use it on another stream
         LC_CUDA(cudaStreamSynchronize(c->ctx->stream()));
         *out = p.release();
@@ -559,8 +565,9 @@ int lc_split_bregman(lc_context c, lc_psf p, const float *rhs, float *x,
 namespace lc {
 
 static std::shared_ptr<Toeplitz> make_psf(Context &ctx, const PolarGeometry &g, const long dims[3],
-                                          bool three_d, const PsfProvider *psf, bool *hit) {
+                                          bool three_d, const PsfProvider *psf, bool *hit, bool fp32 = false) {
     if (hit) *hit = false;
+    if (fp32) return std::make_shared<Toeplitz>(ctx, g, dims, three_d, true);
     if (psf && *psf) return (*psf)(ctx, g, dims, three_d, hit);
     return std::make_shared<Toeplitz>(ctx, g, dims, three_d);
 }
@@ -590,7 +597,7 @@ void mbir2d_core(lc_context c, const float *dsino, int ns, int ntheta, int nradi
     psf.owner = c;
     psf.geom = g;
     long dims[3] = {ns, n, n};
-    psf.T = make_psf(ctx, g->g, dims, false, psfp, psf_hit);
+    psf.T = make_psf(ctx, g->g, dims, false, psfp, psf_hit, p->psf_fp32 != 0);
     LC_CUDA(cudaMemsetAsync(drecon, 0, nv * sizeof(float), s));
     run_solver(&psf, p->method, rhs.get(), drecon, &p->solver, stats);
 }
@@ -697,7 +704,7 @@ void mbir3d_core(lc_context c, const float *dprojs_in, int ntheta, int nrows, in
     lc_psf_s psf;
     psf.owner = c;
     psf.geom = g;
-    psf.T = make_psf(ctx, g->g, N, true, psfp, psf_hit);
+    psf.T = make_psf(ctx, g->g, N, true, psfp, psf_hit, p->psf_fp32 != 0);
     if (load_input) load_input();
     DevBuf<unsigned> mx(1, s);
     mx.zero(s);

@@ -333,6 +333,16 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
 // length.  Their values are never reached by the cropped convolution
 // (|i - j| <= n - 1 < P/2), and without them the zero-centred kernel is
 // exactly point-symmetric, so its spectrum is real.
+__global__ void fill_ones_kernel(float2 *__restrict__ c, long n) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        c[i] = make_float2(1.f, 0.f);
+}
+
+__global__ void widen_kernel(const float *__restrict__ a, double *__restrict__ b, long n) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+
 __global__ void zero_unpaired_kernel(double *__restrict__ K, int P1, int P2, int P3) {
     long total = (long)P1 * P2 * P3;
     for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
@@ -414,7 +424,7 @@ void launch_neg_laplacian_axpy(Context &ctx, const float *x, float *y, const lon
 
 static int next_fast_dim(long n) { return (int)next_smooth23(n); }
 
-Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], bool three_d)
+Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], bool three_d, bool psf_fp32)
     : three_d_(three_d), g_(&g) {
     for (int d = 0; d < 3; ++d) n_[d] = dims[d];
     LC_REQUIRE(n_[0] > 0 && n_[1] > 0 && n_[2] > 0, "Toeplitz: dims must be positive");
@@ -433,7 +443,8 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
     }
     cudaStream_t st = ctx.stream();
     DevBuf<double> K;
-    build_kernel(ctx, K);  // unpaired -P/2 planes already zeroed
+    if (psf_fp32) build_kernel_nufft32(ctx, K);
+    else build_kernel(ctx, K);  // unpaired -P/2 planes already zeroed
     // Spectrum of the zero-centred kernel: FFT with the mode placement k -> k mod P.
     // It is real and point-symmetric; keep x in [0, P3/2] (the R2C half) and all
     // of y and z, i.e. a real {P1, P2, P3/2+1} array.
@@ -561,6 +572,30 @@ Toeplitz::Toeplitz(Context &ctx, const Toeplitz &src, bool work)
     cudaStream_t st = ctx.stream();
     t1_.alloc(n_[0] * n_[1] * Ph_[2], st);
     if (three_d_) t2_.alloc(n_[0] * (long)P_[1] * Ph_[2], st);
+}
+
+// The kernel as the reference GPU path builds it (include/gpu/toeplitz2d.h:84-115,
+// include/gpu/toeplitz.h:80-110): Re of a type-1 NUFFT of unit weights at every
+// grid point onto the P grid, here in FP32 at tol 1e-6 (cuFINUFFT's float
+// path runs at 1.2e-6), widened to FP64 for the spectrum FFTs that follow.
+void Toeplitz::build_kernel_nufft32(Context &ctx, DevBuf<double> &K) {
+    cudaStream_t st = ctx.stream();
+    ProfScope ps(ctx, PS_PSF_GEN, 0.0);
+    const int P1 = P_[0], P2 = P_[1], P3 = P_[2];
+    const long total = (long)P1 * P2 * P3;
+    const int modes[3] = {P3, P2, three_d_ ? P1 : 1};
+    NufftPlan plan(ctx, *g_, modes, 1e-6);
+    DevBuf<float2> ones(g_->pts.M, st);
+    fill_ones_kernel<<<grid_for(g_->pts.M, 256, ctx.num_sms()), 256, 0, st>>>(ones.get(), g_->pts.M);
+    LC_CHECK_LAUNCH();
+    DevBuf<float> K32(total, st);
+    plan.type1_real(ctx, ones.get(), 1, K32.get(), 1.0f, PT_PLAIN);
+    K.alloc(total, st);
+    widen_kernel<<<grid_for(total, 256, ctx.num_sms()), 256, 0, st>>>(K32.get(), K.get(), total);
+    LC_CHECK_LAUNCH();
+    kernel_mirror_ = false;
+    zero_unpaired_kernel<<<grid_for(total, 256, ctx.num_sms()), 256, 0, st>>>(K.get(), P1, P2, P3);
+    LC_CHECK_LAUNCH();
 }
 
 void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {

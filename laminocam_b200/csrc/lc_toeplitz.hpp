@@ -26,7 +26,9 @@ class Toeplitz {
     // slices (2D, n2 == n3 required by the reference API).  The spectrum is
     // built in the order of ctx.stream() and may still be in flight on
     // return.
-    Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], bool three_d);
+    // psf_fp32: the kernel K from a FP32 type-1 NUFFT of ones (tol 1e-6), the
+    // reference GPU's construction, in place of the exact FP64 closed form
+    Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], bool three_d, bool psf_fp32 = false);
     // shares src's spectrum (read-only) and, with `work`, owns fresh work
     // buffers on ctx's stream: concurrent jobs on one geometry use one
     // spectrum.  Without work buffers the copy only holds the spectrum (a
@@ -71,6 +73,7 @@ class Toeplitz {
 
   private:
     void build_kernel(Context &ctx, DevBuf<double> &K);
+    void build_kernel_nufft32(Context &ctx, DevBuf<double> &K);
     bool three_d_;
     bool kernel_mirror_ = false;  // the last kernel built is even in its mirror axis (kz in 3D)
     bool zfold_ = false;          // spectrum stored for f1 <= P1/2 only

@@ -8,10 +8,11 @@
 //   ref_bench check_fft   <in.f64> <out.f64>   FFTW-shim transform (tests)
 //   ref_bench check_nufft <in.f64> <out.f64>   FINUFFT-shim transform (tests)
 //   ref_bench lamino <phantom.f32> <n1> <n2> <n3> <nangles> <gamma_deg> <warmup> <steps> [full]
-//   ref_prec  forward2d  <in.f64> <out.f64>     forward2d in double (tol 1e-12)
-//   ref_prec  precision2d <in.f64> <out.f64>    backproj2d, sysmat2d(x, PSF), CG and
-//                                               Split-Bregman in double, for the
-//                                               precision study
+//   ref_prec  forward2d[_f32]  <in.f64> <out.f64>    forward2d in double (FINUFFT
+//                                                    tol 1e-12) or float (5e-4)
+//   ref_prec  precision2d[_f32] <in.f64> <out.f64>   backproj2d, sysmat2d(x, PSF), CG and
+//                                                    Split-Bregman in double or float,
+//                                                    for the precision study
 // (ref_prec is this file built with -DLC_GPU_STENCIL: the zero-padded finite
 // differences of the reference's GPU build, gpu_stencil.h, in place of
 // src/finitediff.cpp, whose interior-only stencil vanishes on single slices.)
@@ -139,6 +140,49 @@ static std::vector<double> check_nufft_t(const std::vector<double> &v, size_t po
     return out;
 }
 
+// n nth nr theta[nth] vol[n n] -> sino[nth nr], in precision T (the FINUFFT
+// tolerance of the reference for T: 1e-12 double, 5e-4 float)
+template <typename T>
+static std::vector<double> forward2d_op(const std::vector<double> &v, size_t pos) {
+    const size_t n = (size_t)v[pos++], nth = (size_t)v[pos++], nr = (size_t)v[pos++];
+    std::vector<T> th(nth);
+    for (size_t i = 0; i < nth; ++i) th[i] = (T)v[pos + i];
+    pos += nth;
+    Array<T> vol(dims_t{1, n, n});
+    for (size_t i = 0; i < n * n; ++i) vol[i] = (T)v[pos + i];
+    cpu::PolarGrid2D<T> pg(th, nr);
+    Array<T> s = forward2d(vol, pg);
+    return std::vector<double>(s.begin(), s.end());
+}
+
+// n nth nr cg_iters sb_outer sb_inner lam mu theta[nth] sino[nth nr] xprobe[n n]
+//   -> backproj2d rhs, sysmat2d(xprobe, PSF), CG recon, Split-Bregman recon
+template <typename T>
+static std::vector<double> precision2d_op(const std::vector<double> &v, size_t pos) {
+    const size_t n = (size_t)v[pos++], nth = (size_t)v[pos++], nr = (size_t)v[pos++];
+    const size_t cg_iters = (size_t)v[pos++], sb_outer = (size_t)v[pos++], sb_inner = (size_t)v[pos++];
+    const T lam = (T)v[pos++], mu = (T)v[pos++];
+    std::vector<T> th(nth);
+    for (size_t i = 0; i < nth; ++i) th[i] = (T)v[pos + i];
+    pos += nth;
+    Array<T> sino(dims_t{1, nth, nr}), xp(dims_t{1, n, n});
+    for (size_t i = 0; i < nth * nr; ++i) sino[i] = (T)v[pos + i];
+    pos += nth * nr;
+    for (size_t i = 0; i < n * n; ++i) xp[i] = (T)v[pos + i];
+    cpu::PolarGrid2D<T> pg(th, nr);
+    const dims_t rd{1, n, n};
+    Array<T> rhs = backproj2d(sino, pg, rd);
+    cpu::PointSpreadFunction2D<T> psf(pg, n);
+    opt::Function<T> A = [&psf](const Array<T> &x) { return sysmat2d(x, psf); };
+    Array<T> ax = A(xp);
+    auto x0 = Array<T>::zeros(rd);
+    Array<T> cg = opt::cgsolver<T>(A, rhs, x0, cg_iters, T(0), T(0));
+    Array<T> sb = opt::split_bregman<T>(A, rhs, x0, lam, mu, sb_outer, sb_inner, T(0), T(0));
+    std::vector<double> out;
+    for (const Array<T> *a : {&rhs, &ax, &cg, &sb}) out.insert(out.end(), a->begin(), a->end());
+    return out;
+}
+
 static int lamino(int argc, char **argv) {
     if (argc < 10) throw std::runtime_error("lamino: arguments missing");
     const char *phantom = argv[2];
@@ -236,7 +280,7 @@ int main(int argc, char **argv) {
     }
     try {
         const std::string op = argv[1];
-        if (op == "lamino" || op == "forward2d" || op == "precision2d") {
+        if (op != "check_fft" && op != "check_nufft") {
             // the reference prints per-iteration progress; keep stdout for the JSON lines
             std::cout.setstate(std::ios::failbit);
         }
@@ -254,37 +298,10 @@ int main(int argc, char **argv) {
             int sign = (int)v[pos++];
             out = prec ? check_fft_t<double>(v, pos, kind, rank, n.data(), sign)
                        : check_fft_t<float>(v, pos, kind, rank, n.data(), sign);
-        } else if (op == "forward2d") {  // n nth nr theta[nth] vol[n n] -> sino[nth nr]
-            const size_t n = (size_t)v[pos++], nth = (size_t)v[pos++], nr = (size_t)v[pos++];
-            std::vector<double> th(v.begin() + pos, v.begin() + pos + nth);
-            pos += nth;
-            Array<double> vol(dims_t{1, n, n});
-            for (size_t i = 0; i < n * n; ++i) vol[i] = v[pos + i];
-            cpu::PolarGrid2D<double> pg(th, nr);
-            Array<double> s = forward2d(vol, pg);
-            out.assign(s.begin(), s.end());
-        } else if (op == "precision2d") {
-            // n nth nr cg_iters sb_outer sb_inner lam mu theta[nth] sino[nth nr] xprobe[n n]
-            //   -> rhs, A^T A xprobe (Toeplitz), CG recon, Split-Bregman recon (each n n)
-            const size_t n = (size_t)v[pos++], nth = (size_t)v[pos++], nr = (size_t)v[pos++];
-            const size_t cg_iters = (size_t)v[pos++], sb_outer = (size_t)v[pos++], sb_inner = (size_t)v[pos++];
-            const double lam = v[pos++], mu = v[pos++];
-            std::vector<double> th(v.begin() + pos, v.begin() + pos + nth);
-            pos += nth;
-            Array<double> sino(dims_t{1, nth, nr}), xp(dims_t{1, n, n});
-            for (size_t i = 0; i < nth * nr; ++i) sino[i] = v[pos + i];
-            pos += nth * nr;
-            for (size_t i = 0; i < n * n; ++i) xp[i] = v[pos + i];
-            cpu::PolarGrid2D<double> pg(th, nr);
-            const dims_t rd{1, n, n};
-            Array<double> rhs = backproj2d(sino, pg, rd);
-            cpu::PointSpreadFunction2D<double> psf(pg, n);
-            opt::Function<double> A = [&psf](const Array<double> &x) { return sysmat2d(x, psf); };
-            Array<double> ax = A(xp);
-            auto x0 = Array<double>::zeros(rd);
-            Array<double> cg = opt::cgsolver<double>(A, rhs, x0, cg_iters, 0.0, 0.0);
-            Array<double> sb = opt::split_bregman<double>(A, rhs, x0, lam, mu, sb_outer, sb_inner, 0.0, 0.0);
-            for (const Array<double> *a : {&rhs, &ax, &cg, &sb}) out.insert(out.end(), a->begin(), a->end());
+        } else if (op == "forward2d" || op == "forward2d_f32") {
+            out = op == "forward2d" ? forward2d_op<double>(v, pos) : forward2d_op<float>(v, pos);
+        } else if (op == "precision2d" || op == "precision2d_f32") {
+            out = op == "precision2d" ? precision2d_op<double>(v, pos) : precision2d_op<float>(v, pos);
         } else if (op == "check_nufft") {
             int type = (int)v[pos++], dim = (int)v[pos++];
             int64_t nm[3] = {(int64_t)v[pos], (int64_t)v[pos + 1], (int64_t)v[pos + 2]};

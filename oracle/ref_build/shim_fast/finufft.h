@@ -142,13 +142,15 @@ void make_schedule(NuPlan &p) {
     for (int64_t j = 0; j < p.M; ++j) p.perm[cnt[key[j]]++] = (int32_t)j;
 }
 
-inline void es_weights(double u, int w, double beta, int64_t &l0, float *wt) {
+// kernel weights in the transform's precision R
+template <typename R>
+inline void es_weights(double u, int w, double beta, int64_t &l0, R *wt) {
     l0 = first_cell(u, w);
     const double hw = 0.5 * w;
     for (int m = 0; m < w; ++m) {
         const double z = ((double)(l0 + m) - u) / hw;
         const double t = 1.0 - z * z;
-        wt[m] = t > 0 ? (float)std::exp(beta * (std::sqrt(t) - 1.0)) : 0.0f;
+        wt[m] = t > 0 ? (R)std::exp(beta * (std::sqrt(t) - 1.0)) : R(0);
     }
 }
 
@@ -156,13 +158,13 @@ inline void es_weights(double u, int w, double beta, int64_t &l0, float *wt) {
 template <typename R>
 inline void spread_one(const NuPlan &p, int64_t j, std::complex<R> v, std::complex<R> *g) {
     const int w = p.w;
-    float wx[16], wy[16], wz[16];
+    R wx[16], wy[16], wz[16];
     int64_t l0[3] = {0, 0, 0};
     es_weights(fine_coord(coord_of<R>(p, 0, j), p.nf[0]), w, p.beta, l0[0], wx);
     if (p.dim > 1) es_weights(fine_coord(coord_of<R>(p, 1, j), p.nf[1]), w, p.beta, l0[1], wy);
-    else wy[0] = 1.f;
+    else wy[0] = R(1);
     if (p.dim > 2) es_weights(fine_coord(coord_of<R>(p, 2, j), p.nf[2]), w, p.beta, l0[2], wz);
-    else wz[0] = 1.f;
+    else wz[0] = R(1);
     const int wyn = p.dim > 1 ? w : 1, wzn = p.dim > 2 ? w : 1;
     const int64_t nx = p.nf[0], ny = p.nf[1], nz = p.nf[2];
     const bool xin = l0[0] >= 0 && l0[0] + w <= nx;
@@ -170,15 +172,15 @@ inline void spread_one(const NuPlan &p, int64_t j, std::complex<R> v, std::compl
         const int64_t iz = p.dim > 2 ? wrapi(l0[2] + dz, nz) : 0;
         for (int dy = 0; dy < wyn; ++dy) {
             const int64_t iy = p.dim > 1 ? wrapi(l0[1] + dy, ny) : 0;
-            const R f = (R)(wz[dz] * wy[dy]);
+            const R f = wz[dz] * wy[dy];
             const R vr = v.real() * f, vi = v.imag() * f;
             std::complex<R> *row = g + (iz * ny + iy) * nx;
             if (xin) {
                 R *r = reinterpret_cast<R *>(row + l0[0]);
 #pragma omp simd
                 for (int dx = 0; dx < w; ++dx) {
-                    r[2 * dx] += vr * (R)wx[dx];
-                    r[2 * dx + 1] += vi * (R)wx[dx];
+                    r[2 * dx] += vr * wx[dx];
+                    r[2 * dx + 1] += vi * wx[dx];
                 }
             } else {
                 for (int dx = 0; dx < w; ++dx) row[wrapi(l0[0] + dx, nx)] += std::complex<R>(vr * wx[dx], vi * wx[dx]);
@@ -190,13 +192,13 @@ inline void spread_one(const NuPlan &p, int64_t j, std::complex<R> v, std::compl
 template <typename R>
 inline std::complex<R> interp_one(const NuPlan &p, int64_t j, const std::complex<R> *g) {
     const int w = p.w;
-    float wx[16], wy[16], wz[16];
+    R wx[16], wy[16], wz[16];
     int64_t l0[3] = {0, 0, 0};
     es_weights(fine_coord(coord_of<R>(p, 0, j), p.nf[0]), w, p.beta, l0[0], wx);
     if (p.dim > 1) es_weights(fine_coord(coord_of<R>(p, 1, j), p.nf[1]), w, p.beta, l0[1], wy);
-    else wy[0] = 1.f;
+    else wy[0] = R(1);
     if (p.dim > 2) es_weights(fine_coord(coord_of<R>(p, 2, j), p.nf[2]), w, p.beta, l0[2], wz);
-    else wz[0] = 1.f;
+    else wz[0] = R(1);
     const int wyn = p.dim > 1 ? w : 1, wzn = p.dim > 2 ? w : 1;
     const int64_t nx = p.nf[0], ny = p.nf[1], nz = p.nf[2];
     R ar = 0, ai = 0;
@@ -211,7 +213,7 @@ inline std::complex<R> interp_one(const NuPlan &p, int64_t j, const std::complex
                 rr += c.real() * wx[dx];
                 ri += c.imag() * wx[dx];
             }
-            const R f = (R)(wz[dz] * wy[dy]);
+            const R f = wz[dz] * wy[dy];
             ar += rr * f;
             ai += ri * f;
         }

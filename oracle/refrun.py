@@ -143,3 +143,41 @@ def fast_nufft(nu_type: int, dim: int, modes, iflag: int, tol: float, x, y, z, d
                                      np.stack([d.real, d.imag], axis=-1).ravel()])
     out = out.view(np.complex128)
     return out.reshape(nm[2], nm[1], nm[0])[:, :, :] if nu_type == 1 else out
+
+
+def prec_path() -> str:
+    return os.path.join(REF_DIR, "ref_prec")
+
+
+def prec_available() -> bool:
+    return os.path.exists(prec_path())
+
+
+def _run_prec(op: str, values) -> np.ndarray:
+    flat = np.concatenate([np.ravel(np.asarray(v, dtype=np.float64)) for v in values])
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.f64")
+        fout = os.path.join(td, "out.f64")
+        flat.tofile(fin)
+        subprocess.run([prec_path(), op, fin, fout], check=True,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1)))
+        return np.fromfile(fout, dtype=np.float64)
+
+
+def ref_forward2d(vol, theta, nr, double=True):
+    """The reference's forward2d (src/projection.cpp:146-160) in double (FINUFFT
+    tol 1e-12) or float (tol 5e-4), on the timing build's FFT/NUFFT stand-ins
+    (the zero-padded GPU finite differences)."""
+    n = vol.shape[-1]
+    out = _run_prec("forward2d" if double else "forward2d_f32", [[n, len(theta), nr], theta, vol])
+    return out.reshape(1, len(theta), nr)
+
+
+def ref_precision2d(sino, theta, n, xprobe, cg_iters, sb_outer, sb_inner, lam, mu, double=True):
+    """The reference's backproj2d, sysmat2d(xprobe, PSF), cgsolver and
+    split_bregman in double (FINUFFT tol 1e-12) or float (5e-4).  Returns
+    (rhs, A^T A xprobe, CG recon, Split-Bregman recon), each {1, n, n}."""
+    nth, nr = sino.shape[-2], sino.shape[-1]
+    out = _run_prec("precision2d" if double else "precision2d_f32",
+                    [[n, nth, nr, cg_iters, sb_outer, sb_inner, lam, mu], theta, sino, xprobe])
+    return tuple(out[k * n * n:(k + 1) * n * n].reshape(1, n, n) for k in range(4))
