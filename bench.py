@@ -643,14 +643,50 @@ def run_reference(args, rank, world):
 
 
 def kernel_case(case: str, reps: int):
-    """Reduced cases for profiler captures of one kernel family at the
-    workload's padded volume [29, 721, 721] (P = [64, 1458, 1458]); prints
-    timings, not a benchmark line.
+    """Reduced cases for profiler captures of one kernel family; prints
+    timings, not a benchmark line.  At the workload's padded volume
+    [29, 721, 721] (P = [64, 1458, 1458]):
       toeplitz       PSF from the workload's 360 angles, then `reps` A^T A applies
       split_bregman  PSF from 12 of the angles (cheap to build), then
-                     Split-Bregman with `reps` outer iterations, one CG each"""
+                     Split-Bregman with `reps` outer iterations, one CG each
+    and for the 2D paths:
+      batch          the 64-job uneven mix through lc_mbir2d_batch with `reps`
+                     CG iterations (no graph, so each launch is visible)
+      noalloc        `reps` allocation-free Toeplitz applies of 2 slices of
+                     1023 x 1023 (P = 2048)"""
     import torch
     import laminocam_b200 as lc
+    if case == "batch":
+        jobs = mix_jobs(lc)
+        p = lc.ReconParams(regularizer="unconstrained", recon_dims=(1, 1, 1), max_iters=reps, tol=0.0, xtol=0.0)
+        lc.MBIR2D_batch(jobs, p)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        lc.MBIR2D_batch(jobs, p)
+        print(json.dumps({"kernel_case": case, "jobs": len(jobs), "iters": reps,
+                          "ms": (time.time() - t0) * 1e3}), flush=True)
+        return
+    if case == "noalloc":
+        import ctypes as C
+        n, nth, ns = 1023, 720, 2
+        th = np.arange(nth) * np.pi / nth
+        psf = lc.PointSpreadFunction2D(lc.PolarGrid2D(th, n), n, ns)
+        spec = torch.as_tensor(psf.spectrum(), device="cuda").contiguous()
+        x = torch.rand((ns, n, n), device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+        y = torch.empty_like(x)
+        lib = lc._lib.load()
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream or 1)
+        assert lib.lc_sysmat2d_toeplitz_noalloc(None, None, 0, None, None, 0, 0) == 0
+        torch.cuda.synchronize()
+        t0 = time.time()
+        for _ in range(reps):
+            rc = lib.lc_sysmat2d_toeplitz_noalloc(stream, C.c_void_p(spec.data_ptr()), psf.P[2],
+                                                  C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), ns, n)
+            assert rc == 0, rc
+        torch.cuda.synchronize()
+        print(json.dumps({"kernel_case": case, "P": psf.P[2], "reps": reps,
+                          "ms_per_rep": (time.time() - t0) * 1e3 / reps}), flush=True)
+        return
     n1, n = 29, 721
     nth = NANGLES if case == "toeplitz" else 12
     th = np.arange(nth) * 2 * np.pi / nth
@@ -693,7 +729,7 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="reduced case for profiler captures: recon_dims [15,255,255], 180 angles, "
                          "255x255 detector, 5 outer iterations (not a benchmark line)")
-    ap.add_argument("--kernel-case", choices=["toeplitz", "split_bregman"],
+    ap.add_argument("--kernel-case", choices=["toeplitz", "split_bregman", "batch", "noalloc"],
                     help="reduced case for a profiler capture of one kernel family (not a benchmark line)")
     ap.add_argument("--reps", type=int, default=3, help="applies or outer iterations of --kernel-case")
     ap.add_argument("--precision-study", action="store_true",

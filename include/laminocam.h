@@ -149,6 +149,24 @@ int lc_cgsolver(lc_context ctx, lc_psf psf, const float *rhs, float *x, const lc
 int lc_split_bregman(lc_context ctx, lc_psf psf, const float *rhs, float *x,
                      const lc_solver_params *p, lc_solver_stats *stats);
 
+/* The solvers over any linear operator, given as a callback: the
+ * opt::Function<T> argument of opt::cgsolver / opt::split_bregman
+ * (include/optimize.h:30-31, 74-91), e.g. the NUFFT normal operator of
+ * tests/test_cg_normal.cpp:47-101 or a preconditioned one.  Each application
+ * calls op(user, in, out, n, stream): in and out are device vectors of n
+ * floats, stream the cudaStream_t to issue the work on; return 0 on success
+ * (any other value stops the solve with LC_ERR_INVALID).  With
+ * p->use_graph = 1 the iterations are captured into a CUDA graph, so op must
+ * then only enqueue work on stream (no synchronisation, allocation or host
+ * copies); with use_graph = 0 it may do anything.  The split-Bregman operator
+ * is A^T A alone (mu times the negative Laplacian is added by the solver);
+ * dims {n1, n2, n3} shape the finite differences. */
+typedef int (*lc_operator_fn)(void *user, const float *in, float *out, long n, void *stream);
+int lc_cgsolver_op(lc_context ctx, lc_operator_fn op, void *user, long n, const float *rhs, float *x,
+                   const lc_solver_params *p, lc_solver_stats *stats);
+int lc_split_bregman_op(lc_context ctx, lc_operator_fn op, void *user, const int *dims, const float *rhs,
+                        float *x, const lc_solver_params *p, lc_solver_stats *stats);
+
 /* ---- reconstruction drivers (host buffers) ------------------------------ */
 typedef struct {
     int method;           /* 0: CG (UNCONSTRAINED), 1: Split-Bregman */

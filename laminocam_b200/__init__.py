@@ -407,6 +407,78 @@ def split_bregman(A: _PSFBase, yT, x0, lam: float, mu: float, outer_max: int, in
     return (x, _info(st)) if return_info else x
 
 
+def _operator_callback(ctx, A, shape):
+    """Wraps A(x) -> y (torch CUDA tensors of `shape`) as an lc_operator_fn;
+    the exception of a failing A is kept and re-raised by the caller."""
+    torch = _torch()
+    from ._lib import OperatorFn
+    err = []
+
+    def fn(user, pin, pout, n, stream):
+        try:
+            x = _tensor_view(pin, shape, torch)
+            y = _tensor_view(pout, shape, torch)
+            # 0 and 1 are the legacy default stream (cudaStreamLegacy), 2 the
+            # per-thread default stream; torch names the first as its default
+            st = torch.cuda.ExternalStream(stream) if (stream or 0) > 2 else torch.cuda.default_stream()
+            with torch.cuda.stream(st):
+                y.copy_(A(x).reshape(shape))
+            return 0
+        except Exception as ex:  # reported through the status code
+            err.append(ex)
+            return 1
+    return OperatorFn(fn), err
+
+
+def _tensor_view(ptr, shape, torch):
+    """A torch CUDA float32 tensor over device memory at ptr (not owned)."""
+    n = int(np.prod(shape))
+    cls = type("Ptr", (), {"__cuda_array_interface__": {"shape": (n,), "typestr": "<f4", "data": (ptr, False),
+                                                        "version": 3}})
+    return torch.as_tensor(cls(), device="cuda").view(*shape)
+
+
+def cgsolver_op(A, y, x0, max_iter: int, tol: float, xtol: float, ctx: Optional[Context] = None,
+                return_info=False):
+    """opt::cgsolver (include/optimize.h:89-91) over any operator A: a callable
+    taking and returning torch CUDA tensors shaped like y.  Called once per
+    iteration from the solver, with the solver's iteration scalars on the
+    device (no graph capture)."""
+    ctx = ctx or Context.default()
+    ctx.sync_stream()
+    yv = _dev(y, device=ctx.device)
+    x = _dev(x0, device=ctx.device).clone()
+    st = SolverStats()
+    p = _solver_params(max_iter, 1, tol, xtol, 0.0, 1.0)
+    cb, err = _operator_callback(ctx, A, tuple(yv.shape))
+    rc = ctx.lib.lc_cgsolver_op(ctx.handle, cb, None, yv.numel(), _ptr(yv), _ptr(x), C.byref(p), C.byref(st))
+    if err:
+        raise err[0]
+    _check(rc, ctx)
+    return (x, _info(st)) if return_info else x
+
+
+def split_bregman_op(AtA, yT, x0, lam: float, mu: float, outer_max: int, inner_max: int, tol: float,
+                     xtol: float, ctx: Optional[Context] = None, return_info=False):
+    """opt::split_bregman (include/optimize.h:74-77) over any normal operator
+    AtA (a callable on torch CUDA tensors shaped like yT, {n1, n2, n3} or
+    {n2, n3}); mu times the negative Laplacian is added by the solver."""
+    ctx = ctx or Context.default()
+    ctx.sync_stream()
+    yv = _dev(yT, device=ctx.device)
+    x = _dev(x0, device=ctx.device).clone()
+    shape = tuple(yv.shape)
+    dims = (C.c_int * 3)(*((1,) * (3 - len(shape)) + shape))
+    st = SolverStats()
+    p = _solver_params(outer_max, inner_max, tol, xtol, lam, mu)
+    cb, err = _operator_callback(ctx, AtA, shape)
+    rc = ctx.lib.lc_split_bregman_op(ctx.handle, cb, None, dims, _ptr(yv), _ptr(x), C.byref(p), C.byref(st))
+    if err:
+        raise err[0]
+    _check(rc, ctx)
+    return (x, _info(st)) if return_info else x
+
+
 @dataclass
 class ReconParams:
     """ReconParams (include/recon_params.h:45-55)."""

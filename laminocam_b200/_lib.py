@@ -56,6 +56,8 @@ class Job2D(C.Structure):
                 ("theta", C.POINTER(C.c_double)), ("n", C.c_int), ("recon", C.POINTER(C.c_float))]
 
 
+OperatorFn = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p)
+
 vp = C.c_void_p
 i32 = C.c_int
 f64 = C.c_double
@@ -96,6 +98,10 @@ SIGNATURES = {
                         C.POINTER(ReconParamsC), fptr, C.POINTER(SolverStats)]),
     "lc_mbir3d_device": (i32, [vp, vp, i32, i32, i32, dptr, dptr, dptr, fptr, C.POINTER(C.c_int),
                                C.POINTER(ReconParamsC), vp, C.POINTER(SolverStats)]),
+    "lc_cgsolver_op": (i32, [vp, OperatorFn, vp, C.c_long, vp, vp, C.POINTER(SolverParams),
+                             C.POINTER(SolverStats)]),
+    "lc_split_bregman_op": (i32, [vp, OperatorFn, vp, C.POINTER(C.c_int), vp, vp, C.POINTER(SolverParams),
+                                  C.POINTER(SolverStats)]),
     "lc_mbir2d_batch": (i32, [vp, C.POINTER(Job2D), i32, C.POINTER(ReconParamsC), i32,
                               C.POINTER(SolverStats)]),
     "lc_profile_enable": (i32, [vp, i32]),

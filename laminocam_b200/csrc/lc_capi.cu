@@ -1,5 +1,6 @@
 // extern "C" boundary of laminocam_b200 (declared in include/laminocam.h).
 #include <algorithm>
+#include <chrono>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -557,6 +558,55 @@ int lc_split_bregman(lc_context c, lc_psf p, const float *rhs, float *x,
     return guarded(c, [&] {
         LC_REQUIRE(p && rhs && x, "NULL argument");
         run_solver(p, 1, rhs, x, prm, stats);
+    });
+}
+
+// The solvers over an operator given as a callback (opt::Function<T>,
+// include/optimize.h:30-31): each application calls op(user, in, out, n,
+// stream) with device vectors of n floats; a nonzero return stops the solve
+// with LC_ERR_INVALID and the callback's code in the message.
+static void run_solver_op(lc_context c, int method, lc_operator_fn op, void *user, const long dims[3],
+                          const float *rhs, float *x, const lc_solver_params *prm, lc_solver_stats *stats) {
+    LC_REQUIRE(op && rhs && x, "NULL argument");
+    check_solver_params(prm);
+    if (method == 1) LC_REQUIRE(prm->mu != 0.0f, "split_bregman: mu must be non-zero");
+    Context &ctx = *c->ctx;
+    const long n = dims[0] * dims[1] * dims[2];
+    LC_REQUIRE(n > 0, "operator size must be positive");
+    Solver solver(ctx, n);
+    Operator A = [&ctx, op, user, n](const float *in, float *out) {
+        const int rc = op(user, in, out, n, (void *)ctx.stream());
+        if (rc) throw Error(1, "operator callback returned " + std::to_string(rc));
+    };
+    SolverStats st;
+    const auto t0 = std::chrono::steady_clock::now();
+    if (method == 0) solver.cg(ctx, A, rhs, x, to_sp(prm), &st, nullptr);
+    else solver.split_bregman(ctx, A, dims, rhs, x, to_sp(prm), &st);
+    LC_CUDA(cudaStreamSynchronize(ctx.stream()));
+    if (stats) {
+        stats->iters = st.iters;
+        stats->cg_iters_total = st.cg_iters_total;
+        stats->residual = st.residual;
+        stats->dx = st.dx;
+        stats->stop_reason = st.stop_reason;
+        stats->elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+}
+
+int lc_cgsolver_op(lc_context c, lc_operator_fn op, void *user, long n, const float *rhs, float *x,
+                   const lc_solver_params *prm, lc_solver_stats *stats) {
+    return guarded(c, [&] {
+        const long dims[3] = {1, 1, n};
+        run_solver_op(c, 0, op, user, dims, rhs, x, prm, stats);
+    });
+}
+
+int lc_split_bregman_op(lc_context c, lc_operator_fn op, void *user, const int *dims, const float *rhs,
+                        float *x, const lc_solver_params *prm, lc_solver_stats *stats) {
+    return guarded(c, [&] {
+        LC_REQUIRE(dims && dims[0] > 0 && dims[1] > 0 && dims[2] > 0, "dims must be positive");
+        const long d[3] = {dims[0], dims[1], dims[2]};
+        run_solver_op(c, 1, op, user, d, rhs, x, prm, stats);
     });
 }
 
