@@ -568,16 +568,23 @@ def serving_stream(lc, workers=32, count=STREAM_REQUESTS, rates=STREAM_RATES):
             st = sv.stats()
             slat = [lag * 1e3 + r.latency_ms for (_, lag), r in zip(subs, res)]
             diffs = [O.rel_l2(r.recon, p) for r, p in zip(res, plain_out)]
+
+            def by_class(lats, kind):
+                v = [x for x, (_, key, _) in zip(lats, reqs) if key[0] == kind]
+                return {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99))} if v else None
             out["rates"].append({
                 "rate_req_s": rate,
                 "plain": {"recons_per_s": count / t_plain, "seconds": t_plain,
                           "latency_ms_p50": float(np.percentile(lat, 50)),
                           "latency_ms_p99": float(np.percentile(lat, 99)),
+                          "latency_ms_2d": by_class(lat, "2d"), "latency_ms_3d": by_class(lat, "3d"),
                           "service_ms_by_kind": {k: {"requests": v[0], "total_ms": round(v[1], 1)}
                                                  for k, v in sorted(service.items())}},
                 "served": {"recons_per_s": count / t_served, "seconds": t_served,
                            "latency_ms_p50": float(np.percentile(slat, 50)),
                            "latency_ms_p99": float(np.percentile(slat, 99)),
+                           "latency_ms_2d": by_class(slat, "2d"), "latency_ms_3d": by_class(slat, "3d"),
+                           "backfilled": st["backfilled"],
                            "peak_running": st["peak_running"],
                            "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9,
                            "psf_hits": st["psf_hits"], "psf_misses": st["psf_misses"],

@@ -277,7 +277,9 @@ int lc_sysmat2d_toeplitz_noalloc(void *stream, const float *spectrum, int P, con
  * one GPU.  Jobs submitted from any thread queue in FIFO order; a fixed set of
  * workers (one context and stream each) starts the head job once its
  * estimated device footprint fits the HBM budget next to the running jobs, so
- * jobs that arrive while others run overlap with them on the device.  Toeplitz
+ * jobs that arrive while others run overlap with them on the device.  While
+ * the head does not fit, later jobs that do fit may start first (backfill, at
+ * most `backfill` of them per head, so the head is not starved).  Toeplitz
  * spectra are kept in a geometry-keyed cache (key: the exact angles, the
  * detector size and the padded dims); a job whose geometry is cached skips
  * the PSF construction.  A job computes what lc_mbir2d / lc_mbir3d compute for
@@ -292,6 +294,10 @@ typedef struct {
     double hbm_budget_bytes; /* admission budget; 0: 85% of the free memory at creation */
     double psf_cache_bytes;  /* cap of the Toeplitz spectrum cache; 0: 16 GiB */
     int psf_cache;           /* 0 disables the cache */
+    int backfill;            /* max jobs that may start ahead of a queue head that does not
+                                fit the budget yet (0: strict FIFO; default 16) */
+    int priority_2d;         /* 1 (default): 2D jobs run on high-priority streams, so a slice
+                                next to a running volume gets SMs first */
 } lc_server_params;
 
 typedef struct {
@@ -312,6 +318,9 @@ typedef struct {
     double hbm_budget_bytes, peak_admitted_bytes;
     long psf_hits, psf_misses, psf_cache_entries;
     double psf_cache_bytes;
+    double p50_2d_ms, p99_2d_ms;    /* latency of the completed 2D jobs */
+    double p50_3d_ms, p99_3d_ms;    /* latency of the completed laminography jobs */
+    long backfilled;                /* jobs that started ahead of a waiting queue head */
 } lc_server_stats;
 
 void lc_server_params_default(lc_server_params *p);

@@ -631,19 +631,25 @@ class Server:
 
     Jobs are gpu::MBIR2D / gpu::MBIR reconstructions with the arguments of
     MBIR2D and MBIR.  They queue in FIFO order, and up to `workers` of them run
-    at once when their device footprint fits the HBM budget.  Toeplitz spectra
-    are cached per geometry.  `submit2d` / `submit3d` return a job id; `wait`
-    returns a JobResult or raises LaminocamError with the job's message.
+    at once when their device footprint fits the HBM budget; while the head of
+    the queue waits for memory, up to `backfill` later jobs that fit may start
+    ahead of it.  2D jobs run on high-priority streams (`priority_2d`).
+    Toeplitz spectra are cached per geometry.  `submit2d` / `submit3d` return
+    a job id; `wait` returns a JobResult or raises LaminocamError with the
+    job's message.
     """
 
     def __init__(self, device: int = 0, workers: int = 4, hbm_budget_bytes: float = 0.0,
-                 psf_cache_bytes: float = 0.0, psf_cache: bool = True):
+                 psf_cache_bytes: float = 0.0, psf_cache: bool = True, backfill: int = 16,
+                 priority_2d: bool = True):
         self.lib = _lib.load()
         p = _lib.ServerParams()
         self.lib.lc_server_params_default(C.byref(p))
         p.device, p.workers = int(device), int(workers)
         p.hbm_budget_bytes, p.psf_cache_bytes = float(hbm_budget_bytes), float(psf_cache_bytes)
         p.psf_cache = int(bool(psf_cache))
+        p.backfill = int(backfill)
+        p.priority_2d = int(bool(priority_2d))
         h = C.c_void_p()
         rc = self.lib.lc_server_create(C.byref(p), C.byref(h))
         if rc != 0:

@@ -32,7 +32,8 @@ class ProfileEntry(C.Structure):
 
 class ServerParams(C.Structure):
     _fields_ = [("device", C.c_int), ("workers", C.c_int), ("hbm_budget_bytes", C.c_double),
-                ("psf_cache_bytes", C.c_double), ("psf_cache", C.c_int)]
+                ("psf_cache_bytes", C.c_double), ("psf_cache", C.c_int), ("backfill", C.c_int),
+                ("priority_2d", C.c_int)]
 
 
 class JobInfo(C.Structure):
@@ -48,7 +49,8 @@ class ServerStats(C.Structure):
                 ("recons_per_s", C.c_double), ("hbm_budget_bytes", C.c_double),
                 ("peak_admitted_bytes", C.c_double), ("psf_hits", C.c_long),
                 ("psf_misses", C.c_long), ("psf_cache_entries", C.c_long),
-                ("psf_cache_bytes", C.c_double)]
+                ("psf_cache_bytes", C.c_double), ("p50_2d_ms", C.c_double), ("p99_2d_ms", C.c_double),
+                ("p50_3d_ms", C.c_double), ("p99_3d_ms", C.c_double), ("backfilled", C.c_long)]
 
 
 class Job2D(C.Structure):

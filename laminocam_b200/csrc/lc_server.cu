@@ -8,7 +8,12 @@
 //  * admission: the head job starts only when its estimated device footprint
 //    fits in the HBM budget next to the jobs already running, so requests
 //    that arrive while others run are admitted as workers and memory free up,
-//    and their kernels overlap on the device;
+//    and their kernels overlap on the device; while the head waits for
+//    memory, later jobs that fit start ahead of it (backfill), at most
+//    `backfill` of them per head so that it cannot starve;
+//  * 2D jobs run on high-priority streams: a slice submitted next to a
+//    running laminography volume gets SMs as soon as CTAs of the volume
+//    retire, instead of waiting behind its whole launches;
 //  * a geometry-keyed cache keeps the FP32 Toeplitz spectra resident: a job on
 //    a geometry seen before skips the PSF construction and shares the cached
 //    spectrum read-only (only its work buffers are its own);
@@ -216,19 +221,41 @@ struct lc_server_s {
     long long next_id = 1;
     size_t budget = 0, in_use = 0, peak_in_use = 0;
     int running = 0, peak_running = 0;
+    int head_bypassed = 0;  // jobs started ahead of the current head
+    long backfilled = 0;
+    std::vector<cudaStream_t> hi_streams;  // per worker, for 2D jobs
     bool stopping = false;
     std::unique_ptr<PsfCache> cache;
     PsfProvider provider;
     std::string err;
     // finished jobs
-    std::vector<double> latencies;
+    std::vector<double> latencies, lat2d, lat3d;
     long completed = 0, failed = 0;
     bool have_first = false;
     Clock::time_point t_first_submit, t_last_end;
 
+    ~lc_server_s() {
+        // the contexts' buffers may be ordered on the high-priority streams
+        ctxs.clear();
+        for (cudaStream_t x : hi_streams)
+            if (x) cudaStreamDestroy(x);
+    }
     void worker_loop(int w);
     void run_job(int w, Job &j);
+    // the queued job to start now (queue.end() if none), called under mu
+    std::deque<std::shared_ptr<Job>>::iterator pick();
 };
+
+std::deque<std::shared_ptr<Job>>::iterator lc_server_s::pick() {
+    if (queue.empty()) return queue.end();
+    // a job alone always starts; the head starts when it fits the budget
+    if (running == 0 || in_use + queue.front()->bytes <= budget) return queue.begin();
+    // backfill: the first later job that fits, while the head may still be bypassed
+    if (head_bypassed >= prm.backfill) return queue.end();
+    for (auto it = std::next(queue.begin()); it != queue.end(); ++it)
+        if (in_use + (*it)->bytes <= budget) return it;
+    return queue.end();
+}
 
 void lc_server_s::run_job(int w, Job &j) {
     lc_context c = ctxs[w].get();
@@ -238,6 +265,16 @@ void lc_server_s::run_job(int w, Job &j) {
     const PsfProvider *pp = cache ? &provider : nullptr;
     const long nin = (long)j.d0 * j.d1 * j.d2;
     const long nv = (long)j.recon_dims[0] * j.recon_dims[1] * j.recon_dims[2];
+    // the job's stream: the worker's high-priority one for 2D jobs
+    struct StreamSwap {
+        Context &ctx;
+        cudaStream_t prev;
+        ~StreamSwap() { ctx.set_stream(prev); }
+    } swap{ctx, s};
+    if (!j.three_d && w < (int)hi_streams.size() && hi_streams[w]) {
+        ctx.set_stream(hi_streams[w]);
+        s = hi_streams[w];
+    }
     DevBuf<float> din, dout(nv, s);
     if (!j.three_d) {
         din.upload(j.in, nin, s);
@@ -261,15 +298,23 @@ void lc_server_s::worker_loop(int w) {
         std::shared_ptr<Job> j;
         {
             std::unique_lock<std::mutex> lk(mu);
-            // FIFO: only the head may start, and only when it fits the budget
-            // next to the running jobs (a job alone always starts)
+            // the head when it fits the budget next to the running jobs (a job
+            // alone always starts), else a later job that fits (backfill)
+            std::deque<std::shared_ptr<Job>>::iterator it;
             cv_work.wait(lk, [&] {
                 if (queue.empty()) return stopping;
-                return running == 0 || in_use + queue.front()->bytes <= budget;
+                it = pick();
+                return it != queue.end();
             });
             if (queue.empty()) return;
-            j = queue.front();
-            queue.pop_front();
+            if (it == queue.begin()) {
+                head_bypassed = 0;
+            } else {
+                ++head_bypassed;
+                ++backfilled;
+            }
+            j = *it;
+            queue.erase(it);
             in_use += j->bytes;
             peak_in_use = std::max(peak_in_use, in_use);
             ++running;
@@ -296,7 +341,9 @@ void lc_server_s::worker_loop(int w) {
             --running;
             if (rc == LC_OK) {
                 ++completed;
-                latencies.push_back(ms_between(j->t_submit, j->t_end));
+                const double lat = ms_between(j->t_submit, j->t_end);
+                latencies.push_back(lat);
+                (j->three_d ? lat3d : lat2d).push_back(lat);
             } else {
                 ++failed;
             }
@@ -360,13 +407,15 @@ void lc_server_params_default(lc_server_params *p) {
     p->hbm_budget_bytes = 0;  // 0: 85% of the free device memory at creation
     p->psf_cache_bytes = 0;   // 0: 16 GiB
     p->psf_cache = 1;
+    p->backfill = 16;
+    p->priority_2d = 1;
 }
 
 int lc_server_create(const lc_server_params *prm, lc_server *out) {
     if (!prm || !out) return LC_ERR_INVALID;
     *out = nullptr;
     if (prm->workers < 1 || prm->workers > 64) return LC_ERR_INVALID;
-    if (prm->hbm_budget_bytes < 0 || prm->psf_cache_bytes < 0) return LC_ERR_INVALID;
+    if (prm->hbm_budget_bytes < 0 || prm->psf_cache_bytes < 0 || prm->backfill < 0) return LC_ERR_INVALID;
     auto sv = std::make_unique<lc_server_s>();
     std::string msg;
     const int rc = run_guarded(msg, [&] {
@@ -387,6 +436,13 @@ int lc_server_create(const lc_server_params *prm, lc_server *out) {
             auto c = std::make_unique<lc_context_s>();
             c->ctx = std::make_unique<Context>(prm->device, nullptr);
             sv->ctxs.push_back(std::move(c));
+        }
+        if (prm->priority_2d) {
+            int lo = 0, hi = 0;
+            LC_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));  // hi: greatest priority
+            sv->hi_streams.assign(prm->workers, nullptr);
+            for (int w = 0; w < prm->workers; ++w)
+                LC_CUDA(cudaStreamCreateWithPriority(&sv->hi_streams[w], cudaStreamNonBlocking, hi));
         }
         lc_server_s *raw = sv.get();
         for (int w = 0; w < prm->workers; ++w) sv->workers.emplace_back([raw, w] { raw->worker_loop(w); });
@@ -416,6 +472,10 @@ int lc_server_destroy(lc_server sv) {
         DeviceGuard dg(sv->prm.device);
         if (sv->cache) sv->cache->clear();
         sv->ctxs.clear();
+        for (cudaStream_t &x : sv->hi_streams) {
+            if (x) cudaStreamDestroy(x);
+            x = nullptr;
+        }
     }
     delete sv;
     return LC_OK;
@@ -524,6 +584,11 @@ int lc_server_get_stats(lc_server sv, lc_server_stats *out) {
         }
         out->hbm_budget_bytes = (double)sv->budget;
         out->peak_admitted_bytes = (double)sv->peak_in_use;
+        out->p50_2d_ms = percentile(sv->lat2d, 0.50);
+        out->p99_2d_ms = percentile(sv->lat2d, 0.99);
+        out->p50_3d_ms = percentile(sv->lat3d, 0.50);
+        out->p99_3d_ms = percentile(sv->lat3d, 0.99);
+        out->backfilled = sv->backfilled;
     }
     if (sv->cache) {
         size_t used = 0;
@@ -537,6 +602,9 @@ int lc_server_reset_stats(lc_server sv) {
     if (!sv) return LC_ERR_INVALID;
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->latencies.clear();
+    sv->lat2d.clear();
+    sv->lat3d.clear();
+    sv->backfilled = 0;
     sv->completed = sv->failed = 0;
     sv->have_first = false;
     sv->peak_in_use = sv->in_use;

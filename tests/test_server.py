@@ -218,3 +218,35 @@ def test_server_admission_respects_budget(lc):
     assert 1 <= st["peak_running"] <= 2
     for r in res[1:]:
         assert np.array_equal(r.recon, res[0].recon)
+
+
+def test_server_backfill_starts_small_jobs_ahead_of_a_waiting_head(lc):
+    """Budget for one large job: while the second large job waits at the head
+    of the queue for memory, small jobs behind it start on the free workers
+    (backfill) instead of waiting; with backfill 0 the order is strict FIFO.
+    Results are the same either way."""
+    # (the footprint estimate holds a fixed 64 MiB per job, so the large job
+    # must be large for two small ones to fit beside it)
+    sb, thb = sino2d(lc, 1023, 90, 61)
+    ss, ths = sino2d(lc, 63, 60, 62)
+    big = params2d(lc, 1023, "unconstrained", 50)
+    small = params2d(lc, 63, "unconstrained", 50)
+    with lc.Server(workers=1) as probe:
+        one = probe.wait(probe.submit2d(sb, thb, big), WAIT_S).device_bytes
+        ref_small = probe.wait(probe.submit2d(ss, ths, small), WAIT_S).recon
+    for backfill in (16, 0):
+        with lc.Server(workers=4, hbm_budget_bytes=1.5 * one, backfill=backfill) as sv:
+            ids = [sv.submit2d(sb, thb, big), sv.submit2d(sb, thb, big)]
+            ids += [sv.submit2d(ss, ths, small) for _ in range(4)]
+            res = [sv.wait(j, WAIT_S) for j in ids]
+            st = sv.stats()
+        assert st["completed"] == 6 and st["failed"] == 0
+        for r in res[2:]:
+            assert np.array_equal(r.recon, ref_small)
+        if backfill:
+            assert st["backfilled"] >= 1
+            # the small jobs did not wait for the second large job to finish
+            assert max(r.queue_ms for r in res[2:]) < res[1].queue_ms + res[1].run_ms
+        else:
+            assert st["backfilled"] == 0
+        assert st["p50_2d_ms"] > 0 and st["p99_2d_ms"] >= st["p50_2d_ms"] and st["p50_3d_ms"] == 0
