@@ -28,7 +28,10 @@
 namespace lc {
 namespace {
 
-constexpr int kCols = 4;  // columns per CTA: 32-byte row segments
+#ifndef LC_COL_LINES
+#define LC_COL_LINES 4
+#endif
+constexpr int kCols = LC_COL_LINES;  // columns per CTA: 32-byte row segments
 
 enum ColMode { CM_PLAIN = 0, CM_PLAIN_MID = 1, CM_SPLIT_IN = 2, CM_SPLIT_OUT = 3, CM_SPLIT_MID = 4 };
 

@@ -26,6 +26,10 @@
 #include "lc_fft.hpp"
 #include "lc_regfft.cuh"
 
+#ifndef LC_Z64_COLS
+#define LC_Z64_COLS 32  // columns per CTA of the 64-point z convolution
+#endif
+
 namespace lc {
 namespace {
 
@@ -156,7 +160,7 @@ bool launch_zconv(cudaStream_t st, float2 *data, long n_inner, int L, int n_in, 
         case 32: launch_z<8, 4, 32>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
         case 36: launch_z<6, 6, 32>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
         case 48: launch_z<8, 6, 32>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
-        case 64: launch_z<8, 8, 32>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
+        case 64: launch_z<8, 8, LC_Z64_COLS>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
         case 72: launch_z<8, 9, 16>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
         case 96: launch_z<8, 12, 16>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
         case 128: launch_z<8, 16, 16>(st, data, n_inner, n_in, n_out, spec, fold ? 1 : 0); return true;
