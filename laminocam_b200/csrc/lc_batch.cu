@@ -29,11 +29,14 @@
 //
 // The setup of every job (sinogram upload, bin sort, backprojection, FP64
 // PSF) runs on a pool of worker contexts, each with its own stream; the
-// batched iterations then run on the caller's context, replayed from a CUDA
-// graph of eight iterations.
+// batched iterations run on the caller's context, replayed from a CUDA graph
+// of eight iterations.  Batches of eight jobs or more run in two waves: the
+// larger half (by pixels x angles) iterates while the workers still set up
+// the other half, so setup and iterations overlap on the GPU.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -550,12 +553,34 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
         std::vector<DevBuf<float>> rhs(njobs), xs(njobs);
         std::vector<std::shared_ptr<Toeplitz>> ops(njobs);
         std::vector<std::string> errs(njobs);
+        // Two waves: the larger jobs (by pixels x angles, about half the
+        // setup work) are set up first and iterate on the caller's stream
+        // while the workers set up the rest.  A job's result does not depend
+        // on the batch it runs in.
+        std::vector<int> order(njobs);
+        for (int j = 0; j < njobs; ++j) order[j] = j;
+        auto cost = [&](int j) { return (double)jobs[j].n * jobs[j].n * (double)jobs[j].ntheta; };
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+        std::vector<int> wave_end;
+        if (njobs >= 8) {
+            double tot = 0, acc = 0;
+            for (int j = 0; j < njobs; ++j) tot += cost(j);
+            int h = 0;
+            while (h < njobs - 1 && acc < 0.5 * tot) acc += cost(order[h++]);
+            wave_end = {h, njobs};
+        } else {
+            wave_end = {njobs};
+        }
+        std::mutex mu;
+        std::condition_variable cv;
+        std::vector<char> ready(njobs, 0);
         std::atomic<int> next{0};
         auto work = [&](int w) {
             lc_context wc = wctx[w].get();
             Context &wx = *wc->ctx;
             DeviceGuard dg(wx.device());
-            for (int j = next++; j < njobs; j = next++) {
+            for (int t = next++; t < njobs; t = next++) {
+                const int j = order[t];
                 const lc_job2d &q = jobs[j];
                 const int rc = run_guarded(errs[j], [&] {
                     LC_BATCH_T0();
@@ -581,6 +606,11 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
                     LC_BATCH_T(3);
                 });
                 if (rc && errs[j].empty()) errs[j] = "setup failed";
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    ready[t] = 1;
+                }
+                cv.notify_all();
             }
         };
 #ifdef LC_BATCH_TRACE
@@ -588,36 +618,66 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
         const auto lc_t0 = std::chrono::steady_clock::now();
 #endif
         std::vector<std::thread> th;
-        for (int w = 1; w < nw; ++w) th.emplace_back(work, w);
-        work(0);
+        for (int w = 0; w < nw; ++w) th.emplace_back(work, w);
+        // the workers finish every setup even when a wave fails: on every exit
+        // path join them and drain the caller's stream before the buffers go
+        struct Joiner {
+            std::vector<std::thread> &t;
+            cudaStream_t s;
+            ~Joiner() {
+                for (auto &x : t)
+                    if (x.joinable()) x.join();
+                cudaStreamSynchronize(s);
+            }
+        } joiner{th, s};
+        int begin = 0;
+        for (const int end : wave_end) {
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&] {
+                    for (int t = begin; t < end; ++t)
+                        if (!ready[t]) return false;
+                    return true;
+                });
+            }
+#ifdef LC_BATCH_TRACE
+            std::fprintf(stderr, "batch wave [%d, %d) set up at %.2f ms\n", begin, end,
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - lc_t0).count());
+#endif
+            for (int t = begin; t < end; ++t)
+                if (!errs[order[t]].empty())
+                    throw Error(1, "job " + std::to_string(order[t]) + ": " + errs[order[t]]);
+            std::vector<BatchCG2D::Job> bj;
+            for (int t = begin; t < end; ++t) {
+                const int j = order[t];
+                bj.push_back({ops[j], rhs[j].get(), xs[j].get(), p->solver.max_iters, p->solver.tol, p->solver.xtol});
+            }
+            std::vector<CGState> fin;
+            {
+                BatchCG2D batch(ctx, std::move(bj));
+                batch.run(ctx, p->solver.use_graph != 0, &fin);
+            }
+            for (int t = begin; t < end; ++t) {
+                const int j = order[t];
+                const long nv = (long)jobs[j].n * jobs[j].n;
+                LC_CUDA(cudaMemcpyAsync(jobs[j].recon, xs[j].get(), nv * sizeof(float), cudaMemcpyDeviceToHost, s));
+                if (stats) {
+                    const CGState &f = fin[t - begin];
+                    stats[j].iters = f.iters;
+                    stats[j].cg_iters_total = f.iters;
+                    stats[j].residual = f.res;
+                    stats[j].dx = f.dx;
+                    stats[j].stop_reason = f.reason;
+                    stats[j].elapsed_ms = 0.0;
+                }
+            }
+            begin = end;
+        }
         for (auto &t : th) t.join();
 #ifdef LC_BATCH_TRACE
-        std::fprintf(stderr, "batch setup wall %.2f ms; summed over jobs: geometry %.2f backproj %.2f psf %.2f drain %.2f\n",
-                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - lc_t0).count(),
+        std::fprintf(stderr, "batch setup summed over jobs: geometry %.2f backproj %.2f psf %.2f drain %.2f\n",
                      g_batch_t[0], g_batch_t[1], g_batch_t[2], g_batch_t[3]);
 #endif
-        for (int j = 0; j < njobs; ++j)
-            if (!errs[j].empty()) throw Error(1, "job " + std::to_string(j) + ": " + errs[j]);
-        std::vector<BatchCG2D::Job> bj(njobs);
-        for (int j = 0; j < njobs; ++j)
-            bj[j] = {ops[j], rhs[j].get(), xs[j].get(), p->solver.max_iters, p->solver.tol, p->solver.xtol};
-        std::vector<CGState> fin;
-        {
-            BatchCG2D batch(ctx, std::move(bj));
-            batch.run(ctx, p->solver.use_graph != 0, &fin);
-        }
-        for (int j = 0; j < njobs; ++j) {
-            const long nv = (long)jobs[j].n * jobs[j].n;
-            LC_CUDA(cudaMemcpyAsync(jobs[j].recon, xs[j].get(), nv * sizeof(float), cudaMemcpyDeviceToHost, s));
-            if (stats) {
-                stats[j].iters = fin[j].iters;
-                stats[j].cg_iters_total = fin[j].iters;
-                stats[j].residual = fin[j].res;
-                stats[j].dx = fin[j].dx;
-                stats[j].stop_reason = fin[j].reason;
-                stats[j].elapsed_ms = 0.0;
-            }
-        }
         LC_CUDA(cudaStreamSynchronize(s));
         // worker-owned buffers are released in the order of the workers' streams
         for (auto &o : ops) o.reset();

@@ -149,6 +149,17 @@ void launch_axis_fft(Context &ctx, const AxisFFT &a);
 bool launch_zconv(cudaStream_t st, float2 *data, long n_inner, int L, int n_in, int n_out,
                   const float *spec, bool fold = false);
 
+// The z stage of a Toeplitz kernel that is even in z, as the direct product
+// with a real symmetric Toeplitz matrix per column, in place:
+//     data[z][c] <- sum_{z' < n} taps[|z - z'|][c] data[z'][c],   z < n,
+// taps = the first n planes of the kernel's z-profile per (ky, kx) column
+// (times L).  Returns false for n above zdirect_max_rows() (the caller then
+// runs the FFT form, launch_zconv).
+bool launch_zdirect(cudaStream_t st, float2 *data, long n_inner, int n, const float *taps);
+int zdirect_max_rows();
+// false when the environment sets LC_ZDIRECT=0 (the FFT form everywhere)
+bool zdirect_enabled();
+
 // Column transforms (n_inner > 1) without index maps, per-index factors or
 // scale, in FP32 complex, as register-resident kernels with compile-time
 // radix plans; even lengths whose input or output fits in half the line run

@@ -355,6 +355,17 @@ __global__ void zero_unpaired_kernel(double *__restrict__ K, int P1, int P2, int
     }
 }
 
+// taps[d][c] = L * Re b[(L/2 + d)][c], d < n: the planes of the kernel after
+// its x and y transforms at z offsets 0..n-1 (b is in mode order along z)
+__global__ void zdirect_taps_kernel(const double2 *__restrict__ b, float *__restrict__ taps, long plane, int n,
+                                    int L) {
+    const long total = (long)n * plane;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long d = i / plane, c = i - d * plane;
+        taps[i] = (float)((double)L * b[(L / 2 + d) * plane + c].x);
+    }
+}
+
 __global__ void d2f_kernel(const double *__restrict__ in, float *__restrict__ out, long n) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         out[i] = (float)in[i];
@@ -518,6 +529,13 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
     // an FFT along z of a kernel even in kz is even in f1: keep the planes
     // f1 <= P1/2 (a prefix of the plane-major array)
     zfold_ = three_d && kernel_mirror_;
+    if (zfold_ && zdirect_enabled() && n_[0] <= zdirect_max_rows()) {
+        const long plane = (long)P2 * P3h;
+        Kz_ = std::make_shared<DevBuf<float>>(n_[0] * plane, st);
+        zdirect_taps_kernel<<<grid_for(n_[0] * plane, 256, ctx.num_sms()), 256, 0, st>>>(b.get(), Kz_->get(),
+                                                                                         plane, (int)n_[0], P1);
+        LC_CHECK_LAUNCH();
+    }
     long nR = stored_spectrum_elems();
     R_ = std::make_shared<DevBuf<float>>(nR, st);
     d2f_kernel<<<grid_for(nR, 256, ctx.num_sms()), 256, 0, st>>>(Rd.get(), R_->get(), nR);
@@ -554,15 +572,18 @@ size_t Toeplitz::work_bytes(const long dims[3], bool three_d) {
 size_t Toeplitz::build_peak_bytes(const long dims[3], bool three_d) {
     long P[3], Ph[3];
     psf_sizes(dims, three_d, P, Ph);
-    // FP64 kernel, two complex FP64 FFT buffers, FP64 and FP32 real spectra
+    // FP64 kernel, two complex FP64 FFT buffers, FP64 and FP32 real spectra,
+    // and the direct z-stage taps (3D, at most n1 planes)
     const size_t full = (size_t)P[0] * P[1] * P[2];
     const size_t half = (size_t)P[0] * P[1] * Ph[2];
-    return full * sizeof(double) + 2 * half * sizeof(double2) + half * (sizeof(double) + sizeof(float));
+    const size_t taps = three_d ? (size_t)dims[0] * P[1] * Ph[2] : 0;
+    return full * sizeof(double) + 2 * half * sizeof(double2) + half * (sizeof(double) + sizeof(float)) +
+           taps * sizeof(float);
 }
 
 Toeplitz::Toeplitz(Context &ctx, const Toeplitz &src, bool work)
     : three_d_(src.three_d_), kernel_mirror_(src.kernel_mirror_), zfold_(src.zfold_), g_(nullptr), R_(src.R_),
-      scale_(src.scale_) {
+      Kz_(src.Kz_), scale_(src.scale_) {
     for (int d = 0; d < 3; ++d) {
         n_[d] = src.n_[d];
         P_[d] = src.P_[d];
@@ -744,8 +765,8 @@ void Toeplitz::kernel_fp64(Context &ctx, double *host_out) {
 }
 
 double Toeplitz::algorithmic_bytes() const {
-    // read x, write y, read the real spectrum octant once
-    return 8.0 * (double)nvox() + 4.0 * (double)stored_spectrum_elems();
+    // read x, write y, read the real spectrum octant (or the z taps) once
+    return 8.0 * (double)nvox() + 4.0 * (double)(Kz_ ? (long)Kz_->size() : stored_spectrum_elems());
 }
 
 unsigned Toeplitz::cg_caps() const {
@@ -830,7 +851,10 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y, const CGFusion *f, 
             a.sign = -1;
             launch_axis_fft(ctx, a);
         }
-        if (ProfScope ps(ctx, PS_TOEP_Z_MID, 2.0 * T2 + Rb);
+        if (Kz_) {
+            ProfScope ps(ctx, PS_TOEP_Z_MID, 2.0 * T2 + 4.0 * (double)Kz_->size());
+            launch_zdirect(ctx.stream(), t2_.get(), (long)P2 * P3h, (int)n1, Kz_->get());
+        } else if (ProfScope ps(ctx, PS_TOEP_Z_MID, 2.0 * T2 + Rb);
             !(line_kernels_enabled() &&
               launch_zconv(ctx.stream(), t2_.get(), (long)P2 * P3h, P1, (int)n1, (int)n1, R_->get(),
                            zfold_))) {

@@ -61,7 +61,11 @@ class Toeplitz {
     size_t device_bytes() const {
         return spectrum_bytes() + (t1_.size() + t2_.size()) * sizeof(float2);
     }
-    size_t spectrum_bytes() const { return R_->size() * sizeof(float); }
+    // the spectrum and, when the z stage runs in direct form, its taps
+    size_t spectrum_bytes() const { return (R_->size() + (Kz_ ? Kz_->size() : 0)) * sizeof(float); }
+    // the z stage runs as the direct Toeplitz product (kernel even in z,
+    // n1 <= zdirect_max_rows()); its taps are {n1, P2, P3/2+1} floats
+    bool z_direct() const { return (bool)Kz_; }
     // device bytes, for given dims, of the work buffers of one apply and of
     // the peak of a spectrum construction
     static size_t work_bytes(const long dims[3], bool three_d);
@@ -82,6 +86,7 @@ class Toeplitz {
     int Ph_[3];
     const PolarGeometry *g_;
     std::shared_ptr<DevBuf<float>> R_;
+    std::shared_ptr<DevBuf<float>> Kz_;  // direct z-stage taps L b(dz), dz < n1 (or null)
     DevBuf<float2> t1_, t2_;
     double scale_;
 };

@@ -23,6 +23,18 @@
 // Y[2m] = DFT_{A/2}(x)[m], Y[2m+1] = DFT_{A/2}(x h)[m] with
 // h(a) = exp(-2 pi i a / A) = w^(B a); inverse
 // x[a] = DFT+_{A/2}(Y_even)[a] + conj h(a) DFT+_{A/2}(Y_odd)[a].
+//
+// Direct form.  When the kernel is even in z (the angle set is closed under
+// the mirror that negates kz), the stage for one column is a real symmetric
+// Toeplitz matrix times the column: with b(dz) = the kernel's z-profile of
+// the column (the kernel after the x and y transforms), the FFT form computes
+// L sum_{z'} b(z - z') x[z'] and b(-dz) = b(dz) is real.  At n = 29 rows
+// that is 2 n^2 = 1682 FMAs per column against about 4100 instructions for
+// the 64-point FFT route, and the column never leaves registers, so the
+// stage runs at the rate its bytes allow.  The taps L b(dz), dz < n, are
+// stored per column (n planes instead of the L/2 + 1 spectrum planes).
+#include <cstdlib>
+
 #include "lc_fft.hpp"
 #include "lc_regfft.cuh"
 
@@ -134,6 +146,44 @@ __global__ void __launch_bounds__(C *(A > B ? A : B))
     }
 }
 
+// Direct z stage, one column per thread.  N is the compile-time row count
+// (n rounded up; rows n..N-1 are zero and not stored).  The column's n
+// values and n taps stay in registers; every output is one fixed-order sum
+// of N products, so the result does not depend on the launch shape.
+template <int N>
+__global__ void __launch_bounds__(128, (N <= 32 ? 4 : 2))
+    zdirect_kernel(float2 *data, long n_inner, int n, const float *__restrict__ taps) {
+    const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= n_inner) return;
+    float2 x[N];
+    float k[N];
+#pragma unroll
+    for (int z = 0; z < N; ++z) {
+        x[z] = z < n ? data[(long)z * n_inner + col] : make_float2(0.f, 0.f);
+        k[z] = z < n ? __ldg(taps + (long)z * n_inner + col) : 0.f;
+    }
+#pragma unroll
+    for (int z = 0; z < N; ++z) {
+        if (z >= n) break;
+        float ax = 0.f, ay = 0.f;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            const float t = k[z > q ? z - q : q - z];
+            ax = fmaf(t, x[q].x, ax);
+            ay = fmaf(t, x[q].y, ay);
+        }
+        data[(long)z * n_inner + col] = make_float2(ax, ay);
+    }
+}
+
+template <int N>
+void launch_zd(cudaStream_t st, float2 *data, long n_inner, int n, const float *taps) {
+    const long blocks = (n_inner + 127) / 128;
+    LC_REQUIRE(blocks < (1L << 31), "direct z stage: grid too large");
+    zdirect_kernel<N><<<(unsigned)blocks, 128, 0, st>>>(data, n_inner, n, taps);
+    LC_CHECK_LAUNCH();
+}
+
 template <int A, int B, int C>
 void launch_z(cudaStream_t st, float2 *data, long n_inner, int n_in, int n_out, const float *spec, int fold) {
     constexpr int TPL = A > B ? A : B;
@@ -149,6 +199,33 @@ void launch_z(cudaStream_t st, float2 *data, long n_inner, int n_in, int n_out, 
 }
 
 }  // namespace
+
+int zdirect_max_rows() { return 48; }
+
+bool zdirect_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("LC_ZDIRECT");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+bool launch_zdirect(cudaStream_t st, float2 *data, long n_inner, int n, const float *taps) {
+    LC_REQUIRE(n >= 0, "direct z stage: bad row count");
+    if (n > zdirect_max_rows()) return false;
+    if (n_inner <= 0 || n == 0) return true;
+    if (n <= 4) launch_zd<4>(st, data, n_inner, n, taps);
+    else if (n <= 8) launch_zd<8>(st, data, n_inner, n, taps);
+    else if (n <= 12) launch_zd<12>(st, data, n_inner, n, taps);
+    else if (n <= 16) launch_zd<16>(st, data, n_inner, n, taps);
+    else if (n <= 20) launch_zd<20>(st, data, n_inner, n, taps);
+    else if (n <= 24) launch_zd<24>(st, data, n_inner, n, taps);
+    else if (n <= 28) launch_zd<28>(st, data, n_inner, n, taps);
+    else if (n <= 32) launch_zd<32>(st, data, n_inner, n, taps);
+    else if (n <= 40) launch_zd<40>(st, data, n_inner, n, taps);
+    else launch_zd<48>(st, data, n_inner, n, taps);
+    return true;
+}
 
 bool launch_zconv(cudaStream_t st, float2 *data, long n_inner, int L, int n_in, int n_out,
                   const float *spec, bool fold) {
