@@ -931,9 +931,9 @@ def main():
                 "traffic": traffic}
 
     # The spreading against its own bound: every cell update of a footprint
-    # is four 32-bit shared-memory reductions (fixed-point high and low words
-    # of the real and imaginary parts), and an SM retires about 31 of them per
-    # clock (a conflict-free probe measured 30.9).
+    # is two 32-bit shared-memory reductions (the fixed-point words of the
+    # real and imaginary parts), and an SM retires about 31 of them per clock
+    # (a conflict-free probe measured 30.9).
     spread_roof = None
     sp = next((u for u in units if u["name"] == "nufft_spread"), None)
     if sp and not args.small:
@@ -941,9 +941,9 @@ def main():
         mhz = clk.summary().get("sm_mhz") or 1965.0
         w = 7  # ES kernel width at NUFFT tolerance 1e-6
         cells = float(NANGLES) * PADDED_DET[0] * PADDED_DET[1] * w ** 3
-        bound_ms = cells * 4.0 / (SHARED_RED_PER_CLK_SM * sms * mhz * 1e6) * 1e3
+        bound_ms = cells * 2.0 / (SHARED_RED_PER_CLK_SM * sms * mhz * 1e6) * 1e3
         spread_roof = {"bound": "shared-memory reductions", "cell_updates": cells,
-                       "reductions_per_cell": 4, "peak_reductions_per_clk_per_sm": SHARED_RED_PER_CLK_SM,
+                       "reductions_per_cell": 2, "peak_reductions_per_clk_per_sm": SHARED_RED_PER_CLK_SM,
                        "bound_ms": bound_ms, "avg_launch_ms": sp["avg_ms"], "frac": bound_ms / sp["avg_ms"],
                        "hbm_gbs": sp["gbs"], "hbm_frac": sp["gbs"] / peak}
 

@@ -287,40 +287,56 @@ __global__ void bin_scatter_kernel(PolarPts pts, GridCfg g, int W, int *cursor, 
 // speed, never the result.
 //
 // The tile accumulates in exact fixed point with 32-bit integer atomics,
-// which run about four times faster than float atomics in shared memory.
-// Each real contribution v (a float) is scaled by one power of two F for the
-// whole launch and split as  v F = h + l / 2^20  with integers h and l: h is
-// v F rounded to an integer and l the remainder times 2^20, rounded.  Both
-// come from adding 1.5 * 2^23, which places the integer in the low mantissa
-// bits (|v F| < 2^22), so no conversion instruction is needed.  F comes from
-// m, the largest |Re c| + |Im c| of all values of the launch (weights are at
-// most 1, and a unit phase keeps each part below |c|), see fix_exponent.  The
-// flush adds the exact tile sum  T = H 2^20 + L  of each cell to a 64-bit
-// integer per real and imaginary part of the fine grid, and a conversion pass
-// forms T / (F 2^20).  Every sum is an exact integer at one scale, so the fine
-// grid depends neither on the order of the atomics nor on how the points of
-// a bin are cut into subproblems: a backprojection is bit-for-bit repeatable.
-// The resolution 1 / (F 2^20) is below 2^-38 m.
+// which run about four times faster than float atomics in shared memory, one
+// 32-bit word per real and imaginary part of a cell.  Each bin has its own
+// scale F_b = 2^e_b from two bounds over all of its points: m_b, the largest
+// |Re c| + |Im c| of their values (weights are at most 1, and a unit phase
+// keeps each part below |c|), measured per launch, and W_b, a bound on the
+// summed kernel weights of the bin's footprints over one tile cell, measured
+// with the plan (the corner histogram of the bin's points, box-summed along
+// each axis with the largest weight each footprint offset can take).
+// Both depend on the bin's point set alone, not on how the bin is cut into
+// subproblems (the cut follows the bin sort's atomic order), so every
+// contribution is rounded the same way in every plan of the geometry.  A
+// contribution v (a float) is rounded to the integer nearest v F_b by adding
+// 1.5 * 2^23, which places it in the low mantissa bits (|v F_b| < 2^22), and
+// the float's bits are added as they are: every contribution then carries
+// the bias 0x4B400000, and the flush subtracts K_cell times it (modulo 2^32)
+// with K_cell the footprints over the cell.  With F_b m_b <= 2^21 and
+// K_b m_b F_b < 2^30 a tile cell's sum stays below 2^31, so the word holds it
+// exactly.  The flush adds each sum, shifted to one scale F_G = 2^e_G for
+// the whole launch (e_b <= e_G, so the shift is exact), to a 64-bit integer
+// per part of the fine grid, and a conversion pass forms the float grid.
+// Every sum is an exact integer, so the fine grid depends neither on the
+// order of the atomics nor on the schedule: a backprojection is bit-for-bit
+// repeatable.  The rounding step 1 / F_b is at most max(W_b 2^-29, 2^-20) m_b:
+// a cell summed from K footprints is within about sqrt(K / 12) of that of its
+// exact value.
 constexpr int kSpreadThreads = 256;
 constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
 constexpr unsigned kRoundMagicBits = 0x4B400000u;
 
-// Exponent e of the launch's fixed-point scale F = 2^e, from m (the largest
-// |Re c| + |Im c|), nmax (most points of one subproblem) and kmax (an upper
-// bound on the footprints that cover one fine-grid cell):
-//   F m <= 2^21            so |v F| < 2^22 for the rounding by 1.5 2^23;
-//   F nmax m < 2^30        so a tile's sums of h stay below 2^31 (the sums of
-//                          l stay below 2^19 nmax <= 2^30 for nmax <= 2^11);
-//   F kmax m 2^20 < 2^61   so a cell's 64-bit sum (plus the rounding terms,
-//                          below kmax 2^20) stays below 2^62.
-__host__ __device__ __forceinline__ int fix_exponent(float m, int nmax, long kmax) {
+// Exponents of the fixed-point scales.  Launch: F_G = 2^e_G with
+// kmax m F_G < 2^61 (kmax bounds the footprints over one fine-grid cell, m
+// the values), so a cell's 64-bit sum stays below 2^62.  Bin: F_b = 2^e_b
+// with F_b m_b <= 2^21 (rounding by 1.5 2^23) and W_b m_b F_b < 2^30, W_b a
+// bound on the sum of the weights of the bin's footprints over one cell, so
+// a tile cell's sum (plus at most 1024 rounding halves) stays below 2^31;
+// and e_b <= e_G.
+__host__ __device__ __forceinline__ int fix_exponent_grid(float m, long kmax) {
     if (!(m > 0.f)) return 0;
-    int e1, e2, e3;
-    frexp((double)m, &e1);                 // m < 2^e1
-    frexp((double)nmax * (double)m, &e2);  // nmax m < 2^e2
+    int e3;
     frexp((double)kmax * (double)m, &e3);  // kmax m < 2^e3
-    const int a = 21 - e1, b = 30 - e2, c = 41 - e3;
-    return a < b ? (a < c ? a : c) : (b < c ? b : c);
+    return 61 - e3;
+}
+
+__device__ __forceinline__ int fix_exponent_tile(float mb, float wb, int eg) {
+    int e1, e2;
+    frexp((double)mb, &e1);               // m_b < 2^e1
+    frexp((double)wb * (double)mb, &e2);  // W_b m_b < 2^e2
+    const int a = 21 - e1, b = 30 - e2;
+    const int e = a < b ? a : b;
+    return e < eg ? e : eg;
 }
 
 // m = max |Re c| + |Im c| over n values, as the bits of a non-negative float
@@ -336,11 +352,10 @@ __global__ void value_bound_kernel(const float2 *__restrict__ c, long n, int *bi
     if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(bits, __float_as_int(m));
 }
 
-// fine grid <- T / (F 2^20) from the two 64-bit fixed-point sums per cell
+// fine grid <- T / F_G from the two 64-bit fixed-point sums per cell
 __global__ void fix_to_float_kernel(const long long *__restrict__ fix, float2 *__restrict__ grid, long n,
-                                    const int *__restrict__ mbits, int nmax, long kmax) {
-    const int e = fix_exponent(__int_as_float(*mbits), nmax, kmax);
-    const double unscale = ldexp(1.0, -(e + 20));
+                                    const int *__restrict__ mbits, long kmax) {
+    const double unscale = ldexp(1.0, -fix_exponent_grid(__int_as_float(*mbits), kmax));
     const longlong2 *f2 = reinterpret_cast<const longlong2 *>(fix);
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         const longlong2 t = f2[i];
@@ -355,25 +370,20 @@ __device__ __forceinline__ void red_shared(unsigned addr, int v) {
     asm volatile("red.shared.add.u32 [%0+%2], %1;" ::"r"(addr), "r"(v), "n"(OFF) : "memory");
 }
 
-// hi += round(a b) + B, lo += round((a b - round(a b)) 2^20) + B, |a b| < 2^22,
-// at cell DX of the rows starting at the shared addresses hi and lo
+// word += round(a b) + B (B = 0x4B400000, the bits of 1.5 2^23), |a b| < 2^22,
+// at cell DX of the row starting at the shared address `row`
 template <int DX>
-__device__ __forceinline__ void fixed_add(unsigned hi, unsigned lo, float a, float b) {
-    const float y1 = fmaf(a, b, kRoundMagic);
-    const float h = y1 - kRoundMagic;
-    const float y2 = fmaf(fmaf(a, b, -h), 1048576.0f, kRoundMagic);
-    red_shared<4 * DX>(hi, __float_as_int(y1));
-    red_shared<4 * DX>(lo, __float_as_int(y2));
+__device__ __forceinline__ void fixed_add(unsigned row, float a, float b) {
+    red_shared<4 * DX>(row, __float_as_int(fmaf(a, b, kRoundMagic)));
 }
 
 // one footprint row of W cells, real and imaginary parts
 template <int W, int DX = 0>
-__device__ __forceinline__ void spread_row(unsigned hr, unsigned lr, unsigned hi, unsigned li, float vr,
-                                           float vi, const float (&wx)[W]) {
+__device__ __forceinline__ void spread_row(unsigned re, unsigned im, float vr, float vi, const float (&wx)[W]) {
     if constexpr (DX < W) {
-        fixed_add<DX>(hr, lr, vr, wx[DX]);
-        fixed_add<DX>(hi, li, vi, wx[DX]);
-        spread_row<W, DX + 1>(hr, lr, hi, li, vr, vi, wx);
+        fixed_add<DX>(re, vr, wx[DX]);
+        fixed_add<DX>(im, vi, wx[DX]);
+        spread_row<W, DX + 1>(re, im, vr, vi, wx);
     }
 }
 
@@ -426,7 +436,7 @@ template <int DIM, int W>
 __device__ __forceinline__ void spread_point(const PolarPts &pts, const GridCfg &g,
                                              const float2 *__restrict__ c, long cstride, int nvol, int j,
                                              int mode, const float2 *__restrict__ shifts, const int (&S)[3],
-                                             int tx, int plane, int tsize, unsigned sm_hre,
+                                             int tx, int plane, int tsize, unsigned sm_re,
                                              unsigned plane_bytes, float fscale, int rot) {
     const float inv_hw = 2.0f / (float)W;
     PointInfo pi;
@@ -462,15 +472,15 @@ __device__ __forceinline__ void spread_point(const PolarPts &pts, const GridCfg 
     for (int s = 0; s < nvol; ++s) {
         float2 v = c[(long)s * cstride + j];
         v = mode == PT_SHIFT ? cmul(v, mult) : make_float2(v.x * fscale, v.y * fscale);
-        // 32-bit shared addresses of the footprint corner in the four planes
-        const unsigned hr = sm_hre + 4u * (unsigned)(s * tsize + corner);
-        const unsigned lr = hr + plane_bytes, hi = lr + plane_bytes, li = hi + plane_bytes;
+        // 32-bit shared addresses of the footprint corner in the two planes
+        const unsigned ar = sm_re + 4u * (unsigned)(s * tsize + corner);
+        const unsigned ai = ar + plane_bytes;
         if constexpr (DIM == 2) {
 #pragma unroll
             for (int dy = 0; dy < W; ++dy) {
                 const float vr = v.x * wk[1][dy], vi = v.y * wk[1][dy];
                 const unsigned row = 4u * (unsigned)(dy * tx);
-                spread_row<W>(hr + row, lr + row, hi + row, li + row, vr, vi, wk[0]);
+                spread_row<W>(ar + row, ai + row, vr, vi, wk[0]);
             }
         } else {
 #pragma unroll 1
@@ -487,20 +497,131 @@ __device__ __forceinline__ void spread_point(const PolarPts &pts, const GridCfg 
                 for (int dy = 0; dy < W; ++dy) {
                     const float vr = zr * wk[1][dy], vi = zi * wk[1][dy];
                     const unsigned row = zo + 4u * (unsigned)(dy * tx);
-                    spread_row<W>(hr + row, lr + row, hi + row, li + row, vr, vi, wk[0]);
+                    spread_row<W>(ar + row, ai + row, vr, vi, wk[0]);
                 }
             }
         }
     }
 }
 
+// Largest kernel weight of each footprint offset m < W (over every position
+// of the point), rounded up, for the weighted footprint bound
+struct OffsetWeights {
+    float w[16];
+};
+
+// Plan: W_b of every bin (one CTA per bin, float bits): the corner histogram
+// of all the bin's points on its tile, summed along each axis with the
+// offset weights (cell q gets sum_d om[d] h[q - d]), and its maximum.  Every
+// line is summed by one thread in a fixed order, so the bound depends on the
+// bin's point set alone.
 template <int DIM, int W>
-__global__ void __launch_bounds__(kSpreadThreads, 2)
+__global__ void __launch_bounds__(256) bin_footprint_kernel(PolarPts pts, GridCfg g, OffsetWeights om,
+                                                            const int *__restrict__ perm,
+                                                            const int2 *__restrict__ bins, int *kbin) {
+    extern __shared__ int hist[];
+    __shared__ int kmx;
+    const int2 br = bins[blockIdx.x];  // (first position in perm, points)
+    if (br.y == 0) {
+        if (threadIdx.x == 0) kbin[blockIdx.x] = 0;
+        return;
+    }
+    int S[3] = {0, 0, 0};
+    {
+        int rr = blockIdx.x;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            S[d] = (rr % g.nb[d]) * g.bs[d] - g.hw[d];
+            rr /= g.nb[d];
+        }
+    }
+    const int tx = g.td[0], ty = g.td[1], tz = DIM == 3 ? g.td[2] : 1;
+    const int plane = tx * ty, tsize = plane * tz;
+    for (int i = threadIdx.x; i < tsize; i += blockDim.x) hist[i] = 0;
+    if (threadIdx.x == 0) kmx = 0;
+    __syncthreads();
+    for (int p = threadIdx.x; p < br.y; p += blockDim.x) {
+        PointInfo pi;
+        point_at(pts, perm[br.x + p], pi);
+        const int stride[3] = {1, tx, plane};
+        int corner = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            int cell, l0;
+            float off;
+            place(pi.c[d], g.nf[d], g.inv_nf[d], W, cell, l0, off);
+            corner += (l0 - S[d]) * stride[d];
+        }
+        atomicAdd(&hist[corner], 1);
+    }
+    __syncthreads();
+    // weighted sums along x, y, z in place, one thread per line with the
+    // last W inputs in registers
+    float *acc = reinterpret_cast<float *>(hist);
+    for (int i = threadIdx.x; i < tsize; i += blockDim.x) acc[i] = (float)hist[i];
+    __syncthreads();
+#pragma unroll 1
+    for (int d = 0; d < DIM; ++d) {
+        const int n = d == 0 ? tx : (d == 1 ? ty : tz);
+        const int stride = d == 0 ? 1 : (d == 1 ? tx : plane);
+        const int nlines = tsize / n;
+        for (int line = threadIdx.x; line < nlines; line += blockDim.x) {
+            const int base = d == 0 ? line * tx : (d == 1 ? (line % tx) + (line / tx) * plane : line);
+            float r[W];
+#pragma unroll
+            for (int k = 0; k < W; ++k) r[k] = 0.f;
+            for (int q = 0; q < n; ++q) {
+#pragma unroll
+                for (int k = W - 1; k > 0; --k) r[k] = r[k - 1];
+                r[0] = acc[base + q * stride];
+                float v = 0.f;
+#pragma unroll
+                for (int k = 0; k < W; ++k) v = fmaf(om.w[k], r[k], v);
+                acc[base + q * stride] = v;
+            }
+        }
+        __syncthreads();
+    }
+    float km = 0.f;
+    for (int i = threadIdx.x; i < tsize; i += blockDim.x) km = fmaxf(km, acc[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) km = fmaxf(km, __shfl_xor_sync(0xffffffffu, km, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&kmx, __float_as_int(km));
+    __syncthreads();
+    // float rounding of the sums (relative 2^-24 per step): a margin of 1e-4
+    if (threadIdx.x == 0) kbin[blockIdx.x] = __float_as_int(__int_as_float(kmx) * 1.0001f);
+}
+
+// Per launch: m_b of every bin (float bits, binm zeroed first) over all
+// values of the bin's points (one CTA per subproblem)
+__global__ void __launch_bounds__(256) bin_value_bound_kernel(const float2 *__restrict__ c, long cstride,
+                                                              int nvol, const int *__restrict__ perm,
+                                                              const int4 *__restrict__ subs, int *binm) {
+    const int4 sp = subs[blockIdx.x];
+    float m = 0.f;
+    for (int p = threadIdx.x; p < sp.z; p += blockDim.x) {
+        const int j = perm[sp.y + p];
+        for (int s = 0; s < nvol; ++s) {
+            const float2 v = c[(long)s * cstride + j];
+            m = fmaxf(m, fabsf(v.x) + fabsf(v.y));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(&binm[sp.x], __float_as_int(m));
+}
+
+#ifndef LC_SPREAD_MIN_BLOCKS
+#define LC_SPREAD_MIN_BLOCKS 3  // CTAs per SM the spreading kernel's registers are sized for
+#endif
+
+template <int DIM, int W>
+__global__ void __launch_bounds__(kSpreadThreads, LC_SPREAD_MIN_BLOCKS)
     spread_kernel(PolarPts pts, GridCfg g, const float2 *__restrict__ c, long cstride, int nvol,
                   const int *__restrict__ perm, const int4 *__restrict__ subs,
                   unsigned long long *__restrict__ fix, long gstride, int mode,
-                  const float2 *__restrict__ shifts, int maxpts, const int *__restrict__ mbits,
-                  long kmax) {
+                  const float2 *__restrict__ shifts, const int *__restrict__ mbits, long kmax,
+                  const int *__restrict__ kbin, const int *__restrict__ binm) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int cnt[32], start[32], mincnt, maxcnt;
     const int4 sp = subs[blockIdx.x];
@@ -520,16 +641,14 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
     const int plane = tx * ty;
     const int tsize = plane * tz;
     const long acc_n = (long)nvol * tsize;
-    int *hre = reinterpret_cast<int *>(smem_raw);  // high words, real parts
-    int *lre = hre + acc_n;                        // low words, real parts
-    int *him = lre + acc_n;
-    int *lim = him + acc_n;
-    int *kcnt = lim + acc_n;  // footprint corners per cell, then footprints per cell
+    int *are = reinterpret_cast<int *>(smem_raw);  // real parts
+    int *aim = are + acc_n;                        // imaginary parts
+    int *kcnt = aim + acc_n;  // footprint corners per cell, then footprints per cell
     unsigned short *order = reinterpret_cast<unsigned short *>(kcnt + tsize);  // points by bank
     constexpr int kKeys = 8;  // points per thread in the bucketing pass (maxpts <= 8 * threads)
     int key[kKeys];
     const int tid = threadIdx.x;
-    for (long idx = tid; idx < 4 * acc_n + tsize; idx += blockDim.x) hre[idx] = 0;
+    for (long idx = tid; idx < 2 * acc_n + tsize; idx += blockDim.x) are[idx] = 0;
     if (tid < 32) cnt[tid] = 0;
     __syncthreads();
 
@@ -582,13 +701,23 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
         const int k = key[q];
         if (k >= 0) order[start[k >> 16] + (k & 0xffff)] = (unsigned short)(tid + q * (int)blockDim.x);
     }
-    // the launch's fixed-point scale F = 2^e (fix_exponent)
-    const float fscale = ldexpf(1.f, fix_exponent(__int_as_float(*mbits), maxpts, kmax));
+    // footprints per cell: box sums of the corner histogram along each axis
     __syncthreads();
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        box_sum_axis(kcnt, d, W, tx, ty, tz);
+        __syncthreads();
+    }
+    const float mb = __int_as_float(binm[sp.x]);
+    if (!(mb > 0.f)) return;  // every value of the bin is zero: nothing to add (uniform over the CTA)
+    // the bin's fixed-point scale F_b = 2^e_b, and the launch's e_G
+    const int eg = fix_exponent_grid(__int_as_float(*mbits), kmax);
+    const int eb = fix_exponent_tile(mb, __int_as_float(kbin[sp.x]), eg);
+    const float fscale = ldexpf(1.f, eb);
 
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    const unsigned sm_hre = (unsigned)__cvta_generic_to_shared(hre);
-    const unsigned plane_bytes = 4u * (unsigned)acc_n;  // bytes between the hre, lre, him, lim planes
+    const unsigned sm_re = (unsigned)__cvta_generic_to_shared(are);
+    const unsigned plane_bytes = 4u * (unsigned)acc_n;  // bytes between the real and imaginary planes
     const int mycnt = cnt[lane], mystart = start[lane], nrounds = maxcnt, nfull = mincnt;
     // ---- rounds 0 .. nrounds-1 in passes; round r holds the banks with more
     // than r points, so the sets shrink with r.  Rounds below nfull hold every
@@ -644,29 +773,25 @@ __global__ void __launch_bounds__(kSpreadThreads, 2)
         }
         if (p >= 0)
             spread_point<DIM, W>(pts, g, c, cstride, nvol, perm[sp.y + p], mode, shifts, S, tx, plane, tsize,
-                                 sm_hre, plane_bytes, fscale, prot);
+                                 sm_re, plane_bytes, fscale, prot);
     }
     __syncthreads();
-    // footprints per cell: box sums of the corner histogram along each axis
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-        box_sum_axis(kcnt, d, W, tx, ty, tz);
-        __syncthreads();
-    }
-    // flush the tile's exact sums (halos overlap neighbouring bins, so add
-    // atomically; integer sums make the order irrelevant)
+    // flush the tile's exact sums at the launch's scale (halos overlap
+    // neighbouring bins, so add atomically; integer sums make the order
+    // irrelevant)
+    const int sh = eg - eb;
     for (int s = 0; s < nvol; ++s) {
         for (int rr = tid; rr < tsize; rr += blockDim.x) {
             const int k = kcnt[rr];
             if (k == 0) continue;
             const unsigned kb = (unsigned)k * kRoundMagicBits;
             const int idx = s * tsize + rr;
-            const int h1 = (int)((unsigned)hre[idx] - kb), l1 = (int)((unsigned)lre[idx] - kb);
-            const int h2 = (int)((unsigned)him[idx] - kb), l2 = (int)((unsigned)lim[idx] - kb);
-            const long long a = (long long)h1 * 1048576 + l1, b = (long long)h2 * 1048576 + l2;
+            const int t1 = (int)((unsigned)are[idx] - kb), t2 = (int)((unsigned)aim[idx] - kb);
+            if ((t1 | t2) == 0) continue;
             unsigned long long *cell = fix + 2 * ((long)s * gstride + tile_cell_to_grid<DIM>(rr, g, S));
-            atomicAdd(cell, (unsigned long long)a);
-            atomicAdd(cell + 1, (unsigned long long)b);
+            // two's-complement sums: shift the 64-bit patterns (sh <= 40)
+            if (t1) atomicAdd(cell, (unsigned long long)(long long)t1 << sh);
+            if (t2) atomicAdd(cell + 1, (unsigned long long)(long long)t2 << sh);
         }
     }
 }
@@ -772,11 +897,20 @@ template <int DIM, int W>
 void launch_spread_w(const Context &ctx, dim3 grid, size_t smem, cudaStream_t st, const PolarPts &pts,
                      const GridCfg &g, const float2 *c, long cstride, int nvol, const int *perm,
                      const int4 *subs, unsigned long long *out, long gstride, int mode,
-                     const float2 *shifts, int maxpts, const int *mbits, long kmax) {
+                     const float2 *shifts, const int *mbits, long kmax, const int *kbin, const int *binm) {
     auto kern = spread_kernel<DIM, W>;
     allow_max_dynamic_smem(ctx, kern);
     kern<<<grid, kSpreadThreads, smem, st>>>(pts, g, c, cstride, nvol, perm, subs, out, gstride,
-                                             mode, shifts, maxpts, mbits, kmax);
+                                             mode, shifts, mbits, kmax, kbin, binm);
+    LC_CHECK_LAUNCH();
+}
+
+template <int DIM, int W>
+void launch_footprint_w(const Context &ctx, unsigned nbins, size_t smem, cudaStream_t st, const PolarPts &pts,
+                        const GridCfg &g, const OffsetWeights &om, const int *perm, const int2 *bins, int *kbin) {
+    auto kern = bin_footprint_kernel<DIM, W>;
+    allow_max_dynamic_smem(ctx, kern);
+    kern<<<nbins, 256, smem, st>>>(pts, g, om, perm, bins, kbin);
     LC_CHECK_LAUNCH();
 }
 
@@ -920,7 +1054,39 @@ void NufftPlan::sort_points(Context &ctx) {
     if (dim_ == 2) bin_scatter_kernel<2><<<(unsigned)blocks, threads, 0, st>>>(pts_, g, w_, cursor.get(), perm_.get());
     else bin_scatter_kernel<3><<<(unsigned)blocks, threads, 0, st>>>(pts_, g, w_, cursor.get(), perm_.get());
     LC_CHECK_LAUNCH();
-    LC_CUDA(cudaStreamSynchronize(st));
+    // K_b of every bin, over all of its points
+    {
+        std::vector<int2> br(nbins);
+        for (long b = 0; b < nbins; ++b) br[b] = make_int2(off[b], hc[b]);
+        DevBuf<int2> dbr;
+        dbr.upload(br.data(), br.size(), st);
+        kbin_.alloc(nbins, st);
+        binm_.alloc(nbins, st);
+        LC_REQUIRE(nbins < (1L << 31), "NUFFT: too many bins");
+        const size_t hsm = (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(int);
+        LC_REQUIRE(hsm <= ctx.max_smem(), "NUFFT: bin tile does not fit shared memory");
+        LC_REQUIRE(w_ <= 16, "NUFFT: kernel too wide");
+        // Offset m of a footprint sees the point at x = (m - off) 2 / w with
+        // off in (w/2 - 1, w/2]: the weight is at most the kernel at the end
+        // of [(m - w/2) 2/w, (m - w/2 + 1) 2/w] nearest 0 (1 when it holds 0),
+        // raised by 1e-3 for the device's exp2 and rounded up to 2^-12.
+        OffsetWeights om{};
+        for (int m = 0; m < w_; ++m) {
+            const double a = (m - 0.5 * w_) * 2.0 / w_, b = (m - 0.5 * w_ + 1.0) * 2.0 / w_;
+            const double x = (a <= 0.0 && b >= 0.0) ? 0.0 : std::min(std::fabs(a), std::fabs(b));
+            const double phi = x < 1.0 ? std::exp(beta_ * (std::sqrt(1.0 - x * x) - 1.0)) : 0.0;
+            om.w[m] = (float)(std::ceil(phi * 1.001 * 4096.0) / 4096.0);
+        }
+        if (dim_ == 2) {
+            LC_W_SWITCH(w_, (launch_footprint_w<2, WW>(ctx, (unsigned)nbins, hsm, st, pts_, g, om, perm_.get(),
+                                                      dbr.get(), kbin_.get())));
+        } else {
+            LC_W_SWITCH(w_, (launch_footprint_w<3, WW>(ctx, (unsigned)nbins, hsm, st, pts_, g, om, perm_.get(),
+                                                      dbr.get(), kbin_.get())));
+        }
+        LC_CHECK_LAUNCH();
+        LC_CUDA(cudaStreamSynchronize(st));
+    }
 }
 
 void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, PtMode mode) {
@@ -929,15 +1095,15 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
     cudaStream_t st = ctx.stream();
     // values read once, fine grid written once (plus the permutation)
     ProfScope ps(ctx, PS_SPREAD, (double)nvol * (8.0 * pts_.M + 8.0 * gvol) + 4.0 * pts_.M);
-    // four 32-bit fixed-point accumulators per cell (high and low words of the
-    // real and imaginary parts) per volume, a footprint count per cell and the
-    // bucketed point order (16 bits per point)
-    const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * 4 * sizeof(int);
+    // two 32-bit fixed-point accumulators per cell (real and imaginary parts)
+    // per volume, a footprint count per cell and the bucketed point order (16
+    // bits per point)
+    const size_t tile_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * 2 * sizeof(int);
     const size_t bucket_bytes = (size_t)g.td[0] * g.td[1] * g.td[2] * sizeof(int) +
                                 (size_t)maxsub_ * sizeof(unsigned short);
     LC_REQUIRE(maxsub_ <= 8 * kSpreadThreads, "NUFFT spread: subproblem larger than the bucketing pass");
     LC_REQUIRE(maxsub_ <= 2048, "NUFFT spread: subproblem too large for the fixed-point sums");
-    // one fixed-point scale for all values of the launch: bound them first
+    // one fixed-point scale for the fine grid of the launch: bound the values first
     mbits_.ensure(1, st);
     fix_.ensure(2 * gvol * nvol, st);
     LC_CUDA(cudaMemsetAsync(mbits_.get(), 0, sizeof(int), st));
@@ -957,21 +1123,24 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
         const float2 *cv = c + (long)v0 * pts_.M;
         unsigned long long *fv = fix + 2 * (long)v0 * gvol;
         dim3 gd(nsub_);
+        // the bins' value bounds over this chunk of volumes
+        LC_CUDA(cudaMemsetAsync(binm_.get(), 0, binm_.size() * sizeof(int), st));
+        bin_value_bound_kernel<<<gd, 256, 0, st>>>(cv, pts_.M, nv, perm_.get(), subs_.get(), binm_.get());
+        LC_CHECK_LAUNCH();
         if (dim_ == 2) {
             LC_W_SWITCH(w_, (launch_spread_w<2, WW>(ctx, gd, smem, st, pts_, g, cv, pts_.M, nv,
                                                    perm_.get(), subs_.get(), fv, gvol, mode, shifts_,
-                                                   maxsub_, mbits_.get(), kmax_)));
+                                                   mbits_.get(), kmax_, kbin_.get(), binm_.get())));
         } else {
             LC_W_SWITCH(w_, (launch_spread_w<3, WW>(ctx, gd, smem, st, pts_, g, cv, pts_.M, nv,
                                                    perm_.get(), subs_.get(), fv, gvol, mode, shifts_,
-                                                   maxsub_, mbits_.get(), kmax_)));
+                                                   mbits_.get(), kmax_, kbin_.get(), binm_.get())));
         }
     }
     {
         const long n = gvol * nvol;
         const long blocks = std::max<long>(1, std::min<long>((n + 255) / 256, (long)ctx.num_sms() * 8));
-        fix_to_float_kernel<<<(unsigned)blocks, 256, 0, st>>>(fix_.get(), grid, n, mbits_.get(), maxsub_,
-                                                               kmax_);
+        fix_to_float_kernel<<<(unsigned)blocks, 256, 0, st>>>(fix_.get(), grid, n, mbits_.get(), kmax_);
         LC_CHECK_LAUNCH();
     }
 }

@@ -114,6 +114,8 @@ class NufftPlan {
     DevBuf<float2> grid_, h1_, h2_;
     DevBuf<long long> fix_;  // 64-bit fixed-point fine grid of the spreading (re, im)
     DevBuf<int> mbits_;      // bound on the spread values (float bits)
+    DevBuf<int> kbin_;       // per bin: bound on the summed weights over one tile cell (float bits)
+    DevBuf<int> binm_;       // per bin: bound on its spread values (float bits), per call
 };
 
 }  // namespace lc

@@ -91,7 +91,9 @@ __device__ __forceinline__ int mirror_index(int j, int P) {
 //   3D  K(kx, ky, -kz) = K(k): rows with ky <= 0 of each plane kz <= 0, and
 //       K(-kx, -ky, kz), K(-k), K(kx, ky, -kz) from them (a per-angle pair
 //       whose a and b differ only in the sign of their kz coefficient);
-//   2D  K(-kx, ky) = K(k): kx <= 0 of each row ky <= 0 (pairs theta, pi - theta).
+//   2D  K(-kx, ky) = K(k): kx <= 0 of each row ky <= 0 (pairs theta, pi - theta);
+//       mirror == 2: the set is also closed under a quarter turn, so
+//       K(ky, kx) = K(k) and only kx <= ky <= 0 is summed (an eighth).
 template <int DIM, int S, bool ONE_GROUP>
 __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const PsfAngle *__restrict__ angles, int ntheta,
                                                       const int *__restrict__ groups, int ngroups,
@@ -103,7 +105,8 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
     for (int i = threadIdx.x; i < ntheta; i += blockDim.x) ang[i] = angles[i];
     for (int i = threadIdx.x; i <= ngroups; i += blockDim.x) gst[i] = groups[i];
     __syncthreads();
-    // x range summed: all of it, or (2D mirror) jx <= P3/2
+    // x range summed: all of it, or (2D mirror) jx <= P3/2; with the
+    // quarter-turn closure (2D, mirror == 2) only jx <= jy of each row
     const int xend = (DIM == 2 && mirror) ? P3 / 2 + 1 : P3;
     const int nseg = (xend + S - 1) / S;
     // rows of the half space: 3D (jz <= P1/2, all jy, or jy <= P2/2 with the
@@ -124,6 +127,7 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
             jy = (int)row;
         }
         const int jx0 = seg * S;
+        if (DIM == 2 && mirror == 2 && jx0 > jy) continue;  // transposed copy of a summed value
         const double kx0 = (double)(jx0 - P3 / 2);
         const double ky = (double)(jy - P2 / 2);
         const double kz = DIM == 3 ? (double)(jz - P1 / 2) : 0.0;
@@ -241,8 +245,49 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
                 }
             }
         } else {
-            // 2D: K = sum_theta D_nx(uX), two angles per division
+            // 2D: K = sum_theta D_nx(uX), four (then two, then one) angles per
+            // division
             int i = 0;
+            for (; i + 3 < ntheta; i += 4) {
+                const PsfAngle &A = ang[i], &B = ang[i + 1], &C = ang[i + 2], &D = ang[i + 3];
+                const double uA = A.a[0] * kx0 + A.a[1] * ky;
+                const double uB = B.a[0] * kx0 + B.a[1] * ky;
+                const double uC = C.a[0] * kx0 + C.a[1] * ky;
+                const double uD = D.a[0] * kx0 + D.a[1] * ky;
+                SinSeq<true> nA, nB, nC, nD;
+                SinSeq<false> dA, dB, dC, dD;
+                nA.init(uA, A.stepA, A.a[0]);
+                dA.init(uA * inv_nx, A.stepB, A.a[0] * inv_nx);
+                nB.init(uB, B.stepA, B.a[0]);
+                dB.init(uB * inv_nx, B.stepB, B.a[0] * inv_nx);
+                nC.init(uC, C.stepA, C.a[0]);
+                dC.init(uC * inv_nx, C.stepB, C.a[0] * inv_nx);
+                nD.init(uD, D.stepA, D.a[0]);
+                dD.init(uD * inv_nx, D.stepB, D.a[0] * inv_nx);
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    if (fabs(dA.cur) > kDenMin && fabs(dB.cur) > kDenMin && fabs(dC.cur) > kDenMin &&
+                        fabs(dD.cur) > kDenMin) {
+                        const double pab = fma(nA.val(s), dB.cur, nB.val(s) * dA.cur), qab = dA.cur * dB.cur;
+                        const double pcd = fma(nC.val(s), dD.cur, nD.val(s) * dC.cur), qcd = dC.cur * dD.cur;
+                        acc[s] += fma(pab, qcd, pcd * qab) / (qab * qcd);
+                    } else {
+                        const double sd = (double)s;
+                        acc[s] += dirichlet_term(nA.val(s), dA.cur, uA + sd * A.a[0], nx) +
+                                  dirichlet_term(nB.val(s), dB.cur, uB + sd * B.a[0], nx) +
+                                  dirichlet_term(nC.val(s), dC.cur, uC + sd * C.a[0], nx) +
+                                  dirichlet_term(nD.val(s), dD.cur, uD + sd * D.a[0], nx);
+                    }
+                    nA.advance();
+                    dA.advance();
+                    nB.advance();
+                    dB.advance();
+                    nC.advance();
+                    dC.advance();
+                    nD.advance();
+                    dD.advance();
+                }
+            }
             for (; i + 1 < ntheta; i += 2) {
                 const PsfAngle &A = ang[i], &B = ang[i + 1];
                 const double uA = A.a[0] * kx0 + A.a[1] * ky;
@@ -312,18 +357,24 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
                 if (mz != jz && my != jy && mz >= 0 && my >= 0 && mx >= 0) put(mz, my, mx, acc[s]);
             }
         } else {
-            // (jy, jx <= P3/2) summed; (jy, mx), (my, mx), (my, jx) copied
+            // (jy, jx <= P3/2) summed; (jy, mx), (my, mx), (my, jx) copied, and
+            // with mirror == 2 (jx <= jy summed) the same four transposed
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const int jx = jx0 + s;
-                if (jx >= xend) break;
+                if (jx >= xend || (mirror == 2 && jx > jy)) break;
                 const int mx = mirror_index(jx, P3);
-                put(0, jy, jx, acc[s]);
-                if (mx != jx && mx >= 0) put(0, jy, mx, acc[s]);
-                if (my != jy && my >= 0) {
-                    put(0, my, jx, acc[s]);
-                    if (mx >= 0) put(0, my, mx, acc[s]);
-                }
+                const double v = acc[s];
+                auto four = [&](int r, int c, int mr, int mc) {
+                    put(0, r, c, v);
+                    if (mc != c && mc >= 0) put(0, r, mc, v);
+                    if (mr != r && mr >= 0) {
+                        put(0, mr, c, v);
+                        if (mc >= 0) put(0, mr, mc, v);
+                    }
+                };
+                four(jy, jx, my, mx);
+                if (mirror == 2 && jx != jy) four(jx, jy, mx, my);
             }
         }
     }
@@ -672,6 +723,7 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
     // (rounded to 1e-10) are compared; a key on a rounding boundary only costs
     // the saving, never the result.
     bool mirror = nth > 0;
+    bool quarter_turn = false;
     {
         // Dirichlet kernels are even, so a and -a (b and -b) give the same term:
         // each vector is compared with the sign of its first nonzero component
@@ -701,6 +753,18 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
         std::sort(k0.begin(), k0.end());
         std::sort(k1.begin(), k1.end());
         mirror = mirror && k0 == k1;
+        if (mirror && !three_d_ && P_[1] == P_[2]) {
+            // 2D: also closed under theta -> theta + pi/2, a -> (-a1, a0)?
+            std::vector<Key> k2(nth);
+            for (int i = 0; i < nth; ++i) {
+                PsfAngle r = tab[i];
+                r.a[0] = -tab[i].a[1];
+                r.a[1] = tab[i].a[0];
+                k2[i] = key(r, false, false);
+            }
+            std::sort(k2.begin(), k2.end());
+            quarter_turn = k0 == k2;
+        }
     }
     kernel_mirror_ = mirror;
     // group the angles by their theta-independent vector a (equal beta and gamma)
@@ -744,7 +808,7 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
         auto kern = psf_rows_kernel<2, S, false>;
         allow_max_dynamic_smem(ctx, kern);
         kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), 0, nx, ny, P1, P2, P3,
-                                        mirror ? 1 : 0, K.get());
+                                        mirror ? (quarter_turn ? 2 : 1) : 0, K.get());
     }
     LC_CHECK_LAUNCH();
     // planes of mode -P/2 have no mirror inside the grid; they are not needed

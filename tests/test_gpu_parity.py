@@ -246,7 +246,8 @@ def test_toeplitz_slice_independence(lc):
 def test_psf_kernel_reflection_paths(lc, symmetric):
     """The FP64 PSF sums a quarter of the grid when the angle set is closed
     under the reflection that makes the kernel even in one more axis (3D:
-    theta -> -theta at beta = 0; 2D: theta -> pi - theta), and half of it
+    theta -> -theta at beta = 0; 2D: theta -> pi - theta), an eighth in 2D
+    when the set is also closed under a quarter turn, and half of it
     otherwise.  Both against the oracle's exact NUDFT kernel, within 1e-10:
     random angles put some Dirichlet terms close to a pole, where the sine
     recurrences' absolute error (~5e-16) is amplified (the golden angle sets
@@ -268,13 +269,18 @@ def test_psf_kernel_reflection_paths(lc, symmetric):
     # in kz) comes back whole: the real FFT of the zero-centred kernel
     R = np.fft.rfftn(np.fft.ifftshift(K)).real
     assert O.rel_l2(psf.spectrum(), R) < 1e-6
-    # 2D
-    nth, n = 20, 31
-    th = np.arange(nth) * np.pi / nth if symmetric else np.sort(rng.uniform(0, np.pi, nth))
-    K = lc.PointSpreadFunction2D(lc.PolarGrid2D(th, n), n, 1).kernel()
-    err = O.rel_l2(K, zero_unpaired(O.psf2d(th, n, n).kernel))
-    print("2D kernel rel. error", symmetric, err)
-    assert err < 1e-10, err
+    # 2D: 20 uniform angles over [0, pi) are also closed under a quarter turn
+    # (the kernel is then symmetric under transposition and an eighth of the
+    # grid is summed); 21 are not
+    for nth in (20, 21):
+        n = 31
+        th = np.arange(nth) * np.pi / nth if symmetric else np.sort(rng.uniform(0, np.pi, nth))
+        K = lc.PointSpreadFunction2D(lc.PolarGrid2D(th, n), n, 1).kernel()
+        err = O.rel_l2(K, zero_unpaired(O.psf2d(th, n, n).kernel))
+        print("2D kernel rel. error", symmetric, nth, err)
+        assert err < 1e-10, (nth, err)
+        if symmetric and nth == 20:
+            assert np.array_equal(K, K.T)
 
 
 def test_cg50_drift_is_the_fp32_drift(lc):
