@@ -523,7 +523,8 @@ int lc_psf_kernel(lc_context c, lc_psf p, double *host_out) {
 int lc_psf_spectrum(lc_context c, lc_psf p, float *host_out) {
     return guarded(c, [&] {
         LC_REQUIRE(p && host_out, "NULL argument");
-        const Toeplitz &T = *p->T;
+        Toeplitz &T = *p->T;
+        T.ensure_spectrum(*c->ctx);
         LC_CUDA(cudaMemcpyAsync(host_out, T.spectrum(), T.stored_spectrum_elems() * sizeof(float),
                                 cudaMemcpyDeviceToHost, c->ctx->stream()));
         LC_CUDA(cudaStreamSynchronize(c->ctx->stream()));

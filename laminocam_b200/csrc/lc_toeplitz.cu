@@ -98,7 +98,7 @@ template <int DIM, int S, bool ONE_GROUP>
 __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const PsfAngle *__restrict__ angles, int ntheta,
                                                       const int *__restrict__ groups, int ngroups,
                                                       int nx, int ny, int P1, int P2, int P3, int mirror,
-                                                      double *__restrict__ K) {
+                                                      int zlo, double *__restrict__ K) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PsfAngle *ang = reinterpret_cast<PsfAngle *>(smem_raw);
     int *gst = reinterpret_cast<int *>(ang + ntheta);
@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
     // rows of the half space: 3D (jz <= P1/2, all jy, or jy <= P2/2 with the
     // mirror); 2D (jy <= P2/2)
     const int rows_per_plane = (DIM == 3 && mirror) ? P2 / 2 + 1 : P2;
-    const long nrows_half = DIM == 3 ? (long)(P1 / 2 + 1) * rows_per_plane : (long)(P2 / 2 + 1);
+    // (3D: only the planes zlo .. P1/2 of the half, the rest is not needed)
+    const long nrows_half = DIM == 3 ? (long)(P1 / 2 + 1 - zlo) * rows_per_plane : (long)(P2 / 2 + 1);
     const long items = nrows_half * nseg;
     const double inv_nx = 1.0 / (double)nx, inv_ny = 1.0 / (double)ny;
     for (long it = (long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
@@ -121,8 +122,9 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
         const int seg = (int)(it - row * nseg);
         int jz = 0, jy;
         if (DIM == 3) {
-            jz = (int)(row / rows_per_plane);
-            jy = (int)(row - (long)jz * rows_per_plane);
+            const int pz = (int)(row / rows_per_plane);
+            jy = (int)(row - (long)pz * rows_per_plane);
+            jz = zlo + pz;
         } else {
             jy = (int)row;
         }
@@ -406,14 +408,14 @@ __global__ void zero_unpaired_kernel(double *__restrict__ K, int P1, int P2, int
     }
 }
 
-// taps[d][c] = L * Re b[(L/2 + d)][c], d < n: the planes of the kernel after
-// its x and y transforms at z offsets 0..n-1 (b is in mode order along z)
+// taps[d][c] = L * Re b[(z0 + d)][c], d < n: the planes of the kernel after
+// its x and y transforms at z offsets 0..n-1 (plane z0 of b holds offset 0)
 __global__ void zdirect_taps_kernel(const double2 *__restrict__ b, float *__restrict__ taps, long plane, int n,
-                                    int L) {
+                                    int L, int z0) {
     const long total = (long)n * plane;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const long d = i / plane, c = i - d * plane;
-        taps[i] = (float)((double)L * b[(L / 2 + d) * plane + c].x);
+        taps[i] = (float)((double)L * b[(z0 + d) * plane + c].x);
     }
 }
 
@@ -504,25 +506,60 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         scale_ = 1.0 / ((double)P_[1] * P_[2] * (double)n_[2]);
     }
     cudaStream_t st = ctx.stream();
-    DevBuf<double> K;
-    if (psf_fp32) build_kernel_nufft32(ctx, K);
-    else build_kernel(ctx, K);  // unpaired -P/2 planes already zeroed
-    // Spectrum of the zero-centred kernel: FFT with the mode placement k -> k mod P.
-    // It is real and point-symmetric; keep x in [0, P3/2] (the R2C half) and all
-    // of y and z, i.e. a real {P1, P2, P3/2+1} array.
-    ProfScope ps(ctx, PS_PSF_FFT, 0.0);
-    DevBuf<double2> a, b;
-    DevBuf<double> Rd(spectrum_elems(), st);
-    const int P1 = P_[0], P2 = P_[1], P3 = P_[2], P3h = Ph_[2];
-    a.alloc((long)P1 * P2 * P3h, st);
+    psf_fp32_ = psf_fp32;
+    // The direct z stage (3D, kernel even in z, n1 small) needs only the
+    // kernel planes |dz| < n1 after the x and y transforms: those are summed
+    // and transformed, and the full spectrum is built when it is asked for.
+    // Otherwise the spectrum is built here.
+    const bool try_direct = three_d && !psf_fp32 && zdirect_enabled() && n_[0] <= zdirect_max_rows();
+    if (try_direct) {
+        DevBuf<double> K;
+        build_kernel(ctx, K, (int)n_[0]);
+        if (kernel_mirror_) {
+            ProfScope ps(ctx, PS_PSF_FFT, 0.0);
+            const int P1 = P_[0], P2 = P_[1], P3 = P_[2], P3h = Ph_[2];
+            const int zlo = P1 / 2 - (int)(n_[0] - 1), nz = P1 - 2 * zlo + (P1 % 2 == 0 ? 1 : 0);
+            // planes zlo .. zlo + nz - 1 hold |dz| <= n1 - 1 (dz = plane - P1/2)
+            DevBuf<double2> a((long)nz * P2 * P3h, st), b((long)nz * P2 * P3h, st);
+            kernel_xy_fft(ctx, K.get() + (long)zlo * P2 * P3, nz, a.get(), b.get());
+            K.release();
+            a.release();
+            const long plane = (long)P2 * P3h;
+            Kz_ = std::make_shared<DevBuf<float>>(n_[0] * plane, st);
+            zdirect_taps_kernel<<<grid_for(n_[0] * plane, 256, ctx.num_sms()), 256, 0, st>>>(
+                b.get(), Kz_->get(), plane, (int)n_[0], P1, P1 / 2 - zlo);
+            LC_CHECK_LAUNCH();
+            zfold_ = true;
+        } else {
+            // not even in z: the whole kernel and the FFT z stage
+            build_spectrum(ctx, &K);
+        }
+    } else {
+        build_spectrum(ctx, nullptr);
+    }
+    // the spectrum is complete in the order of st; callers that hand it to
+    // other streams synchronise first (buffers here are freed in stream order)
+    // work buffers
+    if (three_d) {
+        t1_.alloc(n_[0] * n_[1] * Ph_[2], st);
+        t2_.alloc(n_[0] * (long)P_[1] * Ph_[2], st);
+    } else {
+        t1_.alloc(n_[0] * n_[1] * Ph_[2], st);
+    }
+}
+
+// x (real to half spectrum) and y transforms, FP64, of nz kernel planes of
+// {P2, P3} in mode order: K -> a -> b ({nz, P2, P3/2+1} complex)
+void Toeplitz::kernel_xy_fft(Context &ctx, const double *K, int nz, double2 *a, double2 *b) {
+    const int P2 = P_[1], P3 = P_[2], P3h = Ph_[2];
     {
         AxisFFT x;
-        x.in = K.get();
+        x.in = K;
         x.in_t = E_F64;
-        x.out = a.get();
+        x.out = a;
         x.out_t = E_C128;
         x.fp64 = true;
-        x.n_outer = (long)P1 * P2;
+        x.n_outer = (long)nz * P2;
         x.n_inner = 1;
         x.in_ostride = P3;
         x.out_ostride = P3h;
@@ -533,13 +570,12 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         x.sign = -1;
         launch_axis_fft(ctx, x);
     }
-    K.release();
     {
         AxisFFT y;
-        y.in = a.get();
+        y.in = a;
         y.in_t = E_C128;
         y.fp64 = true;
-        y.n_outer = P1;
+        y.n_outer = nz;
         y.n_inner = P3h;
         y.in_ostride = (long)P2 * P3h;
         y.out_ostride = (long)P2 * P3h;
@@ -548,18 +584,34 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         y.L = P2;
         y.n_out = P2;
         y.sign = -1;
-        if (three_d) {
-            b.alloc((long)P1 * P2 * P3h, st);
-            y.out = b.get();
-            y.out_t = E_C128;
-        } else {
-            y.out = Rd.get();
-            y.out_t = E_F64;
-        }
+        y.out = b;
+        y.out_t = E_C128;
         launch_axis_fft(ctx, y);
     }
-    a.release();
-    if (three_d) {
+}
+
+// The real spectrum R_ of the whole kernel (built here unless *Kin holds it)
+void Toeplitz::build_spectrum(Context &ctx, DevBuf<double> *Kin) {
+    cudaStream_t st = ctx.stream();
+    DevBuf<double> Kown;
+    DevBuf<double> &K = Kin ? *Kin : Kown;
+    if (!Kin) {
+        if (psf_fp32_) build_kernel_nufft32(ctx, K);
+        else build_kernel(ctx, K, 0);  // unpaired -P/2 planes already zeroed
+    }
+    // Spectrum of the zero-centred kernel: FFT with the mode placement k -> k mod P.
+    // It is real and point-symmetric; keep x in [0, P3/2] (the R2C half) and all
+    // of y and z, i.e. a real {P1, P2, P3/2+1} array.
+    ProfScope ps(ctx, PS_PSF_FFT, 0.0);
+    DevBuf<double2> a, b;
+    DevBuf<double> Rd(spectrum_elems(), st);
+    const int P1 = P_[0], P2 = P_[1], P3h = Ph_[2];
+    a.alloc((long)P1 * P2 * P3h, st);
+    if (three_d_) {
+        b.alloc((long)P1 * P2 * P3h, st);
+        kernel_xy_fft(ctx, K.get(), P1, a.get(), b.get());
+        K.release();
+        a.release();
         AxisFFT z;
         z.in = b.get();
         z.in_t = E_C128;
@@ -576,30 +628,55 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         z.n_out = P1;
         z.sign = -1;
         launch_axis_fft(ctx, z);
+    } else {
+        const int P3 = P_[2];
+        AxisFFT x;
+        x.in = K.get();
+        x.in_t = E_F64;
+        x.out = a.get();
+        x.out_t = E_C128;
+        x.fp64 = true;
+        x.n_outer = (long)P1 * P2;
+        x.n_inner = 1;
+        x.in_ostride = P3;
+        x.out_ostride = P3h;
+        x.n_in = P3;
+        x.in_map = IN_MODES;
+        x.L = P3;
+        x.n_out = P3h;
+        x.sign = -1;
+        launch_axis_fft(ctx, x);
+        K.release();
+        AxisFFT y;
+        y.in = a.get();
+        y.in_t = E_C128;
+        y.fp64 = true;
+        y.n_outer = P1;
+        y.n_inner = P3h;
+        y.in_ostride = (long)P2 * P3h;
+        y.out_ostride = (long)P2 * P3h;
+        y.n_in = P2;
+        y.in_map = IN_MODES;
+        y.L = P2;
+        y.n_out = P2;
+        y.sign = -1;
+        y.out = Rd.get();
+        y.out_t = E_F64;
+        launch_axis_fft(ctx, y);
     }
     // an FFT along z of a kernel even in kz is even in f1: keep the planes
     // f1 <= P1/2 (a prefix of the plane-major array)
-    zfold_ = three_d && kernel_mirror_;
-    if (zfold_ && zdirect_enabled() && n_[0] <= zdirect_max_rows()) {
-        const long plane = (long)P2 * P3h;
-        Kz_ = std::make_shared<DevBuf<float>>(n_[0] * plane, st);
-        zdirect_taps_kernel<<<grid_for(n_[0] * plane, 256, ctx.num_sms()), 256, 0, st>>>(b.get(), Kz_->get(),
-                                                                                         plane, (int)n_[0], P1);
-        LC_CHECK_LAUNCH();
-    }
+    zfold_ = three_d_ && kernel_mirror_;
     long nR = stored_spectrum_elems();
     R_ = std::make_shared<DevBuf<float>>(nR, st);
     d2f_kernel<<<grid_for(nR, 256, ctx.num_sms()), 256, 0, st>>>(Rd.get(), R_->get(), nR);
     LC_CHECK_LAUNCH();
-    // the spectrum is complete in the order of st; callers that hand it to
-    // other streams synchronise first (buffers here are freed in stream order)
-    // work buffers
-    if (three_d) {
-        t1_.alloc(n_[0] * n_[1] * Ph_[2], st);
-        t2_.alloc(n_[0] * (long)P_[1] * Ph_[2], st);
-    } else {
-        t1_.alloc(n_[0] * n_[1] * Ph_[2], st);
-    }
+}
+
+void Toeplitz::ensure_spectrum(Context &ctx) {
+    if (R_) return;
+    LC_REQUIRE(g_ != nullptr, "PSF spectrum export needs the PSF's own geometry");
+    build_spectrum(ctx, nullptr);
 }
 
 static void psf_sizes(const long dims[3], bool three_d, long P[3], long Ph[3]) {
@@ -670,7 +747,7 @@ void Toeplitz::build_kernel_nufft32(Context &ctx, DevBuf<double> &K) {
     LC_CHECK_LAUNCH();
 }
 
-void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
+void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K, int zkeep) {
     cudaStream_t st = ctx.stream();
     ProfScope ps(ctx, PS_PSF_GEN, 0.0);
     const int nth = g_->pts.ntheta;
@@ -795,7 +872,11 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
     K.alloc(total, st);
     constexpr int S = 16;
     const long nseg = ((!three_d_ && mirror ? P3 / 2 + 1 : P3) + S - 1) / S;
-    const long items = (three_d_ ? (long)(P1 / 2 + 1) * (mirror ? P2 / 2 + 1 : P2) : (long)(P2 / 2 + 1)) * nseg;
+    // with zkeep > 0 and the kz mirror, only the planes |kz| < zkeep are summed
+    // (and their mirrors filled); the other planes are left unset
+    const int zlo = (three_d_ && mirror && zkeep > 0) ? std::max(0, P1 / 2 - (zkeep - 1)) : 0;
+    const long items =
+        (three_d_ ? (long)(P1 / 2 + 1 - zlo) * (mirror ? P2 / 2 + 1 : P2) : (long)(P2 / 2 + 1)) * nseg;
     size_t smem = sizeof(PsfAngle) * nth + sizeof(int) * groups.size();
     LC_REQUIRE(smem <= 220 * 1024, "Toeplitz: too many angles for one PSF launch");
     unsigned blocks = (unsigned)std::max<long>(1, std::min<long>((items + 127) / 128, (long)ctx.num_sms() * 16));
@@ -803,12 +884,12 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
         auto kern = ngroups == 1 ? psf_rows_kernel<3, S, true> : psf_rows_kernel<3, S, false>;
         allow_max_dynamic_smem(ctx, kern);
         kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), ngroups, nx, ny, P1, P2, P3,
-                                        mirror ? 1 : 0, K.get());
+                                        mirror ? 1 : 0, zlo, K.get());
     } else {
         auto kern = psf_rows_kernel<2, S, false>;
         allow_max_dynamic_smem(ctx, kern);
         kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), 0, nx, ny, P1, P2, P3,
-                                        mirror ? (quarter_turn ? 2 : 1) : 0, K.get());
+                                        mirror ? (quarter_turn ? 2 : 1) : 0, 0, K.get());
     }
     LC_CHECK_LAUNCH();
     // planes of mode -P/2 have no mirror inside the grid; they are not needed
@@ -821,7 +902,7 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K) {
 void Toeplitz::kernel_fp64(Context &ctx, double *host_out) {
     LC_REQUIRE(g_ != nullptr, "PSF kernel export needs the PSF's own geometry");
     DevBuf<double> K;
-    build_kernel(ctx, K);
+    build_kernel(ctx, K, 0);
     long total = three_d_ ? (long)P_[0] * P_[1] * P_[2] : (long)P_[2] * P_[2];
     LC_CUDA(cudaMemcpyAsync(host_out, K.get(), total * sizeof(double), cudaMemcpyDeviceToHost,
                             ctx.stream()));

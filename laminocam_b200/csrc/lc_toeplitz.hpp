@@ -55,14 +55,19 @@ class Toeplitz {
     // the kernel is even in kz (then R(P1 - f1) = R(f1), spectrum_zfold())
     long stored_spectrum_elems() const { return (long)(zfold_ ? P_[0] / 2 + 1 : P_[0]) * P_[1] * Ph_[2]; }
     bool spectrum_zfold() const { return zfold_; }
-    const float *spectrum() const { return R_->get(); }
+    // the spectrum (built on first use when the z stage is direct: that
+    // needs the PSF's own geometry, as kernel_fp64 does)
+    void ensure_spectrum(Context &ctx);
+    const float *spectrum() const { return R_ ? R_->get() : nullptr; }
     // factor of the last pass: 1 / (P1 P2 P3 n2 n3) (3D) or 1 / (P^2 n) (2D)
     double scale() const { return scale_; }
     size_t device_bytes() const {
         return spectrum_bytes() + (t1_.size() + t2_.size()) * sizeof(float2);
     }
     // the spectrum and, when the z stage runs in direct form, its taps
-    size_t spectrum_bytes() const { return (R_->size() + (Kz_ ? Kz_->size() : 0)) * sizeof(float); }
+    size_t spectrum_bytes() const {
+        return ((R_ ? R_->size() : 0) + (Kz_ ? Kz_->size() : 0)) * sizeof(float);
+    }
     // the z stage runs as the direct Toeplitz product (kernel even in z,
     // n1 <= zdirect_max_rows()); its taps are {n1, P2, P3/2+1} floats
     bool z_direct() const { return (bool)Kz_; }
@@ -76,8 +81,12 @@ class Toeplitz {
     double algorithmic_bytes() const;
 
   private:
-    void build_kernel(Context &ctx, DevBuf<double> &K);
+    // zkeep > 0: with the kz mirror, sum only the planes |kz| < zkeep
+    void build_kernel(Context &ctx, DevBuf<double> &K, int zkeep);
     void build_kernel_nufft32(Context &ctx, DevBuf<double> &K);
+    void kernel_xy_fft(Context &ctx, const double *K, int nz, double2 *a, double2 *b);
+    void build_spectrum(Context &ctx, DevBuf<double> *K);
+    bool psf_fp32_ = false;
     bool three_d_;
     bool kernel_mirror_ = false;  // the last kernel built is even in its mirror axis (kz in 3D)
     bool zfold_ = false;          // spectrum stored for f1 <= P1/2 only
