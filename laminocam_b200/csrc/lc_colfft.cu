@@ -32,6 +32,7 @@ namespace {
 #define LC_COL_LINES 4
 #endif
 constexpr int kCols = LC_COL_LINES;  // columns per CTA: 32-byte row segments
+static_assert(kCols % 2 == 0, "the twiddle tables after the line buffers need 16-byte alignment");
 
 enum ColMode { CM_PLAIN = 0, CM_PLAIN_MID = 1, CM_SPLIT_IN = 2, CM_SPLIT_OUT = 3, CM_SPLIT_MID = 4 };
 
