@@ -257,8 +257,14 @@ void run_solver(lc_psf psf, int method, const float *rhs, float *x, const lc_sol
     Context &ctx = *psf->owner->ctx;
     check_solver_params(p);
     if (method == 1) LC_REQUIRE(p->mu != 0.0f, "split_bregman: mu must be non-zero");
-    if (!psf->solver) psf->solver = std::make_unique<Solver>(ctx, psf->T->nvox());
     Toeplitz *T = psf->T.get();
+    // Split-Bregman runs on rows padded to a multiple of 4 values (zeros past
+    // the row), so that its stencil kernels take four voxels per thread
+    const long *d = T->dims();
+    const long pitch = (d[2] + 3) / 4 * 4;
+    const bool padded = method == 1 && pitch != d[2];
+    const long need = padded ? d[0] * d[1] * pitch : T->nvox();
+    if (!psf->solver || psf->solver->size() != need) psf->solver = std::make_unique<Solver>(ctx, need);
     Operator A = [&ctx, T](const float *in, float *out) { T->apply(ctx, in, out); };
     // CG iterations fuse the direction update and p.Ap into the x passes
     FusedOperator F;
@@ -274,8 +280,23 @@ void run_solver(lc_psf psf, int method, const float *rhs, float *x, const lc_sol
     LC_CUDA(cudaEventRecord(e0, ctx.stream()));
     SolverStats st;
     SolverParams sp = to_sp(p);
-    if (method == 0) psf->solver->cg(ctx, A, rhs, x, sp, &st, &F);
-    else psf->solver->split_bregman(ctx, A, T->dims(), rhs, x, sp, &st);
+    if (method == 0) {
+        psf->solver->cg(ctx, A, rhs, x, sp, &st, &F);
+    } else if (!padded) {
+        psf->solver->split_bregman(ctx, A, d, rhs, x, sp, &st);
+    } else {
+        cudaStream_t s = ctx.stream();
+        const long rows = d[0] * d[1], np = need;
+        DevBuf<float> yp(np, s), xp(np, s);
+        yp.zero(s);
+        xp.zero(s);
+        const size_t w = (size_t)d[2] * sizeof(float), wp = (size_t)pitch * sizeof(float);
+        LC_CUDA(cudaMemcpy2DAsync(yp.get(), wp, rhs, w, w, rows, cudaMemcpyDeviceToDevice, s));
+        LC_CUDA(cudaMemcpy2DAsync(xp.get(), wp, x, w, w, rows, cudaMemcpyDeviceToDevice, s));
+        Operator Ap = [&ctx, T, pitch](const float *in, float *out) { T->apply(ctx, in, out, nullptr, 0, pitch); };
+        psf->solver->split_bregman(ctx, Ap, d, yp.get(), xp.get(), sp, &st, pitch);
+        LC_CUDA(cudaMemcpy2DAsync(x, w, xp.get(), wp, w, rows, cudaMemcpyDeviceToDevice, s));
+    }
     LC_CUDA(cudaEventRecord(e1, ctx.stream()));
     LC_CUDA(cudaEventSynchronize(e1));
     float ms = 0;

@@ -2,6 +2,8 @@
 // CTA (deterministic fixed-order sum of per-CTA partials), and the
 // Split-Bregman stencil kernels (right-hand side, shrinkage + Bregman update).
 #include <algorithm>
+#include <cstdint>
+#include <cstdlib>
 #include <memory>
 
 #include "lc_solver.hpp"
@@ -235,8 +237,10 @@ __global__ void __launch_bounds__(kThreads) p_update_kernel(float *__restrict__ 
         p[i] = fmaf(b, p[i], r[i]);
 }
 
+// n3 values of a row, stored at a row pitch p3 >= n3 (the values past n3 are
+// kept zero)
 struct Dims {
-    int n1, n2, n3;
+    int n1, n2, n3, p3;
 };
 
 // The stencil kernels walk the volume in tiles of 32 (along n3) x kTileRows
@@ -307,8 +311,8 @@ __device__ __forceinline__ float lap_at(const float *__restrict__ x, int idx, in
     const float c = x[idx];
     float lap = 0.f;
     lap += lap_term(x, idx, k, dm.n3, 1, c);
-    lap += lap_term(x, idx, j, dm.n2, dm.n3, c);
-    lap += lap_term(x, idx, i, dm.n1, dm.n2 * dm.n3, c);
+    lap += lap_term(x, idx, j, dm.n2, dm.p3, c);
+    lap += lap_term(x, idx, i, dm.n1, dm.n2 * dm.p3, c);
     return lap;
 }
 
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(kThreads)
         return;
     }
     A v[2] = {A(0), A(0)};
-    const int sj = dm.n3, si = dm.n2 * dm.n3;
+    const int sj = dm.p3, si = dm.n2 * dm.p3;
     for_voxels(tl, dm, [&](int i, int j, int k) {
         const int idx = i * si + j * sj + k;
         const float dk = (k + 1 < dm.n3 ? q0[idx + 1] : 0.f) - (k >= 1 ? q0[idx - 1] : 0.f);
@@ -377,7 +381,7 @@ __global__ void __launch_bounds__(kThreads) lap_dot_kernel(const float *__restri
                                                           unsigned *counter, CGState *st) {
     if (st->done) return;
     A v[1] = {A(0)};
-    const int sj = dm.n3, si = dm.n2 * dm.n3;
+    const int sj = dm.p3, si = dm.n2 * dm.p3;
     for_voxels(tl, dm, [&](int i, int j, int k) {
         const int idx = i * si + j * sj + k;
         const float a = fmaf(-mu, lap_at(p, idx, i, j, k, dm), ap[idx]);
@@ -415,7 +419,7 @@ __global__ void __launch_bounds__(kThreads)
                           double *part, unsigned *counter, CGState *st, float xtol) {
     if (st->sb_done) return;
     A v[2] = {A(0), A(0)};
-    const int sj = dm.n3, si = dm.n2 * dm.n3;
+    const int sj = dm.p3, si = dm.n2 * dm.p3;
     for_voxels(tl, dm, [&](int i, int j, int k) {
         const int idx = i * si + j * sj + k;
         // every load first (the buffers are distinct), then the stores
@@ -442,6 +446,294 @@ __global__ void __launch_bounds__(kThreads)
             v[1] += (A)xo * (A)xo;
             xold[idx] = xi;
         }
+    });
+    if (block_partials<A, 2>(v, part, counter)) {
+        double d2s = XOLD ? total<A>(part, 0, gridDim.x) : st->sb_diff2;
+        double o2 = XOLD ? total<A>(part, 1, gridDim.x) : st->sb_old2;
+        if (threadIdx.x == 0) {
+            double rel = sqrt(d2s) / (sqrt(o2) + 1e-8);
+            st->sb_rel = rel;
+            st->sb_iters += 1;
+            if (rel < (double)xtol) st->sb_done = 1;
+            *counter = 0;
+        }
+    }
+}
+
+// ---- the same three stencil kernels on four voxels per thread ----
+// With the row pitch a multiple of 4 every row starts 16-byte aligned: a
+// thread takes the four voxels k0 .. k0+3 of its row as one float4 (a warp
+// one row segment of 128 voxels, a CTA eight rows), their neighbours along
+// k come from the next lanes by shuffles (the warp's end lanes load the one
+// or two values past the segment), and those along n2 and n1 are float4
+// loads of the neighbouring rows.  The arithmetic per voxel is that of the
+// scalar kernels; values at k >= n3 are stored as 0 and left out of the sums.
+struct Quad {
+    float v[4];
+};
+
+__device__ __forceinline__ Quad ld4(const float *__restrict__ a, long idx) {
+    const float4 t = *reinterpret_cast<const float4 *>(a + idx);
+    return Quad{{t.x, t.y, t.z, t.w}};
+}
+
+__device__ __forceinline__ void st4(float *__restrict__ a, long idx, const Quad &q) {
+    *reinterpret_cast<float4 *>(a + idx) = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
+}
+
+// values at k - 1 and k + 1 (and k - 2, k + 2 with TWO) of the four values c
+// at k0 .. k0+3 of a row (row-relative k0; zero before the row and past its
+// pitch).  Every lane of the warp calls it (shuffles).
+template <bool TWO>
+__device__ __forceinline__ void k_neighbours(const float *__restrict__ row, int k0, int p3, const Quad &c,
+                                             Quad &m1, Quad &p1, Quad &m2, Quad &p2) {
+    const int lane = (int)(threadIdx.x & 31);
+    float w3 = __shfl_up_sync(0xffffffffu, c.v[3], 1);
+    float n0 = __shfl_down_sync(0xffffffffu, c.v[0], 1);
+    float w2 = 0.f, n1 = 0.f;
+    if constexpr (TWO) {
+        w2 = __shfl_up_sync(0xffffffffu, c.v[2], 1);
+        n1 = __shfl_down_sync(0xffffffffu, c.v[1], 1);
+    }
+    if (lane == 0) {
+        w3 = k0 >= 1 && k0 - 1 < p3 ? row[k0 - 1] : 0.f;
+        if constexpr (TWO) w2 = k0 >= 2 && k0 - 2 < p3 ? row[k0 - 2] : 0.f;
+    }
+    if (lane == 31) {
+        n0 = k0 + 4 < p3 ? row[k0 + 4] : 0.f;
+        if constexpr (TWO) n1 = k0 + 5 < p3 ? row[k0 + 5] : 0.f;
+    }
+    m1 = Quad{{w3, c.v[0], c.v[1], c.v[2]}};
+    p1 = Quad{{c.v[1], c.v[2], c.v[3], n0}};
+    if constexpr (TWO) {
+        m2 = Quad{{w2, w3, c.v[0], c.v[1]}};
+        p2 = Quad{{c.v[2], c.v[3], n0, n1}};
+    }
+}
+
+// per-axis term of the negative Laplacian (lap_term) from the values at
+// pos - 2, pos, pos + 2 along an axis of length n
+__device__ __forceinline__ float lap_term_v(float m2, float c, float p2, int pos, int n) {
+    const float pp = (pos + 2 < n) ? p2 : 0.f;
+    const float mm = (pos >= 2) ? m2 : 0.f;
+    const float gp = (pos + 1 < n) ? 0.5f * (pp - c) : 0.f;
+    const float gm = (pos >= 1) ? 0.5f * (c - mm) : 0.f;
+    return 0.5f * (gp - gm);
+}
+
+// body(i, j, k0, act): every (row, four-voxel group) of this thread's tiles;
+// act is false for lanes past the row's pitch (they still join the shuffles)
+template <typename F>
+__device__ __forceinline__ void for_quads(const Tiles &tl, const Dims &dm, F &&body) {
+    const int per = tl.tk * tl.tj;
+    int t = (int)blockIdx.x;
+    int i = t / per;
+    int jb = (t - i * per) / tl.tk;
+    int kb = t - i * per - jb * tl.tk;
+    const int ty = (int)(threadIdx.x >> 5), tx = (int)(threadIdx.x & 31);
+    for (; t < tl.count; t += (int)gridDim.x) {
+        const int j = jb * kTileRows + ty;
+        const int k0 = (kb * 32 + tx) * 4;
+        if (j < dm.n2) body(i, j, k0, k0 < dm.p3);  // uniform over the warp but for act
+        kb += tl.qk;
+        if (kb >= tl.tk) {
+            kb -= tl.tk;
+            ++jb;
+        }
+        jb += tl.qj;
+        if (jb >= tl.tj) {
+            jb -= tl.tj;
+            ++i;
+        }
+        i += tl.qi;
+    }
+}
+
+__device__ __forceinline__ Quad lap4(const float *__restrict__ x, long idx, int i, int j, int k0, const Dims &dm,
+                                     const Quad &c, const Quad &m2k, const Quad &p2k) {
+    const int sj = dm.p3, si = dm.n2 * dm.p3;
+    const Quad jm = j >= 2 ? ld4(x, idx - 2 * sj) : Quad{{0.f, 0.f, 0.f, 0.f}};
+    const Quad jp = j + 2 < dm.n2 ? ld4(x, idx + 2 * sj) : Quad{{0.f, 0.f, 0.f, 0.f}};
+    const Quad im = i >= 2 ? ld4(x, idx - 2 * si) : Quad{{0.f, 0.f, 0.f, 0.f}};
+    const Quad ip = i + 2 < dm.n1 ? ld4(x, idx + 2 * si) : Quad{{0.f, 0.f, 0.f, 0.f}};
+    Quad out;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        float lap = 0.f;
+        lap += lap_term_v(m2k.v[e], c.v[e], p2k.v[e], k0 + e, dm.n3);
+        lap += lap_term_v(jm.v[e], c.v[e], jp.v[e], j, dm.n2);
+        lap += lap_term_v(im.v[e], c.v[e], ip.v[e], i, dm.n1);
+        out.v[e] = lap;
+    }
+    return out;
+}
+
+template <typename A>
+__global__ void __launch_bounds__(kThreads)
+    sb_begin4_kernel(const float *__restrict__ yT, const float *__restrict__ q0, const float *__restrict__ q1,
+                     const float *__restrict__ q2, const float *__restrict__ tx, const float *__restrict__ x,
+                     float *__restrict__ ax, float *__restrict__ r, float *__restrict__ p, Dims dm, Tiles tl,
+                     float mu, double *part, unsigned *counter, CGState *st) {
+    if (st->sb_done) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->done = 1;
+        return;
+    }
+    A v[2] = {A(0), A(0)};
+    const int sj = dm.p3, si = dm.n2 * dm.p3;
+    const Quad zero{{0.f, 0.f, 0.f, 0.f}};
+    for_quads(tl, dm, [&](int i, int j, int k0, bool act) {
+        const long base = (long)i * si + (long)j * sj;
+        const long idx = base + k0;
+        const Quad c0 = act ? ld4(q0, idx) : zero;
+        Quad m1, p1, m2, p2;
+        k_neighbours<false>(q0 + base, k0, dm.p3, c0, m1, p1, m2, p2);
+        Quad xc = zero, xm2 = zero, xp2 = zero, xm1, xp1;
+        if (tx) {
+            xc = act ? ld4(x, idx) : zero;
+            k_neighbours<true>(x + base, k0, dm.p3, xc, xm1, xp1, xm2, xp2);
+        }
+        if (!act) return;
+        const Quad jm = j >= 1 ? ld4(q1, idx - sj) : zero, jp = j + 1 < dm.n2 ? ld4(q1, idx + sj) : zero;
+        const Quad im = i >= 1 ? ld4(q2, idx - si) : zero, ip = i + 1 < dm.n1 ? ld4(q2, idx + si) : zero;
+        const Quad y = ld4(yT, idx);
+        Quad a = tx ? ld4(tx, idx) : ld4(ax, idx);
+        if (tx) {
+            const Quad lp = lap4(x, idx, i, j, k0, dm, xc, xm2, xp2);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) a.v[e] = k0 + e < dm.n3 ? fmaf(-mu, lp.v[e], a.v[e]) : 0.f;
+            st4(ax, idx, a);
+        }
+        Quad rr;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float dk = p1.v[e] - m1.v[e];
+            const float dj = jp.v[e] - jm.v[e];
+            const float di = ip.v[e] - im.v[e];
+            const float rhs = fmaf(-mu, 0.5f * dk + 0.5f * dj + 0.5f * di, y.v[e]);
+            const float ri = rhs - a.v[e];
+            const bool in = k0 + e < dm.n3;
+            rr.v[e] = in ? ri : 0.f;
+            if (in) {
+                v[0] += (A)rhs * (A)rhs;
+                v[1] += (A)ri * (A)ri;
+            }
+        }
+        st4(r, idx, rr);
+        if (p) st4(p, idx, rr);
+    });
+    if (block_partials<A, 2>(v, part, counter)) {
+        double y2 = total<A>(part, 0, gridDim.x);
+        double r2 = total<A>(part, 1, gridDim.x);
+        if (threadIdx.x == 0) {
+            st->y2 = y2;
+            st->rs_old = r2;
+            st->iters = 0;
+            st->done = 0;
+            st->reason = 0;
+            st->res = 0;
+            st->dx = 0;
+            st->sb_diff2 = 0;  // an update skipped by the |p.Ap| stop leaves x unchanged
+            st->sb_old2 = 0;
+            *counter = 0;
+        }
+    }
+}
+
+template <typename A>
+__global__ void __launch_bounds__(kThreads) lap_dot4_kernel(const float *__restrict__ p, float *__restrict__ ap,
+                                                           Dims dm, Tiles tl, float mu, double *part,
+                                                           unsigned *counter, CGState *st) {
+    if (st->done) return;
+    A v[1] = {A(0)};
+    const int sj = dm.p3, si = dm.n2 * dm.p3;
+    const Quad zero{{0.f, 0.f, 0.f, 0.f}};
+    for_quads(tl, dm, [&](int i, int j, int k0, bool act) {
+        const long base = (long)i * si + (long)j * sj;
+        const long idx = base + k0;
+        const Quad c = act ? ld4(p, idx) : zero;
+        Quad m1, p1, m2, p2;
+        k_neighbours<true>(p + base, k0, dm.p3, c, m1, p1, m2, p2);
+        if (!act) return;
+        const Quad lp = lap4(p, idx, i, j, k0, dm, c, m2, p2);
+        Quad a = ld4(ap, idx);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const bool in = k0 + e < dm.n3;
+            a.v[e] = in ? fmaf(-mu, lp.v[e], a.v[e]) : 0.f;
+            if (in) v[0] += (A)c.v[e] * (A)a.v[e];
+        }
+        st4(ap, idx, a);
+    });
+    if (block_partials<A, 1>(v, part, counter)) {
+        double pap = total<A>(part, 0, gridDim.x);
+        if (threadIdx.x == 0) {
+            st->pAp = pap;
+            if (fabs(pap) < 1e-10) {
+                st->done = 1;
+                st->reason = 3;
+            } else {
+                st->alpha = (double)((A)st->rs_old / (A)pap);
+            }
+            *counter = 0;
+        }
+    }
+}
+
+template <typename A, bool XOLD>
+__global__ void __launch_bounds__(kThreads)
+    sb_shrink4_kernel(const float *__restrict__ x, float *__restrict__ xold, float *__restrict__ q0,
+                      float *__restrict__ q1, float *__restrict__ q2, float *__restrict__ b0,
+                      float *__restrict__ b1, float *__restrict__ b2, Dims dm, Tiles tl, float thresh,
+                      double *part, unsigned *counter, CGState *st, float xtol) {
+    if (st->sb_done) return;
+    A v[2] = {A(0), A(0)};
+    const int sj = dm.p3, si = dm.n2 * dm.p3;
+    const Quad zero{{0.f, 0.f, 0.f, 0.f}};
+    for_quads(tl, dm, [&](int i, int j, int k0, bool act) {
+        const long base = (long)i * si + (long)j * sj;
+        const long idx = base + k0;
+        const Quad xc = act ? ld4(x, idx) : zero;
+        Quad m1, p1, m2, p2;
+        k_neighbours<false>(x + base, k0, dm.p3, xc, m1, p1, m2, p2);
+        if (!act) return;
+        const Quad xo = XOLD ? ld4(xold, idx) : zero;
+        const Quad c0 = ld4(b0, idx), c1 = ld4(b1, idx), c2 = ld4(b2, idx);
+        const Quad jm = j >= 1 ? ld4(x, idx - sj) : zero, jp = j + 1 < dm.n2 ? ld4(x, idx + sj) : zero;
+        const Quad im = i >= 1 ? ld4(x, idx - si) : zero, ip = i + 1 < dm.n1 ? ld4(x, idx + si) : zero;
+        Quad o0, o1, o2, n0, n1, n2;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const bool in = k0 + e < dm.n3;
+            const float g0 = 0.5f * ((k0 + e + 1 < dm.n3 ? p1.v[e] : 0.f) - (k0 + e >= 1 ? m1.v[e] : 0.f));
+            const float g1 = 0.5f * (jp.v[e] - jm.v[e]);
+            const float g2 = 0.5f * (ip.v[e] - im.v[e]);
+            const float t0 = g0 + c0.v[e], t1 = g1 + c1.v[e], t2 = g2 + c2.v[e];
+            const float s = sqrtf(t0 * t0 + t1 * t1 + t2 * t2);
+            const float m = fmaxf(0.f, s - thresh);
+            const float inv = 1.0f / (s + 1e-8f);
+            const float e0 = m * (t0 * inv), e1 = m * (t1 * inv), e2 = m * (t2 * inv);
+            const float d0 = c0.v[e] + (g0 - e0), d1 = c1.v[e] + (g1 - e1), d2 = c2.v[e] + (g2 - e2);
+            o0.v[e] = in ? e0 - d0 : 0.f;
+            o1.v[e] = in ? e1 - d1 : 0.f;
+            o2.v[e] = in ? e2 - d2 : 0.f;
+            n0.v[e] = in ? d0 : 0.f;
+            n1.v[e] = in ? d1 : 0.f;
+            n2.v[e] = in ? d2 : 0.f;
+            if constexpr (XOLD) {
+                if (in) {
+                    const float df = xc.v[e] - xo.v[e];
+                    v[0] += (A)df * (A)df;
+                    v[1] += (A)xo.v[e] * (A)xo.v[e];
+                }
+            }
+        }
+        st4(q0, idx, o0);
+        st4(q1, idx, o1);
+        st4(q2, idx, o2);
+        st4(b0, idx, n0);
+        st4(b1, idx, n1);
+        st4(b2, idx, n2);
+        if constexpr (XOLD) st4(xold, idx, xc);
     });
     if (block_partials<A, 2>(v, part, counter)) {
         double d2s = XOLD ? total<A>(part, 0, gridDim.x) : st->sb_diff2;
@@ -626,12 +918,25 @@ void Solver::cg(Context &ctx, const Operator &A, const float *y, float *x, const
     }
 }
 
+bool sb_vec4_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("LC_SB_VEC4");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3], const float *yT,
-                           float *x, const SolverParams &p, SolverStats *stats) {
+                           float *x, const SolverParams &p, SolverStats *stats, long pitch) {
     cudaStream_t s = ctx.stream();
-    LC_REQUIRE(dims[0] * dims[1] * dims[2] == n_, "split_bregman: dims do not match the solver size");
-    LC_REQUIRE(n_ < (1L << 31) && dims[1] < (1L << 24) && dims[2] < (1L << 24),
+    if (pitch <= 0) pitch = dims[2];
+    LC_REQUIRE(pitch >= dims[2], "split_bregman: row pitch below the row length");
+    LC_REQUIRE(dims[0] * dims[1] * pitch == n_, "split_bregman: dims do not match the solver size");
+    LC_REQUIRE(n_ < (1L << 31) && dims[1] < (1L << 24) && pitch < (1L << 24),
                "split_bregman: volume too large for 32-bit indexing");
+    // four voxels per thread when every row starts 16-byte aligned
+    const bool vec4 = pitch % 4 == 0 && sb_vec4_enabled() &&
+                      ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(yT)) & 15) == 0;
     host_st_ = static_cast<CGState *>(ctx.pinned_scratch(sizeof(CGState)));
     const int inner = std::max(0, p.inner_iters);
     for (int a = 0; a < 3; ++a) {
@@ -651,9 +956,16 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
     reset_state_kernel<<<1, 1, 0, s>>>(st_.get());
     LC_CHECK_LAUNCH();
     const float mu = p.mu;
-    const Dims dm{(int)dims[0], (int)dims[1], (int)dims[2]};
+    const Dims dm{(int)dims[0], (int)dims[1], (int)dims[2], (int)pitch};
+    // the values past the row length stay zero in every work vector
+    if (pitch != dims[2]) {
+        ap_.zero(s);
+        r_.zero(s);
+        ax_.zero(s);
+        if (inner > 1) p_.zero(s);
+    }
     Tiles tl;
-    tl.tk = (int)((dims[2] + 31) / 32);
+    tl.tk = vec4 ? (int)((pitch / 4 + 31) / 32) : (int)((dims[2] + 31) / 32);
     tl.tj = (int)((dims[1] + kTileRows - 1) / kTileRows);
     const long ntiles = (long)tl.tk * tl.tj * dims[0];
     LC_REQUIRE(ntiles < (1L << 31), "split_bregman: too many tiles");
@@ -673,12 +985,19 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
         return g;
     };
     const bool f32 = p.fp32_scalars != 0;
-    const TileGrid g_begin = grid_for_kernel(f32 ? (const void *)sb_begin_kernel<float> : (const void *)sb_begin_kernel<double>);
-    const TileGrid g_lap = grid_for_kernel(f32 ? (const void *)lap_dot_kernel<float> : (const void *)lap_dot_kernel<double>);
-    const TileGrid g_shrink = grid_for_kernel(
-        f32 ? (keep_xold ? (const void *)sb_shrink_diff_kernel<float, true> : (const void *)sb_shrink_diff_kernel<float, false>)
-            : (keep_xold ? (const void *)sb_shrink_diff_kernel<double, true>
-                         : (const void *)sb_shrink_diff_kernel<double, false>));
+    const void *k_begin = vec4 ? (f32 ? (const void *)sb_begin4_kernel<float> : (const void *)sb_begin4_kernel<double>)
+                               : (f32 ? (const void *)sb_begin_kernel<float> : (const void *)sb_begin_kernel<double>);
+    const void *k_lap = vec4 ? (f32 ? (const void *)lap_dot4_kernel<float> : (const void *)lap_dot4_kernel<double>)
+                             : (f32 ? (const void *)lap_dot_kernel<float> : (const void *)lap_dot_kernel<double>);
+    const void *k_shrink =
+        vec4 ? (f32 ? (keep_xold ? (const void *)sb_shrink4_kernel<float, true> : (const void *)sb_shrink4_kernel<float, false>)
+                    : (keep_xold ? (const void *)sb_shrink4_kernel<double, true> : (const void *)sb_shrink4_kernel<double, false>))
+             : (f32 ? (keep_xold ? (const void *)sb_shrink_diff_kernel<float, true> : (const void *)sb_shrink_diff_kernel<float, false>)
+                    : (keep_xold ? (const void *)sb_shrink_diff_kernel<double, true>
+                                 : (const void *)sb_shrink_diff_kernel<double, false>));
+    const TileGrid g_begin = grid_for_kernel(k_begin);
+    const TileGrid g_lap = grid_for_kernel(k_lap);
+    const TileGrid g_shrink = grid_for_kernel(k_shrink);
     const int sblk = std::max(g_begin.blocks, std::max(g_lap.blocks, g_shrink.blocks));
     part_.ensure((long)std::max(sblk, nblk_) * kParts, s);
     // With one CG iteration per outer iteration its direction is the residual
@@ -700,11 +1019,11 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
             const float *tx = exact ? ap_.get() : nullptr;
             float *pinit = inner > 1 ? p_.get() : nullptr;
             if (fp32)
-                sb_begin_kernel<float><<<g_begin.blocks, kThreads, 0, os>>>(
+                (vec4 ? sb_begin4_kernel<float> : sb_begin_kernel<float>)<<<g_begin.blocks, kThreads, 0, os>>>(
                     yT, q_[0].get(), q_[1].get(), q_[2].get(), tx, x,
                     ax_.get(), r_.get(), pinit, dm, g_begin.tl, mu, part_.get(), counter_.get(), st_.get());
             else
-                sb_begin_kernel<double><<<g_begin.blocks, kThreads, 0, os>>>(
+                (vec4 ? sb_begin4_kernel<double> : sb_begin_kernel<double>)<<<g_begin.blocks, kThreads, 0, os>>>(
                     yT, q_[0].get(), q_[1].get(), q_[2].get(), tx, x,
                     ax_.get(), r_.get(), pinit, dm, g_begin.tl, mu, part_.get(), counter_.get(), st_.get());
             LC_CHECK_LAUNCH();
@@ -713,7 +1032,7 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
             AtA(pp, ap_.get());
             ProfScope ps(ctx, PS_CG_VEC, 4.0 * n_ * (inner > 1 ? 13.0 : 10.0));
             if (fp32) {
-                lap_dot_kernel<float><<<g_lap.blocks, kThreads, 0, os>>>(pp, ap_.get(), dm, g_lap.tl, mu, part_.get(),
+                (vec4 ? lap_dot4_kernel<float> : lap_dot_kernel<float>)<<<g_lap.blocks, kThreads, 0, os>>>(pp, ap_.get(), dm, g_lap.tl, mu, part_.get(),
                                                                 counter_.get(), st_.get());
                 LC_CHECK_LAUNCH();
                 if (inner > 1)
@@ -725,7 +1044,7 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
                         x, r_.get(), pp, ap_.get(), ax_.get(), n_, part_.get(), counter_.get(), st_.get(), p.tol,
                         p.xtol);
             } else {
-                lap_dot_kernel<double><<<g_lap.blocks, kThreads, 0, os>>>(pp, ap_.get(), dm, g_lap.tl, mu, part_.get(),
+                (vec4 ? lap_dot4_kernel<double> : lap_dot_kernel<double>)<<<g_lap.blocks, kThreads, 0, os>>>(pp, ap_.get(), dm, g_lap.tl, mu, part_.get(),
                                                                  counter_.get(), st_.get());
                 LC_CHECK_LAUNCH();
                 if (inner > 1)
@@ -749,20 +1068,20 @@ void Solver::split_bregman(Context &ctx, const Operator &AtA, const long dims[3]
         const float th = p.lambda / p.mu;
         if (fp32) {
             if (keep_xold)
-                sb_shrink_diff_kernel<float, true><<<g_shrink.blocks, kThreads, 0, os>>>(
+                (vec4 ? sb_shrink4_kernel<float, true> : sb_shrink_diff_kernel<float, true>)<<<g_shrink.blocks, kThreads, 0, os>>>(
                     x, xo, q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
                     g_shrink.tl, th, part_.get(), counter_.get(), st_.get(), p.xtol);
             else
-                sb_shrink_diff_kernel<float, false><<<g_shrink.blocks, kThreads, 0, os>>>(
+                (vec4 ? sb_shrink4_kernel<float, false> : sb_shrink_diff_kernel<float, false>)<<<g_shrink.blocks, kThreads, 0, os>>>(
                     x, xo, q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
                     g_shrink.tl, th, part_.get(), counter_.get(), st_.get(), p.xtol);
         } else {
             if (keep_xold)
-                sb_shrink_diff_kernel<double, true><<<g_shrink.blocks, kThreads, 0, os>>>(
+                (vec4 ? sb_shrink4_kernel<double, true> : sb_shrink_diff_kernel<double, true>)<<<g_shrink.blocks, kThreads, 0, os>>>(
                     x, xo, q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
                     g_shrink.tl, th, part_.get(), counter_.get(), st_.get(), p.xtol);
             else
-                sb_shrink_diff_kernel<double, false><<<g_shrink.blocks, kThreads, 0, os>>>(
+                (vec4 ? sb_shrink4_kernel<double, false> : sb_shrink_diff_kernel<double, false>)<<<g_shrink.blocks, kThreads, 0, os>>>(
                     x, xo, q_[0].get(), q_[1].get(), q_[2].get(), b_[0].get(), b_[1].get(), b_[2].get(), dm,
                     g_shrink.tl, th, part_.get(), counter_.get(), st_.get(), p.xtol);
         }

@@ -54,6 +54,7 @@ class Solver {
     Solver(Context &ctx, long n);
     ~Solver();
     Solver(const Solver &) = delete;
+    long size() const { return n_; }
     Solver &operator=(const Solver &) = delete;
     // x (in: x0, out: solution); y = right-hand side
     // With F, each iteration applies F (fusing the direction update and the
@@ -61,8 +62,12 @@ class Solver {
     void cg(Context &ctx, const Operator &A, const float *y, float *x, const SolverParams &p,
             SolverStats *stats, const FusedOperator *F = nullptr);
     // A is the normal operator A^T A alone; mu * (-laplacian) is added here.
+    // pitch: the row stride of x, yT and of the vectors AtA gets and returns
+    // (>= dims[2], the values past dims[2] zero; 0 = dims[2]); the solver's
+    // size is dims[0] * dims[1] * pitch.  A multiple of 4 lets the stencil
+    // kernels take four voxels per thread.
     void split_bregman(Context &ctx, const Operator &AtA, const long dims[3], const float *yT,
-                       float *x, const SolverParams &p, SolverStats *stats);
+                       float *x, const SolverParams &p, SolverStats *stats, long pitch = 0);
 
   private:
     void cg_run(Context &ctx, const Operator &A, const float *y, float *x, int iters, float tol,

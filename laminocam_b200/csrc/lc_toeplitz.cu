@@ -922,9 +922,11 @@ unsigned Toeplitz::cg_caps() const {
 
 long Toeplitz::cg_partials() const { return row_fft_ctas(n_[0] * n_[1]); }
 
-void Toeplitz::apply(Context &ctx, const float *x, float *y, const CGFusion *f, unsigned parts) {
+void Toeplitz::apply(Context &ctx, const float *x, float *y, const CGFusion *f, unsigned parts, long pitch) {
     LC_REQUIRE((parts & ~cg_caps()) == 0, "Toeplitz: CG fusion not available for this size");
     const long n1 = n_[0], n2 = n_[1], n3 = n_[2];
+    if (pitch <= 0) pitch = n3;
+    LC_REQUIRE(pitch >= n3, "Toeplitz: row pitch below the row length");
     const int P1 = P_[0], P2 = P_[1], P3 = P_[2];
     const int P3h = Ph_[2];
     const double N = (double)n1 * n2 * n3;
@@ -941,7 +943,7 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y, const CGFusion *f, 
         a.out_t = E_C64;
         a.n_outer = n1 * n2;
         a.n_inner = 1;
-        a.in_ostride = n3;
+        a.in_ostride = pitch;
         a.out_ostride = P3h;
         a.n_in = (int)n3;
         a.L = P3;
@@ -1054,7 +1056,7 @@ void Toeplitz::apply(Context &ctx, const float *x, float *y, const CGFusion *f, 
         a.n_outer = n1 * n2;
         a.n_inner = 1;
         a.in_ostride = P3h;
-        a.out_ostride = n3;
+        a.out_ostride = pitch;
         a.n_in = P3h;
         a.in_map = IN_HERM;
         a.L = P3;

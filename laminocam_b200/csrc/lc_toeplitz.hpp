@@ -37,7 +37,10 @@ class Toeplitz {
     // y = A^T A x.  With f, the parts of `parts` (a subset of cg_caps()) of the
     // surrounding CG iteration are fused into the x passes: x is then the
     // direction f->p, updated in place.
-    void apply(Context &ctx, const float *x, float *y, const CGFusion *f = nullptr, unsigned parts = 0);
+    // pitch: the row stride of x and y (>= n3; 0 = n3); y's values past n3
+    // are not written
+    void apply(Context &ctx, const float *x, float *y, const CGFusion *f = nullptr, unsigned parts = 0,
+               long pitch = 0);
     // CG work the apply can fuse (its x passes run the register-plan row kernel)
     unsigned cg_caps() const;
     // CTAs whose partials a fused dot product writes

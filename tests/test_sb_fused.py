@@ -80,3 +80,37 @@ def test_graph_replay_matches_eager_with_refresh(lc, problem, refresh, inner):
     a = lc.split_bregman(A, y, x0, 0.05, 2.0, 10, inner, 0.0, 0.0, residual_refresh=refresh)
     b = lc.split_bregman(A, y, x0, 0.05, 2.0, 10, inner, 0.0, 0.0, residual_refresh=refresh, use_graph=True)
     assert torch.equal(a, b)
+
+
+SCRIPT = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import torch
+import laminocam_b200 as lc
+n1, n, nth = 5, 61, 36
+th = np.arange(nth) * 2 * np.pi / nth
+pg = lc.PolarGrid(th, np.full(nth, -np.deg2rad(30.0)), np.zeros(nth), n, n)
+A = lc.PointSpreadFunction(pg, (n1, n, n))
+y = torch.as_tensor(np.random.default_rng(3).random((n1, n, n)), dtype=torch.float32, device="cuda")
+x = lc.split_bregman(A, y, torch.zeros_like(y), 0.05, 2.0, 12, int(sys.argv[3]), 0.0, 0.0, residual_refresh=4)
+np.save(sys.argv[2], x.cpu().numpy())
+"""
+
+
+@pytest.mark.parametrize("inner", [1, 2])
+def test_four_voxel_kernels_match_scalar(cuda, tmp_path, inner):
+    """Rows of 61 voxels are solved at a row pitch of 64 with the four-voxel
+    stencil kernels (default) or the scalar ones (LC_SB_VEC4=0): the same
+    arithmetic per voxel, reductions summed in another order."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = {}
+    for flag in ("1", "0"):
+        path = str(tmp_path / f"x{flag}_{inner}.npy")
+        subprocess.run([sys.executable, "-c", SCRIPT, root, path, str(inner)],
+                       env=dict(os.environ, LC_SB_VEC4=flag), check=True, timeout=600)
+        outs[flag] = np.load(path).astype(np.float64)
+    assert O.rel_l2(outs["1"], outs["0"]) < 1e-5
