@@ -213,9 +213,10 @@ def cpu_baseline():
 
 
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one Toeplitz apply at the
-# padded workload volume [29, 721, 721]: x rows 60 + 64 MB, y forward 122 + 193,
-# z 387 + 203, y inverse 247 + 98, x inverse 122 + 31
-TOEPLITZ_APPLY_DRAM_BYTES = 1527e6
+# padded workload volume [29, 721, 721] (--kernel-case toeplitz): x rows 60 + 62 MB,
+# y forward 122 + 190, direct z stage 370 + 189, y inverse 247 + 96, x inverse
+# 122 + 32 (writes still in L2 when a pass ends are not counted)
+TOEPLITZ_APPLY_DRAM_BYTES = 1492e6
 
 # padded detector of the workload (511 -> int(511 * 1.4142) forced odd)
 PADDED_DET = (721, 721)
