@@ -568,8 +568,12 @@ __device__ __forceinline__ Quad lap4(const float *__restrict__ x, long idx, int 
     return out;
 }
 
+#ifndef LC_SB_BEGIN_MIN_BLOCKS
+#define LC_SB_BEGIN_MIN_BLOCKS 4  // CTAs per SM sb_begin4's registers are sized for
+#endif
+
 template <typename A>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, LC_SB_BEGIN_MIN_BLOCKS)
     sb_begin4_kernel(const float *__restrict__ yT, const float *__restrict__ q0, const float *__restrict__ q1,
                      const float *__restrict__ q2, const float *__restrict__ tx, const float *__restrict__ x,
                      float *__restrict__ ax, float *__restrict__ r, float *__restrict__ p, Dims dm, Tiles tl,
