@@ -105,7 +105,9 @@ int lc_psf_info(lc_psf psf, int *P, long *spectrum_elems);
  * reads them) */
 int lc_psf_kernel(lc_context ctx, lc_psf psf, double *host_out);
 /* real R2C half spectrum {P0, P1, P2/2+1} of the zero-centred PSF (its
- * unpaired -P/2 planes zeroed), host buffer */
+ * unpaired -P/2 planes zeroed), host buffer.  A 3D PSF whose kernel is even
+ * in z applies its z stage from taps and builds this spectrum on the first
+ * call: like lc_psf_kernel, it needs the PSF's geometry then. */
 int lc_psf_spectrum(lc_context ctx, lc_psf psf, float *host_out);
 /* sysmat(x, PSF) / sysmat2d(x, PSF2D) (src/gradient.cpp:49-52,76-79):
  * y = A^T A x, x and y device {n1, n2, n3} */
