@@ -56,10 +56,13 @@ constexpr size_t col_smem() {
 
 // CTAs per SM the register budget is sized for: three for the small CTAs,
 // fewer for the long lines (whose threads hold up to 2 x 16 elements)
+#ifndef LC_COL_MIN_BLOCKS_SMALL
+#define LC_COL_MIN_BLOCKS_SMALL 3  // CTAs per SM for CTAs of up to 352 threads
+#endif
 template <int R0, int R1, int R2>
 constexpr int col_min_blocks() {
     constexpr int t = RegPlan<R0, R1, R2>::NT * kCols;
-    return t <= 352 ? 3 : (t <= 448 ? 2 : 1);
+    return t <= 352 ? LC_COL_MIN_BLOCKS_SMALL : (t <= 448 ? 2 : 1);
 }
 
 template <int R0, int R1, int R2, int MODE>
