@@ -76,7 +76,10 @@ BIN = os.path.join(HERE, "bin")
 DRIVER_COMMON = ["lc_toml.cpp", "lc_io.cpp", "lc_config.cpp"]
 EXECUTABLES = {"recon_lamino": DRIVER_COMMON + ["recon_lamino.cpp"],
                "recon_tomo": DRIVER_COMMON + ["recon_tomo.cpp"],
+               "forward_scalar": ["lc_toml.cpp", "lc_io.cpp", "forward_scalar.cpp"],
                "lc_convert": ["lc_io.cpp", "lc_convert.cpp"]}
+# drivers that also call the CUDA runtime (device buffers of their own)
+CUDART_DRIVERS = {"forward_scalar"}
 
 
 def host_cxx() -> str:
@@ -99,6 +102,10 @@ def build_drivers() -> None:
                *[os.path.join(DRIVERS, s) for s in srcs]]
         if exe != "lc_convert":
             cmd += ["-L", HERE, "-llaminocam_b200", "-Wl,-rpath,$ORIGIN/.."]
+        if exe in CUDART_DRIVERS:
+            cuda = os.path.dirname(os.path.dirname(os.path.realpath(nvcc())))
+            cmd += ["-I", os.path.join(cuda, "include"), "-L", os.path.join(cuda, "lib64"), "-lcudart",
+                    "-Wl,-rpath," + os.path.join(cuda, "lib64")]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"building {exe} failed:\n{r.stdout}\n{r.stderr}")

@@ -1,4 +1,4 @@
-"""The TOML-driven drivers (recon_lamino, recon_tomo) and their file formats.
+"""The TOML-driven drivers (recon_lamino, recon_tomo, forward_scalar) and their file formats.
 
 CPU tests run the drivers with --dry-run, which parses the config, loads and
 prepares the inputs exactly as a reconstruction would and prints a summary,
@@ -24,7 +24,7 @@ BIN = os.path.join(ROOT, "laminocam_b200", "bin")
 def bins():
     from laminocam_b200 import build
     build.build()
-    return {k: os.path.join(BIN, k) for k in ("recon_lamino", "recon_tomo", "lc_convert")}
+    return {k: os.path.join(BIN, k) for k in ("recon_lamino", "recon_tomo", "forward_scalar", "lc_convert")}
 
 
 def write_tiff(path, vol, big_endian=False, rows_per_strip=None, dtype=np.float32):
@@ -347,3 +347,62 @@ recon_dims = [3, 63, 63]
     ref = lc.MBIR2D(prepared, np.deg2rad(th),
                     lc.ReconParams(regularizer="unconstrained", recon_dims=(3, n, n), max_iters=5, tol=0, xtol=0))
     assert O.rel_l2(got, ref) < 1e-4
+
+
+FORWARD_CFG = """[input]
+filename = "vol.tiff"
+[output]
+basedir = "fwd"
+pad_factor = 1.5
+proj_angles = { min = -90, max = 90, n = 30 }
+[[projections]]
+gamma = 0
+filename = "g0.tiff"
+[[projections]]
+gamma = 25.5
+filename = "sub/g25.tiff"
+"""
+
+
+def test_forward_scalar_config(bins, tmp_path):
+    """src/radon.cpp: [min, max) in n float steps, every axis padded to
+    int(n pad) forced odd, one output file per [[projections]] entry."""
+    vol = np.random.default_rng(4).random((9, 21, 23)).astype(np.float32)
+    write_tiff(tmp_path / "vol.tiff", vol)
+    (tmp_path / "f.toml").write_text(FORWARD_CFG)
+    rc, out, err = dry(bins["forward_scalar"], str(tmp_path / "f.toml"))
+    assert rc == 0, err
+    assert out["volume"] == [9, 21, 23]
+    assert out["padded"] == [13, 31, 33]  # int(1.5 n) -> 13, 31, 34 -> 33
+    assert out["angles"] == 30 and out["angle0"] == -90.0 and out["angle_last"] == 84.0
+    assert [p["gamma"] for p in out["projections"]] == [0.0, 25.5]
+    assert out["projections"][1]["file"].endswith("fwd/sub/g25.tiff")
+    assert abs(out["sum"] - float(vol.astype(np.float64).sum())) < 1e-3 * vol.size
+    (tmp_path / "g.toml").write_text("[output]\nbasedir = 'x'\n")
+    rc, _, err = dry(bins["forward_scalar"], str(tmp_path / "g.toml"))
+    assert rc != 0 and "input and output sections are required" in err
+
+
+@pytest.mark.gpu
+def test_forward_scalar_matches_python_api(bins, tmp_path, cuda):
+    """The tool's files against lc.forward of the same padded volume, cropped."""
+    import laminocam_b200 as lc
+    from oracle import oracle as O
+    vol = np.random.default_rng(5).random((9, 21, 23)).astype(np.float32)
+    write_tiff(tmp_path / "vol.tiff", vol)
+    (tmp_path / "f.toml").write_text(FORWARD_CFG)
+    r = subprocess.run([bins["forward_scalar"], str(tmp_path / "f.toml")], capture_output=True, text=True,
+                       cwd=tmp_path, timeout=600)
+    assert r.returncode == 0, r.stderr
+    ang = np.loadtxt(tmp_path / "fwd" / "angles.txt")
+    assert ang.shape == (30,) and ang[0] == -90 and ang[-1] == 84
+    vp = np.zeros((13, 31, 33), np.float32)
+    vp[2:11, 5:26, 5:28] = vol
+    th = (np.float32(-90) + np.arange(30, dtype=np.float32) * np.float32(6)) * np.float32(np.pi) / np.float32(180)
+    for gamma, name in ((0.0, "g0.tiff"), (25.5, "sub/g25.tiff")):
+        g = np.float32(gamma) * np.float32(np.pi) / np.float32(180)
+        pg = lc.PolarGrid(th.astype(np.float64), np.full(30, float(g)), np.zeros(30), 31, 33)
+        want = lc.forward(vp, pg).cpu().numpy()[:, 5:26, 5:28]
+        got = read_tiff(tmp_path / "fwd" / name)
+        assert got.shape == (30, 21, 23)
+        assert O.rel_l2(got, want) < 1e-6, name
