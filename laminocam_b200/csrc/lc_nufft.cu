@@ -245,13 +245,38 @@ __global__ void bin_count_kernel(PolarPts pts, GridCfg g, int W, int *counts) {
     }
 }
 
+// the bin of a point and its footprint corner in the bin's tile (x fastest):
+// l0 - S per axis, S = bin start - hw, as the spreading kernel places it
 template <int DIM>
-__global__ void bin_scatter_kernel(PolarPts pts, GridCfg g, int W, int *cursor, int *perm) {
+__device__ __forceinline__ int bin_corner_of(const PointInfo &pi, const GridCfg &g, int W, int &corner) {
+    int b = 0, mul = 1, stride = 1;
+    corner = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        int cell, l0;
+        float off;
+        place(pi.c[d], g.nf[d], g.inv_nf[d], W, cell, l0, off);
+        const int bd = cell / g.bs[d];
+        b += bd * mul;
+        mul *= g.nb[d];
+        corner += (l0 - (bd * g.bs[d] - g.hw[d])) * stride;
+        stride *= g.td[d];
+    }
+    return b;
+}
+
+// perm[k] = the point at sorted position k; corners[k] its footprint corner
+// in its bin's tile (read by the footprint bound and the spreading's
+// bucketing)
+template <int DIM>
+__global__ void bin_scatter_kernel(PolarPts pts, GridCfg g, int W, int *cursor, int *perm,
+                                   unsigned short *corners) {
     for (long j = (long)blockIdx.x * blockDim.x + threadIdx.x; j < pts.M;
          j += (long)gridDim.x * blockDim.x) {
         PointInfo pi;
         point_at(pts, j, pi);
-        int b = bin_of<DIM>(pi, g, W);
+        int corner;
+        int b = bin_corner_of<DIM>(pi, g, W, corner);
         unsigned act = __activemask();
         unsigned peers = __match_any_sync(act, b);
         int lane = threadIdx.x & 31;
@@ -261,6 +286,7 @@ __global__ void bin_scatter_kernel(PolarPts pts, GridCfg g, int W, int *cursor, 
         if (lane == leader) base = atomicAdd(&cursor[b], __popc(peers));
         base = __shfl_sync(peers, base, leader);
         perm[base + rank] = (int)j;
+        corners[base + rank] = (unsigned short)corner;
     }
 }
 
@@ -516,8 +542,8 @@ struct OffsetWeights {
 // line is summed by one thread in a fixed order, so the bound depends on the
 // bin's point set alone.
 template <int DIM, int W>
-__global__ void __launch_bounds__(256) bin_footprint_kernel(PolarPts pts, GridCfg g, OffsetWeights om,
-                                                            const int *__restrict__ perm,
+__global__ void __launch_bounds__(256) bin_footprint_kernel(GridCfg g, OffsetWeights om,
+                                                            const unsigned short *__restrict__ corners,
                                                             const int2 *__restrict__ bins, int *kbin) {
     extern __shared__ int hist[];
     __shared__ int kmx;
@@ -526,34 +552,12 @@ __global__ void __launch_bounds__(256) bin_footprint_kernel(PolarPts pts, GridCf
         if (threadIdx.x == 0) kbin[blockIdx.x] = 0;
         return;
     }
-    int S[3] = {0, 0, 0};
-    {
-        int rr = blockIdx.x;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            S[d] = (rr % g.nb[d]) * g.bs[d] - g.hw[d];
-            rr /= g.nb[d];
-        }
-    }
     const int tx = g.td[0], ty = g.td[1], tz = DIM == 3 ? g.td[2] : 1;
     const int plane = tx * ty, tsize = plane * tz;
     for (int i = threadIdx.x; i < tsize; i += blockDim.x) hist[i] = 0;
     if (threadIdx.x == 0) kmx = 0;
     __syncthreads();
-    for (int p = threadIdx.x; p < br.y; p += blockDim.x) {
-        PointInfo pi;
-        point_at(pts, perm[br.x + p], pi);
-        const int stride[3] = {1, tx, plane};
-        int corner = 0;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            int cell, l0;
-            float off;
-            place(pi.c[d], g.nf[d], g.inv_nf[d], W, cell, l0, off);
-            corner += (l0 - S[d]) * stride[d];
-        }
-        atomicAdd(&hist[corner], 1);
-    }
+    for (int p = threadIdx.x; p < br.y; p += blockDim.x) atomicAdd(&hist[corners[br.x + p]], 1);
     __syncthreads();
     // weighted sums along x, y, z in place, one thread per line with the
     // last W inputs in registers
@@ -618,7 +622,8 @@ __global__ void __launch_bounds__(256) bin_value_bound_kernel(const float2 *__re
 template <int DIM, int W>
 __global__ void __launch_bounds__(kSpreadThreads, LC_SPREAD_MIN_BLOCKS)
     spread_kernel(PolarPts pts, GridCfg g, const float2 *__restrict__ c, long cstride, int nvol,
-                  const int *__restrict__ perm, const int4 *__restrict__ subs,
+                  const int *__restrict__ perm, const unsigned short *__restrict__ corners,
+                  const int4 *__restrict__ subs,
                   unsigned long long *__restrict__ fix, long gstride, int mode,
                   const float2 *__restrict__ shifts, const int *__restrict__ mbits, long kmax,
                   const int *__restrict__ kbin, const int *__restrict__ binm) {
@@ -658,20 +663,15 @@ __global__ void __launch_bounds__(kSpreadThreads, LC_SPREAD_MIN_BLOCKS)
         const int p = tid + q * (int)blockDim.x;
         key[q] = -1;
         if (p >= sp.z) continue;
-        const int j = perm[sp.y + p];
-        PointInfo pi;
-        point_at(pts, j, pi);
+        bool use = true;
+        if (mode != PT_PLAIN) {
+            PointInfo pi;
+            point_at(pts, perm[sp.y + p], pi);
+            use = in_band(pi);
+        }
         int k = -1;
-        if (mode == PT_PLAIN || in_band(pi)) {
-            const int stride[3] = {1, tx, plane};
-            int corner = 0;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                int cell, l0;
-                float off;
-                place(pi.c[d], g.nf[d], g.inv_nf[d], W, cell, l0, off);
-                corner += (l0 - S[d]) * stride[d];
-            }
+        if (use) {
+            const int corner = corners[sp.y + p];  // from the bin sort
             const int b = corner & 31;
             k = (b << 16) | atomicAdd(&cnt[b], 1);
             atomicAdd(&kcnt[corner], 1);
@@ -896,21 +896,22 @@ __global__ void __launch_bounds__(256) interp_kernel(PolarPts pts, GridCfg g,
 template <int DIM, int W>
 void launch_spread_w(const Context &ctx, dim3 grid, size_t smem, cudaStream_t st, const PolarPts &pts,
                      const GridCfg &g, const float2 *c, long cstride, int nvol, const int *perm,
-                     const int4 *subs, unsigned long long *out, long gstride, int mode,
-                     const float2 *shifts, const int *mbits, long kmax, const int *kbin, const int *binm) {
+                     const unsigned short *corners, const int4 *subs, unsigned long long *out, long gstride,
+                     int mode, const float2 *shifts, const int *mbits, long kmax, const int *kbin,
+                     const int *binm) {
     auto kern = spread_kernel<DIM, W>;
     allow_max_dynamic_smem(ctx, kern);
-    kern<<<grid, kSpreadThreads, smem, st>>>(pts, g, c, cstride, nvol, perm, subs, out, gstride,
+    kern<<<grid, kSpreadThreads, smem, st>>>(pts, g, c, cstride, nvol, perm, corners, subs, out, gstride,
                                              mode, shifts, mbits, kmax, kbin, binm);
     LC_CHECK_LAUNCH();
 }
 
 template <int DIM, int W>
-void launch_footprint_w(const Context &ctx, unsigned nbins, size_t smem, cudaStream_t st, const PolarPts &pts,
-                        const GridCfg &g, const OffsetWeights &om, const int *perm, const int2 *bins, int *kbin) {
+void launch_footprint_w(const Context &ctx, unsigned nbins, size_t smem, cudaStream_t st, const GridCfg &g,
+                        const OffsetWeights &om, const unsigned short *corners, const int2 *bins, int *kbin) {
     auto kern = bin_footprint_kernel<DIM, W>;
     allow_max_dynamic_smem(ctx, kern);
-    kern<<<nbins, 256, smem, st>>>(pts, g, om, perm, bins, kbin);
+    kern<<<nbins, 256, smem, st>>>(g, om, corners, bins, kbin);
     LC_CHECK_LAUNCH();
 }
 
@@ -1051,8 +1052,14 @@ void NufftPlan::sort_points(Context &ctx) {
     DevBuf<int> cursor;
     cursor.upload(off.data(), off.size(), st);
     perm_.alloc(pts_.M, st);
-    if (dim_ == 2) bin_scatter_kernel<2><<<(unsigned)blocks, threads, 0, st>>>(pts_, g, w_, cursor.get(), perm_.get());
-    else bin_scatter_kernel<3><<<(unsigned)blocks, threads, 0, st>>>(pts_, g, w_, cursor.get(), perm_.get());
+    corner_.alloc(pts_.M, st);
+    LC_REQUIRE((long)g.td[0] * g.td[1] * g.td[2] <= 65536, "NUFFT: bin tile too large for 16-bit corners");
+    if (dim_ == 2)
+        bin_scatter_kernel<2><<<(unsigned)blocks, threads, 0, st>>>(pts_, g, w_, cursor.get(), perm_.get(),
+                                                                    corner_.get());
+    else
+        bin_scatter_kernel<3><<<(unsigned)blocks, threads, 0, st>>>(pts_, g, w_, cursor.get(), perm_.get(),
+                                                                    corner_.get());
     LC_CHECK_LAUNCH();
     // K_b of every bin, over all of its points
     {
@@ -1078,10 +1085,10 @@ void NufftPlan::sort_points(Context &ctx) {
             om.w[m] = (float)(std::ceil(phi * 1.001 * 4096.0) / 4096.0);
         }
         if (dim_ == 2) {
-            LC_W_SWITCH(w_, (launch_footprint_w<2, WW>(ctx, (unsigned)nbins, hsm, st, pts_, g, om, perm_.get(),
+            LC_W_SWITCH(w_, (launch_footprint_w<2, WW>(ctx, (unsigned)nbins, hsm, st, g, om, corner_.get(),
                                                       dbr.get(), kbin_.get())));
         } else {
-            LC_W_SWITCH(w_, (launch_footprint_w<3, WW>(ctx, (unsigned)nbins, hsm, st, pts_, g, om, perm_.get(),
+            LC_W_SWITCH(w_, (launch_footprint_w<3, WW>(ctx, (unsigned)nbins, hsm, st, g, om, corner_.get(),
                                                       dbr.get(), kbin_.get())));
         }
         LC_CHECK_LAUNCH();
@@ -1129,11 +1136,11 @@ void NufftPlan::spread(Context &ctx, const float2 *c, int nvol, float2 *grid, Pt
         LC_CHECK_LAUNCH();
         if (dim_ == 2) {
             LC_W_SWITCH(w_, (launch_spread_w<2, WW>(ctx, gd, smem, st, pts_, g, cv, pts_.M, nv,
-                                                   perm_.get(), subs_.get(), fv, gvol, mode, shifts_,
+                                                   perm_.get(), corner_.get(), subs_.get(), fv, gvol, mode, shifts_,
                                                    mbits_.get(), kmax_, kbin_.get(), binm_.get())));
         } else {
             LC_W_SWITCH(w_, (launch_spread_w<3, WW>(ctx, gd, smem, st, pts_, g, cv, pts_.M, nv,
-                                                   perm_.get(), subs_.get(), fv, gvol, mode, shifts_,
+                                                   perm_.get(), corner_.get(), subs_.get(), fv, gvol, mode, shifts_,
                                                    mbits_.get(), kmax_, kbin_.get(), binm_.get())));
         }
     }

@@ -107,6 +107,7 @@ class NufftPlan {
     DevBuf<float> corr_[3];
     DevBuf<float> corr_xy_;  // corr_y (x) corr_x, 3D type 2
     DevBuf<int> perm_;
+    DevBuf<unsigned short> corner_;  // per sorted point: footprint corner in its bin's tile
     DevBuf<int4> subs_;
     int nsub_ = 0;
     int maxsub_ = 1024;  // most points of one spreading subproblem
