@@ -97,15 +97,25 @@ class ClockSampler:
         self.source = None
         self._stop = threading.Event()
         self._t = threading.Thread(target=self._run, daemon=True)
+        # NVML is initialised here, before the timed region: nvmlInit on a
+        # host with several GPUs takes long enough to disturb a timed step
+        self._nvml_state = None
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.index)
+            mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            get = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons",
+                          getattr(N, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
+            masks = [(name, getattr(N, attr, 0)) for name, attr in self.REASONS]
+            self._nvml_state = (N, h, mx, get, masks)
+        except Exception:
+            self._nvml_state = None
 
     def _nvml(self):
-        import pynvml as N
-        N.nvmlInit()
-        h = N.nvmlDeviceGetHandleByIndex(self.index)
-        mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
-        get = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons",
-                      getattr(N, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
-        masks = [(name, getattr(N, attr, 0)) for name, attr in self.REASONS]
+        if self._nvml_state is None:
+            raise RuntimeError("NVML unavailable")
+        N, h, mx, get, masks = self._nvml_state
         self.source = "nvml"
         while not self._stop.is_set():
             sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
@@ -725,7 +735,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--clock-interval", type=float, default=1.0,
+    ap.add_argument("--clock-interval", type=float, default=0.25,
                     help="seconds between clock samples during the timed region")
     ap.add_argument("--residual-refresh", type=int, default=16,
                     help="Split-Bregman: recompute A x of the warm-started residual every this many "
@@ -867,11 +877,13 @@ def main():
             total = float(t.item())
         return total, lats
 
+    # the clock sampler's NVML set-up runs before the warm-up steps
+    clk = ClockSampler(local, args.clock_interval)
     for _ in range(args.warmup):
         step_device()
     torch.cuda.synchronize()
 
-    with ClockSampler(local, args.clock_interval) as clk:
+    with clk:
         launches0 = lib.lc_kernel_launches()
         total_ms, lats = timed(step_device, args.steps)
         launches = lib.lc_kernel_launches() - launches0
