@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdlib>
 #include <tuple>
 
 #include "lc_regfft.cuh"
@@ -81,20 +82,17 @@ __device__ __forceinline__ int mirror_index(int j, int P) {
     return P - 1 - j;
 }
 
-// Rows of K (all kx of one (kz, ky)) in segments of S values of kx.  The sum over
-// angles uses the Dirichlet closed form, with sin(pi u) and sin(pi u / n)
-// advanced along kx by the three-term sine recurrence (FP64) and evaluated in
-// closed form whenever the denominator is small.
-// Only the half space kz <= 0 (2D: ky <= 0) is summed; K(-k) = K(k) fills the
-// rest.  With `mirror` the angle set is also closed under a reflection that
-// makes K even in one more axis, and a quarter of the grid is summed:
-//   3D  K(kx, ky, -kz) = K(k): rows with ky <= 0 of each plane kz <= 0, and
-//       K(-kx, -ky, kz), K(-k), K(kx, ky, -kz) from them (a per-angle pair
-//       whose a and b differ only in the sign of their kz coefficient);
-//   2D  K(-kx, ky) = K(k): kx <= 0 of each row ky <= 0 (pairs theta, pi - theta);
-//       mirror == 2: the set is also closed under a quarter turn, so
-//       K(ky, kx) = K(k) and only kx <= ky <= 0 is summed (an eighth).
-template <int DIM, int S, bool ONE_GROUP>
+// Rows of K (all kx of one (kz, ky)) in segments of S values of kx, 3D.  The
+// sum over angles uses the Dirichlet closed form, with sin(pi u) and
+// sin(pi u / n) advanced along kx by the three-term sine recurrence (FP64) and
+// evaluated in closed form whenever the denominator is small.
+// Only the half space kz <= 0 is summed; K(-k) = K(k) fills the rest.  With
+// `mirror` the angle set is also closed under the reflection that negates the
+// kz coefficients, K(kx, ky, -kz) = K(k), and a quarter of the grid is summed:
+// rows with ky <= 0 of each plane kz <= 0, and K(-kx, -ky, kz), K(-k),
+// K(kx, ky, -kz) from them (a per-angle pair whose a and b differ only in the
+// sign of their kz coefficient).
+template <int S, bool ONE_GROUP>
 __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const PsfAngle *__restrict__ angles, int ntheta,
                                                       const int *__restrict__ groups, int ngroups,
                                                       int nx, int ny, int P1, int P2, int P3, int mirror,
@@ -105,34 +103,24 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
     for (int i = threadIdx.x; i < ntheta; i += blockDim.x) ang[i] = angles[i];
     for (int i = threadIdx.x; i <= ngroups; i += blockDim.x) gst[i] = groups[i];
     __syncthreads();
-    // x range summed: all of it, or (2D mirror) jx <= P3/2; with the
-    // quarter-turn closure (2D, mirror == 2) only jx <= jy of each row
-    const int xend = (DIM == 2 && mirror) ? P3 / 2 + 1 : P3;
-    const int nseg = (xend + S - 1) / S;
-    // rows of the half space: 3D (jz <= P1/2, all jy, or jy <= P2/2 with the
-    // mirror); 2D (jy <= P2/2)
-    const int rows_per_plane = (DIM == 3 && mirror) ? P2 / 2 + 1 : P2;
-    // (3D: only the planes zlo .. P1/2 of the half, the rest is not needed)
-    const long nrows_half = DIM == 3 ? (long)(P1 / 2 + 1 - zlo) * rows_per_plane : (long)(P2 / 2 + 1);
+    const int nseg = (P3 + S - 1) / S;
+    // rows of the half space: jz <= P1/2, all jy (jy <= P2/2 with the mirror);
+    // only the planes zlo .. P1/2 of the half, the rest is not needed
+    const int rows_per_plane = mirror ? P2 / 2 + 1 : P2;
+    const long nrows_half = (long)(P1 / 2 + 1 - zlo) * rows_per_plane;
     const long items = nrows_half * nseg;
     const double inv_nx = 1.0 / (double)nx, inv_ny = 1.0 / (double)ny;
     for (long it = (long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
          it += (long)gridDim.x * blockDim.x) {
         const long row = it / nseg;
         const int seg = (int)(it - row * nseg);
-        int jz = 0, jy;
-        if (DIM == 3) {
-            const int pz = (int)(row / rows_per_plane);
-            jy = (int)(row - (long)pz * rows_per_plane);
-            jz = zlo + pz;
-        } else {
-            jy = (int)row;
-        }
+        const int pz = (int)(row / rows_per_plane);
+        const int jy = (int)(row - (long)pz * rows_per_plane);
+        const int jz = zlo + pz;
         const int jx0 = seg * S;
-        if (DIM == 2 && mirror == 2 && jx0 > jy) continue;  // transposed copy of a summed value
         const double kx0 = (double)(jx0 - P3 / 2);
         const double ky = (double)(jy - P2 / 2);
-        const double kz = DIM == 3 ? (double)(jz - P1 / 2) : 0.0;
+        const double kz = (double)(jz - P1 / 2);
         // one group (every angle of equal beta and gamma): acc is formed from ay
         // after the angle sum, so the two arrays are never live together
         double acc[S];
@@ -140,145 +128,48 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
 #pragma unroll
             for (int s = 0; s < S; ++s) acc[s] = 0.0;
         }
-        if constexpr (DIM == 3) {
-            // uX = a . k does not depend on theta (a is the first column of
-            // transpose(Rx(theta) Ry(beta) Rz(gamma)), which Rx leaves alone), so
-            // within a group of angles of equal (beta, gamma) the sum factors:
-            // K = sum_groups D_nx(uX) * sum_{theta in group} D_ny(uY).  Four
-            // (then two, then one) angles share one division.
-            for (int gi = 0; gi < (ONE_GROUP ? 1 : ngroups); ++gi) {
-                const int i0 = gst[gi], i1 = gst[gi + 1];
-                double ay[S];
+        // uX = a . k does not depend on theta (a is the first column of
+        // transpose(Rx(theta) Ry(beta) Rz(gamma)), which Rx leaves alone), so
+        // within a group of angles of equal (beta, gamma) the sum factors:
+        // K = sum_groups D_nx(uX) * sum_{theta in group} D_ny(uY).  Four
+        // (then two, then one) angles share one division.
+        for (int gi = 0; gi < (ONE_GROUP ? 1 : ngroups); ++gi) {
+            const int i0 = gst[gi], i1 = gst[gi + 1];
+            double ay[S];
 #pragma unroll
-                for (int s = 0; s < S; ++s) ay[s] = 0.0;
-                int i = i0;
-                // four angles per division:
-                // a/b + c/d + e/f + g/h = ((a d + c b) f h + (e h + g f) b d) / (b d f h)
-                for (; i + 3 < i1; i += 4) {
-                    const PsfAngle &A = ang[i], &B = ang[i + 1], &C = ang[i + 2], &D = ang[i + 3];
-                    const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
-                    const double uB = B.b[0] * kx0 + B.b[1] * ky + B.b[2] * kz;
-                    const double uC = C.b[0] * kx0 + C.b[1] * ky + C.b[2] * kz;
-                    const double uD = D.b[0] * kx0 + D.b[1] * ky + D.b[2] * kz;
-                    SinSeq<true> nA, nB, nC, nD;
-                    SinSeq<false> dA, dB, dC, dD;
-                    nA.init(uA, A.stepC, A.b[0]);
-                    dA.init(uA * inv_ny, A.stepD, A.b[0] * inv_ny);
-                    nB.init(uB, B.stepC, B.b[0]);
-                    dB.init(uB * inv_ny, B.stepD, B.b[0] * inv_ny);
-                    nC.init(uC, C.stepC, C.b[0]);
-                    dC.init(uC * inv_ny, C.stepD, C.b[0] * inv_ny);
-                    nD.init(uD, D.stepC, D.b[0]);
-                    dD.init(uD * inv_ny, D.stepD, D.b[0] * inv_ny);
-#pragma unroll
-                    for (int s = 0; s < S; ++s) {
-                        if (fabs(dA.cur) > kDenMin && fabs(dB.cur) > kDenMin && fabs(dC.cur) > kDenMin &&
-                            fabs(dD.cur) > kDenMin) {
-                            const double pab = fma(nA.val(s), dB.cur, nB.val(s) * dA.cur), qab = dA.cur * dB.cur;
-                            const double pcd = fma(nC.val(s), dD.cur, nD.val(s) * dC.cur), qcd = dC.cur * dD.cur;
-                            ay[s] += fma(pab, qcd, pcd * qab) / (qab * qcd);
-                        } else {
-                            const double sd = (double)s;
-                            ay[s] += dirichlet_term(nA.val(s), dA.cur, uA + sd * A.b[0], ny) +
-                                     dirichlet_term(nB.val(s), dB.cur, uB + sd * B.b[0], ny) +
-                                     dirichlet_term(nC.val(s), dC.cur, uC + sd * C.b[0], ny) +
-                                     dirichlet_term(nD.val(s), dD.cur, uD + sd * D.b[0], ny);
-                        }
-                        nA.advance();
-                        dA.advance();
-                        nB.advance();
-                        dB.advance();
-                        nC.advance();
-                        dC.advance();
-                        nD.advance();
-                        dD.advance();
-                    }
-                }
-                for (; i + 1 < i1; i += 2) {
-                    const PsfAngle &A = ang[i], &B = ang[i + 1];
-                    const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
-                    const double uB = B.b[0] * kx0 + B.b[1] * ky + B.b[2] * kz;
-                    SinSeq<true> nA, nB;
-                    SinSeq<false> dA, dB;
-                    nA.init(uA, A.stepC, A.b[0]);
-                    dA.init(uA * inv_ny, A.stepD, A.b[0] * inv_ny);
-                    nB.init(uB, B.stepC, B.b[0]);
-                    dB.init(uB * inv_ny, B.stepD, B.b[0] * inv_ny);
-#pragma unroll
-                    for (int s = 0; s < S; ++s) {
-                        if (fabs(dA.cur) > kDenMin && fabs(dB.cur) > kDenMin) {
-                            ay[s] += fma(nA.val(s), dB.cur, nB.val(s) * dA.cur) / (dA.cur * dB.cur);
-                        } else {
-                            ay[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.b[0], ny) +
-                                     dirichlet_term(nB.val(s), dB.cur, uB + (double)s * B.b[0], ny);
-                        }
-                        nA.advance();
-                        dA.advance();
-                        nB.advance();
-                        dB.advance();
-                    }
-                }
-                if (i < i1) {
-                    const PsfAngle &A = ang[i];
-                    const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
-                    SinSeq<true> nA;
-                    SinSeq<false> dA;
-                    nA.init(uA, A.stepC, A.b[0]);
-                    dA.init(uA * inv_ny, A.stepD, A.b[0] * inv_ny);
-#pragma unroll
-                    for (int s = 0; s < S; ++s) {
-                        ay[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.b[0], ny);
-                        nA.advance();
-                        dA.advance();
-                    }
-                }
-                const PsfAngle &A = ang[i0];
-                const double uX0 = A.a[0] * kx0 + A.a[1] * ky + A.a[2] * kz;
-                SinSeq<true> nX;
-                SinSeq<false> dX;
-                nX.init(uX0, A.stepA, A.a[0]);
-                dX.init(uX0 * inv_nx, A.stepB, A.a[0] * inv_nx);
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    const double tX = dirichlet_term(nX.val(s), dX.cur, uX0 + (double)s * A.a[0], nx);
-                    acc[s] = ONE_GROUP ? tX * ay[s] : fma(tX, ay[s], acc[s]);
-                    nX.advance();
-                    dX.advance();
-                }
-            }
-        } else {
-            // 2D: K = sum_theta D_nx(uX), four (then two, then one) angles per
-            // division
-            int i = 0;
-            for (; i + 3 < ntheta; i += 4) {
+            for (int s = 0; s < S; ++s) ay[s] = 0.0;
+            int i = i0;
+            // four angles per division:
+            // a/b + c/d + e/f + g/h = ((a d + c b) f h + (e h + g f) b d) / (b d f h)
+            for (; i + 3 < i1; i += 4) {
                 const PsfAngle &A = ang[i], &B = ang[i + 1], &C = ang[i + 2], &D = ang[i + 3];
-                const double uA = A.a[0] * kx0 + A.a[1] * ky;
-                const double uB = B.a[0] * kx0 + B.a[1] * ky;
-                const double uC = C.a[0] * kx0 + C.a[1] * ky;
-                const double uD = D.a[0] * kx0 + D.a[1] * ky;
+                const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
+                const double uB = B.b[0] * kx0 + B.b[1] * ky + B.b[2] * kz;
+                const double uC = C.b[0] * kx0 + C.b[1] * ky + C.b[2] * kz;
+                const double uD = D.b[0] * kx0 + D.b[1] * ky + D.b[2] * kz;
                 SinSeq<true> nA, nB, nC, nD;
                 SinSeq<false> dA, dB, dC, dD;
-                nA.init(uA, A.stepA, A.a[0]);
-                dA.init(uA * inv_nx, A.stepB, A.a[0] * inv_nx);
-                nB.init(uB, B.stepA, B.a[0]);
-                dB.init(uB * inv_nx, B.stepB, B.a[0] * inv_nx);
-                nC.init(uC, C.stepA, C.a[0]);
-                dC.init(uC * inv_nx, C.stepB, C.a[0] * inv_nx);
-                nD.init(uD, D.stepA, D.a[0]);
-                dD.init(uD * inv_nx, D.stepB, D.a[0] * inv_nx);
+                nA.init(uA, A.stepC, A.b[0]);
+                dA.init(uA * inv_ny, A.stepD, A.b[0] * inv_ny);
+                nB.init(uB, B.stepC, B.b[0]);
+                dB.init(uB * inv_ny, B.stepD, B.b[0] * inv_ny);
+                nC.init(uC, C.stepC, C.b[0]);
+                dC.init(uC * inv_ny, C.stepD, C.b[0] * inv_ny);
+                nD.init(uD, D.stepC, D.b[0]);
+                dD.init(uD * inv_ny, D.stepD, D.b[0] * inv_ny);
 #pragma unroll
                 for (int s = 0; s < S; ++s) {
                     if (fabs(dA.cur) > kDenMin && fabs(dB.cur) > kDenMin && fabs(dC.cur) > kDenMin &&
                         fabs(dD.cur) > kDenMin) {
                         const double pab = fma(nA.val(s), dB.cur, nB.val(s) * dA.cur), qab = dA.cur * dB.cur;
                         const double pcd = fma(nC.val(s), dD.cur, nD.val(s) * dC.cur), qcd = dC.cur * dD.cur;
-                        acc[s] += fma(pab, qcd, pcd * qab) / (qab * qcd);
+                        ay[s] += fma(pab, qcd, pcd * qab) / (qab * qcd);
                     } else {
                         const double sd = (double)s;
-                        acc[s] += dirichlet_term(nA.val(s), dA.cur, uA + sd * A.a[0], nx) +
-                                  dirichlet_term(nB.val(s), dB.cur, uB + sd * B.a[0], nx) +
-                                  dirichlet_term(nC.val(s), dC.cur, uC + sd * C.a[0], nx) +
-                                  dirichlet_term(nD.val(s), dD.cur, uD + sd * D.a[0], nx);
+                        ay[s] += dirichlet_term(nA.val(s), dA.cur, uA + sd * A.b[0], ny) +
+                                 dirichlet_term(nB.val(s), dB.cur, uB + sd * B.b[0], ny) +
+                                 dirichlet_term(nC.val(s), dC.cur, uC + sd * C.b[0], ny) +
+                                 dirichlet_term(nD.val(s), dD.cur, uD + sd * D.b[0], ny);
                     }
                     nA.advance();
                     dA.advance();
@@ -290,23 +181,23 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
                     dD.advance();
                 }
             }
-            for (; i + 1 < ntheta; i += 2) {
+            for (; i + 1 < i1; i += 2) {
                 const PsfAngle &A = ang[i], &B = ang[i + 1];
-                const double uA = A.a[0] * kx0 + A.a[1] * ky;
-                const double uB = B.a[0] * kx0 + B.a[1] * ky;
+                const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
+                const double uB = B.b[0] * kx0 + B.b[1] * ky + B.b[2] * kz;
                 SinSeq<true> nA, nB;
-                    SinSeq<false> dA, dB;
-                nA.init(uA, A.stepA, A.a[0]);
-                dA.init(uA * inv_nx, A.stepB, A.a[0] * inv_nx);
-                nB.init(uB, B.stepA, B.a[0]);
-                dB.init(uB * inv_nx, B.stepB, B.a[0] * inv_nx);
+                SinSeq<false> dA, dB;
+                nA.init(uA, A.stepC, A.b[0]);
+                dA.init(uA * inv_ny, A.stepD, A.b[0] * inv_ny);
+                nB.init(uB, B.stepC, B.b[0]);
+                dB.init(uB * inv_ny, B.stepD, B.b[0] * inv_ny);
 #pragma unroll
                 for (int s = 0; s < S; ++s) {
                     if (fabs(dA.cur) > kDenMin && fabs(dB.cur) > kDenMin) {
-                        acc[s] += fma(nA.val(s), dB.cur, nB.val(s) * dA.cur) / (dA.cur * dB.cur);
+                        ay[s] += fma(nA.val(s), dB.cur, nB.val(s) * dA.cur) / (dA.cur * dB.cur);
                     } else {
-                        acc[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.a[0], nx) +
-                                  dirichlet_term(nB.val(s), dB.cur, uB + (double)s * B.a[0], nx);
+                        ay[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.b[0], ny) +
+                                 dirichlet_term(nB.val(s), dB.cur, uB + (double)s * B.b[0], ny);
                     }
                     nA.advance();
                     dA.advance();
@@ -314,27 +205,40 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
                     dB.advance();
                 }
             }
-            if (i < ntheta) {
+            if (i < i1) {
                 const PsfAngle &A = ang[i];
-                const double uA = A.a[0] * kx0 + A.a[1] * ky;
+                const double uA = A.b[0] * kx0 + A.b[1] * ky + A.b[2] * kz;
                 SinSeq<true> nA;
-                    SinSeq<false> dA;
-                nA.init(uA, A.stepA, A.a[0]);
-                dA.init(uA * inv_nx, A.stepB, A.a[0] * inv_nx);
+                SinSeq<false> dA;
+                nA.init(uA, A.stepC, A.b[0]);
+                dA.init(uA * inv_ny, A.stepD, A.b[0] * inv_ny);
 #pragma unroll
                 for (int s = 0; s < S; ++s) {
-                    acc[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.a[0], nx);
+                    ay[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.b[0], ny);
                     nA.advance();
                     dA.advance();
                 }
             }
+            const PsfAngle &A = ang[i0];
+            const double uX0 = A.a[0] * kx0 + A.a[1] * ky + A.a[2] * kz;
+            SinSeq<true> nX;
+            SinSeq<false> dX;
+            nX.init(uX0, A.stepA, A.a[0]);
+            dX.init(uX0 * inv_nx, A.stepB, A.a[0] * inv_nx);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const double tX = dirichlet_term(nX.val(s), dX.cur, uX0 + (double)s * A.a[0], nx);
+                acc[s] = ONE_GROUP ? tX * ay[s] : fma(tX, ay[s], acc[s]);
+                nX.advance();
+                dX.advance();
+            }
         }
         const long plane = (long)P2 * P3;
-        const int mz = DIM == 3 ? mirror_index(jz, P1) : 0;
+        const int mz = mirror_index(jz, P1);
         const int my = mirror_index(jy, P2);
         auto put = [&](int z, int y, int x, double v) { K[(long)z * plane + (long)y * P3 + x] = v; };
         if (!mirror) {
-            const bool self_plane = DIM == 3 ? (mz == jz) : (my == jy);
+            const bool self_plane = mz == jz;
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const int jx = jx0 + s;
@@ -342,10 +246,10 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
                 put(jz, jy, jx, acc[s]);
                 if (self_plane) continue;  // its mirror is summed by another row of the half space
                 const int mx = mirror_index(jx, P3);
-                if ((DIM == 3 && mz < 0) || my < 0 || mx < 0) continue;
+                if (mz < 0 || my < 0 || mx < 0) continue;
                 put(mz, my, mx, acc[s]);
             }
-        } else if constexpr (DIM == 3) {
+        } else {
             // (jz, jy, jx) summed; (jz, my, mx), (mz, my, mx), (mz, jy, jx) copied.
             // A copy that lands on a summed row or plane is left to the sum.
 #pragma unroll
@@ -358,25 +262,333 @@ __global__ void __launch_bounds__(128, ONE_GROUP ? 3 : 1) psf_rows_kernel(const 
                 if (mz != jz && mz >= 0) put(mz, jy, jx, acc[s]);
                 if (mz != jz && my != jy && mz >= 0 && my >= 0 && mx >= 0) put(mz, my, mx, acc[s]);
             }
+        }
+    }
+}
+
+// ---- 2D kernel: K(kx, ky) = sum_theta D_nx(cos(theta) kx + sin(theta) ky) ----
+// Rows ky <= 0 in segments of S values of kx (with the mirror, kx <= 0 only;
+// with the quarter-turn closure, mirror == 2, only kx <= ky; the other
+// entries are copies).  G lanes of one warp share a segment: each sums a
+// contiguous share of the angle quads (the last lane also the 1 to 3 angles
+// left over), and a butterfly of shuffles adds the shares, so that every lane
+// of the group holds the same total.  The summation order depends on G, and
+// G on the grid size and the angle count alone, so a kernel does not depend
+// on what else runs beside it.  Small grids (a few hundred segments) split
+// the angle sum over up to 32 lanes and still fill the GPU.
+template <int S>
+__device__ __forceinline__ void psf2d_sum_quads(const PsfAngle *ang, int i0, int i1, double kx0, double ky, int nx,
+                                                double inv_nx, double (&acc)[S]) {
+    for (int i = i0; i < i1; i += 4) {
+        const PsfAngle &A = ang[i], &B = ang[i + 1], &C = ang[i + 2], &D = ang[i + 3];
+        const double uA = A.a[0] * kx0 + A.a[1] * ky;
+        const double uB = B.a[0] * kx0 + B.a[1] * ky;
+        const double uC = C.a[0] * kx0 + C.a[1] * ky;
+        const double uD = D.a[0] * kx0 + D.a[1] * ky;
+        SinSeq<true> nA, nB, nC, nD;
+        SinSeq<false> dA, dB, dC, dD;
+        nA.init(uA, A.stepA, A.a[0]);
+        dA.init(uA * inv_nx, A.stepB, A.a[0] * inv_nx);
+        nB.init(uB, B.stepA, B.a[0]);
+        dB.init(uB * inv_nx, B.stepB, B.a[0] * inv_nx);
+        nC.init(uC, C.stepA, C.a[0]);
+        dC.init(uC * inv_nx, C.stepB, C.a[0] * inv_nx);
+        nD.init(uD, D.stepA, D.a[0]);
+        dD.init(uD * inv_nx, D.stepB, D.a[0] * inv_nx);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            if (fabs(dA.cur) > kDenMin && fabs(dB.cur) > kDenMin && fabs(dC.cur) > kDenMin &&
+                fabs(dD.cur) > kDenMin) {
+                const double pab = fma(nA.val(s), dB.cur, nB.val(s) * dA.cur), qab = dA.cur * dB.cur;
+                const double pcd = fma(nC.val(s), dD.cur, nD.val(s) * dC.cur), qcd = dC.cur * dD.cur;
+                acc[s] += fma(pab, qcd, pcd * qab) / (qab * qcd);
+            } else {
+                const double sd = (double)s;
+                acc[s] += dirichlet_term(nA.val(s), dA.cur, uA + sd * A.a[0], nx) +
+                          dirichlet_term(nB.val(s), dB.cur, uB + sd * B.a[0], nx) +
+                          dirichlet_term(nC.val(s), dC.cur, uC + sd * C.a[0], nx) +
+                          dirichlet_term(nD.val(s), dD.cur, uD + sd * D.a[0], nx);
+            }
+            nA.advance();
+            dA.advance();
+            nB.advance();
+            dB.advance();
+            nC.advance();
+            dC.advance();
+            nD.advance();
+            dD.advance();
+        }
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void psf2d_sum_tail(const PsfAngle *ang, int i, int ntheta, double kx0, double ky, int nx,
+                                               double inv_nx, double (&acc)[S]) {
+    for (; i < ntheta; ++i) {
+        const PsfAngle &A = ang[i];
+        const double uA = A.a[0] * kx0 + A.a[1] * ky;
+        SinSeq<true> nA;
+        SinSeq<false> dA;
+        nA.init(uA, A.stepA, A.a[0]);
+        dA.init(uA * inv_nx, A.stepB, A.a[0] * inv_nx);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            acc[s] += dirichlet_term(nA.val(s), dA.cur, uA + (double)s * A.a[0], nx);
+            nA.advance();
+            dA.advance();
+        }
+    }
+}
+
+// Segments of 16 summed in rows 0 .. J-1: with mirror == 2 row jy holds
+// jy / 16 + 1 of them (kx <= ky), otherwise nseg.
+__host__ __device__ __forceinline__ long psf2d_first_seg(long J, long nseg, int mirror) {
+    if (mirror != 2) return J * nseg;
+    const long A = J / 16, R = J % 16;
+    return J + 16 * A * (A - 1) / 2 + R * A;
+}
+
+template <int S, int G>
+__global__ void __launch_bounds__(128) psf2d_kernel(const PsfAngle *__restrict__ angles, int ntheta, int nx, int P2,
+                                                    int P3, int mirror, double *__restrict__ K) {
+    static_assert(S == 16, "psf2d_first_seg counts segments of 16");
+    static_assert(G >= 1 && G <= 32 && (G & (G - 1)) == 0, "G lanes per segment: a power of two up to 32");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PsfAngle *ang = reinterpret_cast<PsfAngle *>(smem_raw);
+    for (int i = threadIdx.x; i < ntheta; i += blockDim.x) ang[i] = angles[i];
+    __syncthreads();
+    const int xend = mirror ? P3 / 2 + 1 : P3;
+    const int nseg = (xend + S - 1) / S;
+    const int nrows = P2 / 2 + 1;
+    const long items = psf2d_first_seg(nrows, nseg, mirror);
+    const double inv_nx = 1.0 / (double)nx;
+    constexpr int IPW = 32 / G;  // segments per warp
+    const int lane = threadIdx.x & 31, sub = lane % G;
+    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    // this lane's angle quads; the angles after the last quad go to lane G - 1
+    const int nq = ntheta / 4;
+    const int i0 = 4 * (int)((long)sub * nq / G), i1 = 4 * (int)((long)(sub + 1) * nq / G);
+    // the loop is warp-uniform: every lane reaches the shuffles
+    for (long base = warp * IPW; base < items; base += nwarps * IPW) {
+        const long it = base + lane / G;
+        const bool active = it < items;
+        // row of segment it: the last row whose first segment is <= it
+        int jy = 0, seg = 0;
+        if (active) {
+            int lo = 0, hi = nrows - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (psf2d_first_seg(mid, nseg, mirror) <= it) lo = mid;
+                else hi = mid - 1;
+            }
+            jy = lo;
+            seg = (int)(it - psf2d_first_seg(jy, nseg, mirror));
+        }
+        const int jx0 = seg * S;
+        const double kx0 = (double)(jx0 - P3 / 2);
+        const double ky = (double)(jy - P2 / 2);
+        double acc[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) acc[s] = 0.0;
+        if (active) {
+            psf2d_sum_quads<S>(ang, i0, i1, kx0, ky, nx, inv_nx, acc);
+            if (sub == G - 1) psf2d_sum_tail<S>(ang, 4 * nq, ntheta, kx0, ky, nx, inv_nx, acc);
+        }
+#pragma unroll
+        for (int off = G / 2; off >= 1; off >>= 1) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) acc[s] += __shfl_xor_sync(0xffffffffu, acc[s], off);
+        }
+        if (!active) continue;
+        const int my = mirror_index(jy, P2);
+        auto put = [&](int y, int x, double v) { K[(long)y * P3 + x] = v; };
+        if (!mirror) {
+            const bool self_row = my == jy;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const int jx = jx0 + s;
+                if (s % G != sub) continue;
+                if (jx >= P3) break;
+                put(jy, jx, acc[s]);
+                if (self_row) continue;  // its mirror is summed in this row
+                const int mx = mirror_index(jx, P3);
+                if (my < 0 || mx < 0) continue;
+                put(my, mx, acc[s]);
+            }
         } else {
             // (jy, jx <= P3/2) summed; (jy, mx), (my, mx), (my, jx) copied, and
             // with mirror == 2 (jx <= jy summed) the same four transposed
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const int jx = jx0 + s;
+                if (s % G != sub) continue;
                 if (jx >= xend || (mirror == 2 && jx > jy)) break;
                 const int mx = mirror_index(jx, P3);
                 const double v = acc[s];
                 auto four = [&](int r, int c, int mr, int mc) {
-                    put(0, r, c, v);
-                    if (mc != c && mc >= 0) put(0, r, mc, v);
+                    put(r, c, v);
+                    if (mc != c && mc >= 0) put(r, mc, v);
                     if (mr != r && mr >= 0) {
-                        put(0, mr, c, v);
-                        if (mc >= 0) put(0, mr, mc, v);
+                        put(mr, c, v);
+                        if (mc >= 0) put(mr, mc, v);
                     }
                 };
                 four(jy, jx, my, mx);
                 if (mirror == 2 && jx != jy) four(jx, jy, mx, my);
+            }
+        }
+    }
+}
+
+// ---- tabulated 3D kernel for one tilt and beta = 0 (laminography) ----
+// With beta = 0 and one gamma for every angle, a = (cg, -sg, 0) and
+// b_theta = (ct sg, ct cg, -st), so
+//     K(k) = D_nx(w) * S(u, kz),  w = cg kx - sg ky,  u = sg kx + cg ky,
+//     S(u, kz) = sum_theta D_ny(ct u - st kz).
+// Each Dirichlet term is a sum of exponentials of u with frequencies below pi,
+// so S(., kz) is band-limited: it is summed exactly (FP64, the recurrences of
+// psf_rows_kernel) on a grid of u of spacing 1/32 for every needed kz <= 0
+// and interpolated with ten equispaced points (Lagrange, barycentric form).
+// The interpolation error is below (pi h)^10 |omega| / 10! of the kernel's
+// peak, about 1e-14 at h = 1/32.  With the kz mirror S(u, -kz) = S(u, kz).
+struct TabAngle {
+    double ct, st;
+    double2 stepN, stepD;  // (4 sin^2(t/2), sin t) of the u steps ct h and ct h / ny
+};
+
+constexpr int kTabSeg = 16;     // table samples per thread (one recurrence run)
+constexpr int kTabPoints = 10;  // interpolation stencil
+
+// table[r * nu + j] = S(u0 + j h, -r), r < nr, j < nu
+__global__ void __launch_bounds__(128) psf_table_kernel(const TabAngle *__restrict__ angles, int ntheta, int ny,
+                                                        double u0, double h, int nu, int nr,
+                                                        double *__restrict__ table) {
+    extern __shared__ __align__(16) unsigned char tab_smem[];
+    TabAngle *ang = reinterpret_cast<TabAngle *>(tab_smem);
+    for (int i = threadIdx.x; i < ntheta; i += blockDim.x) ang[i] = angles[i];
+    __syncthreads();
+    constexpr int S = kTabSeg;
+    const int nseg = (nu + S - 1) / S;
+    const double inv_ny = 1.0 / (double)ny;
+    for (long it = (long)blockIdx.x * blockDim.x + threadIdx.x; it < (long)nr * nseg;
+         it += (long)gridDim.x * blockDim.x) {
+        const int r = (int)(it / nseg), seg = (int)(it - (long)r * nseg);
+        const int j0 = seg * S;
+        const double kz = -(double)r;
+        const double ub = u0 + (double)j0 * h;
+        double acc[S];
+#pragma unroll
+        for (int q = 0; q < S; ++q) acc[q] = 0.0;
+        int i = 0;
+        for (; i + 3 < ntheta; i += 4) {
+            const TabAngle &A = ang[i], &B = ang[i + 1], &C = ang[i + 2], &D = ang[i + 3];
+            const double vA = A.ct * ub - A.st * kz, vB = B.ct * ub - B.st * kz;
+            const double vC = C.ct * ub - C.st * kz, vD = D.ct * ub - D.st * kz;
+            SinSeq<false> nA, nB, nC, nD, dA, dB, dC, dD;
+            nA.init(vA, A.stepN, A.ct * h);
+            dA.init(vA * inv_ny, A.stepD, A.ct * h * inv_ny);
+            nB.init(vB, B.stepN, B.ct * h);
+            dB.init(vB * inv_ny, B.stepD, B.ct * h * inv_ny);
+            nC.init(vC, C.stepN, C.ct * h);
+            dC.init(vC * inv_ny, C.stepD, C.ct * h * inv_ny);
+            nD.init(vD, D.stepN, D.ct * h);
+            dD.init(vD * inv_ny, D.stepD, D.ct * h * inv_ny);
+#pragma unroll
+            for (int q = 0; q < S; ++q) {
+                if (fabs(dA.cur) > kDenMin && fabs(dB.cur) > kDenMin && fabs(dC.cur) > kDenMin &&
+                    fabs(dD.cur) > kDenMin) {
+                    const double pab = fma(nA.cur, dB.cur, nB.cur * dA.cur), qab = dA.cur * dB.cur;
+                    const double pcd = fma(nC.cur, dD.cur, nD.cur * dC.cur), qcd = dC.cur * dD.cur;
+                    acc[q] += fma(pab, qcd, pcd * qab) / (qab * qcd);
+                } else {
+                    const double qd = (double)q * h;
+                    acc[q] += dirichlet_term(nA.cur, dA.cur, vA + qd * A.ct, ny) +
+                              dirichlet_term(nB.cur, dB.cur, vB + qd * B.ct, ny) +
+                              dirichlet_term(nC.cur, dC.cur, vC + qd * C.ct, ny) +
+                              dirichlet_term(nD.cur, dD.cur, vD + qd * D.ct, ny);
+                }
+                nA.advance();
+                dA.advance();
+                nB.advance();
+                dB.advance();
+                nC.advance();
+                dC.advance();
+                nD.advance();
+                dD.advance();
+            }
+        }
+        for (; i < ntheta; ++i) {
+            const TabAngle &A = ang[i];
+            const double vA = A.ct * ub - A.st * kz;
+            SinSeq<false> nA, dA;
+            nA.init(vA, A.stepN, A.ct * h);
+            dA.init(vA * inv_ny, A.stepD, A.ct * h * inv_ny);
+#pragma unroll
+            for (int q = 0; q < S; ++q) {
+                acc[q] += dirichlet_term(nA.cur, dA.cur, vA + (double)q * h * A.ct, ny);
+                nA.advance();
+                dA.advance();
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < S; ++q)
+            if (j0 + q < nu) table[(long)r * nu + j0 + q] = acc[q];
+    }
+}
+
+// K from the table on the planes zs .. zs + nzc - 1, rows ky <= 0, and by the
+// symmetries of the scan on the rest: K(-kx, -ky, kz) = K(k) always (u and w
+// change sign, and S(-u, kz) = S(u, -kz) = S(u, kz)), and with zmirror the
+// planes P1 - jz as well (K(kx, ky, -kz) = K(k)).  A copy that lands on a
+// computed entry is left to it, so every entry has one writer.
+//   K = D_nx(cg kx - sg ky) * S(sg kx + cg ky, -|kz|)
+// The ten Lagrange weights are formed as c_q prod_{m != q} (t - m) from prefix
+// and suffix products: no division, and exact at the nodes.
+__global__ void __launch_bounds__(256) psf_interp_kernel(const double *__restrict__ table, double u0, double inv_h,
+                                                         int nu, int nr, double sg, double cg, int nx, int P1, int P2,
+                                                         int P3, int zs, int nzc, int zmirror, double *__restrict__ K) {
+    // 1 / prod_{m != q} (q - m) = (-1)^(9-q) / (q! (9-q)!)
+    constexpr double c[kTabPoints] = {-1.0 / 362880.0, 1.0 / 40320.0, -1.0 / 10080.0, 1.0 / 4320.0,
+                                      -1.0 / 2880.0,   1.0 / 2880.0, -1.0 / 4320.0,  1.0 / 10080.0,
+                                      -1.0 / 40320.0,  1.0 / 362880.0};
+    const int rows = P2 / 2 + 1;
+    const long plane = (long)P2 * P3, half = (long)rows * P3, total = (long)nzc * half;
+    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long)gridDim.x * blockDim.x) {
+        const int pz = (int)(idx / half);
+        const long rem = idx - (long)pz * half;
+        const int jy = (int)(rem / P3), jx = (int)(rem - (long)jy * P3);
+        const int jz = zs + pz;
+        const double kx = (double)(jx - P3 / 2), ky = (double)(jy - P2 / 2);
+        const int r = abs(jz - P1 / 2);
+        const double u = sg * kx + cg * ky, w = cg * kx - sg * ky;
+        const double t = (u - u0) * inv_h;
+        const int j = (int)floor(t) - 4;
+        const double tt = t - (double)j;  // in [4, 5)
+        const double *row = table + (long)min(r, nr - 1) * nu + j;
+        double d[kTabPoints], pre[kTabPoints];
+#pragma unroll
+        for (int q = 0; q < kTabPoints; ++q) d[q] = tt - (double)q;
+        pre[0] = 1.0;
+#pragma unroll
+        for (int q = 1; q < kTabPoints; ++q) pre[q] = pre[q - 1] * d[q - 1];
+        double suf = 1.0, sv = 0.0;
+#pragma unroll
+        for (int q = kTabPoints - 1; q >= 0; --q) {
+            sv = fma(c[q] * pre[q] * suf, row[q], sv);
+            suf *= d[q];
+        }
+        const double v = dirichlet(w, nx) * sv;
+        const int my = mirror_index(jy, P2), mx = mirror_index(jx, P3);
+        const bool ycopy = my != jy && my >= 0 && mx >= 0;
+        K[(long)jz * plane + rem] = v;
+        if (ycopy) K[(long)jz * plane + (long)my * P3 + mx] = v;
+        if (zmirror) {
+            const int mz = mirror_index(jz, P1);
+            if (mz != jz && mz >= 0) {
+                K[(long)mz * plane + rem] = v;
+                if (ycopy) K[(long)mz * plane + (long)my * P3 + mx] = v;
             }
         }
     }
@@ -396,12 +608,12 @@ __global__ void widen_kernel(const float *__restrict__ a, double *__restrict__ b
         b[i] = (double)a[i];
 }
 
-__global__ void zero_unpaired_kernel(double *__restrict__ K, int P1, int P2, int P3) {
-    long total = (long)P1 * P2 * P3;
-    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+__global__ void zero_unpaired_kernel(double *__restrict__ K, int P1, int P2, int P3, int z0, int nz) {
+    const long plane = (long)P2 * P3, end = (long)(z0 + nz) * plane;
+    for (long idx = (long)z0 * plane + (long)blockIdx.x * blockDim.x + threadIdx.x; idx < end;
          idx += (long)gridDim.x * blockDim.x) {
-        int jz = (int)(idx / ((long)P2 * P3));
-        long r = idx - (long)jz * P2 * P3;
+        int jz = (int)(idx / plane);
+        long r = idx - (long)jz * plane;
         int jy = (int)(r / P3), jx = (int)(r - (long)jy * P3);
         if ((P1 % 2 == 0 && jz == 0) || (P2 % 2 == 0 && jy == 0) || (P3 % 2 == 0 && jx == 0))
             K[idx] = 0.0;
@@ -488,6 +700,15 @@ void launch_neg_laplacian_axpy(Context &ctx, const float *x, float *y, const lon
 
 static int next_fast_dim(long n) { return (int)next_smooth23(n); }
 
+// false when the environment sets LC_PSF_TABLE=0 (the direct sum everywhere)
+static bool psf_table_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("LC_PSF_TABLE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], bool three_d, bool psf_fp32)
     : three_d_(three_d), g_(&g) {
     for (int d = 0; d < 3; ++d) n_[d] = dims[d];
@@ -518,16 +739,17 @@ Toeplitz::Toeplitz(Context &ctx, const PolarGeometry &g, const long dims[3], boo
         if (kernel_mirror_) {
             ProfScope ps(ctx, PS_PSF_FFT, 0.0);
             const int P1 = P_[0], P2 = P_[1], P3 = P_[2], P3h = Ph_[2];
-            const int zlo = P1 / 2 - (int)(n_[0] - 1), nz = P1 - 2 * zlo + (P1 % 2 == 0 ? 1 : 0);
-            // planes zlo .. zlo + nz - 1 hold |dz| <= n1 - 1 (dz = plane - P1/2)
+            // planes P1/2 .. P1/2 + n1 - 1 hold dz = 0 .. n1 - 1 (the kernel is
+            // even in dz, so these are all the taps)
+            const int nz = (int)n_[0];
             DevBuf<double2> a((long)nz * P2 * P3h, st), b((long)nz * P2 * P3h, st);
-            kernel_xy_fft(ctx, K.get() + (long)zlo * P2 * P3, nz, a.get(), b.get());
+            kernel_xy_fft(ctx, K.get() + (long)(P1 / 2) * P2 * P3, nz, a.get(), b.get());
             K.release();
             a.release();
             const long plane = (long)P2 * P3h;
             Kz_ = std::make_shared<DevBuf<float>>(n_[0] * plane, st);
             zdirect_taps_kernel<<<grid_for(n_[0] * plane, 256, ctx.num_sms()), 256, 0, st>>>(
-                b.get(), Kz_->get(), plane, (int)n_[0], P1, P1 / 2 - zlo);
+                b.get(), Kz_->get(), plane, (int)n_[0], P1, 0);
             LC_CHECK_LAUNCH();
             zfold_ = true;
         } else {
@@ -743,7 +965,7 @@ void Toeplitz::build_kernel_nufft32(Context &ctx, DevBuf<double> &K) {
     widen_kernel<<<grid_for(total, 256, ctx.num_sms()), 256, 0, st>>>(K32.get(), K.get(), total);
     LC_CHECK_LAUNCH();
     kernel_mirror_ = false;
-    zero_unpaired_kernel<<<grid_for(total, 256, ctx.num_sms()), 256, 0, st>>>(K.get(), P1, P2, P3);
+    zero_unpaired_kernel<<<grid_for(total, 256, ctx.num_sms()), 256, 0, st>>>(K.get(), P1, P2, P3, 0, P1);
     LC_CHECK_LAUNCH();
 }
 
@@ -872,28 +1094,97 @@ void Toeplitz::build_kernel(Context &ctx, DevBuf<double> &K, int zkeep) {
     K.alloc(total, st);
     constexpr int S = 16;
     const long nseg = ((!three_d_ && mirror ? P3 / 2 + 1 : P3) + S - 1) / S;
-    // with zkeep > 0 and the kz mirror, only the planes |kz| < zkeep are summed
-    // (and their mirrors filled); the other planes are left unset
-    const int zlo = (three_d_ && mirror && zkeep > 0) ? std::max(0, P1 / 2 - (zkeep - 1)) : 0;
+    // with zkeep > 0 and the kz mirror, only the planes 0 <= kz < zkeep are
+    // set (the direct sum sums -zkeep < kz <= 0 and mirrors them); the other
+    // planes are left unset
+    const bool zpart = three_d_ && mirror && zkeep > 0;
+    const int zlo = zpart ? std::max(0, P1 / 2 - (zkeep - 1)) : 0;
+    const int zbeg = zpart ? P1 / 2 : 0, zcnt = zpart ? std::min(zkeep, P1 - P1 / 2) : P1;
     const long items =
         (three_d_ ? (long)(P1 / 2 + 1 - zlo) * (mirror ? P2 / 2 + 1 : P2) : (long)(P2 / 2 + 1)) * nseg;
     size_t smem = sizeof(PsfAngle) * nth + sizeof(int) * groups.size();
     LC_REQUIRE(smem <= 220 * 1024, "Toeplitz: too many angles for one PSF launch");
     unsigned blocks = (unsigned)std::max<long>(1, std::min<long>((items + 127) / 128, (long)ctx.num_sms() * 16));
-    if (three_d_) {
-        auto kern = ngroups == 1 ? psf_rows_kernel<3, S, true> : psf_rows_kernel<3, S, false>;
+    // laminography (one tilt, beta = 0, the kz mirror): the tabulated form
+    bool tabulated = three_d_ && ngroups == 1 && mirror && psf_table_enabled();
+    for (int i = 0; tabulated && i < nth; ++i) tabulated = sorted[i].a[2] == 0.0;
+    if (tabulated) {
+        const double cg = sorted[0].a[0], sg = -sorted[0].a[1];
+        const double h = 1.0 / 32.0;
+        // u over the grid's corners, with the stencil's margin
+        double umin = 1e300, umax = -1e300;
+        for (int cx = 0; cx < 2; ++cx)
+            for (int cy = 0; cy < 2; ++cy) {
+                const double kx = cx ? (double)(P3 - 1 - P3 / 2) : (double)(-P3 / 2);
+                const double ky = cy ? (double)(P2 - 1 - P2 / 2) : (double)(-P2 / 2);
+                const double u = sg * kx + cg * ky;
+                umin = std::min(umin, u);
+                umax = std::max(umax, u);
+            }
+        const double u0 = umin - 6.0 * h;
+        const int nu = (int)std::ceil((umax - u0) / h) + 8;
+        // the planes 0 <= kz < zkeep, or kz <= 0 and their mirrors
+        const int zs = zkeep > 0 ? P1 / 2 : 0;
+        const int nzc = zkeep > 0 ? std::min(zkeep, P1 - P1 / 2) : P1 / 2 + 1;
+        const int nr = zkeep > 0 ? nzc : P1 / 2 + 1;
+        std::vector<TabAngle> ta(nth);
+        for (int i = 0; i < nth; ++i) {
+            // b = (ct sg, ct cg, -st): ct from the ky coefficient over cg, or the kx one over sg
+            const PsfAngle &A = sorted[i];
+            const double ct = std::fabs(cg) >= std::fabs(sg) ? A.b[1] / cg : A.b[0] / sg;
+            ta[i].ct = ct;
+            ta[i].st = -A.b[2];
+            ta[i].stepN = step(ct * h);
+            ta[i].stepD = step(ct * h / ny);
+        }
+        DevBuf<TabAngle> dta;
+        dta.upload(ta.data(), ta.size(), st);
+        DevBuf<double> table((long)nr * nu, st);
+        const size_t tsm = sizeof(TabAngle) * nth;
+        LC_REQUIRE(tsm <= 220 * 1024, "Toeplitz: too many angles for one PSF launch");
+        allow_max_dynamic_smem(ctx, psf_table_kernel);
+        const long titems = (long)nr * ((nu + kTabSeg - 1) / kTabSeg);
+        const unsigned tb = (unsigned)std::max<long>(1, std::min<long>((titems + 127) / 128, (long)ctx.num_sms() * 16));
+        psf_table_kernel<<<tb, 128, tsm, st>>>(dta.get(), nth, ny, u0, h, nu, nr, table.get());
+        LC_CHECK_LAUNCH();
+        const long npts = (long)nzc * (P2 / 2 + 1) * P3;
+        psf_interp_kernel<<<grid_for(npts, 256, ctx.num_sms()), 256, 0, st>>>(
+            table.get(), u0, 1.0 / h, nu, nr, sg, cg, nx, P1, P2, P3, zs, nzc, zkeep > 0 ? 0 : 1, K.get());
+        LC_CHECK_LAUNCH();
+    } else if (three_d_) {
+        auto kern = ngroups == 1 ? psf_rows_kernel<S, true> : psf_rows_kernel<S, false>;
         allow_max_dynamic_smem(ctx, kern);
         kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), ngroups, nx, ny, P1, P2, P3,
                                         mirror ? 1 : 0, zlo, K.get());
     } else {
-        auto kern = psf_rows_kernel<2, S, false>;
-        allow_max_dynamic_smem(ctx, kern);
-        kern<<<blocks, 128, smem, st>>>(dtab.get(), nth, dgroups.get(), 0, nx, ny, P1, P2, P3,
-                                        mirror ? (quarter_turn ? 2 : 1) : 0, 0, K.get());
+        // lanes per segment: the fewest that give about 1024 threads per SM,
+        // at least one angle quad per lane
+        const int m2 = mirror ? (quarter_turn ? 2 : 1) : 0;
+        const long nseg2 = ((mirror ? P3 / 2 + 1 : P3) + S - 1) / S;
+        const long segs = psf2d_first_seg(P2 / 2 + 1, nseg2, m2);
+        int G = 1;
+        while (G < 32 && segs * G < (long)ctx.num_sms() * 1024 && 2 * G <= nth / 4) G *= 2;
+        const size_t smem2 = sizeof(PsfAngle) * nth;
+        LC_REQUIRE(smem2 <= 220 * 1024, "Toeplitz: too many angles for one PSF launch");
+        const unsigned blocks2 =
+            (unsigned)std::max<long>(1, std::min<long>((segs * G + 127) / 128, (long)ctx.num_sms() * 16));
+        auto launch = [&](auto kern) {
+            allow_max_dynamic_smem(ctx, kern);
+            kern<<<blocks2, 128, smem2, st>>>(dtab.get(), nth, nx, P2, P3, m2, K.get());
+        };
+        switch (G) {
+        case 1: launch(psf2d_kernel<S, 1>); break;
+        case 2: launch(psf2d_kernel<S, 2>); break;
+        case 4: launch(psf2d_kernel<S, 4>); break;
+        case 8: launch(psf2d_kernel<S, 8>); break;
+        case 16: launch(psf2d_kernel<S, 16>); break;
+        default: launch(psf2d_kernel<S, 32>); break;
+        }
     }
     LC_CHECK_LAUNCH();
     // planes of mode -P/2 have no mirror inside the grid; they are not needed
-    zero_unpaired_kernel<<<grid_for(total, 256, ctx.num_sms()), 256, 0, st>>>(K.get(), P1, P2, P3);
+    zero_unpaired_kernel<<<grid_for((long)zcnt * P2 * P3, 256, ctx.num_sms()), 256, 0, st>>>(K.get(), P1, P2, P3,
+                                                                                         zbeg, zcnt);
     LC_CHECK_LAUNCH();
     // the angle table is freed in the order of st; the host tables were
     // staged by their uploads

@@ -84,7 +84,7 @@ class Toeplitz {
     double algorithmic_bytes() const;
 
   private:
-    // zkeep > 0: with the kz mirror, sum only the planes |kz| < zkeep
+    // zkeep > 0: with the kz mirror, only the planes 0 <= kz < zkeep are set
     void build_kernel(Context &ctx, DevBuf<double> &K, int zkeep);
     void build_kernel_nufft32(Context &ctx, DevBuf<double> &K);
     void kernel_xy_fft(Context &ctx, const double *K, int nz, double2 *a, double2 *b);
