@@ -7,17 +7,18 @@
 // one cuFINUFFT execute per slice, include/gpu/toeplitz2d.h:68-76 one Thrust
 // multiply per slice, src/gpu/conjgrad.cu:45-108 a handful of launches and
 // host syncs per iteration per job.  Here an iteration is:
-//   p = r + beta p                      one launch, (job, chunk) work items
 //   per grid size P, in parallel graph branches, over the jobs of that P:
-//     Toeplitz x rows (R2C)             one launch, (job, row group) CTAs
+//     Toeplitz x rows (R2C)             one launch, (job, row group) CTAs;
+//                                       p = r + beta p on the way in
 //     Toeplitz y columns x spectrum     one launch, (job, column group) CTAs
-//     Toeplitz x rows (C2R, scaled)     one launch
-//   p.Ap and alpha                      one launch, (job, chunk) items
+//     Toeplitz x rows (C2R, scaled)     one launch; p.Ap and alpha on the
+//                                       way out (per-job partials and ticket)
 //   x += alpha p, r -= alpha Ap, beta   one launch, (job, chunk) items
 // The FFT passes use the register-plan row and column kernels (batched over
 // an item table) where a plan covers P, else the generic shared-memory kernel
-// (AxisFFTBatch); a launch per P keeps the compile-time plan of those
-// kernels, and the branches run concurrently.
+// (AxisFFTBatch), whose jobs take the direction update and p.Ap as vector
+// launches of their own at the ends of their branch.  A launch per P keeps
+// the compile-time plan of those kernels, and the branches run concurrently.
 //
 // Every job keeps its own FP64 scalars (CGState) and stopping tests in device
 // memory; a job whose test fired, or whose iteration budget is spent, turns
@@ -44,6 +45,7 @@
 
 #include "../../include/laminocam.h"
 #include "lc_internal.hpp"
+#include "lc_reduce.cuh"
 #include "lc_solver.hpp"
 #include "lc_toeplitz.hpp"
 
@@ -273,8 +275,8 @@ class BatchCG2D {
         cudaStream_t s = ctx.stream();
         const int J = (int)jobs_.size();
         LC_REQUIRE(J > 0, "batch: no jobs");
-        std::vector<long> voff(J), hoff(J);
-        long vtot = 0, htot = 0;
+        std::vector<long> voff(J), hoff(J), roff(J);
+        long vtot = 0, htot = 0, rtot = 0;
         int chunks = 0;
         for (int j = 0; j < J; ++j) {
             const Toeplitz &T = *jobs_[j].T;
@@ -284,6 +286,8 @@ class BatchCG2D {
             vtot += (n + 3) & ~3L;  // 16-byte aligned vectors
             hoff[j] = htot;
             htot += T.dims()[1] * (T.P()[2] / 2 + 1);
+            roff[j] = rtot;
+            rtot += row_fft_ctas(T.dims()[1]);
             chunks += (int)((n + kChunk - 1) / kChunk);
         }
         vec_.alloc(3 * vtot, s);  // r, p, Ap
@@ -292,6 +296,7 @@ class BatchCG2D {
         counters_.alloc(J, s);
         counters_.zero(s);
         part_.alloc((size_t)chunks * 4, s);
+        rpart_.alloc((size_t)rtot * kRedParts, s);  // p.Ap partials of the fused row passes
         std::vector<VecJob> vj(J);
         std::vector<int2> items;
         items.reserve(chunks);
@@ -314,13 +319,23 @@ class BatchCG2D {
             for (int c = 0; c < v.nchunks; ++c) items.push_back(make_int2(j, c));
             part0 += v.nchunks;
             Group &g = group_for(T.P()[2]);
-            add_toeplitz(ctx, g, T, v.p, v.ap, h_.get() + hoff[j], &st_.get()[j].done);
+            CGFusion f;
+            f.p = v.p;
+            f.r = v.r;
+            f.st = st_.get() + j;
+            f.part = rpart_.get() + roff[j] * kRedParts;
+            f.counter = counters_.get() + j;
+            f.fp32 = 0;
+            if (!add_toeplitz(ctx, g, T, v.p, v.ap, h_.get() + hoff[j], &st_.get()[j].done, f))
+                for (int c = 0; c < v.nchunks; ++c) g.plain.push_back(make_int2(j, c));
         }
         vjobs_.upload(vj.data(), J, s);
         items_.upload(items.data(), items.size(), s);
         nitems_ = (int)items.size();
-        for (auto &g : groups_)
+        for (auto &g : groups_) {
             for (Stage *st : {&g->fwd, &g->col, &g->inv}) st->finalize(ctx);
+            if (!g->plain.empty()) g->dplain.upload(g->plain.data(), g->plain.size(), s);
+        }
         // side streams of the per-grid branches (created here, outside any capture)
         const int nside = (int)std::min<size_t>(groups_.size(), 8);
         side_.resize(nside, nullptr);
@@ -361,10 +376,19 @@ class BatchCG2D {
             const int k = std::min(chunk, maxit - done);
             if (use_graph && k == chunk) {
                 if (!graph.ready()) {
+#ifdef LC_BATCH_TRACE
+                    const auto tc = std::chrono::steady_clock::now();
+#endif
                     const cudaStream_t cs = ctx.capture_stream();
                     graph.capture(cs, [&] {
                         for (int i = 0; i < chunk; ++i) iteration(cs);
                     });
+#ifdef LC_BATCH_TRACE
+                    std::fprintf(stderr, "batch graph of %d iterations, %zu grid sizes: captured in %.2f ms\n", chunk,
+                                 groups_.size(),
+                                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc)
+                                     .count());
+#endif
                 }
                 graph.launch(s);
             } else {
@@ -393,11 +417,17 @@ class BatchCG2D {
         RegLineBatch reg;
         AxisFFTBatch gen;
         bool generic = false;
-        void add(Context &ctx, const AxisFFT &a, const int *skip) {
-            if (!generic && reg.add(a, skip)) return;
+        // true when the register kernels took the transform with its fused
+        // CG work; the generic kernel takes it without
+        bool add(Context &ctx, const AxisFFT &a, const int *skip) {
+            if (!generic && reg.add(a, skip)) return true;
             LC_REQUIRE(reg.empty(), "batch: the jobs of one grid size take different kernels");
             generic = true;
-            gen.add(ctx, a, skip);
+            AxisFFT b = a;
+            b.cg = nullptr;
+            b.cg_parts = 0;
+            gen.add(ctx, b, skip);
+            return false;
         }
         void finalize(Context &ctx) {
             if (generic) gen.finalize(ctx);
@@ -411,6 +441,10 @@ class BatchCG2D {
     struct Group {
         int P = 0;
         Stage fwd, col, inv;
+        // (job, chunk) items of the jobs whose row passes do not fuse the
+        // direction update and p.Ap (the generic kernel)
+        std::vector<int2> plain;
+        DevBuf<int2> dplain;
     };
 
     Group &group_for(int P) {
@@ -422,24 +456,30 @@ class BatchCG2D {
     }
 
     void iteration(cudaStream_t s) {
-        batch_p_update_kernel<<<nitems_, kVecThreads, 0, s>>>(vjobs_.get(), items_.get(), st_.get());
-        LC_CHECK_LAUNCH();
         // the grid sizes' Toeplitz passes as parallel branches
         LC_CUDA(cudaEventRecord(fork_, s));
         for (size_t i = 0; i < side_.size(); ++i) LC_CUDA(cudaStreamWaitEvent(side_[i], fork_, 0));
         for (size_t g = 0; g < groups_.size(); ++g) {
             const cudaStream_t b = side_[g % side_.size()];
-            groups_[g]->fwd.launch(b);
-            groups_[g]->col.launch(b);
-            groups_[g]->inv.launch(b);
+            const Group &G = *groups_[g];
+            const unsigned np = (unsigned)G.plain.size();
+            if (np) {
+                batch_p_update_kernel<<<np, kVecThreads, 0, b>>>(vjobs_.get(), G.dplain.get(), st_.get());
+                LC_CHECK_LAUNCH();
+            }
+            G.fwd.launch(b);
+            G.col.launch(b);
+            G.inv.launch(b);
+            if (np) {
+                batch_dot_kernel<<<np, kVecThreads, 0, b>>>(vjobs_.get(), G.dplain.get(), st_.get(), part_.get(),
+                                                            counters_.get());
+                LC_CHECK_LAUNCH();
+            }
         }
         for (size_t i = 0; i < side_.size(); ++i) {
             LC_CUDA(cudaEventRecord(join_[i], side_[i]));
             LC_CUDA(cudaStreamWaitEvent(s, join_[i], 0));
         }
-        batch_dot_kernel<<<nitems_, kVecThreads, 0, s>>>(vjobs_.get(), items_.get(), st_.get(), part_.get(),
-                                                         counters_.get());
-        LC_CHECK_LAUNCH();
         batch_update_kernel<<<nitems_, kVecThreads, 0, s>>>(vjobs_.get(), items_.get(), st_.get(), part_.get(),
                                                             counters_.get());
         LC_CHECK_LAUNCH();
@@ -449,8 +489,9 @@ class BatchCG2D {
     // the group's three launches.  Real rows of an even grid run as complex
     // rows of half the length (even/odd packing), of an odd grid (3^q) as
     // complex rows of the full length.
-    void add_toeplitz(Context &ctx, Group &g, const Toeplitz &T, const float *p, float *ap, float2 *h,
-                      const int *skip) {
+    // Returns true when the row passes fuse the direction update and p.Ap (f).
+    bool add_toeplitz(Context &ctx, Group &g, const Toeplitz &T, const float *p, float *ap, float2 *h,
+                      const int *skip, const CGFusion &f) {
         const long n = T.dims()[1];
         const int P = T.P()[2], Ph = P / 2 + 1;
         const bool even = P % 2 == 0;
@@ -469,7 +510,9 @@ class BatchCG2D {
         a.in_map = even ? IN_REAL_PACKED : IN_DIRECT;
         a.out_map = even ? OUT_R2C_UNPACK : OUT_DIRECT;
         a.sign = -1;
-        g.fwd.add(ctx, a, skip);
+        a.cg = &f;
+        a.cg_parts = kFusedUpdate;
+        const bool fwd_fused = g.fwd.add(ctx, a, skip);
         AxisFFT b;
         b.in = h;
         b.in_t = E_C64;
@@ -506,7 +549,11 @@ class BatchCG2D {
         c.out_off = 0;
         c.sign = +1;
         c.scale = T.scale();
-        g.inv.add(ctx, c, skip);
+        c.cg = &f;
+        c.cg_parts = kFusedDot;
+        const bool inv_fused = g.inv.add(ctx, c, skip);
+        LC_REQUIRE(fwd_fused == inv_fused, "batch: the row passes of one job take different kernels");
+        return fwd_fused;
     }
 
     std::vector<Job> jobs_;
@@ -515,6 +562,7 @@ class BatchCG2D {
     DevBuf<CGState> st_;
     DevBuf<unsigned> counters_;
     DevBuf<double> part_;
+    DevBuf<double> rpart_;
     DevBuf<VecJob> vjobs_;
     DevBuf<int2> items_;
     int nitems_ = 0;
@@ -542,6 +590,15 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
         }
         Context &ctx = *c->ctx;
         cudaStream_t s = ctx.stream();
+#ifdef LC_BATCH_TRACE
+        const auto lc_t00 = std::chrono::steady_clock::now();
+        auto lc_tr = [&](const char *what) {
+            std::fprintf(stderr, "batch %s at %.2f ms\n", what,
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - lc_t00).count());
+        };
+#else
+        auto lc_tr = [](const char *) {};
+#endif
         const int nw = std::max(1, std::min(setup_workers > 0 ? setup_workers : 8, njobs));
         // per job: right-hand side and Toeplitz operator, built on the workers
         // (contexts kept in the caller's context for later calls)
@@ -617,6 +674,7 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
         for (double &v : g_batch_t) v = 0;
         const auto lc_t0 = std::chrono::steady_clock::now();
 #endif
+        lc_tr("workers start");
         std::vector<std::thread> th;
         for (int w = 0; w < nw; ++w) th.emplace_back(work, w);
         // the workers finish every setup even when a wave fails: on every exit
@@ -655,7 +713,17 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
             std::vector<CGState> fin;
             {
                 BatchCG2D batch(ctx, std::move(bj));
+#ifdef LC_BATCH_TRACE
+                std::fprintf(stderr, "batch wave [%d, %d) built at %.2f ms\n", begin, end,
+                             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - lc_t0)
+                                 .count());
+#endif
                 batch.run(ctx, p->solver.use_graph != 0, &fin);
+#ifdef LC_BATCH_TRACE
+                std::fprintf(stderr, "batch wave [%d, %d) iterated at %.2f ms\n", begin, end,
+                             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - lc_t0)
+                                 .count());
+#endif
             }
             for (int t = begin; t < end; ++t) {
                 const int j = order[t];
@@ -671,6 +739,7 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
                     stats[j].elapsed_ms = 0.0;
                 }
             }
+            lc_tr("results copied");
             begin = end;
         }
         for (auto &t : th) t.join();
@@ -679,10 +748,12 @@ extern "C" int lc_mbir2d_batch(lc_context c, const lc_job2d *jobs, int njobs, co
                      g_batch_t[0], g_batch_t[1], g_batch_t[2], g_batch_t[3]);
 #endif
         LC_CUDA(cudaStreamSynchronize(s));
+        lc_tr("joined");
         // worker-owned buffers are released in the order of the workers' streams
         for (auto &o : ops) o.reset();
         for (auto &b : rhs) b.release();
         for (auto &b : xs) b.release();
         for (int w = 0; w < nw; ++w) LC_CUDA(cudaStreamSynchronize(wctx[w]->ctx->stream()));
+        lc_tr("released");
     });
 }

@@ -18,10 +18,11 @@ __device__ __forceinline__ A warp_sum_red(A v) {
 }
 
 // Block-reduce K (<= kRedParts) sums of any CTA size up to 1024 threads and
-// store them as this CTA's partials.  Returns true in every thread of the CTA
-// that finished last.  Every thread of the CTA must call it.
+// store them as partial slot `slot` of `nslots` (one per CTA taking part).
+// Returns true in every thread of the CTA that finished last.  Every thread of
+// the CTA must call it.
 template <typename A, int K>
-__device__ bool red_block_partials(A (&v)[K], double *part, unsigned *counter) {
+__device__ bool red_block_partials_at(A (&v)[K], double *part, unsigned *counter, long slot, long nslots) {
     __shared__ A sh[K][32];
     __shared__ bool last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -37,16 +38,22 @@ __device__ bool red_block_partials(A (&v)[K], double *part, unsigned *counter) {
         for (int k = 0; k < K; ++k) {
             A s = lane < nw ? sh[k][lane] : A(0);
             s = warp_sum_red(s);
-            if (lane == 0) part[(long)blockIdx.x * kRedParts + k] = (double)s;
+            if (lane == 0) part[slot * kRedParts + k] = (double)s;
         }
     }
     __threadfence();
     if (threadIdx.x == 0) {
         unsigned t = atomicAdd(counter, 1u);
-        last = (t == gridDim.x - 1);
+        last = ((long)t == nslots - 1);
     }
     __syncthreads();
     return last;
+}
+
+// The same over the whole grid: one slot per CTA
+template <typename A, int K>
+__device__ bool red_block_partials(A (&v)[K], double *part, unsigned *counter) {
+    return red_block_partials_at<A, K>(v, part, counter, (long)blockIdx.x, (long)gridDim.x);
 }
 
 // Fixed-order total of partial k over all CTAs (called by the last CTA, all

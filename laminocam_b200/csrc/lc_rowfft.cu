@@ -161,17 +161,20 @@ __device__ __forceinline__ void row_fft_body(const RowArgs &a, long bid) {
             }
         }
         if constexpr (HOOK) if (dot) {
-            // p.Ap over the grid, then alpha and the |p.Ap| stop (as the CG dot kernel)
+            // p.Ap over the transform's blocks (all of the grid in a plain
+            // launch, the item's blocks in a batched one), then alpha and the
+            // |p.Ap| stop (as the CG dot kernel)
+            const long nblk = (a.n_lines + kRowLines - 1) / kRowLines;
             double pap = 0.0;
             bool last;
             if (a.cg.fp32) {
                 float vv[1] = {accf};
-                last = red_block_partials<float, 1>(vv, a.cg.part, a.cg.counter);
-                if (last) pap = red_total<float>(a.cg.part, 0, gridDim.x);
+                last = red_block_partials_at<float, 1>(vv, a.cg.part, a.cg.counter, bid, nblk);
+                if (last) pap = red_total<float>(a.cg.part, 0, (int)nblk);
             } else {
                 double vv[1] = {accd};
-                last = red_block_partials<double, 1>(vv, a.cg.part, a.cg.counter);
-                if (last) pap = red_total<double>(a.cg.part, 0, gridDim.x);
+                last = red_block_partials_at<double, 1>(vv, a.cg.part, a.cg.counter, bid, nblk);
+                if (last) pap = red_total<double>(a.cg.part, 0, (int)nblk);
             }
             if (last && threadIdx.x == 0) {
                 CGState *st = a.cg.st;
@@ -188,14 +191,14 @@ __device__ __forceinline__ void row_fft_body(const RowArgs &a, long bid) {
     }
 }
 
-// (HOOK's fused dot reduces over the whole grid: the plain launch only)
 template <int R0, int R1, int R2, int MODE, bool HOOK>
 __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines) row_fft_kernel(RowArgs a) {
     row_fft_body<R0, R1, R2, MODE, HOOK>(a, (long)blockIdx.x);
 }
 
-// one launch over several row transforms of one plan and mode (no fused CG
-// work): CTA b runs block b - first_block of the item whose range holds b
+// one launch over several row transforms of one plan and mode: CTA b runs
+// block b - first_block of the item whose range holds b, with the item's
+// fused CG work (its partials and ticket are the item's own)
 struct RowBatchItem {
     RowArgs a;
     long first_block;
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kRowLines)
         else hi = mid - 1;
     }
     if (items[lo].skip && *items[lo].skip) return;
-    row_fft_body<R0, R1, R2, MODE, false>(items[lo].a, b - items[lo].first_block);
+    row_fft_body<R0, R1, R2, MODE, true>(items[lo].a, b - items[lo].first_block);
 }
 
 template <int R0, int R1, int R2, int MODE>
@@ -314,10 +317,15 @@ bool launch_row_fft(cudaStream_t st, const AxisFFT &a) {
 
 bool row_batch_item(const AxisFFT &a, const int *skip, long first_block, RegBatchKey &key,
                     std::vector<unsigned char> &item, long &blocks) {
-    if (a.cg_parts) return false;
     int M = 0, mode = 0;
     RowArgs ra;
     if (!row_plan_args(a, M, mode, ra)) return false;
+    if (a.cg_parts) {
+        LC_REQUIRE(a.cg != nullptr, "row FFT: fused CG work without its state");
+        ra.cg = *a.cg;
+        ra.cg_upd = (mode == RM_R2C && (a.cg_parts & kFusedUpdate)) ? 1 : 0;
+        ra.cg_dot = (mode == RM_C2R && (a.cg_parts & kFusedDot)) ? 1 : 0;
+    }
     key.kind = 2;
     key.M = M;
     key.mode = mode;
