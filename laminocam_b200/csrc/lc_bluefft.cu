@@ -13,8 +13,12 @@
 // The fftshift/ifftshift rolls are index maps at the load and the store
 // (value j of the line is in[(j + d_pre) mod n]; out[k] = X[(k + d_post) mod n]).
 // A CTA takes 4 lines: adjacent rows (contiguous lines) or 4 adjacent columns
-// (32-byte row segments).
+// (32-byte row segments).  Real rows go two to a line: rows a and b are
+// transformed as the complex line a + i b, whose DFT Z gives
+//   A[k] = (Z[k] + conj Z[n-k]) / 2,   B[k] = (Z[k] - conj Z[n-k]) / (2i)
+// (the DFT of a real sequence is Hermitian), paired through shared memory.
 #include <atomic>
+#include <type_traits>
 
 #include "lc_fft.hpp"
 #include "lc_regfft.cuh"
@@ -57,9 +61,18 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kBlueLines) blue_kern
     // with c fastest (adjacent columns)
     const int t = ROWS ? (int)threadIdx.x % NT : (int)threadIdx.x / C;
     const int c = ROWS ? (int)threadIdx.x / NT : (int)threadIdx.x % C;
+    // real rows, two to a line (rows 2 line and 2 line + 1)
+    constexpr bool PACK = ROWS && std::is_same_v<TI, float>;
     long base_in, base_out, step;
-    bool valid;
-    if constexpr (ROWS) {
+    bool valid, valid_b = false;
+    if constexpr (PACK) {
+        const long line = (long)blockIdx.x * C + c;
+        valid = 2 * line < a.n_outer;
+        valid_b = 2 * line + 1 < a.n_outer;
+        base_in = (valid ? 2 * line : 0) * a.in_ostride;
+        base_out = (valid ? 2 * line : 0) * a.out_ostride;
+        step = 1;
+    } else if constexpr (ROWS) {
         const long line = (long)blockIdx.x * C + c;
         valid = line < a.n_outer;
         base_in = (valid ? line : 0) * a.in_ostride;
@@ -87,7 +100,13 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kBlueLines) blue_kern
             if (valid && j < a.n) {
                 int s = j + a.d_pre;
                 if (s >= a.n) s -= a.n;
-                x = cmul(load_c<TI>(in + (long)s * step), __ldg(a.chirp + j));
+                if constexpr (PACK) {
+                    const float xa = static_cast<const float *>(a.in)[base_in + s];
+                    const float xb = valid_b ? static_cast<const float *>(a.in)[base_in + a.in_ostride + s] : 0.f;
+                    x = cmul(make_float2(xa, xb), __ldg(a.chirp + j));
+                } else {
+                    x = cmul(load_c<TI>(in + (long)s * step), __ldg(a.chirp + j));
+                }
             }
             v[0][r] = x;
         }
@@ -109,6 +128,37 @@ __global__ void __launch_bounds__(RegPlan<R0, R1, R2>::NT *kBlueLines) blue_kern
     }
     xform3<M, R2, R1, R0>(v, at, t, tw, +1);
     constexpr int NF = M / R0;
+    if constexpr (PACK) {
+        // Z[q] of the line into its shared-memory row, then the two rows'
+        // values from the pairs (q, n - q)
+        __syncthreads();  // the transform's last shared-memory reads are done
+        if (t < NF) {
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int q = t + r * NF;
+                if (q < a.n) {
+                    const float2 h = th[q];
+                    const float2 y = cadd(v[0][r], cmul(make_float2(h.x, -h.y), v[1][r]));
+                    at(0, q) = cscale(cmul(y, __ldg(a.chirp + q)), 0.5f * a.scale);
+                }
+            }
+        }
+        __syncthreads();
+        if (t < NF && valid) {
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int q = t + r * NF;
+                if (q < a.n) {
+                    const float2 zq = at(0, q), zm = at(0, q == 0 ? 0 : a.n - q);
+                    int k = q - a.d_post;
+                    if (k < 0) k += a.n;
+                    a.out[base_out + k] = make_float2(zq.x + zm.x, zq.y - zm.y);
+                    if (valid_b) a.out[base_out + a.out_ostride + k] = make_float2(zq.y + zm.y, zm.x - zq.x);
+                }
+            }
+        }
+        return;
+    }
     if (t < NF && valid) {
 #pragma unroll
         for (int r = 0; r < R0; ++r) {
@@ -171,7 +221,9 @@ bool launch_bluestein_lines(cudaStream_t st, const AxisDFT &a, const BluesteinEn
     const bool rows = a.n_inner == 1;
     long blocks;
     if (rows) {
-        blocks = (a.n_outer + kBlueLines - 1) / kBlueLines;
+        // real rows go two to a line
+        const long lines = a.in_t == E_F32 ? (a.n_outer + 1) / 2 : a.n_outer;
+        blocks = (lines + kBlueLines - 1) / kBlueLines;
         b.bpo = 1;
     } else {
         b.bpo = (a.n_inner + kBlueLines - 1) / kBlueLines;
