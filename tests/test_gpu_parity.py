@@ -135,10 +135,12 @@ def test_projection_ops_3d_golden(lc, f):
     assert O.rel_l2(to_np(lc.sysmat(vol, pg)), g["sysmat3d_nufft"]) < PROJ_TOL
 
 
-def test_projection_ops_3d_bluestein_detector(lc):
-    """Detector lines of 33 and 40 samples take the Bluestein (chirp-z) DFT path."""
+@pytest.mark.parametrize("nth", [12, 11])
+def test_projection_ops_3d_bluestein_detector(lc, nth):
+    """Detector lines of 33 and 40 samples take the Bluestein (chirp-z) DFT path.
+    Real detector rows go two to a line; 11 angles leave an odd row count
+    (363), so the last line carries one row."""
     rng = np.random.default_rng(31)
-    nth = 12
     th = np.arange(nth) * 2 * np.pi / nth
     ga, be = np.full(nth, -0.45), np.full(nth, 0.05)
     vol = rng.random((5, 24, 24)).astype(np.float32)
