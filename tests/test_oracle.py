@@ -127,6 +127,59 @@ def test_dirichlet_closed_form_psf_matches_nudft():
     assert np.abs(K - K_exact).max() / np.abs(K_exact).max() < 1e-12
 
 
+def _dirichlet(u, n):
+    den = np.sin(np.pi * u / n)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return np.where(np.abs(den) < 1e-13, n * np.cos(np.pi * u) / np.cos(np.pi * u / n),
+                        np.sin(np.pi * u) / den)
+
+
+def test_laminography_psf_factorisation_and_table():
+    """The tabulated laminography PSF of the CUDA generator, restated in
+    numpy: with beta = 0 and one tilt gamma,
+        K(k) = D_nx(cg kx - sg ky) * S(sg kx + cg ky, kz),
+        S(u, kz) = sum_theta D_ny(cos(theta) u - sin(theta) kz),
+    S sampled at spacing 1/32 in u and read back by ten-point Lagrange
+    interpolation (weights c_q prod_{m != q} (t - m)).  Against the oracle's
+    exact NUDFT kernel (the reference's angle-by-angle sum)."""
+    import math
+    nth, nr, nc, dims = 40, 29, 31, (5, 30, 30)
+    th = -np.pi / 2 + np.arange(nth) * np.pi / nth
+    gam = np.deg2rad(-25.0)
+    grid = O.Grid3D(th, np.full(nth, gam), np.zeros(nth), nr, nc)
+    K_exact = O.psf3d(grid, dims).kernel
+    P1, P2, P3 = K_exact.shape
+    cg, sg = np.cos(gam), np.sin(gam)
+    kz, ky, kx = np.meshgrid(np.arange(P1) - P1 // 2, np.arange(P2) - P2 // 2, np.arange(P3) - P3 // 2,
+                             indexing="ij")
+    # the table S(u0 + j h, -r), r = |kz|
+    h = 1.0 / 32.0
+    us = [sg * x + cg * y for x in (-(P3 // 2), P3 - 1 - P3 // 2) for y in (-(P2 // 2), P2 - 1 - P2 // 2)]
+    u0 = min(us) - 6 * h
+    nu = int(np.ceil((max(us) - u0) / h)) + 8
+    uu = u0 + np.arange(nu) * h
+    nrz = P1 // 2 + 1
+    T = np.zeros((nrz, nu))
+    for r in range(nrz):
+        for t in th:
+            T[r] += _dirichlet(np.cos(t) * uu + np.sin(t) * r, nr)
+    # ten-point interpolation
+    c = np.array([(-1) ** (9 - q) / (math.factorial(q) * math.factorial(9 - q)) for q in range(10)])
+    u, w = sg * kx + cg * ky, cg * kx - sg * ky
+    t = (u - u0) / h
+    j = np.floor(t).astype(int) - 4
+    d = (t - j)[..., None] - np.arange(10)
+    pre = np.cumprod(np.concatenate([np.ones(d.shape[:-1] + (1,)), d[..., :-1]], axis=-1), axis=-1)
+    suf = np.flip(np.cumprod(np.concatenate([np.ones(d.shape[:-1] + (1,)), np.flip(d, -1)[..., :-1]], axis=-1),
+                             axis=-1), -1)
+    idx = j[..., None] + np.arange(10)
+    vals = T[np.abs(kz)[..., None], idx]
+    S = np.sum(c * pre * suf * vals, axis=-1)
+    K = _dirichlet(w, nc) * S
+    err = np.abs(K - K_exact).max() / np.abs(K_exact).max()
+    assert err < 1e-12, err
+
+
 @pytest.mark.parametrize("three_d", [False, True])
 def test_zero_centred_spectrum_is_real_after_dropping_unpaired_planes(three_d):
     """The CUDA PSF keeps Re(FFT(K0)) with K0 the zero-centred kernel whose -P/2
